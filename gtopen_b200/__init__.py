@@ -1,0 +1,400 @@
+"""gtopen_b200 -- B200 discounted-CFR engine for heads-up postflop spots.
+
+Python mirror of the reference solver crate's API for the GPU hot path
+(MatthewPDingle/GTOpen crates/solver: game.rs Spot, cfr.rs Solver state,
+gpu/mod.rs GpuSolver, save.rs), bound over the C ABI in include/gtob.h
+(libgtob.so, built in place by gtopen_b200/csrc/Makefile).  There is no CPU
+fallback: every call goes through libgtob, and importing the bindings fails
+loudly if the library is missing.
+"""
+import ctypes as C
+import json
+import os
+
+import numpy as np
+
+__all__ = ["Spot", "Solver", "GpuSolver", "GtobError", "KERNEL_NAMES", "estimate_vram", "vram_info_mb",
+           "evaluate7", "parse_range", "lib", "LIB_PATH"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgtob.so")
+_LIB = None
+
+STORAGE = {"f32": 0, "compressed": 1, "i16": 1}
+ALGO = {"dcfr": 0, "cfr+": 1, "cfrplus": 1, "pcfr+": 2, "pcfrplus": 2}
+DEVICE_FORMAT = {None: -1, "follow": -1, "f32": 0, "i16": 1}
+KERNEL_NAMES = ["copy_root", "down_action", "down_chance", "up_fold", "up_show", "up_chance", "up_action"]
+
+
+class GtobError(RuntimeError):
+    """A failed libgtob call (the reference's Result::Err(String))."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+class SpotInfo(C.Structure):
+    _fields_ = [("num_nodes", C.c_uint64), ("num_action_nodes", C.c_uint64), ("num_children", C.c_uint64),
+                ("num_actions", C.c_uint64), ("data_size", C.c_uint64 * 2), ("num_hands", C.c_uint32 * 2),
+                ("root_street", C.c_uint32), ("num_suit_perms", C.c_uint32)]
+
+
+class GpuInfo(C.Structure):
+    _fields_ = [("device_bytes", C.c_uint64), ("visited_nodes", C.c_uint64), ("cfv_slots", C.c_uint64),
+                ("reach_slots", C.c_uint64 * 2), ("device_action_nodes", C.c_uint64 * 2),
+                ("visited_terminals", C.c_uint64), ("num_levels", C.c_uint32), ("num_river_slots", C.c_uint32),
+                ("arena_format", C.c_int32), ("iter_bytes", C.c_double)]
+
+
+class Profile(C.Structure):
+    _fields_ = [("ms", C.c_double * 7), ("launches", C.c_uint32 * 7)]
+
+    def as_dict(self):
+        return {KERNEL_NAMES[k]: (self.ms[k], self.launches[k]) for k in range(7)}
+
+
+def lib():
+    """Load libgtob.so (raises if it has not been built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libgtob.so is not built: run `make -C gtopen_b200/csrc` (or __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    P, I, U32, U64, D = C.c_void_p, C.c_int, C.c_uint32, C.c_uint64, C.c_double
+    sig = {
+        "gtob_last_error": (C.c_char_p, []),
+        "gtob_kernel_name": (C.c_char_p, [I]),
+        "gtob_version": (C.c_char_p, []),
+        "gtob_spot_from_json": (I, [C.c_char_p, U64, I, C.POINTER(P)]),
+        "gtob_spot_free": (None, [P]),
+        "gtob_spot_info_get": (I, [P, C.POINTER(SpotInfo)]),
+        "gtob_spot_tree": (I, [P] + [P] * 12),
+        "gtob_spot_children": (I, [P, P]),
+        "gtob_spot_actions": (I, [P, P, P]),
+        "gtob_spot_hands": (I, [P, I, P, P, P, P]),
+        "gtob_spot_suit_perms": (I, [P, P, P, P]),
+        "gtob_spot_river": (I, [P, I, P, I, P, P]),
+        "gtob_spot_pair_weight_sum": (D, [P]),
+        "gtob_evaluate7": (U32, [P]),
+        "gtob_parse_range": (I, [C.c_char_p, P]),
+        "gtob_estimate_vram": (U64, [P]),
+        "gtob_vram_info_mb": (I, [C.POINTER(U64), C.POINTER(U64)]),
+        "gtob_solver_new": (I, [P, I, I, I, C.POINTER(P)]),
+        "gtob_solver_free": (None, [P]),
+        "gtob_solver_iteration": (U32, [P]),
+        "gtob_solver_set_iteration": (I, [P, U32]),
+        "gtob_solver_arena_bytes": (U64, [P]),
+        "gtob_solver_get_arena": (I, [P, I, I, P]),
+        "gtob_solver_set_arena": (I, [P, I, I, P]),
+        "gtob_solver_average_strategy": (I, [P, U32, P]),
+        "gtob_solver_solved_strategy": (I, [P, U32, P]),
+        "gtob_solver_lock_node": (I, [P, P, I, I, P, I, C.c_char_p, C.c_char_p, C.POINTER(U32)]),
+        "gtob_solver_set_lock": (I, [P, U32, P, U64, C.c_char_p]),
+        "gtob_solver_clear_locks": (I, [P]),
+        "gtob_solver_num_locks": (I, [P]),
+        "gtob_solver_ensure_symmetric": (I, [P]),
+        "gtob_save": (I, [P, C.c_char_p]),
+        "gtob_load": (I, [C.c_char_p, I, C.POINTER(P)]),
+        "gtob_gpu_new": (I, [P, I, C.POINTER(P)]),
+        "gtob_gpu_free": (None, [P]),
+        "gtob_gpu_iterate": (I, [P, I]),
+        "gtob_gpu_iterate_profiled": (I, [P, C.POINTER(Profile)]),
+        "gtob_gpu_exploitability": (I, [P, P, C.POINTER(D)]),
+        "gtob_gpu_sync_to_cpu": (I, [P, P]),
+        "gtob_gpu_sync_strategy": (I, [P, P]),
+        "gtob_gpu_synchronize": (I, [P]),
+        "gtob_gpu_update_locks": (I, [P, P]),
+        "gtob_gpu_iteration": (U32, [P]),
+        "gtob_gpu_info_get": (I, [P, C.POINTER(GpuInfo)]),
+        "gtob_gpu_root_cfv": (I, [P, I, I, P]),
+        "gtob_gpu_export_arena": (I, [P, I, I, P]),
+        "gtob_gpu_discounts": (I, [P, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _LIB = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _check(rc):
+    if rc < 0:
+        raise GtobError(rc, lib().gtob_last_error().decode(errors="replace"))
+    return rc
+
+
+def evaluate7(cards):
+    c = np.ascontiguousarray(cards, np.uint8)
+    return int(lib().gtob_evaluate7(_ptr(c)))
+
+
+def parse_range(text):
+    w = np.zeros(1326, np.float32)
+    _check(lib().gtob_parse_range(text.encode(), _ptr(w)))
+    return w
+
+
+class Spot:
+    """game.rs Spot: tree, hand lists, river tables, suit symmetries."""
+
+    def __init__(self, config, max_nodes=0, lenient=False):
+        text = config if isinstance(config, str) else json.dumps(config)
+        h = C.c_void_p()
+        _check(lib().gtob_spot_from_json(text.encode(), int(max_nodes), int(lenient), C.byref(h)))
+        self._h = h
+        self.config = json.loads(text)
+        info = SpotInfo()
+        _check(lib().gtob_spot_info_get(self._h, C.byref(info)))
+        self.num_nodes = info.num_nodes
+        self.num_action_nodes = info.num_action_nodes
+        self.num_children = info.num_children
+        self.num_actions = info.num_actions
+        self.data_size = [info.data_size[0], info.data_size[1]]
+        self.nh = [info.num_hands[0], info.num_hands[1]]
+        self.root_street = info.root_street
+        self.num_suit_perms = info.num_suit_perms
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gtob_spot_free(self._h)
+            self._h = None
+
+    def tree(self):
+        n = self.num_nodes
+        out = dict(kind=np.zeros(n, np.uint8), player=np.zeros(n, np.uint8), street=np.zeros(n, np.uint8),
+                   nchild=np.zeros(n, np.uint8), child_start=np.zeros(n, np.uint32),
+                   action_start=np.zeros(n, np.uint32), data_off=np.zeros(n, np.uint64),
+                   put0=np.zeros(n), put1=np.zeros(n), twin=np.zeros(n), tlose=np.zeros(n), ttie=np.zeros(n))
+        keys = ("kind", "player", "street", "nchild", "child_start", "action_start", "data_off", "put0", "put1",
+                "twin", "tlose", "ttie")
+        _check(lib().gtob_spot_tree(self._h, *[_ptr(out[k]) for k in keys]))
+        return out
+
+    def children(self):
+        a = np.zeros(self.num_children, np.uint32)
+        _check(lib().gtob_spot_children(self._h, _ptr(a)))
+        return a
+
+    def actions(self):
+        k = np.zeros(self.num_actions, np.int32)
+        amt = np.zeros(self.num_actions)
+        _check(lib().gtob_spot_actions(self._h, _ptr(k), _ptr(amt)))
+        return k, amt
+
+    def hands(self, p):
+        n = self.nh[p]
+        c1, c2 = np.zeros(n, np.uint8), np.zeros(n, np.uint8)
+        w, same = np.zeros(n, np.float32), np.zeros(n, np.uint32)
+        _check(lib().gtob_spot_hands(self._h, p, _ptr(c1), _ptr(c2), _ptr(w), _ptr(same)))
+        return c1, c2, w, same
+
+    def suit_perms(self):
+        k = self.num_suit_perms
+        pm = np.zeros((k, 4), np.uint8)
+        h0, h1 = np.zeros((k, self.nh[0]), np.uint16), np.zeros((k, self.nh[1]), np.uint16)
+        _check(lib().gtob_spot_suit_perms(self._h, _ptr(pm), _ptr(h0), _ptr(h1)))
+        return pm, h0, h1
+
+    def river(self, p, dealt):
+        d = np.array(list(dealt) + [0, 0], np.uint8)
+        st, ix = np.zeros(self.nh[p], np.uint32), np.zeros(self.nh[p], np.uint16)
+        n = _check(lib().gtob_spot_river(self._h, p, _ptr(d), len(dealt), _ptr(st), _ptr(ix)))
+        return st[:n], ix[:n]
+
+    def pair_weight_sum(self):
+        return lib().gtob_spot_pair_weight_sum(self._h)
+
+    def estimate_vram(self):
+        return int(lib().gtob_estimate_vram(self._h))
+
+
+def estimate_vram(spot):
+    return spot.estimate_vram()
+
+
+def vram_info_mb():
+    f, t = C.c_uint64(), C.c_uint64()
+    if lib().gtob_vram_info_mb(C.byref(f), C.byref(t)) != 0:
+        return None
+    return f.value, t.value
+
+
+class Solver:
+    """cfr.rs Solver state: arenas, locks, iteration (the CFR loop runs on the GPU)."""
+
+    def __init__(self, spot, storage="f32", algo="dcfr", use_iso=True, _handle=None):
+        self.spot = spot
+        self.storage = storage
+        self.algo = algo
+        if _handle is not None:
+            self._h = _handle
+            return
+        h = C.c_void_p()
+        _check(lib().gtob_solver_new(spot._h, STORAGE[storage], ALGO[algo], int(use_iso), C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gtob_solver_free(self._h)
+            self._h = None
+
+    @property
+    def iteration(self):
+        return int(lib().gtob_solver_iteration(self._h))
+
+    @iteration.setter
+    def iteration(self, v):
+        _check(lib().gtob_solver_set_iteration(self._h, int(v)))
+
+    def arena_bytes(self):
+        return int(lib().gtob_solver_arena_bytes(self._h))
+
+    def arena(self, which, p):
+        out = np.zeros(self.spot.data_size[p], np.float32)
+        _check(lib().gtob_solver_get_arena(self._h, int(which), int(p), _ptr(out)))
+        return out
+
+    def set_arena(self, which, p, data):
+        d = np.ascontiguousarray(data, np.float32)
+        assert d.size == self.spot.data_size[p]
+        _check(lib().gtob_solver_set_arena(self._h, int(which), int(p), _ptr(d)))
+
+    def _na_nh(self, node):
+        t = self.spot.tree()
+        return int(t["nchild"][node]), self.spot.nh[int(t["player"][node])]
+
+    def average_strategy(self, node, na=None, nh=None):
+        if na is None:
+            na, nh = self._na_nh(node)
+        out = np.zeros(na * nh, np.float32)
+        _check(lib().gtob_solver_average_strategy(self._h, int(node), _ptr(out)))
+        return out
+
+    def solved_strategy(self, node, na=None, nh=None):
+        if na is None:
+            na, nh = self._na_nh(node)
+        out = np.zeros(na * nh, np.float32)
+        _check(lib().gtob_solver_solved_strategy(self._h, int(node), _ptr(out)))
+        return out
+
+    def lock_node(self, path, mode, freqs=None, edits=None, label=""):
+        """query.rs lock_node. path: list of ints (action index) or card strings;
+        mode: "freeze" | "range" | "hands"."""
+        steps = []
+        for s in path:
+            if isinstance(s, str):
+                r, su = "23456789TJQKA".index(s[0].upper()), "cdhs".index(s[1].lower())
+                steps.append(-1 - (r * 4 + su))
+            else:
+                steps.append(int(s))
+        st = np.array(steps + [0], np.int32)
+        m = {"freeze": 0, "range": 1, "hands": 2}[mode]
+        fr = np.array((freqs or []) + [0.0], np.float32)
+        ej = json.dumps([[c, list(map(float, f))] for c, f in (edits or [])]).encode()
+        node = C.c_uint32()
+        _check(lib().gtob_solver_lock_node(self._h, _ptr(st), len(steps), m, _ptr(fr), len(freqs or []), ej,
+                                           label.encode(), C.byref(node)))
+        return node.value
+
+    def set_lock(self, node, sigma, label=""):
+        s = np.ascontiguousarray(sigma, np.float32)
+        _check(lib().gtob_solver_set_lock(self._h, int(node), _ptr(s), s.size, label.encode()))
+
+    def clear_locks(self):
+        _check(lib().gtob_solver_clear_locks(self._h))
+
+    @property
+    def num_locks(self):
+        return lib().gtob_solver_num_locks(self._h)
+
+    def ensure_symmetric(self):
+        _check(lib().gtob_solver_ensure_symmetric(self._h))
+
+    def save(self, path):
+        _check(lib().gtob_save(self._h, os.fspath(path).encode()))
+
+    @staticmethod
+    def load(path, storage="f32"):
+        h = C.c_void_p()
+        _check(lib().gtob_load(os.fspath(path).encode(), STORAGE[storage], C.byref(h)))
+        # the loaded solver owns a spot rebuilt from the header; expose it too
+        with open(path, "rb") as f:
+            f.read(10)
+            header = json.loads(f.readline())
+        spot = Spot(header["config"], lenient=True)
+        return Solver(spot, storage=storage, _handle=h)
+
+
+class GpuSolver:
+    """gpu/mod.rs GpuSolver: device buffers, CUDA-graph iterations, BR checks, syncs."""
+
+    def __init__(self, solver, device_format=None):
+        h = C.c_void_p()
+        _check(lib().gtob_gpu_new(solver._h, DEVICE_FORMAT[device_format], C.byref(h)))
+        self._h = h
+        self.solver = solver
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gtob_gpu_free(self._h)
+            self._h = None
+
+    def close(self):
+        self.__del__()
+
+    def iterate(self, n=1):
+        _check(lib().gtob_gpu_iterate(self._h, int(n)))
+
+    def iterate_profiled(self):
+        p = Profile()
+        _check(lib().gtob_gpu_iterate_profiled(self._h, C.byref(p)))
+        return p
+
+    def exploitability(self, solver=None):
+        v = C.c_double()
+        _check(lib().gtob_gpu_exploitability(self._h, (solver or self.solver)._h, C.byref(v)))
+        return v.value
+
+    def sync_to_cpu(self, solver=None):
+        _check(lib().gtob_gpu_sync_to_cpu(self._h, (solver or self.solver)._h))
+
+    def sync_strategy(self, solver=None):
+        _check(lib().gtob_gpu_sync_strategy(self._h, (solver or self.solver)._h))
+
+    def synchronize(self):
+        _check(lib().gtob_gpu_synchronize(self._h))
+
+    def update_locks(self, solver=None):
+        _check(lib().gtob_gpu_update_locks(self._h, (solver or self.solver)._h))
+
+    @property
+    def iteration(self):
+        return int(lib().gtob_gpu_iteration(self._h))
+
+    def info(self):
+        i = GpuInfo()
+        _check(lib().gtob_gpu_info_get(self._h, C.byref(i)))
+        return {k: (list(getattr(i, k)) if k in ("reach_slots", "device_action_nodes") else getattr(i, k))
+                for k, _ in GpuInfo._fields_}
+
+    def root_cfv(self, p, mode=0):
+        out = np.zeros(self.solver.spot.nh[p], np.float32)
+        _check(lib().gtob_gpu_root_cfv(self._h, int(p), int(mode), _ptr(out)))
+        return out
+
+    def export_arena(self, which, p):
+        out = np.zeros(self.solver.spot.data_size[p], np.float32)
+        _check(lib().gtob_gpu_export_arena(self._h, int(which), int(p), _ptr(out)))
+        return out
+
+    def discounts(self):
+        out = np.zeros(3, np.float32)
+        _check(lib().gtob_gpu_discounts(self._h, _ptr(out)))
+        return out

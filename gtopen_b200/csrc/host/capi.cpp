@@ -1,0 +1,355 @@
+// C ABI (include/gtob.h): thin wrappers turning C++ exceptions into status
+// codes plus a thread-local message, the way the reference's Result<_, String>
+// errors reach its callers.
+#include "../../../include/gtob.h"
+
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../kernels/engine.hpp"
+#include "core.hpp"
+#include "solver.hpp"
+
+using namespace gtob;
+
+struct gtob_spot { std::shared_ptr<Spot> s; };
+struct gtob_solver { std::unique_ptr<HostSolver> v; };
+struct gtob_gpu { std::unique_ptr<GpuEngine> e; };
+
+static thread_local std::string g_err;
+
+template <class T>
+static void put(T* dst, const std::vector<T>& v) {
+    if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(T));
+}
+
+static int classify(const std::string& m) {
+    if (m.rfind("cuda: out of memory", 0) == 0 || m.find("out of memory") != std::string::npos) return GTOB_ENOMEM_DEVICE;
+    if (m.rfind("cuda:", 0) == 0) return GTOB_ECUDA;
+    if (m.rfind("io:", 0) == 0 || m.find("cannot open") != std::string::npos || m.find("write failed") != std::string::npos ||
+        m.find("rename failed") != std::string::npos || m.find("cannot create") != std::string::npos)
+        return GTOB_EIO;
+    return GTOB_EINVAL;
+}
+#define API_BEGIN try {
+#define API_END                              \
+    }                                        \
+    catch (const std::exception& ex) {       \
+        g_err = ex.what();                   \
+        return classify(g_err);              \
+    }                                        \
+    catch (...) {                            \
+        g_err = "unknown error";             \
+        return GTOB_EINVAL;                  \
+    }                                        \
+    return GTOB_OK;
+#define REQUIRE(c)                                               \
+    if (!(c)) {                                                  \
+        g_err = "invalid argument: " #c;                         \
+        return GTOB_EINVAL;                                      \
+    }
+
+extern "C" {
+
+const char* gtob_last_error(void) { return g_err.c_str(); }
+const char* gtob_kernel_name(int k) { return (k >= 0 && k < 7) ? kKernelNames[k] : ""; }
+const char* gtob_version(void) { return "gtob 0.1 sm_100a"; }
+
+int gtob_spot_from_json(const char* js, uint64_t max_nodes, int lenient, gtob_spot** out) {
+    REQUIRE(js && out);
+    *out = nullptr;
+    API_BEGIN
+    SpotConfig cfg = config_from_json(json::parse(js));
+    auto s = build_spot(cfg, max_nodes, lenient != 0);
+    *out = new gtob_spot{std::shared_ptr<Spot>(s.release())};
+    API_END
+}
+void gtob_spot_free(gtob_spot* s) { delete s; }
+int gtob_spot_info_get(const gtob_spot* s, gtob_spot_info* o) {
+    REQUIRE(s && o);
+    const Spot& sp = *s->s;
+    o->num_nodes = sp.tree.size();
+    o->num_action_nodes = sp.num_action_nodes();
+    o->num_children = sp.tree.children.size();
+    o->num_actions = sp.tree.act_kind.size();
+    o->data_size[0] = sp.tree.data_size[0];
+    o->data_size[1] = sp.tree.data_size[1];
+    o->num_hands[0] = (uint32_t)sp.hands[0].size();
+    o->num_hands[1] = (uint32_t)sp.hands[1].size();
+    o->root_street = (uint32_t)sp.tree.root_street;
+    o->num_suit_perms = (uint32_t)sp.perms.size();
+    return GTOB_OK;
+}
+int gtob_spot_tree(const gtob_spot* s, uint8_t* kind, uint8_t* player, uint8_t* street, uint8_t* nchild,
+                   uint32_t* cs, uint32_t* as, uint64_t* doff, double* p0, double* p1, double* tw, double* tl,
+                   double* tt) {
+    REQUIRE(s);
+    const Tree& t = s->s->tree;
+    put(kind, t.kind); put(player, t.player); put(street, t.street); put(nchild, t.nchild);
+    put(cs, t.child_start); put(as, t.action_start); put(doff, t.data_off);
+    put(p0, t.put0); put(p1, t.put1); put(tw, t.twin); put(tl, t.tlose); put(tt, t.ttie);
+    return GTOB_OK;
+}
+int gtob_spot_children(const gtob_spot* s, uint32_t* out) {
+    REQUIRE(s && out);
+    put(out, s->s->tree.children);
+    return GTOB_OK;
+}
+int gtob_spot_actions(const gtob_spot* s, int32_t* kind, double* amount) {
+    REQUIRE(s);
+    const Tree& t = s->s->tree;
+    for (size_t i = 0; i < t.act_kind.size(); i++) {
+        if (kind) kind[i] = t.act_kind[i];
+        if (amount) amount[i] = t.act_amount[i];
+    }
+    return GTOB_OK;
+}
+int gtob_spot_hands(const gtob_spot* s, int p, uint8_t* c1, uint8_t* c2, float* w, uint32_t* same) {
+    REQUIRE(s && (p == 0 || p == 1));
+    const Hands& h = s->s->hands[p];
+    put(c1, h.c1); put(c2, h.c2); put(w, h.w); put(same, s->s->same[p]);
+    return GTOB_OK;
+}
+int gtob_spot_suit_perms(const gtob_spot* s, uint8_t* perms4, uint16_t* hp0, uint16_t* hp1) {
+    REQUIRE(s);
+    const Spot& sp = *s->s;
+    for (size_t k = 0; k < sp.perms.size(); k++) {
+        if (perms4) std::memcpy(perms4 + 4 * k, sp.perms[k].data(), 4);
+        if (hp0) std::memcpy(hp0 + k * sp.hands[0].size(), sp.hand_perm[0][k].data(), 2 * sp.hands[0].size());
+        if (hp1) std::memcpy(hp1 + k * sp.hands[1].size(), sp.hand_perm[1][k].data(), 2 * sp.hands[1].size());
+    }
+    return GTOB_OK;
+}
+int gtob_spot_river(const gtob_spot* s, int p, const uint8_t* dealt, int nd, uint32_t* str, uint16_t* idx) {
+    REQUIRE(s && (p == 0 || p == 1) && nd >= 0 && nd <= 2);
+    API_BEGIN
+    const RiverBoard& rb = s->s->river_at(dealt, nd);
+    put(str, rb.str[p]);
+    put(idx, rb.idx[p]);
+    return (int)rb.str[p].size();
+    API_END
+}
+double gtob_spot_pair_weight_sum(const gtob_spot* s) { return s ? s->s->pair_weight_sum() : 0.0; }
+uint32_t gtob_evaluate7(const uint8_t* c) { return eval7(c); }
+int gtob_parse_range(const char* text, float* w) {
+    REQUIRE(text && w);
+    API_BEGIN
+    auto v = parse_range_weights(text);
+    std::memcpy(w, v.data(), sizeof(float) * 1326);
+    API_END
+}
+uint64_t gtob_estimate_vram(const gtob_spot* s) {
+    if (!s) return 0;
+    try {
+        return estimate_vram(*s->s);
+    } catch (...) {
+        return 0;
+    }
+}
+int gtob_vram_info_mb(uint64_t* f, uint64_t* t) {
+    REQUIRE(f && t);
+    if (!vram_info_mb(f, t)) {
+        g_err = "cuda: no device";
+        return GTOB_ECUDA;
+    }
+    return GTOB_OK;
+}
+
+int gtob_solver_new(gtob_spot* s, int storage, int algo, int use_iso, gtob_solver** out) {
+    REQUIRE(s && out && (storage == 0 || storage == 1) && algo >= 0 && algo <= 2);
+    *out = nullptr;
+    API_BEGIN
+    *out = new gtob_solver{std::make_unique<HostSolver>(s->s, storage, algo, use_iso != 0)};
+    API_END
+}
+void gtob_solver_free(gtob_solver* v) { delete v; }
+uint32_t gtob_solver_iteration(const gtob_solver* v) { return v ? v->v->iteration : 0; }
+int gtob_solver_set_iteration(gtob_solver* v, uint32_t it) {
+    REQUIRE(v);
+    v->v->iteration = it;
+    return GTOB_OK;
+}
+uint64_t gtob_solver_arena_bytes(const gtob_solver* v) { return v ? v->v->arena_bytes() : 0; }
+int gtob_solver_get_arena(const gtob_solver* v, int which, int p, float* out) {
+    REQUIRE(v && out && which >= 0 && which <= 2 && (p == 0 || p == 1));
+    API_BEGIN
+    v->v->arena_f32(which, p, out);
+    API_END
+}
+int gtob_solver_set_arena(gtob_solver* v, int which, int p, const float* in) {
+    REQUIRE(v && in && which >= 0 && which <= 2 && (p == 0 || p == 1));
+    API_BEGIN
+    v->v->set_arena_f32(which, p, in);
+    API_END
+}
+static int check_action_node(const gtob_solver* v, uint32_t node) {
+    const Tree& t = v->v->spot->tree;
+    if (node >= t.size() || t.kind[node] != kAction) {
+        g_err = "node " + std::to_string(node) + " is not an action node";
+        return GTOB_EINVAL;
+    }
+    return GTOB_OK;
+}
+int gtob_solver_average_strategy(const gtob_solver* v, uint32_t node, float* out) {
+    REQUIRE(v && out);
+    if (int r = check_action_node(v, node)) return r;
+    v->v->average_strategy(node, out);
+    return GTOB_OK;
+}
+int gtob_solver_solved_strategy(const gtob_solver* v, uint32_t node, float* out) {
+    REQUIRE(v && out);
+    if (int r = check_action_node(v, node)) return r;
+    v->v->solved_strategy(node, out);
+    return GTOB_OK;
+}
+int gtob_solver_lock_node(gtob_solver* v, const int32_t* steps, int ns, int mode, const float* freqs, int nf,
+                          const char* edits_json, const char* label, uint32_t* node_out) {
+    REQUIRE(v && ns >= 0 && (ns == 0 || steps) && mode >= 0 && mode <= 2 && (nf == 0 || freqs));
+    API_BEGIN
+    std::vector<int> st(steps, steps + ns);
+    std::vector<float> fr(freqs, freqs + nf);
+    std::vector<std::pair<std::string, std::vector<float>>> edits;
+    if (mode == 2) {
+        if (!edits_json) throw Error("hand edits required");
+        json::Value e = json::parse(edits_json);
+        for (auto& x : e.arr) {
+            if (x.kind != json::Value::ARR || x.arr.size() != 2 || x.arr[0].kind != json::Value::STR)
+                throw Error("edit must be [combo, [freqs...]]");
+            std::vector<float> f;
+            for (auto& y : x.arr[1].arr) f.push_back((float)y.num);
+            edits.push_back({x.arr[0].str, f});
+        }
+    }
+    uint32_t n = v->v->lock_node(st, mode, fr, edits, label ? label : "");
+    if (node_out) *node_out = n;
+    API_END
+}
+int gtob_solver_set_lock(gtob_solver* v, uint32_t node, const float* sigma, uint64_t n, const char* label) {
+    REQUIRE(v && sigma);
+    API_BEGIN
+    std::vector<std::pair<uint32_t, std::vector<float>>> l{{node, std::vector<float>(sigma, sigma + n)}};
+    validate_locks(*v->v->spot, l);
+    v->v->locks[node] = l[0].second;
+    v->v->lock_labels[node] = label ? label : "";
+    v->v->sym_dirty = true;
+    API_END
+}
+int gtob_solver_clear_locks(gtob_solver* v) {
+    REQUIRE(v);
+    if (!v->v->locks.empty()) v->v->sym_dirty = true;
+    v->v->locks.clear();
+    v->v->lock_labels.clear();
+    return GTOB_OK;
+}
+int gtob_solver_num_locks(const gtob_solver* v) { return v ? (int)v->v->locks.size() : 0; }
+int gtob_solver_ensure_symmetric(gtob_solver* v) {
+    REQUIRE(v);
+    API_BEGIN
+    v->v->ensure_symmetric();
+    API_END
+}
+int gtob_save(const gtob_solver* v, const char* path) {
+    REQUIRE(v && path);
+    API_BEGIN
+    v->v->save(path);
+    API_END
+}
+int gtob_load(const char* path, int storage, gtob_solver** out) {
+    REQUIRE(path && out && (storage == 0 || storage == 1));
+    *out = nullptr;
+    API_BEGIN
+    *out = new gtob_solver{HostSolver::load(path, storage)};
+    API_END
+}
+
+int gtob_gpu_new(const gtob_solver* v, int fmt, gtob_gpu** out) {
+    REQUIRE(v && out && fmt >= -1 && fmt <= 1);
+    *out = nullptr;
+    API_BEGIN
+    *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt)};
+    API_END
+}
+void gtob_gpu_free(gtob_gpu* g) { delete g; }
+int gtob_gpu_iterate(gtob_gpu* g, int n) {
+    REQUIRE(g && n >= 0);
+    API_BEGIN
+    g->e->iterate(n);
+    API_END
+}
+int gtob_gpu_iterate_profiled(gtob_gpu* g, gtob_profile* out) {
+    REQUIRE(g && out);
+    API_BEGIN
+    Profile p = g->e->iterate_profiled();
+    std::memcpy(out->ms, p.ms, sizeof(p.ms));
+    std::memcpy(out->launches, p.launches, sizeof(p.launches));
+    API_END
+}
+int gtob_gpu_exploitability(gtob_gpu* g, const gtob_solver* v, double* chips) {
+    REQUIRE(g && v && chips);
+    API_BEGIN
+    *chips = g->e->exploitability(*v->v);
+    API_END
+}
+int gtob_gpu_sync_to_cpu(gtob_gpu* g, gtob_solver* v) {
+    REQUIRE(g && v);
+    API_BEGIN
+    g->e->sync_to_cpu(*v->v, false);
+    API_END
+}
+int gtob_gpu_sync_strategy(gtob_gpu* g, gtob_solver* v) {
+    REQUIRE(g && v);
+    API_BEGIN
+    g->e->sync_to_cpu(*v->v, true);
+    API_END
+}
+int gtob_gpu_synchronize(gtob_gpu* g) {
+    REQUIRE(g);
+    API_BEGIN
+    g->e->synchronize();
+    API_END
+}
+int gtob_gpu_update_locks(gtob_gpu* g, const gtob_solver* v) {
+    REQUIRE(g && v);
+    API_BEGIN
+    g->e->update_locks(*v->v);
+    API_END
+}
+uint32_t gtob_gpu_iteration(const gtob_gpu* g) { return g ? g->e->iteration() : 0; }
+int gtob_gpu_info_get(gtob_gpu* g, gtob_gpu_info* o) {
+    REQUIRE(g && o);
+    const Plan& P = g->e->plan();
+    o->device_bytes = g->e->device_bytes();
+    o->visited_nodes = P.num_visited;
+    o->cfv_slots = P.n_cslots;
+    o->reach_slots[0] = P.n_rslots[0];
+    o->reach_slots[1] = P.n_rslots[1];
+    o->device_action_nodes[0] = P.n_anodes[0];
+    o->device_action_nodes[1] = P.n_anodes[1];
+    o->visited_terminals = P.visited_terminals;
+    o->num_levels = (uint32_t)P.num_levels;
+    o->num_river_slots = P.num_slots;
+    o->arena_format = g->e->format();
+    o->iter_bytes = g->e->iter_bytes();
+    return GTOB_OK;
+}
+int gtob_gpu_root_cfv(gtob_gpu* g, int p, int mode, float* out) {
+    REQUIRE(g && out && (p == 0 || p == 1) && (mode == 0 || mode == 1));
+    API_BEGIN
+    g->e->root_cfv(p, mode, out);
+    API_END
+}
+int gtob_gpu_export_arena(gtob_gpu* g, int which, int p, float* out) {
+    REQUIRE(g && out && which >= 0 && which <= 2 && (p == 0 || p == 1));
+    API_BEGIN
+    g->e->export_arena(which, p, out);
+    API_END
+}
+int gtob_gpu_discounts(gtob_gpu* g, float* out3) {
+    REQUIRE(g && out3);
+    API_BEGIN
+    g->e->discounts(out3);
+    API_END
+}
+
+}  // extern "C"

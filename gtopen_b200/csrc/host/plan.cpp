@@ -1,0 +1,261 @@
+// Device plan builder: see plan.hpp.  Traversal and orbit folding follow the
+// reference's gpu/plan.rs:100-198 (levels = depth, representative chance
+// branches only, card -> (representative, suit permutation) tables).
+#include "plan.hpp"
+
+#include <algorithm>
+#include <unordered_map>
+
+namespace gtob {
+
+namespace {
+struct Visit {
+    uint32_t node, level;
+    uint8_t dealt[2];
+    int ndealt;
+    uint32_t cslot;
+    uint32_t rs[2];
+};
+template <class T>
+void flatten(std::vector<std::vector<std::pair<uint32_t, T>>>& by_level, std::vector<T>& flat, std::vector<Span>& span) {
+    for (auto& lst : by_level) {
+        std::sort(lst.begin(), lst.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        span.push_back({(uint32_t)flat.size(), (uint32_t)lst.size()});
+        for (auto& x : lst) flat.push_back(x.second);
+    }
+}
+}  // namespace
+
+Plan build_plan(const Spot& sp, bool use_iso) {
+    const Tree& t = sp.tree;
+    Plan P;
+    P.nh[0] = (int)sp.hands[0].size();
+    P.nh[1] = (int)sp.hands[1].size();
+    P.nh_max = std::max(P.nh[0], P.nh[1]);
+    P.iso_active = use_iso && sp.perms.size() > 1;
+    const size_t n = t.size();
+
+    std::vector<std::vector<std::pair<uint32_t, ActItem>>> act_l;
+    std::vector<std::vector<std::pair<uint32_t, EdgeItem>>> edge_l;
+    std::vector<std::vector<std::pair<uint32_t, FoldItem>>> fold_l;
+    std::vector<std::vector<std::pair<uint32_t, ShowItem>>> show_l;
+    std::vector<std::vector<std::pair<uint32_t, ChanceItem>>> chance_l;
+    auto grow = [&](uint32_t lv) {
+        if (act_l.size() <= lv) {
+            act_l.resize(lv + 1);
+            edge_l.resize(lv + 1);
+            fold_l.resize(lv + 1);
+            show_l.resize(lv + 1);
+            chance_l.resize(lv + 1);
+        }
+    };
+    std::unordered_map<size_t, uint32_t> slot_of_key;
+    std::vector<uint8_t> visited(n, 0);
+
+    uint64_t next_c = 1, next_r[2] = {1, 1};
+    std::vector<Visit> stack;
+    stack.push_back({0, 0, {0, 0}, 0, 0, {0, 0}});
+    while (!stack.empty()) {
+        Visit v = stack.back();
+        stack.pop_back();
+        const uint32_t nd = v.node;
+        visited[nd] = 1;
+        grow(v.level);
+        P.num_visited++;
+        switch (t.kind[nd]) {
+            case kAction: {
+                const int a = t.player[nd], na = t.nchild[nd];
+                ActItem it{};
+                it.node = nd;
+                it.cslot = v.cslot;
+                it.child_cslot = (uint32_t)next_c;
+                it.rslot = v.rs[a];
+                it.child_rslot = (uint32_t)next_r[a];
+                it.actor = (uint32_t)a;
+                it.na = (uint32_t)na;
+                next_c += na;
+                next_r[a] += na;
+                act_l[v.level].push_back({nd, it});
+                for (int k = na - 1; k >= 0; k--) {  // push reversed so pops run in action order
+                    Visit c = v;
+                    c.node = t.child(nd, k);
+                    c.level = v.level + 1;
+                    c.cslot = it.child_cslot + k;
+                    c.rs[a] = it.child_rslot + k;
+                    stack.push_back(c);
+                }
+                break;
+            }
+            case kChance: {
+                std::vector<int> valid = P.iso_active ? sp.perms_fixing(v.dealt, v.ndealt) : std::vector<int>{0};
+                struct CardRep { uint8_t card, rep; uint32_t perm; };
+                std::vector<CardRep> cr;
+                for (int c = 0; c < 52; c++) {
+                    uint32_t ch = t.children[t.child_start[nd] + c];
+                    bool dealt = false;
+                    for (int i = 0; i < v.ndealt; i++) dealt = dealt || v.dealt[i] == c;
+                    if (ch == kSentinel || dealt) continue;
+                    uint8_t rep = (uint8_t)c;
+                    uint32_t krep = 0;
+                    for (int k : valid) {
+                        uint8_t pc = card_permute((uint8_t)c, sp.perms[k]);
+                        if (pc < rep) { rep = pc; krep = (uint32_t)k; }
+                    }
+                    cr.push_back({(uint8_t)c, rep, krep});
+                }
+                uint32_t rep_slot[52];
+                uint32_t nreps = 0;
+                const uint64_t cbase = next_c, rbase0 = next_r[0], rbase1 = next_r[1];
+                for (auto& x : cr)
+                    if (x.card == x.rep) rep_slot[x.card] = nreps++;
+                next_c += nreps;
+                next_r[0] += nreps;
+                next_r[1] += nreps;
+                ChanceItem ci{};
+                ci.cslot = v.cslot;
+                ci.cc_start = (uint32_t)P.cards.size();
+                ci.cc_count = (uint32_t)cr.size();
+                ci.inv = 1.0f / (float)(46 - (int)t.street[nd]);
+                for (auto& x : cr) P.cards.push_back({x.card, (uint32_t)(cbase + rep_slot[x.rep]), x.perm, 0});
+                chance_l[v.level].push_back({nd, ci});
+                for (int k = (int)cr.size() - 1; k >= 0; k--) {
+                    const auto& x = cr[k];
+                    if (x.card != x.rep) continue;
+                    uint32_t r = rep_slot[x.card];
+                    Visit c = v;
+                    c.node = t.children[t.child_start[nd] + x.card];
+                    c.level = v.level + 1;
+                    c.dealt[c.ndealt++] = x.card;
+                    c.cslot = (uint32_t)(cbase + r);
+                    c.rs[0] = (uint32_t)(rbase0 + r);
+                    c.rs[1] = (uint32_t)(rbase1 + r);
+                    EdgeItem e{{v.rs[0], v.rs[1]}, {c.rs[0], c.rs[1]}, x.card, 0};
+                    edge_l[v.level].push_back({c.node, e});
+                    stack.push_back(c);
+                }
+                break;
+            }
+            case kFold: {
+                FoldItem f{v.cslot, {v.rs[0], v.rs[1]}, t.player[nd], (float)t.twin[nd], (float)t.tlose[nd]};
+                fold_l[v.level].push_back({nd, f});
+                P.visited_terminals++;
+                break;
+            }
+            default: {
+                size_t key = sp.river_key(v.dealt, v.ndealt);
+                auto itk = slot_of_key.find(key);
+                uint32_t s;
+                if (itk == slot_of_key.end()) {
+                    s = (uint32_t)P.slot_key.size();
+                    slot_of_key[key] = s;
+                    P.slot_key.push_back((uint32_t)key);
+                } else {
+                    s = itk->second;
+                }
+                ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, s, (float)t.twin[nd], (float)t.tlose[nd], (float)t.ttie[nd], 0};
+                show_l[v.level].push_back({nd, si});
+                P.visited_terminals++;
+                break;
+            }
+        }
+    }
+    P.n_cslots = next_c;
+    P.n_rslots[0] = next_r[0];
+    P.n_rslots[1] = next_r[1];
+    P.num_levels = (int)act_l.size();
+
+    // device arena layout: visited action nodes of each player in node order
+    P.node_sidx.assign(n, -1);
+    for (uint32_t nd = 0; nd < n; nd++) {
+        if (!visited[nd] || t.kind[nd] != kAction) continue;
+        int a = t.player[nd];
+        uint64_t len = (uint64_t)t.nchild[nd] * P.nh[a];
+        P.node_sidx[nd] = (int32_t)P.n_anodes[a];
+        P.anode_id[a].push_back(nd);
+        P.anode_off[a].push_back(P.arena_len[a]);
+        P.n_anodes[a]++;
+        P.arena_len[a] += (len + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
+        P.visited_action_elems[a] += len;
+    }
+    for (auto& lst : act_l)
+        for (auto& x : lst) {
+            int a = (int)x.second.actor;
+            x.second.sidx = (uint32_t)P.node_sidx[x.first];
+            x.second.aoff = P.anode_off[a][x.second.sidx];
+        }
+    flatten(act_l, P.act, P.act_span);
+    flatten(edge_l, P.edge, P.edge_span);
+    flatten(fold_l, P.fold, P.fold_span);
+    flatten(show_l, P.show, P.show_span);
+    flatten(chance_l, P.chance, P.chance_span);
+
+    // per-hand card lists (fold evaluator: hands of player q holding card c)
+    for (int q = 0; q < 2; q++) {
+        std::vector<std::vector<uint16_t>> by(52);
+        for (size_t i = 0; i < sp.hands[q].size(); i++) {
+            by[sp.hands[q].c1[i]].push_back((uint16_t)i);
+            by[sp.hands[q].c2[i]].push_back((uint16_t)i);
+        }
+        for (int c = 0; c < 52; c++) {
+            P.hcard_off[q].push_back((uint32_t)P.hcard_idx[q].size());
+            P.hcard_idx[q].insert(P.hcard_idx[q].end(), by[c].begin(), by[c].end());
+        }
+        P.hcard_off[q].push_back((uint32_t)P.hcard_idx[q].size());
+    }
+
+    // river slot tables
+    P.num_slots = (uint32_t)P.slot_key.size();
+    for (uint32_t s = 0; s < P.num_slots; s++) {
+        const RiverBoard& rb = *sp.river.at(P.slot_key[s]);
+        for (int q = 0; q < 2; q++) {
+            P.sorted_off[q].push_back((uint32_t)P.sorted_idx[q].size());
+            P.sorted_cnt[q].push_back((uint32_t)rb.idx[q].size());
+            P.max_sorted = std::max<uint32_t>(P.max_sorted, (uint32_t)rb.idx[q].size());
+            P.sorted_idx[q].insert(P.sorted_idx[q].end(), rb.idx[q].begin(), rb.idx[q].end());
+            std::vector<std::vector<uint16_t>> by(52);
+            for (size_t k = 0; k < rb.idx[q].size(); k++) {
+                uint16_t h = rb.idx[q][k];
+                by[sp.hands[q].c1[h]].push_back((uint16_t)k);
+                by[sp.hands[q].c2[h]].push_back((uint16_t)k);
+            }
+            for (int c = 0; c < 52; c++) {
+                P.ccard_off[q].push_back((uint32_t)P.ccard_pos[q].size());
+                P.ccard_pos[q].insert(P.ccard_pos[q].end(), by[c].begin(), by[c].end());
+            }
+            P.ccard_off[q].push_back((uint32_t)P.ccard_pos[q].size());
+        }
+        for (int p = 0; p < 2; p++) {
+            const int o = 1 - p;
+            const auto& ms = rb.str[p];
+            const auto& os = rb.str[o];
+            const uint16_t* opos = P.ccard_pos[o].data();
+            const uint32_t* ooff = P.ccard_off[o].data() + (size_t)s * 53;
+            P.rank_off[p].push_back((uint32_t)P.rank[p].size());
+            P.rank_cnt[p].push_back((uint32_t)ms.size());
+            size_t lb = 0, ub = 0;
+            for (size_t k = 0; k < ms.size(); k++) {
+                while (lb < os.size() && os[lb] < ms[k]) lb++;
+                if (ub < lb) ub = lb;
+                while (ub < os.size() && os[ub] <= ms[k]) ub++;
+                uint16_t h = rb.idx[p][k];
+                RankEntry e{};
+                e.idx = h;
+                e.lb = (uint16_t)lb;
+                e.ub = (uint16_t)ub;
+                auto count_below = [&](int card, size_t bound) {
+                    const uint16_t* b = opos + ooff[card];
+                    const uint16_t* en = opos + ooff[card + 1];
+                    return (uint16_t)(std::lower_bound(b, en, (uint16_t)bound) - b);
+                };
+                e.c1lo = count_below(sp.hands[p].c1[h], lb);
+                e.c1hi = count_below(sp.hands[p].c1[h], ub);
+                e.c2lo = count_below(sp.hands[p].c2[h], lb);
+                e.c2hi = count_below(sp.hands[p].c2[h], ub);
+                P.rank[p].push_back(e);
+            }
+        }
+    }
+    return P;
+}
+
+}  // namespace gtob

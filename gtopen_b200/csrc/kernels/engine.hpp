@@ -1,0 +1,54 @@
+// GPU engine for one spot: the role of the reference's gpu::GpuSolver
+// (crates/solver/src/gpu/mod.rs).  Owns every device buffer; copies arenas and
+// locks out of a HostSolver and syncs results back into it.
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+
+#include "../host/plan.hpp"
+#include "../host/solver.hpp"
+
+namespace gtob {
+
+enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1 };
+
+struct Profile {
+    double ms[7];
+    uint32_t launches[7];
+};
+extern const char* const kKernelNames[7];
+
+struct EngineImpl;
+
+class GpuEngine {
+  public:
+    // fmt < 0: follow the host storage (f32 -> f32 arenas, compressed -> i16/u16)
+    GpuEngine(const HostSolver& host, int fmt);
+    ~GpuEngine();
+    void iterate(int n);
+    Profile iterate_profiled();
+    double exploitability(const HostSolver& host);       // chips
+    void root_cfv(int p, int mode, float* out);          // eval sweep root values (mode 0 BR, 1 average)
+    void sync_to_cpu(HostSolver& host, bool strategy_only);
+    void synchronize();
+    void update_locks(const HostSolver& host);
+    uint32_t iteration() const;
+    int format() const;
+    const Plan& plan() const;
+    uint64_t device_bytes() const;
+    // algorithmic bytes of one CFR iteration / one BR check (traffic model)
+    double iter_bytes() const;
+    // device arena exports for tests (reference layout, decoded f32)
+    void export_arena(int which, int p, float* out);
+    // time one kind of level launch set: used by bench for the roofline
+    void discounts(float* out3);
+
+  private:
+    std::unique_ptr<EngineImpl> d_;
+};
+
+uint64_t estimate_vram(const Spot& spot);
+bool vram_info_mb(uint64_t* free_mb, uint64_t* total_mb);
+
+}  // namespace gtob

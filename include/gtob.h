@@ -1,0 +1,166 @@
+/*
+ * gtob -- C ABI of the B200 discounted-CFR engine for heads-up postflop spots.
+ *
+ * This is the drop-in boundary for the reference solver crate's GPU module
+ * (MatthewPDingle/GTOpen, crates/solver/src/gpu/mod.rs) and the parts of the
+ * crate that path needs (game.rs Spot, cfr.rs Solver state, save.rs).  Every
+ * entry point below names the reference item it replaces.  Conventions:
+ *   - every function returns an int status: GTOB_OK (0) or a negative error
+ *     class; gtob_last_error() returns a thread-local message (the reference
+ *     returns Result<_, String> with "cuda: ..." messages, gpu/mod.rs:56-58);
+ *   - handles are opaque and owned by the library (free with gtob_*_free);
+ *   - buffers are plain host pointers and sizes; no handle is thread-safe
+ *     (the reference drives one GpuSolver from one worker thread).
+ */
+#ifndef GTOB_H
+#define GTOB_H
+#include <stdint.h>
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GTOB_OK 0
+#define GTOB_EINVAL (-1)          /* bad argument / config / file: the reference's Err(String) */
+#define GTOB_ENOMEM_DEVICE (-2)   /* device allocation failed */
+#define GTOB_ECUDA (-3)           /* any other CUDA error */
+#define GTOB_ETIMEOUT_QUEUE (-4)  /* a bounded device wait gave up */
+#define GTOB_EIO (-5)             /* save/load I/O */
+
+#define GTOB_STORAGE_F32 0        /* store.rs Storage::F32 */
+#define GTOB_STORAGE_COMPRESSED 1 /* store.rs Storage::Compressed (i16 regrets, u16 sums) */
+#define GTOB_ALGO_DCFR 0          /* cfr.rs Algorithm::Dcfr (alpha 1.5, beta 0, gamma 2) */
+#define GTOB_ALGO_CFRPLUS 1       /* cfr.rs Algorithm::CfrPlus */
+#define GTOB_ALGO_PCFRPLUS 2      /* cfr.rs Algorithm::PcfrPlus */
+#define GTOB_DEVICE_FOLLOW_HOST (-1) /* device arena format follows the host storage */
+#define GTOB_DEVICE_F32 0
+#define GTOB_DEVICE_I16 1
+#define GTOB_ARENA_REGRETS 0
+#define GTOB_ARENA_STRATEGY 1
+#define GTOB_ARENA_PREDICTIONS 2
+
+typedef struct gtob_spot gtob_spot;
+typedef struct gtob_solver gtob_solver;
+typedef struct gtob_gpu gtob_gpu;
+
+/* gpu/mod.rs:22-36 KERNEL_NAMES and Profile{ms:[f64;7], launches:[u32;7]} */
+typedef struct {
+    double ms[7];
+    uint32_t launches[7];
+} gtob_profile;
+
+typedef struct {
+    uint64_t num_nodes;
+    uint64_t num_action_nodes;
+    uint64_t num_children;
+    uint64_t num_actions;
+    uint64_t data_size[2];
+    uint32_t num_hands[2];
+    uint32_t root_street;
+    uint32_t num_suit_perms;
+} gtob_spot_info;
+
+typedef struct {
+    uint64_t device_bytes;
+    uint64_t visited_nodes;
+    uint64_t cfv_slots;
+    uint64_t reach_slots[2];
+    uint64_t device_action_nodes[2];
+    uint64_t visited_terminals;
+    uint32_t num_levels;
+    uint32_t num_river_slots;
+    int32_t arena_format;
+    double iter_bytes; /* algorithmic bytes of one CFR iteration */
+} gtob_gpu_info;
+
+/* Thread-local message of the last failed call (Result::Err text). */
+const char* gtob_last_error(void);
+/* gpu/mod.rs:22-30 KERNEL_NAMES[k], k in 0..7 */
+const char* gtob_kernel_name(int k);
+const char* gtob_version(void);
+
+/* ---- Spot (game.rs) ---------------------------------------------------- */
+/* Spot::new / Spot::new_with_limit / Spot::new_lenient_with_limit (game.rs:103-133):
+ * spot_config_json is the reference SpotConfig JSON (serde conventions:
+ * {"PotPct":33}, {"PrevMult":2.5}, "AllIn"); max_nodes 0 = no budget. */
+int gtob_spot_from_json(const char* spot_config_json, uint64_t max_nodes, int lenient, gtob_spot** out);
+void gtob_spot_free(gtob_spot* spot);
+int gtob_spot_info_get(const gtob_spot* spot, gtob_spot_info* out);
+/* Tree arrays (tree.rs:178-211), each of num_nodes entries; NULL skips. */
+int gtob_spot_tree(const gtob_spot* spot, uint8_t* kind, uint8_t* player, uint8_t* street, uint8_t* nchild,
+                   uint32_t* child_start, uint32_t* action_start, uint64_t* data_offset, double* put0,
+                   double* put1, double* t_win, double* t_lose, double* t_tie);
+int gtob_spot_children(const gtob_spot* spot, uint32_t* out);
+int gtob_spot_actions(const gtob_spot* spot, int32_t* kind, double* amount);
+/* Spot::hands / weights / same_combo (game.rs:82-100) */
+int gtob_spot_hands(const gtob_spot* spot, int player, uint8_t* c1, uint8_t* c2, float* weight, uint32_t* same_combo);
+/* suit_perms (num_suit_perms x 4) and hand_perm[player] (num_suit_perms x num_hands) */
+int gtob_spot_suit_perms(const gtob_spot* spot, uint8_t* perms4, uint16_t* hand_perm0, uint16_t* hand_perm1);
+/* RiverTable::get for dealt cards (game.rs:36-62); returns the count of (strength, index) pairs */
+int gtob_spot_river(const gtob_spot* spot, int player, const uint8_t* dealt, int ndealt, uint32_t* strength,
+                    uint16_t* index);
+double gtob_spot_pair_weight_sum(const gtob_spot* spot);
+/* evaluator::evaluate7 (evaluator.rs:68) */
+uint32_t gtob_evaluate7(const uint8_t* cards7);
+/* range::Range::parse (range.rs:28) into 1326 weights indexed by combo_index */
+int gtob_parse_range(const char* text, float* weights1326);
+/* gpu::estimate_vram (gpu/mod.rs:946) and gpu::vram_info_mb (gpu/mod.rs:953) */
+uint64_t gtob_estimate_vram(const gtob_spot* spot);
+int gtob_vram_info_mb(uint64_t* free_mb, uint64_t* total_mb);
+
+/* ---- host solver state (cfr.rs Solver, save.rs, query.rs locks) --------- */
+/* Solver::with_storage (cfr.rs:122) + algo / use_isomorphism fields */
+int gtob_solver_new(gtob_spot* spot, int storage, int algo, int use_iso, gtob_solver** out);
+void gtob_solver_free(gtob_solver* solver);
+uint32_t gtob_solver_iteration(const gtob_solver* solver);
+int gtob_solver_set_iteration(gtob_solver* solver, uint32_t iteration);
+uint64_t gtob_solver_arena_bytes(const gtob_solver* solver);
+/* whole arena in the reference layout (save.rs:76-90): data_size[player] f32 */
+int gtob_solver_get_arena(const gtob_solver* solver, int which, int player, float* out);
+int gtob_solver_set_arena(gtob_solver* solver, int which, int player, const float* in);
+/* Solver::average_strategy (cfr.rs:729) / solved_strategy_into (cfr.rs:679): na*nh, action-major */
+int gtob_solver_average_strategy(const gtob_solver* solver, uint32_t node, float* out);
+int gtob_solver_solved_strategy(const gtob_solver* solver, uint32_t node, float* out);
+/* Solver::lock_node (query.rs:700-773).  steps: >= 0 action index, < 0 card (-1 - card).
+ * mode 0 Freeze, 1 Range{freqs}, 2 Hands{edits}: edits_json = [["AcAd",[1,0]],...] */
+int gtob_solver_lock_node(gtob_solver* solver, const int32_t* steps, int nsteps, int mode, const float* freqs,
+                          int nfreqs, const char* edits_json, const char* label, uint32_t* node_out);
+int gtob_solver_set_lock(gtob_solver* solver, uint32_t node, const float* sigma, uint64_t n, const char* label);
+int gtob_solver_clear_locks(gtob_solver* solver);
+int gtob_solver_num_locks(const gtob_solver* solver);
+/* Solver::ensure_symmetric (cfr.rs:749) */
+int gtob_solver_ensure_symmetric(gtob_solver* solver);
+/* Solver::save (save.rs:92) / Solver::load_with_storage (save.rs:149) */
+int gtob_save(const gtob_solver* solver, const char* path);
+int gtob_load(const char* path, int storage, gtob_solver** out);
+
+/* ---- GPU engine (gpu/mod.rs GpuSolver) ----------------------------------- */
+/* GpuSolver::new (gpu/mod.rs:146); device_format GTOB_DEVICE_* */
+int gtob_gpu_new(const gtob_solver* solver, int device_format, gtob_gpu** out);
+void gtob_gpu_free(gtob_gpu* gpu);
+/* GpuSolver::iterate (gpu/mod.rs:304), n times */
+int gtob_gpu_iterate(gtob_gpu* gpu, int n);
+/* GpuSolver::iterate_profiled (gpu/mod.rs:351) */
+int gtob_gpu_iterate_profiled(gtob_gpu* gpu, gtob_profile* out);
+/* GpuSolver::exploitability (gpu/mod.rs:367), chips */
+int gtob_gpu_exploitability(gtob_gpu* gpu, const gtob_solver* solver, double* chips);
+/* GpuSolver::sync_to_cpu (gpu/mod.rs:845) / sync_strategy (gpu/mod.rs:871) */
+int gtob_gpu_sync_to_cpu(gtob_gpu* gpu, gtob_solver* solver);
+int gtob_gpu_sync_strategy(gtob_gpu* gpu, gtob_solver* solver);
+/* GpuSolver::synchronize (gpu/mod.rs:889) */
+int gtob_gpu_synchronize(gtob_gpu* gpu);
+/* GpuSolver::update_locks (gpu/mod.rs:894) */
+int gtob_gpu_update_locks(gtob_gpu* gpu, const gtob_solver* solver);
+/* GpuSolver::iteration (pub field) */
+uint32_t gtob_gpu_iteration(const gtob_gpu* gpu);
+int gtob_gpu_info_get(gtob_gpu* gpu, gtob_gpu_info* out);
+/* root counterfactual values of one evaluation sweep (gpu/mod.rs:400-416; mode 0 BR, 1 average) */
+int gtob_gpu_root_cfv(gtob_gpu* gpu, int player, int mode, float* out);
+/* device arena decoded to the reference layout, without touching the host solver */
+int gtob_gpu_export_arena(gtob_gpu* gpu, int which, int player, float* out);
+/* the last discounts the device computed (pos, neg, strat) */
+int gtob_gpu_discounts(gtob_gpu* gpu, float* out3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
