@@ -1,0 +1,339 @@
+#!/usr/bin/env python
+"""Benchmark of the GTOpen postflop discounted-CFR iteration on B200.
+
+A step is one DCFR iteration (both traversals, alternating updates) of one
+spot.  Default workload: the flop single-raised-pot configuration (3-card
+board, OOP top 40% / IP top 55% of combos, pot 55, stack 975, bets
+{33,75,a}, raises {2.5x,a}, 3 raises: 10,835,022 nodes, 470 x 647 hands)
+with i16/u16 arenas, inputs synthesised from a fixed seed.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+value     = iterations/s over all ranks (each rank solves its own replica;
+            weak scaling, no data-path collective), device time from CUDA
+            events on the engine's stream, max over ranks.
+e2e       = the same metric through the C ABI from host arenas: upload
+            (GpuSolver::new), K iterations, one exploitability check, and the
+            arena download (sync_to_cpu), wall clock.
+roofline  = algorithmic bytes per iteration / device time per iteration vs
+            the measured HBM copy bandwidth.
+cpu_baseline / --impl reference = the CPU oracle (the reference CPU engine's
+            algorithm, restated in C++ and run with OpenMP over chance
+            branches) on the host cores.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAK_FALLBACK = 6650.0
+
+
+def load_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return PEAK_FALLBACK, "fallback"
+
+
+def make_config(name):
+    import gtopen_b200 as g
+    from gtopen_b200 import workloads as W
+    if name == "flop":
+        return W.flop_spot(g.evaluate7, seed=3)
+    if name == "turn":
+        return W.turn_spot(g.evaluate7, seed=2)
+    if name == "river":
+        return W.river_spot(seed=1)
+    if name == "bench_spot":
+        with open(os.path.join(ROOT, "tests", "golden", "bench_spot.json")) as f:
+            return json.load(f)
+    raise SystemExit("unknown workload " + name)
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (median SM clock, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(n_gpus):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def allmax(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(cfg, storage, steps, threads=None):
+    """The oracle (reference CPU engine restated, pruning on) on the host cores."""
+    from oracle import pyoracle as po
+    n = threads or os.cpu_count() or 1
+    po.set_threads(n)
+    t0 = time.perf_counter()
+    spot = po.Spot(cfg)
+    build_s = time.perf_counter() - t0
+    sv = po.Solver(spot, compressed=storage != "f32", algo="dcfr", use_iso=True, prune=True)
+    times = []
+    for _ in range(steps):
+        t = time.perf_counter()
+        sv.iterate(1)
+        times.append(time.perf_counter() - t)
+    return {"iter_s": times, "build_s": build_s, "cores": n}
+
+
+def run_reference(args, world, rank):
+    if rank != 0:
+        return
+    cfg = make_config(args.workload)
+    k = max(1, args.steps)
+    w = max(0, args.warmup)
+    r = cpu_baseline(cfg, args.storage, k + w, args.cpu_threads)
+    timed = r["iter_s"][w:]
+    total = sum(timed)
+    value = len(timed) / total
+    line = {
+        "impl": "reference", "metric": "CFR iterations/s (time-to-0.3%-pot exploitability & HBM GB/s vs peak)",
+        "value": value, "unit": "iter/s", "n_gpus": args.gpus, "steps": len(timed), "warmup": w,
+        "ms_per_step": 1000.0 * total / len(timed), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "i16" if args.storage != "f32" else "f32", "data": "synthetic (seeded spot)",
+        "config": workload_config(args, cfg),
+        "cpu_baseline": {"value": value, "unit": "iter/s", "cores": r["cores"], "kind": "port",
+                         "sample": "%d full DCFR iterations of the workload on the CPU oracle "
+                                   "(reference cfr.rs semantics, pruning on, OpenMP over chance cards)" % len(timed)},
+        "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(args, cfg):
+    return {"workload": {"flop": "flop SRP: 3-card board seed 3, OOP top40%/IP top55%, pot 55 stack 975, "
+                                 "bets {33,75,a} raises {2.5x,a} max 3 raises",
+                         "turn": "turn precision study: 4-card board seed 2, top 50% each, pot 100 stack 300",
+                         "river": "river HU: 5-card board seed 1, all 1081 combos each side, pot 100 stack 400",
+                         "bench_spot": "reference bench_spot.json (Ks7h2d, 257 v 319)"}[args.workload],
+            "board": cfg["board"], "arenas": "i16/u16 per-node scale" if args.storage != "f32" else "f32",
+            "algo": "DCFR alpha 1.5 beta 0 gamma 2, alternating", "l2": "inputs larger than L2 (arenas GB-sized)",
+            "parallelism": "replica per GPU (weak scaling)"}
+
+
+def run_ours(args, world, rank, local):
+    import gtopen_b200 as g
+    g.set_device(local)
+    cfg = make_config(args.workload)
+    t0 = time.perf_counter()
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, storage=args.storage, algo="dcfr", use_iso=True)
+    build_s = time.perf_counter() - t0
+    gpu = g.GpuSolver(host)
+    info = gpu.info()
+    gpu.iterate(args.warmup)
+    gpu.synchronize()
+    barrier(world)
+    clocks = Clocks(local)
+    clocks.start()
+    ms = gpu.time_iterations(args.steps)
+    ck = clocks.stop()
+    barrier(world)
+    ms_max = allmax(ms, world)
+    value = world * args.steps / (ms_max / 1000.0)
+    per_iter_s = ms / 1000.0 / args.steps
+    peak, peak_kind = load_peak()
+    achieved = info["iter_bytes"] / per_iter_s / 1e9
+    prof = gpu.iterate_profiled()
+    launches_per_iter = 1 + sum(prof.launches)
+    kinds = {g.KERNEL_NAMES[k]: round(prof.ms[k], 3) for k in range(7)}
+    tot = sum(prof.ms) or 1.0
+    dominant = max(range(7), key=lambda k: prof.ms[k])
+    e_chk = gpu.exploitability(host)
+    gpu.close()
+    del gpu
+
+    # end to end through the C ABI from host arenas
+    e2e = None
+    if not args.no_e2e:
+        barrier(world)
+        t = time.perf_counter()
+        gpu2 = g.GpuSolver(host)
+        gpu2.iterate(args.steps)
+        e = gpu2.exploitability(host)
+        gpu2.sync_to_cpu(host)
+        gpu2.synchronize()
+        dt = time.perf_counter() - t
+        dt_max = allmax(dt, world)
+        b = 2 if args.storage != "f32" else 4
+        arena_bytes = 2 * (spot.data_size[0] + spot.data_size[1]) * b
+        e2e = {"value": world * args.steps / dt_max, "unit": "iter/s",
+               "h2d_bytes_per_step": int(arena_bytes / args.steps),
+               "d2h_bytes_per_step": int((arena_bytes + 16) / args.steps),
+               "includes": "GpuSolver::new upload, %d iterations, 1 exploitability check, sync_to_cpu" % args.steps,
+               "exploitability_pct_pot": e / cfg["tree"]["starting_pot"] * 100}
+        gpu2.close()
+
+    ttt = None
+    if args.ttt and rank == 0:
+        ttt = time_to_target(g, cfg, args)
+
+    if rank != 0:
+        return
+    base = None
+    if not args.no_cpu_baseline:
+        r = cpu_baseline(cfg, args.storage, args.cpu_steps, args.cpu_threads)
+        v = len(r["iter_s"]) / sum(r["iter_s"])
+        base = {"value": v, "unit": "iter/s", "cores": r["cores"], "kind": "port",
+                "sample": "%d DCFR iteration(s) of the same spot on the CPU oracle (reference cfr.rs semantics, "
+                          "i16 arenas, pruning on, OpenMP over chance cards); spot build %.1fs excluded"
+                          % (len(r["iter_s"]), r["build_s"])}
+    line = {
+        "metric": "CFR iterations/s (time-to-0.3%-pot exploitability & HBM GB/s vs peak)",
+        "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "i16" if args.storage != "f32" else "f32", "data": "synthetic (seeded spot)",
+        "config": workload_config(args, cfg),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+                     "traffic": None,
+                     "kernel": "one CFR iteration (CUDA graph of all sweep kernels); dominant kind %s (%.0f%%)"
+                               % (g.KERNEL_NAMES[dominant], 100.0 * prof.ms[dominant] / tot),
+                     "algorithmic_bytes_per_iter": info["iter_bytes"]},
+        "kernel_ms_profiled_iteration": kinds,
+        "gpu_launches": launches_per_iter * args.steps,
+        "clocks": ck,
+        "e2e": e2e,
+        "cpu_baseline": base,
+        "tree": {"nodes": spot.num_nodes, "visited": info["visited_nodes"], "hands": spot.nh,
+                 "levels": info["num_levels"], "device_gb": info["device_bytes"] / 1e9, "build_s": build_s},
+        "exploitability_pct_pot_after": e_chk / cfg["tree"]["starting_pot"] * 100,
+    }
+    if ttt:
+        line["time_to_target"] = ttt
+    print(json.dumps(line), flush=True)
+
+
+def time_to_target(g, cfg, args):
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, storage=args.storage, algo="dcfr", use_iso=True)
+    t = time.perf_counter()
+    gpu = g.GpuSolver(host)
+    pot = cfg["tree"]["starting_pot"]
+    pct = None
+    while gpu.iteration < args.ttt_max:
+        gpu.iterate(args.check_every)
+        pct = gpu.exploitability(host) / pot * 100
+        if pct <= args.target:
+            break
+    gpu.synchronize()
+    dt = time.perf_counter() - t
+    it = gpu.iteration
+    gpu.close()
+    return {"target_pct_pot": args.target, "reached": pct is not None and pct <= args.target, "iterations": it,
+            "wall_s": dt, "final_pct_pot": pct, "check_every": args.check_every}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="flop", choices=["flop", "turn", "river", "bench_spot"])
+    ap.add_argument("--storage", default="compressed", choices=["compressed", "f32"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--cpu-threads", type=int, default=0)
+    ap.add_argument("--ttt", action="store_true", help="also measure wall time to the exploitability target")
+    ap.add_argument("--target", type=float, default=0.3)
+    ap.add_argument("--check-every", type=int, default=10)
+    ap.add_argument("--ttt-max", type=int, default=2000)
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world, rank, local = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, world, rank)
+        else:
+            run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

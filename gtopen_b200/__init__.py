@@ -111,6 +111,8 @@ def lib():
         "gtob_gpu_root_cfv": (I, [P, I, I, P]),
         "gtob_gpu_export_arena": (I, [P, I, I, P]),
         "gtob_gpu_discounts": (I, [P, P]),
+        "gtob_set_device": (I, [I]),
+        "gtob_gpu_time_iterations": (I, [P, I, C.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -398,3 +400,13 @@ class GpuSolver:
         out = np.zeros(3, np.float32)
         _check(lib().gtob_gpu_discounts(self._h, _ptr(out)))
         return out
+
+    def time_iterations(self, n):
+        """Run n iterations; return their device time in ms (CUDA events on the engine stream)."""
+        ms = C.c_double()
+        _check(lib().gtob_gpu_time_iterations(self._h, int(n), C.byref(ms)))
+        return ms.value
+
+
+def set_device(device):
+    _check(lib().gtob_set_device(int(device)))

@@ -3,6 +3,8 @@
 // errors reach its callers.
 #include "../../../include/gtob.h"
 
+#include <cuda_runtime.h>
+
 #include <cstring>
 #include <memory>
 #include <string>
@@ -343,6 +345,20 @@ int gtob_gpu_export_arena(gtob_gpu* g, int which, int p, float* out) {
     REQUIRE(g && out && which >= 0 && which <= 2 && (p == 0 || p == 1));
     API_BEGIN
     g->e->export_arena(which, p, out);
+    API_END
+}
+int gtob_set_device(int device) {
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        g_err = std::string("cuda: ") + cudaGetErrorString(e);
+        return GTOB_ECUDA;
+    }
+    return GTOB_OK;
+}
+int gtob_gpu_time_iterations(gtob_gpu* g, int n, double* ms) {
+    REQUIRE(g && ms && n >= 0);
+    API_BEGIN
+    *ms = g->e->time_iterations(n);
     API_END
 }
 int gtob_gpu_discounts(gtob_gpu* g, float* out3) {

@@ -909,6 +909,26 @@ void GpuEngine::iterate(int n) {
     CK(cudaGetLastError());
 }
 
+double GpuEngine::time_iterations(int n) {
+    EngineImpl& E = *d_;
+    if (!E.g_iter) E.g_iter = E.capture(-1);
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, E.stream));
+    for (int k = 0; k < n; k++) {
+        CK(cudaGraphLaunch(E.g_iter, E.stream));
+        E.iteration++;
+    }
+    CK(cudaEventRecord(b, E.stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
 Profile GpuEngine::iterate_profiled() {
     EngineImpl& E = *d_;
     Profile pr;

@@ -27,6 +27,8 @@ class GpuEngine {
     GpuEngine(const HostSolver& host, int fmt);
     ~GpuEngine();
     void iterate(int n);
+    // n iterations bracketed by CUDA events on the engine's stream; returns ms
+    double time_iterations(int n);
     Profile iterate_profiled();
     double exploitability(const HostSolver& host);       // chips
     void root_cfv(int p, int mode, float* out);          // eval sweep root values (mode 0 BR, 1 average)

@@ -134,6 +134,9 @@ int gtob_save(const gtob_solver* solver, const char* path);
 int gtob_load(const char* path, int storage, gtob_solver** out);
 
 /* ---- GPU engine (gpu/mod.rs GpuSolver) ----------------------------------- */
+/* Device for later gtob_gpu_new calls on this thread (the reference always
+ * opens device 0, gpu/mod.rs:152; one process per GPU sets its own). */
+int gtob_set_device(int device);
 /* GpuSolver::new (gpu/mod.rs:146); device_format GTOB_DEVICE_* */
 int gtob_gpu_new(const gtob_solver* solver, int device_format, gtob_gpu** out);
 void gtob_gpu_free(gtob_gpu* gpu);
@@ -157,6 +160,8 @@ int gtob_gpu_info_get(gtob_gpu* gpu, gtob_gpu_info* out);
 int gtob_gpu_root_cfv(gtob_gpu* gpu, int player, int mode, float* out);
 /* device arena decoded to the reference layout, without touching the host solver */
 int gtob_gpu_export_arena(gtob_gpu* gpu, int which, int player, float* out);
+/* n iterations bracketed by CUDA events on the engine's own stream (ms) */
+int gtob_gpu_time_iterations(gtob_gpu* gpu, int n, double* ms);
 /* the last discounts the device computed (pos, neg, strat) */
 int gtob_gpu_discounts(gtob_gpu* gpu, float* out3);
 
