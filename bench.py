@@ -188,7 +188,7 @@ def workload_config(args, cfg):
                          "bench_spot": "reference bench_spot.json (Ks7h2d, 257 v 319)"}[args.workload],
             "board": cfg["board"], "arenas": "i16/u16 per-node scale" if args.storage != "f32" else "f32",
             "algo": "DCFR alpha 1.5 beta 0 gamma 2, alternating", "l2": "inputs larger than L2 (arenas GB-sized)",
-            "parallelism": "replica per GPU (weak scaling)"}
+            "parallelism": "replica per GPU (weak scaling)", "engine": getattr(args, "engine", "fused")}
 
 
 def run_ours(args, world, rank, local):
@@ -199,7 +199,7 @@ def run_ours(args, world, rank, local):
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage=args.storage, algo="dcfr", use_iso=True)
     build_s = time.perf_counter() - t0
-    gpu = g.GpuSolver(host)
+    gpu = g.GpuSolver(host, engine=args.engine)
     info = gpu.info()
     gpu.iterate(args.warmup)
     gpu.synchronize()
@@ -228,7 +228,7 @@ def run_ours(args, world, rank, local):
     if not args.no_e2e:
         barrier(world)
         t = time.perf_counter()
-        gpu2 = g.GpuSolver(host)
+        gpu2 = g.GpuSolver(host, engine=args.engine)
         gpu2.iterate(args.steps)
         e = gpu2.exploitability(host)
         gpu2.sync_to_cpu(host)
@@ -288,7 +288,7 @@ def time_to_target(g, cfg, args):
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage=args.storage, algo="dcfr", use_iso=True)
     t = time.perf_counter()
-    gpu = g.GpuSolver(host)
+    gpu = g.GpuSolver(host, engine=args.engine)
     pot = cfg["tree"]["starting_pot"]
     pct = None
     while gpu.iteration < args.ttt_max:
@@ -312,6 +312,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="flop", choices=["flop", "turn", "river", "bench_spot"])
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32"])
+    ap.add_argument("--engine", default="fused", choices=["fused", "plain"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=1)

@@ -98,6 +98,7 @@ def lib():
         "gtob_save": (I, [P, C.c_char_p]),
         "gtob_load": (I, [C.c_char_p, I, C.POINTER(P)]),
         "gtob_gpu_new": (I, [P, I, C.POINTER(P)]),
+        "gtob_gpu_new_ex": (I, [P, I, I, C.POINTER(P)]),
         "gtob_gpu_free": (None, [P]),
         "gtob_gpu_iterate": (I, [P, I]),
         "gtob_gpu_iterate_profiled": (I, [P, C.POINTER(Profile)]),
@@ -337,9 +338,13 @@ class Solver:
 class GpuSolver:
     """gpu/mod.rs GpuSolver: device buffers, CUDA-graph iterations, BR checks, syncs."""
 
-    def __init__(self, solver, device_format=None):
+    def __init__(self, solver, device_format=None, engine="fused"):
+        """engine: "fused" (terminals evaluated inside their parents' kernels,
+        f64 terminal sums), "plain" (one launch per node kind and level, f64
+        terminal sums) or "fused32" (fused, f32 terminal sums)."""
         h = C.c_void_p()
-        _check(lib().gtob_gpu_new(solver._h, DEVICE_FORMAT[device_format], C.byref(h)))
+        eng = {"fused": 0, "plain": 1, "fused32": 2}[engine]
+        _check(lib().gtob_gpu_new_ex(solver._h, DEVICE_FORMAT[device_format], eng, C.byref(h)))
         self._h = h
         self.solver = solver
 

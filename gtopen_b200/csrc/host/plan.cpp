@@ -24,11 +24,13 @@ void flatten(std::vector<std::vector<std::pair<uint32_t, T>>>& by_level, std::ve
         for (auto& x : lst) flat.push_back(x.second);
     }
 }
+bool is_terminal(uint8_t k) { return k == kFold || k == kShowdown; }
 }  // namespace
 
-Plan build_plan(const Spot& sp, bool use_iso) {
+Plan build_plan(const Spot& sp, bool use_iso, bool fused) {
     const Tree& t = sp.tree;
     Plan P;
+    P.fused = fused;
     P.nh[0] = (int)sp.hands[0].size();
     P.nh[1] = (int)sp.hands[1].size();
     P.nh_max = std::max(P.nh[0], P.nh[1]);
@@ -50,6 +52,23 @@ Plan build_plan(const Spot& sp, bool use_iso) {
         }
     };
     std::unordered_map<size_t, uint32_t> slot_of_key;
+    auto river_slot = [&](const uint8_t* dealt, int nd) {
+        size_t key = sp.river_key(dealt, nd);
+        auto it = slot_of_key.find(key);
+        if (it != slot_of_key.end()) return it->second;
+        uint32_t s = (uint32_t)P.slot_key.size();
+        slot_of_key[key] = s;
+        P.slot_key.push_back((uint32_t)key);
+        return s;
+    };
+    auto term_of = [&](uint32_t c, const uint8_t* dealt, int nd) {
+        TermInfo ti{(float)t.twin[c], (float)t.tlose[c], (float)t.ttie[c], 0};
+        ti.aux = t.kind[c] == kFold ? t.player[c] : river_slot(dealt, nd);
+        P.terms.push_back(ti);
+        P.visited_terminals++;
+        P.num_visited++;
+        return (uint32_t)(P.terms.size() - 1);
+    };
     std::vector<uint8_t> visited(n, 0);
 
     uint64_t next_c = 1, next_r[2] = {1, 1};
@@ -68,22 +87,31 @@ Plan build_plan(const Spot& sp, bool use_iso) {
                 ActItem it{};
                 it.node = nd;
                 it.cslot = v.cslot;
-                it.child_cslot = (uint32_t)next_c;
                 it.rslot = v.rs[a];
-                it.child_rslot = (uint32_t)next_r[a];
+                it.oslot = v.rs[1 - a];
                 it.actor = (uint32_t)a;
                 it.na = (uint32_t)na;
-                next_c += na;
-                next_r[a] += na;
-                act_l[v.level].push_back({nd, it});
-                for (int k = na - 1; k >= 0; k--) {  // push reversed so pops run in action order
-                    Visit c = v;
-                    c.node = t.child(nd, k);
-                    c.level = v.level + 1;
-                    c.cslot = it.child_cslot + k;
-                    c.rs[a] = it.child_rslot + k;
-                    stack.push_back(c);
+                it.cref = (uint32_t)P.crefs.size();
+                P.max_children = std::max<uint32_t>(P.max_children, (uint32_t)na);
+                std::vector<Visit> kids;
+                for (int k = 0; k < na; k++) {
+                    const uint32_t c = t.child(nd, k);
+                    if (fused && is_terminal(t.kind[c])) {
+                        uint32_t ti = term_of(c, v.dealt, v.ndealt);
+                        P.crefs.push_back({t.kind[c] == kFold ? kChildFold : kChildShow, kNoSlot, kNoSlot, ti});
+                        it.nterm++;
+                        continue;
+                    }
+                    Visit cv = v;
+                    cv.node = c;
+                    cv.level = v.level + 1;
+                    cv.cslot = (uint32_t)next_c++;
+                    cv.rs[a] = (uint32_t)next_r[a]++;
+                    P.crefs.push_back({kChildNode, cv.cslot, cv.rs[a], kNoSlot});
+                    kids.push_back(cv);
                 }
+                act_l[v.level].push_back({nd, it});
+                for (auto k = kids.rbegin(); k != kids.rend(); ++k) stack.push_back(*k);
                 break;
             }
             case kChance: {
@@ -103,36 +131,47 @@ Plan build_plan(const Spot& sp, bool use_iso) {
                     }
                     cr.push_back({(uint8_t)c, rep, krep});
                 }
-                uint32_t rep_slot[52];
-                uint32_t nreps = 0;
-                const uint64_t cbase = next_c, rbase0 = next_r[0], rbase1 = next_r[1];
-                for (auto& x : cr)
-                    if (x.card == x.rep) rep_slot[x.card] = nreps++;
-                next_c += nreps;
-                next_r[0] += nreps;
-                next_r[1] += nreps;
+                uint32_t rep_cslot[52], rep_term[52];
                 ChanceItem ci{};
                 ci.cslot = v.cslot;
+                ci.inv = 1.0f / (float)(46 - (int)t.street[nd]);
+                ci.rs[0] = v.rs[0];
+                ci.rs[1] = v.rs[1];
+                std::vector<Visit> kids;
+                for (auto& x : cr) {
+                    if (x.card != x.rep) continue;
+                    const uint32_t c = t.children[t.child_start[nd] + x.card];
+                    uint8_t d2[2] = {v.ndealt > 0 ? v.dealt[0] : (uint8_t)0, 0};
+                    d2[v.ndealt] = x.card;
+                    if (fused && t.kind[c] == kShowdown) {
+                        rep_term[x.card] = term_of(c, d2, v.ndealt + 1);
+                        rep_cslot[x.card] = kNoSlot;
+                        continue;
+                    }
+                    Visit cv = v;
+                    cv.node = c;
+                    cv.level = v.level + 1;
+                    cv.dealt[0] = d2[0];
+                    cv.dealt[1] = d2[1];
+                    cv.ndealt = v.ndealt + 1;
+                    cv.cslot = (uint32_t)next_c++;
+                    cv.rs[0] = (uint32_t)next_r[0]++;
+                    cv.rs[1] = (uint32_t)next_r[1]++;
+                    rep_cslot[x.card] = cv.cslot;
+                    rep_term[x.card] = kNoSlot;
+                    EdgeItem e{{v.rs[0], v.rs[1]}, {cv.rs[0], cv.rs[1]}, x.card, 0};
+                    edge_l[v.level].push_back({c, e});
+                    kids.push_back(cv);
+                }
                 ci.cc_start = (uint32_t)P.cards.size();
                 ci.cc_count = (uint32_t)cr.size();
-                ci.inv = 1.0f / (float)(46 - (int)t.street[nd]);
-                for (auto& x : cr) P.cards.push_back({x.card, (uint32_t)(cbase + rep_slot[x.rep]), x.perm, 0});
-                chance_l[v.level].push_back({nd, ci});
-                for (int k = (int)cr.size() - 1; k >= 0; k--) {
-                    const auto& x = cr[k];
-                    if (x.card != x.rep) continue;
-                    uint32_t r = rep_slot[x.card];
-                    Visit c = v;
-                    c.node = t.children[t.child_start[nd] + x.card];
-                    c.level = v.level + 1;
-                    c.dealt[c.ndealt++] = x.card;
-                    c.cslot = (uint32_t)(cbase + r);
-                    c.rs[0] = (uint32_t)(rbase0 + r);
-                    c.rs[1] = (uint32_t)(rbase1 + r);
-                    EdgeItem e{{v.rs[0], v.rs[1]}, {c.rs[0], c.rs[1]}, x.card, 0};
-                    edge_l[v.level].push_back({c.node, e});
-                    stack.push_back(c);
+                for (auto& x : cr) {
+                    // low byte: the dealt card; second byte: its orbit representative
+                    P.cards.push_back({(uint32_t)x.card | ((uint32_t)x.rep << 8), rep_cslot[x.rep], x.perm, rep_term[x.rep]});
+                    if (rep_term[x.rep] != kNoSlot) ci.nterm++;
                 }
+                chance_l[v.level].push_back({nd, ci});
+                for (auto k = kids.rbegin(); k != kids.rend(); ++k) stack.push_back(*k);
                 break;
             }
             case kFold: {
@@ -142,17 +181,8 @@ Plan build_plan(const Spot& sp, bool use_iso) {
                 break;
             }
             default: {
-                size_t key = sp.river_key(v.dealt, v.ndealt);
-                auto itk = slot_of_key.find(key);
-                uint32_t s;
-                if (itk == slot_of_key.end()) {
-                    s = (uint32_t)P.slot_key.size();
-                    slot_of_key[key] = s;
-                    P.slot_key.push_back((uint32_t)key);
-                } else {
-                    s = itk->second;
-                }
-                ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, s, (float)t.twin[nd], (float)t.tlose[nd], (float)t.ttie[nd], 0};
+                ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, river_slot(v.dealt, v.ndealt), (float)t.twin[nd],
+                            (float)t.tlose[nd], (float)t.ttie[nd], 0};
                 show_l[v.level].push_back({nd, si});
                 P.visited_terminals++;
                 break;
@@ -242,19 +272,30 @@ Plan build_plan(const Spot& sp, bool use_iso) {
                 e.idx = h;
                 e.lb = (uint16_t)lb;
                 e.ub = (uint16_t)ub;
-                auto count_below = [&](int card, size_t bound) {
+                // Q index = segment base of the card + #entries of its list below the bound
+                auto q_index = [&](int card, size_t bound) {
                     const uint16_t* b = opos + ooff[card];
                     const uint16_t* en = opos + ooff[card + 1];
-                    return (uint16_t)(std::lower_bound(b, en, (uint16_t)bound) - b);
+                    const size_t base = (ooff[card] - ooff[0]) + (size_t)card;
+                    return (uint16_t)(base + (std::lower_bound(b, en, (uint16_t)bound) - b));
                 };
-                e.c1lo = count_below(sp.hands[p].c1[h], lb);
-                e.c1hi = count_below(sp.hands[p].c1[h], ub);
-                e.c2lo = count_below(sp.hands[p].c2[h], lb);
-                e.c2hi = count_below(sp.hands[p].c2[h], ub);
+                const int h1 = sp.hands[p].c1[h], h2 = sp.hands[p].c2[h];
+                e.q1lo = q_index(h1, lb);
+                e.q1hi = q_index(h1, ub);
+                e.q2lo = q_index(h2, lb);
+                e.q2hi = q_index(h2, ub);
+                e.cards = (uint16_t)(h1 | (h2 << 8));
                 P.rank[p].push_back(e);
             }
+            // my hands absent from this board's list (they hold a dealt card): value 0
+            std::vector<uint8_t> on(P.nh[p], 0);
+            for (uint16_t h : rb.idx[p]) on[h] = 1;
+            P.zero_off[p].push_back((uint32_t)P.zero_idx[p].size());
+            for (int h = 0; h < P.nh[p]; h++)
+                if (!on[h]) P.zero_idx[p].push_back((uint16_t)h);
         }
     }
+    for (int p = 0; p < 2; p++) P.zero_off[p].push_back((uint32_t)P.zero_idx[p].size());
     return P;
 }
 

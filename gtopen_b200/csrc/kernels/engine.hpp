@@ -12,6 +12,7 @@
 namespace gtob {
 
 enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1 };
+enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2 };
 
 struct Profile {
     double ms[7];
@@ -23,8 +24,13 @@ struct EngineImpl;
 
 class GpuEngine {
   public:
-    // fmt < 0: follow the host storage (f32 -> f32 arenas, compressed -> i16/u16)
-    GpuEngine(const HostSolver& host, int fmt);
+    // fmt < 0: follow the host storage (f32 -> f32 arenas, compressed -> i16/u16).
+    // engine: kEngineFused (terminals evaluated inside their parents' kernels,
+    // f64 terminal sums as the reference CPU engine), kEnginePlain (one launch
+    // per terminal level, f64 sums), kEngineFused32 (fused, f32 sums as the
+    // reference GPU kernels).
+    GpuEngine(const HostSolver& host, int fmt, int engine = 0);
+    bool fused() const;
     ~GpuEngine();
     void iterate(int n);
     // n iterations bracketed by CUDA events on the engine's stream; returns ms

@@ -34,6 +34,11 @@ extern "C" {
 #define GTOB_DEVICE_FOLLOW_HOST (-1) /* device arena format follows the host storage */
 #define GTOB_DEVICE_F32 0
 #define GTOB_DEVICE_I16 1
+#define GTOB_ENGINE_FUSED 0     /* terminals in their parents' kernels, f64 terminal sums */
+#define GTOB_ENGINE_PLAIN 1     /* one launch per node kind and level, f64 terminal sums */
+#define GTOB_ENGINE_FUSED_F32 2 /* fused with f32 terminal sums (the reference GPU kernels'
+                                   precision; exploitability matches, but near-tied
+                                   regrets may round differently than the CPU engine) */
 #define GTOB_ARENA_REGRETS 0
 #define GTOB_ARENA_STRATEGY 1
 #define GTOB_ARENA_PREDICTIONS 2
@@ -139,6 +144,10 @@ int gtob_load(const char* path, int storage, gtob_solver** out);
 int gtob_set_device(int device);
 /* GpuSolver::new (gpu/mod.rs:146); device_format GTOB_DEVICE_* */
 int gtob_gpu_new(const gtob_solver* solver, int device_format, gtob_gpu** out);
+/* GpuSolver::new with the engine choice: GTOB_ENGINE_FUSED (terminals
+ * evaluated inside their parents' kernels, the default) or GTOB_ENGINE_PLAIN
+ * (one launch per node kind and level, the reference's kernel split). */
+int gtob_gpu_new_ex(const gtob_solver* solver, int device_format, int engine, gtob_gpu** out);
 void gtob_gpu_free(gtob_gpu* gpu);
 /* GpuSolver::iterate (gpu/mod.rs:304), n times */
 int gtob_gpu_iterate(gtob_gpu* gpu, int n);
