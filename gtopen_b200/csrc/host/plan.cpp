@@ -27,10 +27,13 @@ void flatten(std::vector<std::vector<std::pair<uint32_t, T>>>& by_level, std::ve
 bool is_terminal(uint8_t k) { return k == kFold || k == kShowdown; }
 }  // namespace
 
-Plan build_plan(const Spot& sp, bool use_iso, bool fused) {
+Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
     const Tree& t = sp.tree;
     Plan P;
+    const bool fused = fuse_mode == kFuseAll;
     P.fused = fused;
+    P.fuse_folds = fuse_mode != kFuseNone;
+    auto in_place = [&](uint8_t kind) { return kind == kFold ? P.fuse_folds : kind == kShowdown ? fused : false; };
     P.nh[0] = (int)sp.hands[0].size();
     P.nh[1] = (int)sp.hands[1].size();
     P.nh_max = std::max(P.nh[0], P.nh[1]);
@@ -96,7 +99,7 @@ Plan build_plan(const Spot& sp, bool use_iso, bool fused) {
                 std::vector<Visit> kids;
                 for (int k = 0; k < na; k++) {
                     const uint32_t c = t.child(nd, k);
-                    if (fused && is_terminal(t.kind[c])) {
+                    if (is_terminal(t.kind[c]) && in_place(t.kind[c])) {
                         uint32_t ti = term_of(c, v.dealt, v.ndealt);
                         P.crefs.push_back({t.kind[c] == kFold ? kChildFold : kChildShow, kNoSlot, kNoSlot, ti});
                         it.nterm++;
@@ -248,11 +251,25 @@ Plan build_plan(const Spot& sp, bool use_iso, bool fused) {
                 by[sp.hands[q].c1[h]].push_back((uint16_t)k);
                 by[sp.hands[q].c2[h]].push_back((uint16_t)k);
             }
+            const size_t first = P.ccard_pos[q].size();
+            P.bin_off[q].push_back((uint32_t)P.bin_start[q].size());
+            P.bin_start[q].push_back(0);
+            size_t bin_begin = 0;
             for (int c = 0; c < 52; c++) {
                 P.ccard_off[q].push_back((uint32_t)P.ccard_pos[q].size());
+                // close the bin if this card's whole list would not fit in it
+                const size_t here = P.ccard_pos[q].size() - first;
+                if (here - bin_begin + by[c].size() > 64) {
+                    P.bin_start[q].push_back((uint16_t)here);
+                    bin_begin = here;
+                }
                 P.ccard_pos[q].insert(P.ccard_pos[q].end(), by[c].begin(), by[c].end());
+                P.ccard_card[q].insert(P.ccard_card[q].end(), by[c].size(), (uint8_t)c);
             }
             P.ccard_off[q].push_back((uint32_t)P.ccard_pos[q].size());
+            const size_t total = P.ccard_pos[q].size() - first;
+            if (total > bin_begin) P.bin_start[q].push_back((uint16_t)total);
+            P.max_bins = std::max<uint32_t>(P.max_bins, (uint32_t)(P.bin_start[q].size() - P.bin_off[q].back() - 1));
         }
         for (int p = 0; p < 2; p++) {
             const int o = 1 - p;
@@ -295,7 +312,10 @@ Plan build_plan(const Spot& sp, bool use_iso, bool fused) {
                 if (!on[h]) P.zero_idx[p].push_back((uint16_t)h);
         }
     }
-    for (int p = 0; p < 2; p++) P.zero_off[p].push_back((uint32_t)P.zero_idx[p].size());
+    for (int p = 0; p < 2; p++) {
+        P.zero_off[p].push_back((uint32_t)P.zero_idx[p].size());
+        P.bin_off[p].push_back((uint32_t)P.bin_start[p].size());
+    }
     return P;
 }
 

@@ -97,8 +97,13 @@ struct RankEntry {
 
 struct Span { uint32_t start, count; };
 
+// Which terminal children the parent's up-sweep kernel evaluates in place
+// (no slots, no launches of their own).
+enum FuseMode { kFuseNone = 0, kFuseFolds = 1, kFuseAll = 2 };
+
 struct Plan {
-    bool fused = false;
+    bool fused = false;       // showdown children evaluated in place too
+    bool fuse_folds = false;  // fold children evaluated in place
     int num_levels = 0;
     int nh[2] = {0, 0};
     int nh_max = 0;
@@ -130,8 +135,14 @@ struct Plan {
     std::vector<uint32_t> sorted_off[2];
     std::vector<uint32_t> sorted_cnt[2];
     std::vector<uint16_t> sorted_idx[2];
-    std::vector<uint32_t> ccard_off[2];
-    std::vector<uint16_t> ccard_pos[2];
+    std::vector<uint32_t> ccard_off[2];   // [slot*53 + c] -> start of card c's list in ccard_pos
+    std::vector<uint16_t> ccard_pos[2];   // sorted-order positions of the opponent hands holding c
+    std::vector<uint8_t> ccard_card[2];   // card of each ccard_pos entry
+    // Card lists of one board packed, whole cards only, into bins of <= 64
+    // entries (entry offsets relative to the slot's first entry).
+    std::vector<uint32_t> bin_off[2];     // [slot] -> first entry in bin_start (num_slots + 1)
+    std::vector<uint16_t> bin_start[2];   // nbins + 1 offsets per slot
+    uint32_t max_bins = 0;
     std::vector<uint32_t> rank_off[2];
     std::vector<uint32_t> rank_cnt[2];
     std::vector<RankEntry> rank[2];
@@ -144,6 +155,6 @@ struct Plan {
     uint64_t visited_terminals = 0;
 };
 
-Plan build_plan(const Spot& spot, bool use_iso, bool fused);
+Plan build_plan(const Spot& spot, bool use_iso, int fuse_mode);
 
 }  // namespace gtob

@@ -43,6 +43,9 @@ struct Dev {
     const uint16_t* sorted_idx[2];
     const uint32_t* ccard_off[2];
     const uint16_t* ccard_pos[2];
+    const uint8_t* ccard_card[2];
+    const uint32_t* bin_off[2];
+    const uint16_t* bin_start[2];
     const uint32_t* rank_off[2];
     const uint32_t* rank_cnt[2];
     const RankEntry* rank[2];
@@ -343,20 +346,8 @@ __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* r
     T* Q = P + m + 1;
     T* S = Q + 2 * m + 52;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // issue the card-list position loads now; they do not depend on R
-    uint32_t cb[kCardsPerWarp], ce[kCardsPerWarp];
-    uint16_t cp[kCardsPerWarp][2];
-#pragma unroll
-    for (int ci = 0; ci < kCardsPerWarp; ci++) {
-        const int c = warp + ci * kWarps;
-        cb[ci] = c < 52 ? coff[c] : 0;
-        ce[ci] = c < 52 ? coff[c + 1] : 0;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const uint32_t k = cb[ci] + lane + 32 * h;
-            cp[ci][h] = k < ce[ci] ? cpos[k] : (uint16_t)0;
-        }
-    }
+    const uint32_t c0 = coff[0];
+    if (threadIdx.x < 52) Q[(coff[threadIdx.x] - c0) + threadIdx.x] = 0;  // each card's exclusive prefix starts at 0
 #pragma unroll
     for (int u = 0; u < kMaxHpt; u++) {
         const int k = threadIdx.x + u * kThreads;
@@ -364,29 +355,40 @@ __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* r
     }
     __syncthreads();
     block_exclusive_scan<T>(R, P, m, s_w);
-    const uint32_t c0 = coff[0];
-#pragma unroll
-    for (int ci = 0; ci < kCardsPerWarp; ci++) {
-        const int c = warp + ci * kWarps;
-        if (c >= 52) break;
-        const uint32_t b = cb[ci], e = ce[ci];
-        T* q = Q + (b - c0) + c;
+    // Per-card exclusive prefixes: whole card lists are packed into bins of
+    // <= 64 entries (plan time), so one warp scans a bin as two 32-lane
+    // chunks of a segmented scan (segments = cards) with no cross-warp carry.
+    const uint16_t* bs = d.bin_start[o] + d.bin_off[o][slot];
+    const int nbins = (int)(d.bin_off[o][slot + 1] - d.bin_off[o][slot]) - 1;
+    const uint16_t* bpos = cpos + c0;
+    const uint8_t* bcard = d.ccard_card[o] + c0;
+    for (int b = warp; b < nbins; b += kWarps) {
+        const uint32_t t0 = bs[b], t1 = bs[b + 1];
         T carry = 0;
-        if (lane == 0) q[0] = 0;
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-            const uint32_t k = b + lane + 32 * h;
-            T v = k < e ? R[cp[ci][h]] : (T)0;
+            const uint32_t t = t0 + 32 * h + lane;
+            const bool valid = t < t1;
+            const int c = valid ? bcard[t] : 255;
+            const int pc = (valid && t > t0) ? bcard[t - 1] : 255;
+            T s = valid ? R[bpos[t]] : (T)0;
+            unsigned f = valid && pc != c;  // first entry of its card in this bin
 #pragma unroll
             for (int x = 1; x < 32; x <<= 1) {
-                T y = __shfl_up_sync(0xffffffffu, v, x);
-                if (lane >= x) v += y;
+                const T y = __shfl_up_sync(0xffffffffu, s, x);
+                const unsigned g = __shfl_up_sync(0xffffffffu, f, x);
+                if (lane >= x) {
+                    if (!f) s += y;
+                    f |= g;
+                }
             }
-            if (k < e) q[k - b + 1] = carry + v;
-            carry += __shfl_sync(0xffffffffu, v, 31);
+            if (!f) s += carry;  // the card continued from the previous chunk
+            if (valid) Q[t + c + 1] = s;
+            carry = __shfl_sync(0xffffffffu, s, 31);
         }
-        if (lane == 0) S[c] = carry;
     }
+    __syncthreads();
+    if (threadIdx.x < 52) S[threadIdx.x] = Q[(coff[threadIdx.x + 1] - c0) + threadIdx.x];
     __syncthreads();
     const T total = P[m];
     const int mp = (int)d.rank_cnt[p][slot];
@@ -737,6 +739,282 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
 #undef CHILD_V
     __syncthreads();  // every thread has read the old scales
     if (threadIdx.x == 0) {
+        ar.rscale[p][it.sidx] = (rmax > 0.0f && isfinite(rmax)) ? rmax : 0.0f;
+        ar.sscale[p][it.sidx] = (smax > 0.0f && isfinite(smax)) ? smax : 0.0f;
+        if (PQ) ar.pscale[p][it.sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
+    }
+}
+
+// ------------------------------------------------- warp-per-node kernels
+// The fast engine gives each action node (and each plain fold) one warp:
+// eight nodes per CTA, no block barriers, a lane walks hands lane, lane+32,
+// ... so a node's hands are independent and a warp never waits for another.
+
+template <class T>
+__device__ __forceinline__ T warp_sum(T v) {  // fixed xor tree: deterministic
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ float warp_max(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Fold summary of one opponent reach vector by one warp (game.rs:478-485):
+// the total (lane-strided f64 partials, fixed tree) and the 52 per-card sums
+// (lane c and lane c + 32 each sum card c's hand list sequentially in hand
+// order -- the reference CPU engine's order).  S: 52 doubles private to the warp.
+__device__ double warp_fold_sums(const Dev& d, int o, const float* ro, double* S) {
+    const int lane = threadIdx.x & 31, nho = d.nh[o];
+    double t = 0.0;
+#pragma unroll 4
+    for (int j = lane; j < nho; j += 32) t += (double)ro[j];
+#pragma unroll
+    for (int cc = 0; cc < 2; cc++) {
+        const int c = lane + 32 * cc;
+        if (c < 52) {
+            const uint32_t b = d.hcard_off[o][c], e = d.hcard_off[o][c + 1];
+            double s = 0.0;
+#pragma unroll 4
+            for (uint32_t k = b; k < e; k++) s += (double)ro[d.hcard_idx[o][k]];
+            S[c] = s;
+        }
+    }
+    __syncwarp();
+    return warp_sum(t);
+}
+// One hand's fold value from the warp's summary.
+__device__ __forceinline__ float fold_value(const Dev& d, int p, int i, const float* ro, double total, const double* S,
+                                            float amount) {
+    const uint32_t sm = d.same[p][i];
+    const float same_r = sm != kSentinel ? ro[sm] : 0.0f;
+    return amount * ((float)(total - S[d.c1[p][i]] - S[d.c2[p][i]]) + same_r);
+}
+
+#define WARP_ITEM(count)                                              \
+    const int wid = blockIdx.x * kWarps + (int)(threadIdx.x >> 5);   \
+    if (wid >= (count)) return;                                       \
+    const int lane = threadIdx.x & 31;
+
+template <int FMT, int KA>
+__global__ void __launch_bounds__(kThreads) kw_down_action(Dev d, Arenas ar, const ActItem* items, int count, int mode) {
+    WARP_ITEM(count)
+    const ActItem it = items[wid];
+    const int a = (int)it.actor, na = (int)it.na, nh = d.nh[a];
+    uint32_t rs[KA];
+#pragma unroll
+    for (int k = 0; k < KA; k++) rs[k] = k < na ? d.crefs[it.cref + k].rslot : kNoSlot;
+    const float* parent = d.reach[a] + (size_t)it.rslot * nh;
+    float* rbase = d.reach[a];
+    const long long loff = d.lock_off[a][it.sidx];
+    float sig[KA];
+#pragma unroll 2
+    for (int i = lane; i < nh; i += 32) {
+        const float pr = parent[i];
+        node_sigma<FMT, KA>(d, ar, it, loff, i, mode, sig);
+#pragma unroll
+        for (int k = 0; k < KA; k++)
+            if (k < na && rs[k] != kNoSlot) rbase[(size_t)rs[k] * nh + i] = pr * sig[k];
+    }
+}
+
+// Plain-layout fold terminal, one warp per fold: result to its cfv slot.
+__global__ void __launch_bounds__(kThreads) kw_fold(Dev d, const FoldItem* items, int count, int p) {
+    __shared__ double s_S[kWarps][52];
+    WARP_ITEM(count)
+    const FoldItem f = items[wid];
+    const int o = 1 - p;
+    const float* ro = d.reach[o] + (size_t)f.rs[o] * d.nh[o];
+    double* S = s_S[threadIdx.x >> 5];
+    const double total = warp_fold_sums(d, o, ro, S);
+    const float amount = (int)f.folder == p ? f.tlose : f.twin;
+    float* out = d.cfv + (size_t)f.cslot * d.nh_max;
+    for (int i = lane; i < d.nh[p]; i += 32) out[i] = fold_value(d, p, i, ro, total, S, amount);
+}
+
+// Up sweep, action nodes, one warp per node.  Fold children are evaluated in
+// place from a warp fold summary (the node's single fold child, if any);
+// every other child is read from its cfv slot.  EVAL = 0: CFR update
+// (cfr.rs:469-531, 297-409); EVAL = 1: best response (mode 0) or average
+// strategy (mode 1), best_response.rs:69-121, 185-219.  Dynamic smem per
+// warp: the fold child's opponent reach when the opponent acts (nh_pad floats).
+template <int FMT, int EVAL, int KA>
+__global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const ActItem* items, int count, int p,
+                                                         int mode) {
+    extern __shared__ float wsm[];
+    __shared__ double s_S[kWarps][52];
+    WARP_ITEM(count)
+    const int w = threadIdx.x >> 5;
+    const ActItem it = items[wid];
+    const int a = (int)it.actor, na = (int)it.na, nh = d.nh[p], o = 1 - p, nho = d.nh[o];
+    uint32_t cs[KA];
+    int fk = -1;  // the fold child, if evaluated here
+    float famount = 0.0f;
+#pragma unroll
+    for (int k = 0; k < KA; k++) {
+        cs[k] = 0;
+        if (k < na) {
+            const ChildRef c = d.crefs[it.cref + k];
+            cs[k] = c.cslot;
+            if (c.kind == kChildFold) {
+                fk = k;
+                const TermInfo tm = d.terms[c.term];
+                famount = (int)tm.aux == p ? tm.tlose : tm.twin;
+            }
+        }
+    }
+    const long long loff = d.lock_off[a][it.sidx];
+    float sig[KA];
+    double ftotal = 0.0;
+    const double* S = s_S[w];
+    const float* fro = nullptr;
+    if (fk >= 0) {
+        const float* ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * nho;
+        fro = ro;
+        if (a == o) {  // the opponent folds with probability sigma_o[fk]
+            float* rf = wsm + (size_t)w * d.nh_pad;
+            for (int j = lane; j < nho; j += 32) {
+                node_sigma<FMT, KA>(d, ar, it, loff, j, EVAL ? 1 : 0, sig);
+                float sf = 0.0f;
+#pragma unroll
+                for (int k = 0; k < KA; k++)
+                    if (k == fk) sf = sig[k];
+                rf[j] = ro[j] * sf;
+            }
+            __syncwarp();
+            fro = rf;
+        }
+        ftotal = warp_fold_sums(d, o, fro, s_S[w]);
+    }
+    float* out = d.cfv + (size_t)it.cslot * d.nh_max;
+    const float* cfv = d.cfv;
+    const size_t stride = (size_t)d.nh_max;
+#define CHILD_V(k, i) ((k) == fk ? fold_value(d, p, (i), fro, ftotal, S, famount) : cfv[(size_t)cs[k] * stride + (i)])
+    if (a != p) {  // opponent node: sum of children
+        for (int i = lane; i < nh; i += 32) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < KA; k++)
+                if (k < na) acc += CHILD_V(k, i);
+            out[i] = acc;
+        }
+        return;
+    }
+    if (loff >= 0) {  // locked: fixed sigma, no update
+        for (int i = lane; i < nh; i += 32) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < KA; k++)
+                if (k < na) acc += d.lock_sig[loff + (long long)k * nh + i] * CHILD_V(k, i);
+            out[i] = acc;
+        }
+        return;
+    }
+    if (EVAL) {
+        for (int i = lane; i < nh; i += 32) {
+            float acc;
+            if (mode == 0) {
+                acc = CHILD_V(0, i);
+#pragma unroll
+                for (int k = 1; k < KA; k++)
+                    if (k < na) {
+                        const float v = CHILD_V(k, i);
+                        if (v > acc) acc = v;
+                    }
+            } else {
+                average_sigma<FMT, KA>(ar, a, it, i, sig);
+                acc = 0.0f;
+#pragma unroll
+                for (int k = 0; k < KA; k++)
+                    if (k < na) acc += sig[k] * CHILD_V(k, i);
+            }
+            out[i] = acc;
+        }
+        return;
+    }
+    const float pos = d.disc[0], neg = d.disc[1], ds = d.disc[2];
+    const float* reach = d.reach[p] + (size_t)it.rslot * nh;
+    float v[KA];
+    if (FMT == kDevF32) {
+        float* R = (float*)ar.reg[p];
+        float* Sg = (float*)ar.str[p];
+        float* PR = (float*)ar.pred[p];
+        for (int i = lane; i < nh; i += 32) {
+            regret_sigma<FMT, KA>(ar, p, it, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < KA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float rp = reach[i];
+            const size_t b = it.aoff + (size_t)i * na;
+#pragma unroll
+            for (int k = 0; k < KA; k++)
+                if (k < na) {
+                    const float r = R[b + k];
+                    R[b + k] = r * (r > 0.0f ? pos : neg) + (v[k] - o_);
+                    Sg[b + k] = Sg[b + k] * ds + rp * sig[k];
+                    if (PR) PR[b + k] = v[k] - o_;
+                }
+            out[i] = o_;
+        }
+        return;
+    }
+    // 16-bit arenas (cfr.rs:350-407): pass 1 finds the node's new maxima
+    // (warp reduction), pass 2 recomputes and requantises.
+    int16_t* RQ = (int16_t*)ar.reg[p];
+    uint16_t* SQ = (uint16_t*)ar.str[p];
+    int16_t* PQ = (int16_t*)ar.pred[p];
+    const float kr = ar.rscale[p][it.sidx] / 32767.0f;
+    const float kss = ar.sscale[p][it.sidx] / 65535.0f * ds;
+    float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
+    for (int pass = 0; pass < 2; pass++) {
+        float rk = 0.0f, sk = 0.0f, pk = 0.0f;
+        if (pass == 1) {
+            rmax = warp_max(rmax);
+            smax = warp_max(smax);
+            pmax = warp_max(pmax);
+            rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
+            sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
+            pk = (pmax > 0.0f && isfinite(pmax)) ? 32767.0f / pmax : 0.0f;
+        }
+        for (int i = lane; i < nh; i += 32) {
+            regret_sigma<FMT, KA>(ar, p, it, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < KA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float rp = reach[i];
+            const size_t b = it.aoff + (size_t)i * na;
+#pragma unroll
+            for (int k = 0; k < KA; k++)
+                if (k < na) {
+                    const int16_t qv = RQ[b + k];
+                    const float nr = (float)qv * kr * (qv > 0 ? pos : neg) + (v[k] - o_);
+                    const float ns = (float)SQ[b + k] * kss + rp * sig[k];
+                    if (pass == 0) {
+                        rmax = fmaxf(rmax, fabsf(nr));
+                        smax = fmaxf(smax, ns);
+                        if (PQ) pmax = fmaxf(pmax, fabsf(v[k] - o_));
+                    } else {
+                        RQ[b + k] = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
+                        SQ[b + k] = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
+                        if (PQ) PQ[b + k] = pk > 0.0f ? sat_i16((v[k] - o_) * pk) : (int16_t)0;
+                    }
+                }
+            if (pass == 1) out[i] = o_;
+        }
+        __syncwarp();  // every lane has read the old quants of its hands before any scale changes
+    }
+#undef CHILD_V
+    if (lane == 0) {
         ar.rscale[p][it.sidx] = (rmax > 0.0f && isfinite(rmax)) ? rmax : 0.0f;
         ar.sscale[p][it.sidx] = (smax > 0.0f && isfinite(smax)) ? smax : 0.0f;
         if (PQ) ar.pscale[p][it.sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;

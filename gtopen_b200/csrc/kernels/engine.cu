@@ -71,6 +71,7 @@ struct EngineImpl {
     bool pcfr = false;
     bool wide = false;  // some node has more than 8 actions: use the 32-wide kernels
     bool term64 = false;  // terminal sums in f64 (plain engine, or fused on request)
+    bool warp = false;    // warp-per-node action kernels, fold children in place
     uint32_t iteration = 0;
     cudaStream_t stream = nullptr;
     std::vector<void*> owned;
@@ -90,6 +91,7 @@ struct EngineImpl {
     size_t staging_len = 0;
     size_t show_smem = 0;    // plain showdown kernel (f64 scratch)
     size_t act_smem = 0;     // fused up-action dynamic smem
+    size_t warp_smem = 0;    // warp up-action dynamic smem (one staged reach per warp)
     size_t chance_smem = 0;  // runout chance dynamic smem
     cudaGraphExec_t g_iter = nullptr;
     cudaGraphExec_t g_eval[2] = {nullptr, nullptr};
@@ -176,9 +178,36 @@ struct EngineImpl {
     }
     template <int FMT, int KA>
     void down_action(const Span& sa, int mode) {
-        k_down_action<FMT, KA><<<sa.count, kThreads, 0, stream>>>(d, ar, act + sa.start, mode);
+        if (warp) {
+            const unsigned grid = (sa.count + kWarps - 1) / kWarps;
+            kw_down_action<FMT, KA><<<grid, kThreads, 0, stream>>>(d, ar, act + sa.start, (int)sa.count, mode);
+        } else {
+            k_down_action<FMT, KA><<<sa.count, kThreads, 0, stream>>>(d, ar, act + sa.start, mode);
+        }
+    }
+    template <int FMT, int KA>
+    void warp_up_action(const Span& sa, int p, int eval) {
+        const unsigned grid = (sa.count + kWarps - 1) / kWarps;
+        const ActItem* it = act + sa.start;
+        if (eval < 0) kw_up_action<FMT, 0, KA><<<grid, kThreads, warp_smem, stream>>>(d, ar, it, (int)sa.count, p, 0);
+        else kw_up_action<FMT, 1, KA><<<grid, kThreads, warp_smem, stream>>>(d, ar, it, (int)sa.count, p, eval);
+    }
+    template <int FMT, int KA>
+    static void set_warp_smem(size_t bytes) {
+        set_smem((const void*)kw_up_action<FMT, 0, KA>, bytes);
+        set_smem((const void*)kw_up_action<FMT, 1, KA>, bytes);
     }
     void launch_up_action(const Span& sa, int p, int eval) {
+        if (warp) {
+            if (fmt == kFmtF32) {
+                if (wide) warp_up_action<kDevF32, 32>(sa, p, eval);
+                else warp_up_action<kDevF32, 8>(sa, p, eval);
+            } else {
+                if (wide) warp_up_action<kDevI16, 32>(sa, p, eval);
+                else warp_up_action<kDevI16, 8>(sa, p, eval);
+            }
+            return;
+        }
         if (fmt == kFmtF32) {
             if (wide) up_action<kDevF32, 32>(sa, p, eval);
             else up_action<kDevF32, 8>(sa, p, eval);
@@ -261,7 +290,9 @@ struct EngineImpl {
 GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new EngineImpl()) {
     EngineImpl& E = *d_;
     const Spot& sp = *host.spot;
-    const bool fused = engine != kEnginePlain;
+    if (engine < kEngineFused || engine > kEngineWarp) throw Error("unknown engine kind");
+    const int fuse = engine == kEnginePlain ? kFuseNone : engine == kEngineWarp ? kFuseFolds : kFuseAll;
+    E.warp = engine == kEngineWarp;
     E.term64 = engine != kEngineFused32;
     E.spot = &sp;
     E.algo = host.algo;
@@ -269,7 +300,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     E.fmt = fmt < 0 ? (host.storage == kStoreF32 ? kFmtF32 : kFmtI16) : fmt;
     if (E.fmt != kFmtF32 && E.fmt != kFmtI16) throw Error("unknown device arena format");
     E.iteration = host.iteration;
-    E.plan = build_plan(sp, host.use_iso, fused);
+    E.plan = build_plan(sp, host.use_iso, fuse);
     const Plan& P = E.plan;
     if (P.max_children > 32u) throw Error("an action node with more than 32 actions is not supported on the GPU");
     E.wide = P.max_children > 8u;
@@ -305,6 +336,9 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
         d.sorted_idx[q] = dupload(P.sorted_idx[q], O, &B);
         d.ccard_off[q] = dupload(P.ccard_off[q], O, &B);
         d.ccard_pos[q] = dupload(P.ccard_pos[q], O, &B);
+        d.ccard_card[q] = dupload(P.ccard_card[q], O, &B);
+        d.bin_off[q] = dupload(P.bin_off[q], O, &B);
+        d.bin_start[q] = dupload(P.bin_start[q], O, &B);
         d.rank_off[q] = dupload(P.rank_off[q], O, &B);
         d.rank_cnt[q] = dupload(P.rank_cnt[q], O, &B);
         d.rank[q] = dupload(P.rank[q], O, &B);
@@ -327,7 +361,8 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     E.chance = dupload(P.chance, O, &B);
     const size_t tsz = E.term64 ? sizeof(double) : sizeof(float);
     E.show_smem = (size_t)d.scr_elems * sizeof(double);
-    if (max_nterm) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
+    if (E.warp) E.warp_smem = (size_t)kWarps * d.nh_pad * sizeof(float);
+    if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
     set_smem((const void*)k_showdown, E.show_smem);
     set_smem((const void*)k_chance<float>, E.chance_smem);
@@ -340,6 +375,10 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     EngineImpl::set_up_smem<kDevI16, 8, double>(E.act_smem);
     EngineImpl::set_up_smem<kDevF32, 32, double>(E.act_smem);
     EngineImpl::set_up_smem<kDevI16, 32, double>(E.act_smem);
+    EngineImpl::set_warp_smem<kDevF32, 8>(E.warp_smem);
+    EngineImpl::set_warp_smem<kDevI16, 8>(E.warp_smem);
+    EngineImpl::set_warp_smem<kDevF32, 32>(E.warp_smem);
+    EngineImpl::set_warp_smem<kDevI16, 32>(E.warp_smem);
 
     // arenas
     const size_t esz = E.fmt == kFmtF32 ? 4 : 2;
@@ -562,7 +601,7 @@ double GpuEngine::iter_bytes() const {
 }
 
 uint64_t estimate_vram(const Spot& spot) {  // same role as game.rs:365-373, for this engine's layout
-    Plan P = build_plan(spot, true, true);
+    Plan P = build_plan(spot, true, kFuseAll);
     uint64_t b = P.n_cslots * (uint64_t)P.nh_max * 4 + P.n_rslots[0] * (uint64_t)P.nh[0] * 4 +
                  P.n_rslots[1] * (uint64_t)P.nh[1] * 4;
     b += (P.arena_len[0] + P.arena_len[1]) * 2 * 4;

@@ -12,7 +12,7 @@
 namespace gtob {
 
 enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1 };
-enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2 };
+enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2, kEngineWarp = 3 };
 
 struct Profile {
     double ms[7];
@@ -28,7 +28,8 @@ class GpuEngine {
     // engine: kEngineFused (terminals evaluated inside their parents' kernels,
     // f64 terminal sums as the reference CPU engine), kEnginePlain (one launch
     // per terminal level, f64 sums), kEngineFused32 (fused, f32 sums as the
-    // reference GPU kernels).
+    // reference GPU kernels), kEngineWarp (one warp per action node, fold
+    // children evaluated in place by the warp, showdowns one CTA each; f64).
     GpuEngine(const HostSolver& host, int fmt, int engine = 0);
     bool fused() const;
     ~GpuEngine();

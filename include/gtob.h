@@ -39,6 +39,8 @@ extern "C" {
 #define GTOB_ENGINE_FUSED_F32 2 /* fused with f32 terminal sums (the reference GPU kernels'
                                    precision; exploitability matches, but near-tied
                                    regrets may round differently than the CPU engine) */
+#define GTOB_ENGINE_WARP 3      /* one warp per action node with its fold child evaluated
+                                   in the warp; showdowns one CTA each; f64 terminal sums */
 #define GTOB_ARENA_REGRETS 0
 #define GTOB_ARENA_STRATEGY 1
 #define GTOB_ARENA_PREDICTIONS 2
@@ -145,8 +147,9 @@ int gtob_set_device(int device);
 /* GpuSolver::new (gpu/mod.rs:146); device_format GTOB_DEVICE_* */
 int gtob_gpu_new(const gtob_solver* solver, int device_format, gtob_gpu** out);
 /* GpuSolver::new with the engine choice: GTOB_ENGINE_FUSED (terminals
- * evaluated inside their parents' kernels, the default) or GTOB_ENGINE_PLAIN
- * (one launch per node kind and level, the reference's kernel split). */
+ * evaluated inside their parents' kernels, the default), GTOB_ENGINE_PLAIN
+ * (one launch per node kind and level, the reference's kernel split),
+ * GTOB_ENGINE_FUSED_F32 or GTOB_ENGINE_WARP. */
 int gtob_gpu_new_ex(const gtob_solver* solver, int device_format, int engine, gtob_gpu** out);
 void gtob_gpu_free(gtob_gpu* gpu);
 /* GpuSolver::iterate (gpu/mod.rs:304), n times */

@@ -60,7 +60,7 @@ def _compare(spot, osv, host, what):
         assert d <= 1e-4 * scale, "%s: regrets[%d] differ by %g (scale %g)" % (what, p, d, scale)
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
 @pytest.mark.parametrize("name,cfg_fn,iters", [
     ("clairvoyance", W.clairvoyance_spot, 50),
     ("small_flop", W.small_flop_spot, 20),
@@ -77,7 +77,7 @@ def test_f32_dcfr_matches_oracle(name, cfg_fn, iters, engine):
     assert abs(eo - eg) / pot * 100 < EXPL_TOL_PCT, (eo, eg)
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
 def test_turn_config_f32_and_i16(engine):
     cfg = W.turn_spot(g.evaluate7)
     for storage in ("f32", "compressed"):
@@ -87,11 +87,12 @@ def test_turn_config_f32_and_i16(engine):
         assert abs(eo - eg) / 100.0 * 100 < EXPL_TOL_PCT, (storage, eo, eg)
 
 
+@pytest.mark.parametrize("engine", ["fused", "warp"])
 @pytest.mark.parametrize("algo", ["cfr+", "pcfr+"])
 @pytest.mark.parametrize("storage", ["f32", "compressed"])
-def test_cfrplus_pcfrplus_match_oracle(algo, storage):
+def test_cfrplus_pcfrplus_match_oracle(algo, storage, engine):
     cfg = W.small_flop_spot()
-    ospot, osv, spot, host, gpu = _run_pair(cfg, 15, storage=storage, algo=algo)
+    ospot, osv, spot, host, gpu = _run_pair(cfg, 15, storage=storage, algo=algo, engine=engine)
     _compare(spot, osv, host, "%s/%s" % (algo, storage))
 
 
@@ -110,10 +111,11 @@ def test_fused32_exploitability_matches_oracle(name, cfg_fn, iters):
     assert abs(osv.exploitability() - gpu.exploitability(host)) / pot * 100 < EXPL_TOL_PCT
 
 
-def test_i16_quants_match_oracle_bitwise_mostly():
+@pytest.mark.parametrize("engine", ["fused", "warp"])
+def test_i16_quants_match_oracle_bitwise_mostly(engine):
     """16-bit arenas: the device requantises exactly like store.rs; decoded values agree."""
     cfg = W.small_flop_spot()
-    ospot, osv, spot, host, gpu = _run_pair(cfg, 10, storage="compressed")
+    ospot, osv, spot, host, gpu = _run_pair(cfg, 10, storage="compressed", engine=engine)
     for p in (0, 1):
         for which in (0, 1):
             a, b = osv.arena(which, p), host.arena(which, p)
@@ -121,7 +123,7 @@ def test_i16_quants_match_oracle_bitwise_mostly():
             assert frac_equal > 0.999, (which, p, frac_equal)
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
 def test_iso_matches_oracle(engine):
     cfg = W.iso_spot()
     ospot, osv, spot, host, gpu = _run_pair(cfg, 10, use_iso=True, engine=engine)
@@ -186,7 +188,7 @@ def test_locked_always_call_kills_bluffs():
     assert sig[nh + names.index("8h7h")] < 0.05
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
 def test_exploitability_with_rake_matches_oracle(engine):
     cfg = W.small_flop_spot()
     cfg["tree"]["rake_pct"] = 0.05
@@ -208,13 +210,15 @@ def test_root_br_cfv_matches_oracle():
 def test_profile_counts_launches():
     spot = g.Spot(W.small_flop_spot())
     host = g.Solver(spot)
-    for engine in ("fused", "plain"):
+    for engine in ("fused", "plain", "warp"):
         gpu = g.GpuSolver(host, engine=engine)
         pr = gpu.iterate_profiled()
         assert pr.launches[0] == 2 and sum(pr.launches) > 10
         assert gpu.iteration == 1
         if engine == "fused":
             assert pr.launches[3] == 0 and pr.launches[4] == 0  # terminals evaluated in place
+        if engine == "warp":
+            assert pr.launches[3] == 0 and pr.launches[4] > 0  # folds in place, showdowns launched
 
 
 def test_allin_runout_spot_matches_oracle():
@@ -225,7 +229,7 @@ def test_allin_runout_spot_matches_oracle():
         st["bet"] = [{"PotPct": 75.0}, "AllIn"]
         st["raise"] = ["AllIn"]
     cfg["tree"]["effective_stack"] = 120.0
-    for engine in ("fused", "plain"):
+    for engine in ("fused", "plain", "warp"):
         for storage in ("f32", "compressed"):
             ospot, osv, spot, host, gpu = _run_pair(cfg, 12, storage=storage, engine=engine)
             _compare(spot, osv, host, "runout/%s/%s" % (engine, storage))
