@@ -23,6 +23,7 @@ _LIB = None
 STORAGE = {"f32": 0, "compressed": 1, "i16": 1}
 ALGO = {"dcfr": 0, "cfr+": 1, "cfrplus": 1, "pcfr+": 2, "pcfrplus": 2}
 DEVICE_FORMAT = {None: -1, "follow": -1, "f32": 0, "i16": 1}
+NODE_SCRATCH_ELEMS = 16384  # GTOB_NODE_SCRATCH_ELEMS
 KERNEL_NAMES = ["copy_root", "down_action", "down_chance", "up_fold", "up_show", "up_chance", "up_action"]
 
 
@@ -111,6 +112,7 @@ def lib():
         "gtob_gpu_info_get": (I, [P, C.POINTER(GpuInfo)]),
         "gtob_gpu_root_cfv": (I, [P, I, I, P]),
         "gtob_gpu_export_arena": (I, [P, I, I, P]),
+        "gtob_gpu_read_node_static": (I, [P, I, C.c_uint32, P, C.c_uint64, P]),
         "gtob_gpu_discounts": (I, [P, P]),
         "gtob_set_device": (I, [I]),
         "gtob_gpu_time_iterations": (I, [P, I, C.POINTER(D)]),
@@ -401,6 +403,17 @@ class GpuSolver:
         out = np.zeros(self.solver.spot.data_size[p], np.float32)
         _check(lib().gtob_gpu_export_arena(self._h, int(which), int(p), _ptr(out)))
         return out
+
+    def read_node_static(self, which, node):
+        """One action node's arena block through the allocation-free entry
+        point (static device scratch of NODE_SCRATCH_ELEMS floats)."""
+        t = self.solver.spot.tree()
+        n = int(t["nchild"][node]) * self.solver.spot.nh[int(t["player"][node])]
+        out = np.zeros(max(n, 1), np.float32)
+        written = C.c_uint64()
+        _check(lib().gtob_gpu_read_node_static(self._h, int(which), int(node), _ptr(out), out.size,
+                                               C.byref(written)))
+        return out[:written.value]
 
     def discounts(self):
         out = np.zeros(3, np.float32)

@@ -348,6 +348,14 @@ int gtob_gpu_export_arena(gtob_gpu* g, int which, int p, float* out) {
     g->e->export_arena(which, p, out);
     API_END
 }
+int gtob_gpu_read_node_static(gtob_gpu* g, int which, uint32_t node, float* out, uint64_t out_len,
+                              uint64_t* written) {
+    REQUIRE(g && out && which >= 0 && which <= 2);
+    API_BEGIN
+    const size_t n = g->e->read_node_static(which, node, out, (size_t)out_len);
+    if (written) *written = n;
+    API_END
+}
 int gtob_set_device(int device) {
     cudaError_t e = cudaSetDevice(device);
     if (e != cudaSuccess) {

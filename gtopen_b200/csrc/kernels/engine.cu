@@ -24,7 +24,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "cfr_kernels.cuh"
@@ -533,6 +535,82 @@ void GpuEngine::export_arena(int which, int p, float* out) {
     }
     CK(cudaMemcpyAsync(out, E.staging, len * 4, cudaMemcpyDeviceToHost, E.stream));
     CK(cudaStreamSynchronize(E.stream));
+}
+
+// ------------------------------------------------ allocation-free node read
+// Scratch of read_node_static: one action node's block decoded to f32 in the
+// reference layout [action * nh + hand].  File-scope device memory, so a call
+// allocates nothing; every element that is copied out is written by the same
+// call first, so nothing in it has to start at zero.  One array per device,
+// shared by every engine on that device: calls that overlap in time race.
+static __device__ __align__(256) float g_node_scratch[kNodeScratchElems];
+
+// Variant of k_to_host / k_decode_to_host for one node, writing into the
+// scratch at offset 0 (scale == nullptr: an f32 arena, copied as is).
+template <class T>
+__global__ void k_node_to_scratch(const T* dev, const float* scale, float div, float* dst, XNode x, int nh) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nh) return;
+    const float kq = scale ? scale[x.sidx] / div : 1.0f;
+    for (uint32_t k = 0; k < x.na; k++) {
+        const T v = dev[x.dev_off + (size_t)i * x.na + k];
+        dst[(size_t)k * nh + i] = scale ? (float)v * kq : (float)v;
+    }
+}
+constexpr int kMaxDevices = 64;
+
+// Per-device address of g_node_scratch, resolved once with that device current.
+static float* node_scratch_ptr(int device) {
+    static std::mutex mu;
+    static float* ptrs[kMaxDevices] = {};
+    if (device < 0 || device >= kMaxDevices) throw Error("device ordinal out of range");
+    std::lock_guard<std::mutex> lk(mu);
+    if (!ptrs[device]) {
+        void* p = nullptr;
+        const cudaError_t rc = cudaGetSymbolAddress(&p, g_node_scratch);
+        if (rc != cudaSuccess) throw Error(std::string("cuda: cudaGetSymbolAddress(node scratch): ") + cudaGetErrorString(rc));
+        ptrs[device] = (float*)p;
+    }
+    return ptrs[device];
+}
+
+size_t GpuEngine::read_node_static(int which, uint32_t node, float* out, size_t out_len) {
+    EngineImpl& E = *d_;
+    const Spot& sp = *E.spot;
+    if (node >= sp.tree.size() || sp.tree.kind[node] != kAction) throw Error("node " + std::to_string(node) + " is not an action node");
+    const int p = sp.tree.player[node];
+    const int32_t s = E.plan.node_sidx[node];
+    if (s < 0) throw Error("node " + std::to_string(node) + " has no device block (a symmetric branch the engine skips)");
+    if (which == kPreds && !E.pcfr) throw Error("the engine keeps no predictions (not PCFR+)");
+    const XNode x = E.hx[p][(size_t)s];
+    const int nh = E.plan.nh[p];
+    const size_t n = (size_t)x.na * (size_t)nh;
+    if (n > kNodeScratchElems)
+        throw Error("node " + std::to_string(node) + " block has " + std::to_string(n) + " elements, more than the " +
+                    std::to_string(kNodeScratchElems) + "-element static scratch");
+    if (out_len < n) throw Error("invalid argument: output holds " + std::to_string(out_len) + " floats, node needs " +
+                                 std::to_string(n));
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    cudaPointerAttributes attr;
+    CK(cudaPointerGetAttributes(&attr, E.d.cfv));
+    if (attr.device != dev) throw Error("invalid argument: the engine's device is not the current device");
+    float* scratch = node_scratch_ptr(dev);
+    const void* src = which == kRegrets ? E.ar.reg[p] : which == kStrategy ? E.ar.str[p] : E.ar.pred[p];
+    const unsigned grid = (unsigned)((nh + kThreads - 1) / kThreads);
+    if (E.fmt == kFmtF32) {
+        k_node_to_scratch<float><<<grid, kThreads, 0, E.stream>>>((const float*)src, nullptr, 1.0f, scratch, x, nh);
+    } else {
+        const float* sc = which == kRegrets ? E.ar.rscale[p] : which == kStrategy ? E.ar.sscale[p] : E.ar.pscale[p];
+        if (which == kStrategy)
+            k_node_to_scratch<uint16_t><<<grid, kThreads, 0, E.stream>>>((const uint16_t*)src, sc, 65535.0f, scratch, x, nh);
+        else
+            k_node_to_scratch<int16_t><<<grid, kThreads, 0, E.stream>>>((const int16_t*)src, sc, 32767.0f, scratch, x, nh);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, scratch, n * sizeof(float), cudaMemcpyDeviceToHost, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+    return n;
 }
 
 void GpuEngine::sync_to_cpu(HostSolver& host, bool strategy_only) {  // gpu/mod.rs:845-886

@@ -12,6 +12,7 @@
 namespace gtob {
 
 enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1 };
+constexpr size_t kNodeScratchElems = 16384;  // 64 KiB of f32: the read_node_static limit
 enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2, kEngineWarp = 3 };
 
 struct Profile {
@@ -50,6 +51,10 @@ class GpuEngine {
     double iter_bytes() const;
     // device arena exports for tests (reference layout, decoded f32)
     void export_arena(int which, int p, float* out);
+    // One action node's block (reference layout, f32) through a static device
+    // scratch of kNodeScratchElems floats: no allocation, host or device, on
+    // success.  Returns the element count written to out.
+    size_t read_node_static(int which, uint32_t node, float* out, size_t out_len);
     // time one kind of level launch set: used by bench for the roofline
     void discounts(float* out3);
 

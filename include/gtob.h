@@ -177,6 +177,31 @@ int gtob_gpu_time_iterations(gtob_gpu* gpu, int n, double* ms);
 /* the last discounts the device computed (pos, neg, strat) */
 int gtob_gpu_discounts(gtob_gpu* gpu, float* out3);
 
+/* No counterpart in the reference.  One action node's arena block (which:
+ * GTOB_ARENA_*), decoded to f32 in the reference layout [action * nh + hand],
+ * the same values gtob_gpu_export_arena gives for that node, read through a
+ * static device scratch of GTOB_NODE_SCRATCH_ELEMS floats: on success the
+ * call allocates no host or device memory.  It serves callers that must not
+ * allocate while a solve holds the device -- a viewer polling one node
+ * mid-solve, where the arenas were sized to fill HBM (a cudaMalloc there can
+ * fail, and cudaMalloc/cudaFree synchronise the device) and where
+ * gtob_gpu_export_arena would move a whole arena.
+ *   - Blocks of more than GTOB_NODE_SCRATCH_ELEMS elements (nchild * hands)
+ *     are refused with GTOB_EINVAL; so is out_len < the block size.
+ *   - Call it with the solver's device current.  The first call on a device
+ *     resolves the scratch address (cudaGetSymbolAddress) and loads the
+ *     kernel, which may make the CUDA runtime allocate: make that first call
+ *     before capturing any stream.
+ *   - Nothing in the scratch has to start at zero: each call writes every
+ *     element it copies out.
+ *   - The scratch is one array per device: calls that overlap in time (two
+ *     threads, or two solvers on one device) race on it.  The call returns
+ *     after its copy is complete, so calls made one after another are safe.
+ * *written (if not NULL) receives the element count. */
+#define GTOB_NODE_SCRATCH_ELEMS 16384
+int gtob_gpu_read_node_static(gtob_gpu* gpu, int which, uint32_t node, float* out, uint64_t out_len,
+                              uint64_t* written);
+
 #ifdef __cplusplus
 }
 #endif
