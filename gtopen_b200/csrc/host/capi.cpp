@@ -27,6 +27,7 @@ static void put(T* dst, const std::vector<T>& v) {
 }
 
 static int classify(const std::string& m) {
+    if (m.rfind("timeout:", 0) == 0) return GTOB_ETIMEOUT_QUEUE;
     if (m.rfind("cuda: out of memory", 0) == 0 || m.find("out of memory") != std::string::npos) return GTOB_ENOMEM_DEVICE;
     if (m.rfind("cuda:", 0) == 0) return GTOB_ECUDA;
     if (m.rfind("io:", 0) == 0 || m.find("cannot open") != std::string::npos || m.find("write failed") != std::string::npos ||

@@ -217,6 +217,16 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
             x.second.aoff = P.anode_off[a][x.second.sidx];
         }
     flatten(act_l, P.act, P.act_span);
+    // within a level, player 0's nodes first: a down sweep that only has to
+    // refresh one player's reach launches over that player's sub-span
+    for (size_t l = 0; l < P.act_span.size(); l++) {
+        const Span s = P.act_span[l];
+        auto first = P.act.begin() + s.start;
+        auto mid = std::stable_partition(first, first + s.count, [](const ActItem& x) { return x.actor == 0; });
+        const uint32_t n0 = (uint32_t)(mid - first);
+        P.act_span_actor[0].push_back({s.start, n0});
+        P.act_span_actor[1].push_back({s.start + n0, s.count - n0});
+    }
     flatten(edge_l, P.edge, P.edge_span);
     flatten(fold_l, P.fold, P.fold_span);
     flatten(show_l, P.show, P.show_span);

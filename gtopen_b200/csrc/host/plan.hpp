@@ -111,6 +111,7 @@ struct Plan {
     uint64_t num_visited = 0;
     std::vector<ActItem> act;
     std::vector<Span> act_span;
+    std::vector<Span> act_span_actor[2];  // per level: the sub-span of each actor's nodes
     std::vector<EdgeItem> edge;
     std::vector<Span> edge_span;
     std::vector<FoldItem> fold;

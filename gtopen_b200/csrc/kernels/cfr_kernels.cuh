@@ -26,7 +26,8 @@ constexpr int kMaxHpt = 6;  // hands per thread in the runout kernel (nh <= 1536
 
 struct Dev {
     int nh[2];
-    int nh_max;
+    int nh_max;        // cfv slot stride (floats, a multiple of 4: 16-byte aligned slots)
+    int rstr[2];       // reach slot stride per player (floats, a multiple of 4)
     int nh_pad;        // floats per staged hand vector (multiple of 4)
     int scr_elems;     // terminal scratch elements (4 * max_sorted + 105)
     int max_nterm;     // terminal children of one action node (fused smem layout)
@@ -61,6 +62,7 @@ struct Dev {
     float* disc;  // pos, neg, strat
     unsigned* iter;
     double* dot;  // root dot products
+    unsigned* err;  // device error bits (bounded waits that gave up, bad copies)
 };
 struct Arenas {
     void* reg[2];
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(kThreads) k_down_action(Dev d, Arenas ar, cons
     const int a = (int)it.actor, na = (int)it.na, nh = d.nh[a];
     if (threadIdx.x < na) s_rs[threadIdx.x] = d.crefs[it.cref + threadIdx.x].rslot;
     __syncthreads();
-    const float* parent = d.reach[a] + (size_t)it.rslot * nh;
+    const float* parent = d.reach[a] + (size_t)it.rslot * d.rstr[a];
     const long long loff = d.lock_off[a][it.sidx];
     float sig[KA];
     for (int i = threadIdx.x; i < nh; i += blockDim.x) {
@@ -449,17 +451,19 @@ __global__ void __launch_bounds__(kThreads) k_down_action(Dev d, Arenas ar, cons
         node_sigma<FMT, KA>(d, ar, it, loff, i, mode, sig);
 #pragma unroll
         for (int k = 0; k < KA; k++)
-            if (k < na && s_rs[k] != kNoSlot) d.reach[a][(size_t)s_rs[k] * nh + i] = pr * sig[k];
+            if (k < na && s_rs[k] != kNoSlot) d.reach[a][(size_t)s_rs[k] * d.rstr[a] + i] = pr * sig[k];
     }
 }
 
 // Down sweep, chance edges: both players' reach with holders of the card zeroed.
-__global__ void __launch_bounds__(kThreads) k_down_chance(Dev d, const EdgeItem* items) {
+// qmask: the players whose reach is refreshed (bit q)
+__global__ void __launch_bounds__(kThreads) k_down_chance(Dev d, const EdgeItem* items, int qmask) {
     const EdgeItem e = items[blockIdx.x];
     for (int q = 0; q < 2; q++) {
+        if (!(qmask >> q & 1)) continue;
         const int nh = d.nh[q];
-        const float* pr = d.reach[q] + (size_t)e.prs[q] * nh;
-        float* cr = d.reach[q] + (size_t)e.crs[q] * nh;
+        const float* pr = d.reach[q] + (size_t)e.prs[q] * d.rstr[q];
+        float* cr = d.reach[q] + (size_t)e.crs[q] * d.rstr[q];
         for (int i = threadIdx.x; i < nh; i += blockDim.x) cr[i] = (d.mask[q][i] >> e.card & 1ull) ? 0.0f : pr[i];
     }
 }
@@ -470,7 +474,7 @@ __global__ void __launch_bounds__(kThreads) k_fold(Dev d, const FoldItem* items,
     __shared__ double s_red[kWarps];
     const FoldItem f = items[blockIdx.x];
     const int o = 1 - p;
-    const float* ro = d.reach[o] + (size_t)f.rs[o] * d.nh[o];
+    const float* ro = d.reach[o] + (size_t)f.rs[o] * d.rstr[o];
     const double total = fold_sums<double>(d, o, ro, S, s_red);
     fold_write<double>(d, p, ro, total, S, (int)f.folder == p ? f.tlose : f.twin, d.cfv + (size_t)f.cslot * d.nh_max);
 }
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(kThreads) k_showdown(Dev d, const ShowItem* it
     __shared__ double s_w[kWarps];
     const ShowItem s = items[blockIdx.x];
     const int o = 1 - p;
-    const float* ro = d.reach[o] + (size_t)s.rs[o] * d.nh[o];
+    const float* ro = d.reach[o] + (size_t)s.rs[o] * d.rstr[o];
     eval_showdown<double>(d, p, s.slot, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, sh, s_w);
 }
 
@@ -511,7 +515,7 @@ __global__ void __launch_bounds__(kThreads) k_chance(Dev d, const ChanceItem* it
     T* scr = (T*)dsm;
     float* rt = (float*)(scr + d.scr_elems);
     float* tv = rt + d.nh_pad;
-    const float* ro = d.reach[o] + (size_t)c.rs[o] * nho;
+    const float* ro = d.reach[o] + (size_t)c.rs[o] * d.rstr[o];
     float acc[kMaxHpt];
 #pragma unroll
     for (int k = 0; k < kMaxHpt; k++) acc[k] = 0.0f;
@@ -581,7 +585,7 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
         TT* scr = (TT*)dsm;
         float* rts = (float*)(scr + d.scr_elems);
         tv = rts + (size_t)d.max_nterm * d.nh_pad;
-        const float* ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * nho;
+        const float* ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * d.rstr[o];
         if (a == o) {
             // the opponent acts: each terminal child's reach = reach * sigma_o[k]
             for (int j = threadIdx.x; j < nho; j += blockDim.x) {
@@ -659,7 +663,7 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
         return;
     }
     const float pos = d.disc[0], neg = d.disc[1], ds = d.disc[2];
-    const float* reach = d.reach[p] + (size_t)it.rslot * nh;
+    const float* reach = d.reach[p] + (size_t)it.rslot * d.rstr[p];
     float v[KA];
     if (FMT == kDevF32) {
         float* R = (float*)ar.reg[p];
@@ -806,7 +810,7 @@ __global__ void __launch_bounds__(kThreads) kw_down_action(Dev d, Arenas ar, con
     uint32_t rs[KA];
 #pragma unroll
     for (int k = 0; k < KA; k++) rs[k] = k < na ? d.crefs[it.cref + k].rslot : kNoSlot;
-    const float* parent = d.reach[a] + (size_t)it.rslot * nh;
+    const float* parent = d.reach[a] + (size_t)it.rslot * d.rstr[a];
     float* rbase = d.reach[a];
     const long long loff = d.lock_off[a][it.sidx];
     float sig[KA];
@@ -816,7 +820,7 @@ __global__ void __launch_bounds__(kThreads) kw_down_action(Dev d, Arenas ar, con
         node_sigma<FMT, KA>(d, ar, it, loff, i, mode, sig);
 #pragma unroll
         for (int k = 0; k < KA; k++)
-            if (k < na && rs[k] != kNoSlot) rbase[(size_t)rs[k] * nh + i] = pr * sig[k];
+            if (k < na && rs[k] != kNoSlot) rbase[(size_t)rs[k] * d.rstr[a] + i] = pr * sig[k];
     }
 }
 
@@ -826,7 +830,7 @@ __global__ void __launch_bounds__(kThreads) kw_fold(Dev d, const FoldItem* items
     WARP_ITEM(count)
     const FoldItem f = items[wid];
     const int o = 1 - p;
-    const float* ro = d.reach[o] + (size_t)f.rs[o] * d.nh[o];
+    const float* ro = d.reach[o] + (size_t)f.rs[o] * d.rstr[o];
     double* S = s_S[threadIdx.x >> 5];
     const double total = warp_fold_sums(d, o, ro, S);
     const float amount = (int)f.folder == p ? f.tlose : f.twin;
@@ -871,7 +875,7 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
     const double* S = s_S[w];
     const float* fro = nullptr;
     if (fk >= 0) {
-        const float* ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * nho;
+        const float* ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * d.rstr[o];
         fro = ro;
         if (a == o) {  // the opponent folds with probability sigma_o[fk]
             float* rf = wsm + (size_t)w * d.nh_pad;
@@ -935,7 +939,7 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
         return;
     }
     const float pos = d.disc[0], neg = d.disc[1], ds = d.disc[2];
-    const float* reach = d.reach[p] + (size_t)it.rslot * nh;
+    const float* reach = d.reach[p] + (size_t)it.rslot * d.rstr[p];
     float v[KA];
     if (FMT == kDevF32) {
         float* R = (float*)ar.reg[p];

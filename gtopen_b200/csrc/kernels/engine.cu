@@ -74,6 +74,7 @@ struct EngineImpl {
     bool wide = false;  // some node has more than 8 actions: use the 32-wide kernels
     bool term64 = false;  // terminal sums in f64 (plain engine, or fused on request)
     bool warp = false;    // warp-per-node action kernels, fold children in place
+    bool reach_valid = false;  // reach slots hold the current strategies' reach (see prime)
     uint32_t iteration = 0;
     cudaStream_t stream = nullptr;
     std::vector<void*> owned;
@@ -137,6 +138,7 @@ struct EngineImpl {
         d.lock_off[1] = (const long long*)(base + b0);
         d.lock_sig = (const float*)(base + b0 + b1);
         drop_graphs();
+        reach_valid = false;
     }
     void drop_graphs() {
         if (g_iter) { cudaGraphExecDestroy(g_iter); g_iter = nullptr; }
@@ -233,16 +235,38 @@ struct EngineImpl {
         else k_chance<double><<<sc.count, kThreads, chance_smem, stream>>>(d, chance + sc.start, p);
     }
 
-    // One sweep for traverser p.  eval < 0: CFR iteration; 0/1: BR / average.
-    void sweep(int p, int eval, Profile* pr) {
+    // Down sweep.  qmask: the players whose reach vectors are recomputed.  In a
+    // CFR iteration only the opponent's are: the traverser's own reach depends
+    // on its own strategy only, which has not changed since the previous
+    // sweep computed it (that sweep's traverser was the other player), so its
+    // slots still hold exactly the values a full recomputation would write.
+    void down(int qmask, int mode, Profile* pr) {
         timed(pr, 0, [&] { k_copy_root<<<4, kThreads, 0, stream>>>(d); });
         const int L = plan.num_levels;
-        const int down_mode = eval < 0 ? 0 : 1;
         for (int l = 0; l < L; l++) {
-            const Span sa = plan.act_span[l];
-            if (sa.count) timed(pr, 1, [&] { launch_down_action(sa, down_mode); });
+            const Span sa = qmask == 3 ? plan.act_span[l] : plan.act_span_actor[qmask == 1 ? 0 : 1][l];
+            if (sa.count) timed(pr, 1, [&] { launch_down_action(sa, mode); });
             const Span se = plan.edge_span[l];
-            if (se.count) timed(pr, 2, [&] { k_down_chance<<<se.count, kThreads, 0, stream>>>(d, edge + se.start); });
+            if (se.count)
+                timed(pr, 2, [&] { k_down_chance<<<se.count, kThreads, 0, stream>>>(d, edge + se.start, qmask); });
+        }
+    }
+    // Before the first CFR sweep after anything else wrote the reach slots
+    // (engine start, eval sweeps, lock changes): both players' reach.
+    void prime() {
+        if (reach_valid) return;
+        down(3, 0, nullptr);
+        CK(cudaGetLastError());
+        reach_valid = true;
+    }
+    // One sweep for traverser p.  eval < 0: CFR iteration; 0/1: BR / average.
+    void sweep(int p, int eval, Profile* pr) {
+        const int L = plan.num_levels;
+        if (eval < 0) {
+            down(1 << (1 - p), 0, pr);
+        } else {
+            down(3, 1, pr);
+            reach_valid = false;
         }
         for (int l = L - 1; l >= 0; l--) {
             const Span sf = plan.fold_span[l];
@@ -313,8 +337,10 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     Dev& d = E.d;
     d.nh[0] = P.nh[0];
     d.nh[1] = P.nh[1];
-    d.nh_max = P.nh_max;
     d.nh_pad = (P.nh_max + 3) / 4 * 4;
+    d.nh_max = d.nh_pad;  // cfv slot stride: 16-byte aligned slots
+    d.rstr[0] = (P.nh[0] + 3) / 4 * 4;
+    d.rstr[1] = (P.nh[1] + 3) / 4 * 4;
     d.scr_elems = (int)(4 * P.max_sorted + 105);
     uint32_t max_nterm = 0;
     bool runouts = false;
@@ -346,15 +372,16 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
         d.rank[q] = dupload(P.rank[q], O, &B);
         d.zero_off[q] = dupload(P.zero_off[q], O, &B);
         d.zero_idx[q] = dupload(P.zero_idx[q], O, &B);
-        d.reach[q] = (float*)dalloc(P.n_rslots[q] * P.nh[q] * sizeof(float), O, &B);
+        d.reach[q] = (float*)dalloc(P.n_rslots[q] * (size_t)d.rstr[q] * sizeof(float), O, &B);
     }
     d.cards = dupload(P.cards, O, &B);
     d.crefs = dupload(P.crefs, O, &B);
     d.terms = dupload(P.terms, O, &B);
-    d.cfv = (float*)dalloc(P.n_cslots * (size_t)P.nh_max * sizeof(float), O, &B);
+    d.cfv = (float*)dalloc(P.n_cslots * (size_t)d.nh_max * sizeof(float), O, &B);
     d.disc = (float*)dalloc(4 * sizeof(float), O, &B);
     d.iter = (unsigned*)dalloc(sizeof(unsigned), O, &B);
     d.dot = (double*)dalloc(4 * sizeof(double), O, &B);
+    d.err = (unsigned*)dalloc(sizeof(unsigned), O, &B);
     CK(cudaMemcpy(d.iter, &E.iteration, sizeof(unsigned), cudaMemcpyHostToDevice));
     E.act = dupload(P.act, O, &B);
     E.edge = dupload(P.edge, O, &B);
@@ -451,6 +478,7 @@ void GpuEngine::iterate(int n) {
     EngineImpl& E = *d_;
     for (int k = 0; k < n; k++) {
         if (!E.g_iter) E.g_iter = E.capture(-1);
+        E.prime();
         CK(cudaGraphLaunch(E.g_iter, E.stream));
         E.iteration++;
     }
@@ -460,6 +488,7 @@ void GpuEngine::iterate(int n) {
 double GpuEngine::time_iterations(int n) {
     EngineImpl& E = *d_;
     if (!E.g_iter) E.g_iter = E.capture(-1);
+    E.prime();
     cudaEvent_t a, b;
     CK(cudaEventCreate(&a));
     CK(cudaEventCreate(&b));
@@ -482,6 +511,7 @@ Profile GpuEngine::iterate_profiled() {
     Profile pr;
     std::memset(&pr, 0, sizeof(pr));
     CK(cudaStreamSynchronize(E.stream));
+    E.prime();
     k_begin_iteration<<<1, 1, 0, E.stream>>>(E.d.iter, E.d.disc, E.algo);
     E.sweep(0, -1, &pr);
     E.sweep(1, -1, &pr);
@@ -499,6 +529,7 @@ double GpuEngine::exploitability(const HostSolver& host) {  // best_response.rs:
     for (int mode = 0; mode < (raked ? 2 : 1); mode++) {
         if (!E.g_eval[mode]) E.g_eval[mode] = E.capture(mode);
         CK(cudaGraphLaunch(E.g_eval[mode], E.stream));
+        E.reach_valid = false;
         CK(cudaStreamSynchronize(E.stream));
         for (int p = 0; p < 2; p++) (mode == 0 ? br[p] : v[p]) = E.h_dot[p] / denom;
     }
@@ -509,6 +540,7 @@ double GpuEngine::exploitability(const HostSolver& host) {  // best_response.rs:
 void GpuEngine::root_cfv(int p, int mode, float* out) {
     EngineImpl& E = *d_;
     E.sweep(p, mode, nullptr);
+    E.reach_valid = false;
     CK(cudaMemcpyAsync(out, E.d.cfv, E.plan.nh[p] * sizeof(float), cudaMemcpyDeviceToHost, E.stream));
     CK(cudaStreamSynchronize(E.stream));
 }
