@@ -108,7 +108,10 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, backend=None):
+    """One process per GPU (torchrun env).  NCCL on GPUs; gloo when no GPU is
+    visible (the multi-rank plumbing's CPU tests).  A short process-group
+    timeout makes ranks that wait on a missing peer fail instead of hanging."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -117,18 +120,24 @@ def dist_setup(n_gpus):
 
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        timeout = datetime.timedelta(seconds=120)
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=timeout, device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=timeout)
     return world, rank, local
 
 
 def allmax(x, world):
+    """Max over ranks (device times are reported as the slowest rank's)."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([float(x)], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -312,7 +321,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="flop", choices=["flop", "turn", "river", "bench_spot"])
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32"])
-    ap.add_argument("--engine", default="fused", choices=["fused", "plain", "warp", "fused32"])
+    ap.add_argument("--engine", default="fused", choices=["fused", "plain", "warp", "fused32", "staged"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=1)

@@ -1,0 +1,607 @@
+// Staged node kernels (the STAGED engine): one CTA per node stages every
+// vector and arena block the node needs in shared memory with bulk
+// asynchronous copies -- the TMA unit's non-tensor mode, cp.async.bulk --
+// that complete on one mbarrier, then computes from shared memory and writes
+// its results with 16-byte stores.  All of a node's HBM reads are in flight
+// at once (one round trip instead of one per hand chunk and arena field), and
+// a 128-thread CTA with ~32 KB of shared memory leaves room for many nodes
+// per SM.
+//
+// Arithmetic is the same as the generic kernels in cfr_kernels.cuh (the same
+// expressions in the same order, -fmad=false), so results are identical.
+//
+// Every wait is bounded: a copy that does not land within kWaitNs sets bit 0
+// of Dev::err, waits once more (bounded) for the copies in flight and ends the
+// CTA; a source or size the bulk unit cannot take (not 16-byte aligned) sets
+// bit 1 and the CTA issues nothing.  The host reads Dev::err at every
+// synchronisation point and reports a timeout error.
+#pragma once
+#include "cfr_kernels.cuh"
+
+namespace gtob {
+
+constexpr int kSThreads = 128;
+constexpr int kSWarps = kSThreads / 32;
+constexpr int kSKA = 4;                                // staged kernels take nodes with at most 4 actions
+constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait for phase `parity` of the barrier.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = globaltimer_ns();
+    while (!mbar_try_wait(bar, parity))
+        if (globaltimer_ns() - t0 > kWaitNs) return false;
+    return true;
+}
+// Global -> shared bulk copy completing on bar (no multicast).
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Up to 12 copies per node, described by thread 0 and issued together.
+struct CopyList {
+    int n = 0;
+    unsigned total = 0;
+    bool bad = false;
+    void* dst[12];
+    const void* src[12];
+    unsigned bytes[12];
+    __device__ void add(void* d, const void* s, unsigned b) {
+        if (b == 0) return;
+        if ((((uintptr_t)d | (uintptr_t)s | (uintptr_t)b) & 15u) != 0 || n == 12) {
+            bad = true;
+            return;
+        }
+        dst[n] = d;
+        src[n] = s;
+        bytes[n] = b;
+        total += b;
+        n++;
+    }
+};
+__device__ __forceinline__ unsigned round16(unsigned b) { return (b + 15u) & ~15u; }
+
+// Every thread of the CTA calls this once; thread 0 (which initialised bar and
+// filled cl) issues the copies, then all wait.  Returns false, after the
+// error handling described at the top, when the CTA must end.
+__device__ bool stage_and_wait(const Dev& d, uint64_t* bar, const CopyList& cl, int* s_flag) {
+    if (threadIdx.x == 0) {
+        *s_flag = 0;
+        if (cl.bad) {
+            *s_flag = 1;
+            atomicOr(d.err, 2u);
+        } else {
+            mbar_expect_tx(bar, cl.total);
+            for (int k = 0; k < cl.n; k++) bulk_load(cl.dst[k], cl.src[k], cl.bytes[k], bar);
+        }
+    }
+    __syncthreads();
+    if (*s_flag) return false;
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) atomicOr(d.err, 1u);
+        if (!ok) mbar_wait(bar, 0);
+        return false;
+    }
+    return true;
+}
+
+// 16-byte copy of a staged block back to global memory.
+__device__ __forceinline__ void store_block(void* gdst, const void* sblk, unsigned bytes) {
+    int4* g = (int4*)gdst;
+    const int4* s = (const int4*)sblk;
+    for (unsigned k = threadIdx.x; k < bytes / 16; k += blockDim.x) g[k] = s[k];
+}
+
+// Strategies of hand i from staged blocks (same expressions as regret_sigma /
+// average_sigma in cfr_kernels.cuh).
+template <int FMT>
+__device__ __forceinline__ void s_regret_sigma(const void* reg, const void* pred, float kr, float kp, int na, int i,
+                                               float (&sig)[kSKA]) {
+    const int base = i * na;
+    float sum = 0.0f;
+    if (FMT == kDevF32) {
+        const float* r = (const float*)reg + base;
+        const float* pr = (const float*)pred;
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na) {
+                float v = r[k];
+                if (pr) v = fmaxf(v, 0.0f) + pr[base + k];
+                sig[k] = v;
+                sum += fmaxf(v, 0.0f);
+            }
+    } else {
+        const int16_t* q = (const int16_t*)reg + base;
+        if (pred) {
+            const int16_t* qp = (const int16_t*)pred + base;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    sig[k] = (float)max((int)q[k], 0) * kr + (float)qp[k] * kp;
+                    sum += fmaxf(sig[k], 0.0f);
+                }
+        } else {
+            int isum = 0;
+            int qv[kSKA];
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    qv[k] = max((int)q[k], 0);
+                    isum += qv[k];
+                }
+            if (isum > 0) {
+                const float inv = 1.0f / (float)isum;
+#pragma unroll
+                for (int k = 0; k < kSKA; k++)
+                    if (k < na) sig[k] = (float)qv[k] * inv;
+            } else {
+                const float u = 1.0f / (float)na;
+#pragma unroll
+                for (int k = 0; k < kSKA; k++)
+                    if (k < na) sig[k] = u;
+            }
+            return;
+        }
+    }
+    if (sum > 1e-12f) {
+        const float inv = 1.0f / sum;
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na) sig[k] = fmaxf(sig[k], 0.0f) * inv;
+    } else {
+        const float u = 1.0f / (float)na;
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na) sig[k] = u;
+    }
+}
+template <int FMT>
+__device__ __forceinline__ void s_average_sigma(const void* str, int na, int i, float (&sig)[kSKA]) {
+    const int base = i * na;
+    if (FMT == kDevF32) {
+        const float* s = (const float*)str + base;
+        double sum = 0.0;
+        float v[kSKA];
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na) {
+                v[k] = fmaxf(s[k], 0.0f);
+                sum += (double)v[k];
+            }
+        if (sum > 1e-12) {
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) sig[k] = (float)((double)v[k] / sum);
+        } else {
+            const float u = 1.0f / (float)na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) sig[k] = u;
+        }
+    } else {
+        const uint16_t* q = (const uint16_t*)str + base;
+        unsigned sum = 0;
+        unsigned qv[kSKA];
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na) {
+                qv[k] = q[k];
+                sum += qv[k];
+            }
+        if (sum > 0) {
+            const float inv = 1.0f / (float)sum;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) sig[k] = (float)qv[k] * inv;
+        } else {
+            const float u = 1.0f / (float)na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) sig[k] = u;
+        }
+    }
+}
+template <int FMT>
+__device__ __forceinline__ void s_node_sigma(const Dev& d, long long loff, int a, int i, int mode, const void* reg,
+                                             const void* pred, const void* str, float kr, float kp, int na,
+                                             float (&sig)[kSKA]) {
+    if (loff >= 0) {
+        const int nh = d.nh[a];
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na) sig[k] = d.lock_sig[loff + (long long)k * nh + i];
+    } else if (mode == 0) {
+        s_regret_sigma<FMT>(reg, pred, kr, kp, na, i, sig);
+    } else {
+        s_average_sigma<FMT>(str, na, i, sig);
+    }
+}
+
+__device__ __forceinline__ float s_block_max(float v, float* sh) {
+    v = warp_max(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float m = sh[0];
+#pragma unroll
+    for (int k = 1; k < kSWarps; k++) m = fmaxf(m, sh[k]);
+    return m;
+}
+
+// Fold summary of a staged opponent reach vector (game.rs:478-485): total
+// and per-card sums in f64.  Each warp owns cards w, w + 4, ...; lanes split
+// a card's list (<= 51 hands) into two 32-lane chunks.
+__device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, double* s_red) {
+    const int nho = d.nh[o];
+    double t = 0.0;
+    for (int j = threadIdx.x; j < nho; j += kSThreads) t += (double)ro[j];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int c = warp; c < 52; c += kSWarps) {
+        const uint32_t b = d.hcard_off[o][c], e = d.hcard_off[o][c + 1];
+        double s = 0.0;
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+            const uint32_t k = b + lane + 32 * h;
+            s += k < e ? (double)ro[d.hcard_idx[o][k]] : 0.0;
+        }
+        s = warp_sum(s);
+        if (lane == 0) S[c] = s;
+    }
+    t = warp_sum(t);
+    if (lane == 0) s_red[warp] = t;
+    __syncthreads();
+    double total = 0.0;
+#pragma unroll
+    for (int k = 0; k < kSWarps; k++) total += s_red[k];
+    return total;
+}
+
+// Shared-memory layout of the staged action kernels (bytes).
+struct SLayout {
+    unsigned cap, vec;  // arena block capacity; one hand vector (nh_pad floats)
+    __device__ SLayout(const Dev& d, int esz)
+        : cap(round16((unsigned)(kSKA * d.nh_pad * esz))), vec((unsigned)d.nh_pad * 4u) {}
+    __device__ unsigned reg() const { return 16; }
+    __device__ unsigned str() const { return 16 + cap; }
+    __device__ unsigned pred() const { return 16 + 2 * cap; }
+    __device__ unsigned ro() const { return 16 + 3 * cap; }
+    __device__ unsigned rp() const { return 16 + 3 * cap + vec; }
+    __device__ unsigned cv() const { return 16 + 3 * cap + 2 * vec; }
+};
+// Host twins of SLayout's extent: the up kernel uses every region, the down
+// kernel the blocks and one reach vector.
+inline size_t staged_smem_bytes(int nh_pad, int esz) {
+    const size_t cap = ((size_t)kSKA * nh_pad * esz + 15) & ~(size_t)15;
+    return 16 + 3 * cap + (2 + kSKA) * (size_t)nh_pad * 4;
+}
+inline size_t staged_down_smem_bytes(int nh_pad, int esz) {
+    const size_t cap = ((size_t)kSKA * nh_pad * esz + 15) & ~(size_t)15;
+    return 16 + 3 * cap + (size_t)nh_pad * 4;
+}
+
+// Down sweep, one node per CTA: staged sigma source and parent reach; child
+// reach vectors written with coalesced stores (cfr.rs:469-531 push-down).
+template <int FMT>
+__global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const ActItem* items, int mode) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ int s_flag;
+    const ActItem it = items[blockIdx.x];
+    const int a = (int)it.actor, na = (int)it.na, nh = d.nh[a];
+    const int esz = FMT == kDevF32 ? 4 : 2;
+    const SLayout L(d, esz);
+    uint64_t* bar = (uint64_t*)sm;
+    unsigned char* b_reg = sm + L.reg();
+    unsigned char* b_str = sm + L.str();
+    unsigned char* b_pred = sm + L.pred();
+    float* pr = (float*)(sm + L.ro());
+    const long long loff = d.lock_off[a][it.sidx];
+    const bool has_pred = ar.pred[a] != nullptr;
+    const unsigned blk = round16((unsigned)(na * nh * esz));
+    CopyList cl;  // filled and issued by thread 0 only
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        if (loff < 0) {
+            if (mode == 0) {
+                cl.add(b_reg, (const unsigned char*)ar.reg[a] + it.aoff * esz, blk);
+                if (has_pred) cl.add(b_pred, (const unsigned char*)ar.pred[a] + it.aoff * esz, blk);
+            } else {
+                cl.add(b_str, (const unsigned char*)ar.str[a] + it.aoff * esz, blk);
+            }
+        }
+        cl.add(pr, d.reach[a] + (size_t)it.rslot * d.rstr[a], round16((unsigned)nh * 4u));
+    }
+    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
+    uint32_t rs[kSKA];
+#pragma unroll
+    for (int k = 0; k < kSKA; k++) rs[k] = k < na ? d.crefs[it.cref + k].rslot : kNoSlot;
+    float kr = 0.0f, kp = 0.0f;
+    if (FMT != kDevF32 && mode == 0 && loff < 0) {
+        kr = ar.rscale[a][it.sidx] / 32767.0f;
+        if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
+    }
+    float sig[kSKA];
+    for (int i = threadIdx.x; i < nh; i += kSThreads) {
+        s_node_sigma<FMT>(d, loff, a, i, mode, b_reg, has_pred ? b_pred : nullptr, b_str, kr, kp, na, sig);
+        const float p = pr[i];
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na && rs[k] != kNoSlot) d.reach[a][(size_t)rs[k] * d.rstr[a] + i] = p * sig[k];
+    }
+}
+
+// Up sweep, one node per CTA (cfr.rs:469-531 pull-up, 297-409 update;
+// best_response.rs:69-121, 185-219 for EVAL = 1 with mode 0 BR / 1 average).
+// The node's fold child, if any, is evaluated here from the staged opponent
+// reach; every other child's cfv is staged from its slot.
+template <int FMT, int EVAL>
+__global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActItem* items, int p, int mode) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ int s_flag;
+    __shared__ double s_S[52];
+    __shared__ double s_dred[kSWarps];
+    __shared__ float s_red[3 * kSWarps];
+    const ActItem it = items[blockIdx.x];
+    const int a = (int)it.actor, na = (int)it.na, o = 1 - p, nh = d.nh[p], nho = d.nh[o];
+    const int esz = FMT == kDevF32 ? 4 : 2;
+    const SLayout L(d, esz);
+    uint64_t* bar = (uint64_t*)sm;
+    unsigned char* b_reg = sm + L.reg();
+    unsigned char* b_str = sm + L.str();
+    unsigned char* b_pred = sm + L.pred();
+    float* ro = (float*)(sm + L.ro());
+    float* rp = (float*)(sm + L.rp());
+    float* cv = (float*)(sm + L.cv());
+    const int vstride = d.nh_pad;
+
+    uint32_t cs[kSKA];
+    int fk = -1;
+    float famount = 0.0f;
+#pragma unroll
+    for (int k = 0; k < kSKA; k++) {
+        cs[k] = kNoSlot;
+        if (k < na) {
+            const ChildRef c = d.crefs[it.cref + k];
+            cs[k] = c.cslot;
+            if (c.kind == kChildFold) {
+                fk = k;
+                const TermInfo tm = d.terms[c.term];
+                famount = (int)tm.aux == p ? tm.tlose : tm.twin;
+            }
+        }
+    }
+    const long long loff = d.lock_off[a][it.sidx];
+    const bool mine = a == p;
+    const bool has_pred = ar.pred[a] != nullptr;
+    // what the node reads
+    const bool use_reg = loff < 0 && !EVAL && (mine || fk >= 0);
+    const bool use_str = loff < 0 && (EVAL ? (mine ? mode == 1 : fk >= 0) : mine);
+    const bool use_pred = use_reg && has_pred;
+    const bool use_rp = mine && !EVAL && loff < 0;
+    const unsigned blk = round16((unsigned)(na * d.nh[a] * esz));
+    CopyList cl;  // filled and issued by thread 0 only
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        if (use_reg) cl.add(b_reg, (const unsigned char*)ar.reg[a] + it.aoff * esz, blk);
+        if (use_str) cl.add(b_str, (const unsigned char*)ar.str[a] + it.aoff * esz, blk);
+        if (use_pred) cl.add(b_pred, (const unsigned char*)ar.pred[a] + it.aoff * esz, blk);
+        if (use_rp) cl.add(rp, d.reach[p] + (size_t)it.rslot * d.rstr[p], round16((unsigned)nh * 4u));
+        if (fk >= 0)
+            cl.add(ro, d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * d.rstr[o], round16((unsigned)nho * 4u));
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na && k != fk) cl.add(cv + k * vstride, d.cfv + (size_t)cs[k] * d.nh_max, round16((unsigned)nh * 4u));
+    }
+    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
+
+    float sig[kSKA];
+    // scales of the actor's node (16-bit arenas)
+    float kr = 0.0f, kp = 0.0f;
+    if (FMT != kDevF32 && loff < 0) {
+        kr = ar.rscale[a][it.sidx] / 32767.0f;
+        if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
+    }
+    double ftotal = 0.0;
+    if (fk >= 0) {
+        if (a == o) {  // the opponent folds with probability sigma_o[fk]
+            for (int j = threadIdx.x; j < nho; j += kSThreads) {
+                s_node_sigma<FMT>(d, loff, a, j, EVAL ? 1 : 0, b_reg, use_pred ? b_pred : nullptr, b_str, kr, kp, na,
+                                  sig);
+                float sf = 0.0f;
+#pragma unroll
+                for (int k = 0; k < kSKA; k++)
+                    if (k == fk) sf = sig[k];
+                ro[j] = ro[j] * sf;
+            }
+            __syncthreads();
+        }
+        ftotal = s_fold_sums(d, o, ro, s_S, s_dred);
+        __syncthreads();
+    }
+    float* out = d.cfv + (size_t)it.cslot * d.nh_max;
+#define CHILD_V(k, i) ((k) == fk ? fold_value(d, p, (i), ro, ftotal, s_S, famount) : cv[(k) * vstride + (i)])
+    if (!mine) {  // opponent node: sum of children
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) acc += CHILD_V(k, i);
+            out[i] = acc;
+        }
+        return;
+    }
+    if (loff >= 0) {  // locked: fixed sigma, no update
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) acc += d.lock_sig[loff + (long long)k * nh + i] * CHILD_V(k, i);
+            out[i] = acc;
+        }
+        return;
+    }
+    if (EVAL) {
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            float acc;
+            if (mode == 0) {
+                acc = CHILD_V(0, i);
+#pragma unroll
+                for (int k = 1; k < kSKA; k++)
+                    if (k < na) {
+                        const float v = CHILD_V(k, i);
+                        if (v > acc) acc = v;
+                    }
+            } else {
+                s_average_sigma<FMT>(b_str, na, i, sig);
+                acc = 0.0f;
+#pragma unroll
+                for (int k = 0; k < kSKA; k++)
+                    if (k < na) acc += sig[k] * CHILD_V(k, i);
+            }
+            out[i] = acc;
+        }
+        return;
+    }
+    const float pos = d.disc[0], neg = d.disc[1], ds = d.disc[2];
+    const void* predp = use_pred ? b_pred : nullptr;
+    float v[kSKA];
+    if (FMT == kDevF32) {
+        float* R = (float*)b_reg;
+        float* Sg = (float*)b_str;
+        float* PR = (float*)b_pred;
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            s_regret_sigma<FMT>(b_reg, predp, 0.0f, 0.0f, na, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float r_p = rp[i];
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const float r = R[b + k];
+                    R[b + k] = r * (r > 0.0f ? pos : neg) + (v[k] - o_);
+                    Sg[b + k] = Sg[b + k] * ds + r_p * sig[k];
+                    if (use_pred) PR[b + k] = v[k] - o_;
+                }
+            out[i] = o_;
+        }
+        __syncthreads();
+        store_block((unsigned char*)ar.reg[p] + it.aoff * esz, b_reg, blk);
+        store_block((unsigned char*)ar.str[p] + it.aoff * esz, b_str, blk);
+        if (use_pred) store_block((unsigned char*)ar.pred[p] + it.aoff * esz, b_pred, blk);
+        return;
+    }
+    // 16-bit arenas (cfr.rs:350-407): pass 1 finds the node's new maxima,
+    // pass 2 recomputes from the (unchanged) staged quants and requantises in
+    // place; the blocks then go back to HBM.
+    int16_t* RQ = (int16_t*)b_reg;
+    uint16_t* SQ = (uint16_t*)b_str;
+    int16_t* PQ = (int16_t*)b_pred;
+    const float kss = ar.sscale[p][it.sidx] / 65535.0f * ds;
+    float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
+    for (int pass = 0; pass < 2; pass++) {
+        float rk = 0.0f, sk = 0.0f, pk = 0.0f;
+        if (pass == 1) {
+            rmax = s_block_max(rmax, s_red);
+            smax = s_block_max(smax, s_red + kSWarps);
+            if (use_pred) pmax = s_block_max(pmax, s_red + 2 * kSWarps);
+            rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
+            sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
+            pk = (pmax > 0.0f && isfinite(pmax)) ? 32767.0f / pmax : 0.0f;
+        }
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            s_regret_sigma<FMT>(b_reg, predp, kr, kp, na, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float r_p = rp[i];
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const int16_t qv = RQ[b + k];
+                    const float nr = (float)qv * kr * (qv > 0 ? pos : neg) + (v[k] - o_);
+                    const float ns = (float)SQ[b + k] * kss + r_p * sig[k];
+                    if (pass == 0) {
+                        rmax = fmaxf(rmax, fabsf(nr));
+                        smax = fmaxf(smax, ns);
+                        if (use_pred) pmax = fmaxf(pmax, fabsf(v[k] - o_));
+                    } else {
+                        RQ[b + k] = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
+                        SQ[b + k] = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
+                        if (use_pred) PQ[b + k] = pk > 0.0f ? sat_i16((v[k] - o_) * pk) : (int16_t)0;
+                    }
+                }
+            if (pass == 1) out[i] = o_;
+        }
+    }
+#undef CHILD_V
+    __syncthreads();
+    store_block((unsigned char*)ar.reg[p] + it.aoff * esz, b_reg, blk);
+    store_block((unsigned char*)ar.str[p] + it.aoff * esz, b_str, blk);
+    if (use_pred) store_block((unsigned char*)ar.pred[p] + it.aoff * esz, b_pred, blk);
+    if (threadIdx.x == 0) {
+        ar.rscale[p][it.sidx] = (rmax > 0.0f && isfinite(rmax)) ? rmax : 0.0f;
+        ar.sscale[p][it.sidx] = (smax > 0.0f && isfinite(smax)) ? smax : 0.0f;
+        if (use_pred) ar.pscale[p][it.sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
+    }
+}
+
+// Showdown terminal with its opponent reach staged in shared memory (the
+// gather by strength order then reads shared memory, not HBM).
+__global__ void __launch_bounds__(kThreads) ks_showdown(Dev d, const ShowItem* items, int p) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ double s_w[kWarps];
+    __shared__ int s_flag;
+    const ShowItem s = items[blockIdx.x];
+    const int o = 1 - p;
+    uint64_t* bar = (uint64_t*)sm;
+    float* ro = (float*)(sm + 16);
+    double* scr = (double*)(sm + 16 + (size_t)d.nh_pad * 4);
+    CopyList cl;  // filled and issued by thread 0 only
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        cl.add(ro, d.reach[o] + (size_t)s.rs[o] * d.rstr[o], round16((unsigned)d.nh[o] * 4u));
+    }
+    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
+    eval_showdown<double>(d, p, s.slot, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, scr, s_w);
+}
+inline size_t staged_show_smem_bytes(int nh_pad, int scr_elems) {
+    return 16 + (size_t)nh_pad * 4 + (size_t)scr_elems * sizeof(double);
+}
+
+}  // namespace gtob

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "cfr_kernels.cuh"
+#include "cfr_staged.cuh"
 #include "engine.hpp"
 
 namespace gtob {
@@ -74,6 +75,7 @@ struct EngineImpl {
     bool wide = false;  // some node has more than 8 actions: use the 32-wide kernels
     bool term64 = false;  // terminal sums in f64 (plain engine, or fused on request)
     bool warp = false;    // warp-per-node action kernels, fold children in place
+    bool staged = false;  // staged (bulk-copy) node kernels, fold children in place
     bool reach_valid = false;  // reach slots hold the current strategies' reach (see prime)
     uint32_t iteration = 0;
     cudaStream_t stream = nullptr;
@@ -95,6 +97,7 @@ struct EngineImpl {
     size_t show_smem = 0;    // plain showdown kernel (f64 scratch)
     size_t act_smem = 0;     // fused up-action dynamic smem
     size_t warp_smem = 0;    // warp up-action dynamic smem (one staged reach per warp)
+    size_t st_up_smem = 0, st_down_smem = 0, st_show_smem = 0;  // staged kernels
     size_t chance_smem = 0;  // runout chance dynamic smem
     cudaGraphExec_t g_iter = nullptr;
     cudaGraphExec_t g_eval[2] = {nullptr, nullptr};
@@ -182,7 +185,9 @@ struct EngineImpl {
     }
     template <int FMT, int KA>
     void down_action(const Span& sa, int mode) {
-        if (warp) {
+        if (staged) {
+            ks_down<FMT><<<sa.count, kSThreads, st_down_smem, stream>>>(d, ar, act + sa.start, mode);
+        } else if (warp) {
             const unsigned grid = (sa.count + kWarps - 1) / kWarps;
             kw_down_action<FMT, KA><<<grid, kThreads, 0, stream>>>(d, ar, act + sa.start, (int)sa.count, mode);
         } else {
@@ -202,6 +207,17 @@ struct EngineImpl {
         set_smem((const void*)kw_up_action<FMT, 1, KA>, bytes);
     }
     void launch_up_action(const Span& sa, int p, int eval) {
+        if (staged) {
+            const ActItem* it = act + sa.start;
+            if (fmt == kFmtF32) {
+                if (eval < 0) ks_up<kDevF32, 0><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, 0);
+                else ks_up<kDevF32, 1><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, eval);
+            } else {
+                if (eval < 0) ks_up<kDevI16, 0><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, 0);
+                else ks_up<kDevI16, 1><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, eval);
+            }
+            return;
+        }
         if (warp) {
             if (fmt == kFmtF32) {
                 if (wide) warp_up_action<kDevF32, 32>(sa, p, eval);
@@ -273,7 +289,10 @@ struct EngineImpl {
             if (sf.count) timed(pr, 3, [&] { k_fold<<<sf.count, kThreads, 0, stream>>>(d, fold + sf.start, p); });
             const Span ss = plan.show_span[l];
             if (ss.count)
-                timed(pr, 4, [&] { k_showdown<<<ss.count, kThreads, show_smem, stream>>>(d, show + ss.start, p); });
+                timed(pr, 4, [&] {
+                    if (staged) ks_showdown<<<ss.count, kThreads, st_show_smem, stream>>>(d, show + ss.start, p);
+                    else k_showdown<<<ss.count, kThreads, show_smem, stream>>>(d, show + ss.start, p);
+                });
             const Span sc = plan.chance_span[l];
             if (sc.count) timed(pr, 5, [&] { launch_chance(sc, p); });
             const Span sa = plan.act_span[l];
@@ -292,6 +311,19 @@ struct EngineImpl {
             k_root_dot<<<1, kThreads, 0, stream>>>(d, p, p);
         }
         CK(cudaMemcpyAsync(h_dot, d.dot, 2 * sizeof(double), cudaMemcpyDeviceToHost, stream));
+    }
+    // Device error bits (bounded waits that gave up): read at every
+    // synchronisation point; reported once, then cleared.
+    void check_err() {
+        unsigned e = 0;
+        CK(cudaMemcpyAsync(&e, d.err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        if (e) {
+            CK(cudaMemsetAsync(d.err, 0, sizeof(unsigned), stream));
+            CK(cudaStreamSynchronize(stream));
+            throw Error(std::string("timeout: ") + ((e & 1u) ? "a staged copy did not complete within its wait limit"
+                                                              : "a staged copy was refused (misaligned)"));
+        }
     }
     cudaGraphExec_t capture(int which) {
         cudaGraph_t g;
@@ -316,9 +348,11 @@ struct EngineImpl {
 GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new EngineImpl()) {
     EngineImpl& E = *d_;
     const Spot& sp = *host.spot;
-    if (engine < kEngineFused || engine > kEngineWarp) throw Error("unknown engine kind");
-    const int fuse = engine == kEnginePlain ? kFuseNone : engine == kEngineWarp ? kFuseFolds : kFuseAll;
-    E.warp = engine == kEngineWarp;
+    if (engine < kEngineFused || engine > kEngineStaged) throw Error("unknown engine kind");
+    const int fuse = engine == kEnginePlain                               ? kFuseNone
+                     : (engine == kEngineWarp || engine == kEngineStaged) ? kFuseFolds
+                                                                          : kFuseAll;
+    E.warp = engine == kEngineWarp || engine == kEngineStaged;  // staged falls back to warp kernels
     E.term64 = engine != kEngineFused32;
     E.spot = &sp;
     E.algo = host.algo;
@@ -330,6 +364,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     const Plan& P = E.plan;
     if (P.max_children > 32u) throw Error("an action node with more than 32 actions is not supported on the GPU");
     E.wide = P.max_children > 8u;
+    E.staged = engine == kEngineStaged && P.max_children <= (uint32_t)kSKA;
     if (P.nh_max > kThreads * kMaxHpt) throw Error("more than 1536 hands per player is not supported on the GPU");
     CK(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
     size_t& B = E.bytes;
@@ -391,6 +426,19 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     const size_t tsz = E.term64 ? sizeof(double) : sizeof(float);
     E.show_smem = (size_t)d.scr_elems * sizeof(double);
     if (E.warp) E.warp_smem = (size_t)kWarps * d.nh_pad * sizeof(float);
+    if (E.staged) {
+        const int esz = E.fmt == kFmtF32 ? 4 : 2;
+        E.st_up_smem = staged_smem_bytes(d.nh_pad, esz);
+        E.st_down_smem = staged_down_smem_bytes(d.nh_pad, esz);
+        E.st_show_smem = staged_show_smem_bytes(d.nh_pad, d.scr_elems);
+        set_smem((const void*)ks_up<kDevF32, 0>, E.st_up_smem);
+        set_smem((const void*)ks_up<kDevF32, 1>, E.st_up_smem);
+        set_smem((const void*)ks_up<kDevI16, 0>, E.st_up_smem);
+        set_smem((const void*)ks_up<kDevI16, 1>, E.st_up_smem);
+        set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
+        set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
+        set_smem((const void*)ks_showdown, E.st_show_smem);
+    }
     if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
     set_smem((const void*)k_showdown, E.show_smem);
@@ -503,6 +551,7 @@ double GpuEngine::time_iterations(int n) {
     CK(cudaEventElapsedTime(&ms, a, b));
     cudaEventDestroy(a);
     cudaEventDestroy(b);
+    E.check_err();
     return ms;
 }
 
@@ -531,6 +580,7 @@ double GpuEngine::exploitability(const HostSolver& host) {  // best_response.rs:
         CK(cudaGraphLaunch(E.g_eval[mode], E.stream));
         E.reach_valid = false;
         CK(cudaStreamSynchronize(E.stream));
+        E.check_err();
         for (int p = 0; p < 2; p++) (mode == 0 ? br[p] : v[p]) = E.h_dot[p] / denom;
     }
     if (raked) return ((br[0] - v[0]) + (br[1] - v[1])) / 2.0;
@@ -648,6 +698,7 @@ size_t GpuEngine::read_node_static(int which, uint32_t node, float* out, size_t 
 void GpuEngine::sync_to_cpu(HostSolver& host, bool strategy_only) {  // gpu/mod.rs:845-886
     EngineImpl& E = *d_;
     CK(cudaStreamSynchronize(E.stream));
+    E.check_err();
     const Spot& sp = *E.spot;
     const Tree& t = sp.tree;
     for (int p = 0; p < 2; p++) {
@@ -687,7 +738,10 @@ void GpuEngine::sync_to_cpu(HostSolver& host, bool strategy_only) {  // gpu/mod.
     if (E.plan.iso_active) host.sym_dirty = true;
 }
 
-void GpuEngine::synchronize() { CK(cudaStreamSynchronize(d_->stream)); }
+void GpuEngine::synchronize() {
+    CK(cudaStreamSynchronize(d_->stream));
+    d_->check_err();
+}
 void GpuEngine::update_locks(const HostSolver& host) { d_->upload_locks(host); }
 uint32_t GpuEngine::iteration() const { return d_->iteration; }
 int GpuEngine::format() const { return d_->fmt; }

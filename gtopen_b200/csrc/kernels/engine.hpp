@@ -13,7 +13,7 @@ namespace gtob {
 
 enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1 };
 constexpr size_t kNodeScratchElems = 16384;  // 64 KiB of f32: the read_node_static limit
-enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2, kEngineWarp = 3 };
+enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2, kEngineWarp = 3, kEngineStaged = 4 };
 
 struct Profile {
     double ms[7];
@@ -30,7 +30,9 @@ class GpuEngine {
     // f64 terminal sums as the reference CPU engine), kEnginePlain (one launch
     // per terminal level, f64 sums), kEngineFused32 (fused, f32 sums as the
     // reference GPU kernels), kEngineWarp (one warp per action node, fold
-    // children evaluated in place by the warp, showdowns one CTA each; f64).
+    // children evaluated in place by the warp, showdowns one CTA each; f64),
+    // kEngineStaged (one CTA per node staging its blocks and vectors in shared
+    // memory with bulk copies; fold children in place; f64).
     GpuEngine(const HostSolver& host, int fmt, int engine = 0);
     bool fused() const;
     ~GpuEngine();

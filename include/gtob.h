@@ -41,6 +41,10 @@ extern "C" {
                                    regrets may round differently than the CPU engine) */
 #define GTOB_ENGINE_WARP 3      /* one warp per action node with its fold child evaluated
                                    in the warp; showdowns one CTA each; f64 terminal sums */
+#define GTOB_ENGINE_STAGED 4    /* one CTA per node staging its arena blocks and vectors in
+                                   shared memory with bulk copies; fold children in place;
+                                   f64 terminal sums (nodes with more than 4 actions: the
+                                   warp engine's kernels) */
 #define GTOB_ARENA_REGRETS 0
 #define GTOB_ARENA_STRATEGY 1
 #define GTOB_ARENA_PREDICTIONS 2
@@ -149,7 +153,7 @@ int gtob_gpu_new(const gtob_solver* solver, int device_format, gtob_gpu** out);
 /* GpuSolver::new with the engine choice: GTOB_ENGINE_FUSED (terminals
  * evaluated inside their parents' kernels, the default), GTOB_ENGINE_PLAIN
  * (one launch per node kind and level, the reference's kernel split),
- * GTOB_ENGINE_FUSED_F32 or GTOB_ENGINE_WARP. */
+ * GTOB_ENGINE_FUSED_F32, GTOB_ENGINE_WARP or GTOB_ENGINE_STAGED. */
 int gtob_gpu_new_ex(const gtob_solver* solver, int device_format, int engine, gtob_gpu** out);
 void gtob_gpu_free(gtob_gpu* gpu);
 /* GpuSolver::iterate (gpu/mod.rs:304), n times */

@@ -60,7 +60,7 @@ def _compare(spot, osv, host, what):
         assert d <= 1e-4 * scale, "%s: regrets[%d] differ by %g (scale %g)" % (what, p, d, scale)
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp", "staged"])
 @pytest.mark.parametrize("name,cfg_fn,iters", [
     ("clairvoyance", W.clairvoyance_spot, 50),
     ("small_flop", W.small_flop_spot, 20),
@@ -77,7 +77,7 @@ def test_f32_dcfr_matches_oracle(name, cfg_fn, iters, engine):
     assert abs(eo - eg) / pot * 100 < EXPL_TOL_PCT, (eo, eg)
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp", "staged"])
 def test_turn_config_f32_and_i16(engine):
     cfg = W.turn_spot(g.evaluate7)
     for storage in ("f32", "compressed"):
@@ -87,7 +87,7 @@ def test_turn_config_f32_and_i16(engine):
         assert abs(eo - eg) / 100.0 * 100 < EXPL_TOL_PCT, (storage, eo, eg)
 
 
-@pytest.mark.parametrize("engine", ["fused", "warp"])
+@pytest.mark.parametrize("engine", ["fused", "warp", "staged"])
 @pytest.mark.parametrize("algo", ["cfr+", "pcfr+"])
 @pytest.mark.parametrize("storage", ["f32", "compressed"])
 def test_cfrplus_pcfrplus_match_oracle(algo, storage, engine):
@@ -111,7 +111,7 @@ def test_fused32_exploitability_matches_oracle(name, cfg_fn, iters):
     assert abs(osv.exploitability() - gpu.exploitability(host)) / pot * 100 < EXPL_TOL_PCT
 
 
-@pytest.mark.parametrize("engine", ["fused", "warp"])
+@pytest.mark.parametrize("engine", ["fused", "warp", "staged"])
 def test_i16_quants_match_oracle_bitwise_mostly(engine):
     """16-bit arenas: the device requantises exactly like store.rs; decoded values agree."""
     cfg = W.small_flop_spot()
@@ -123,7 +123,7 @@ def test_i16_quants_match_oracle_bitwise_mostly(engine):
             assert frac_equal > 0.999, (which, p, frac_equal)
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp", "staged"])
 def test_iso_matches_oracle(engine):
     cfg = W.iso_spot()
     ospot, osv, spot, host, gpu = _run_pair(cfg, 10, use_iso=True, engine=engine)
@@ -188,7 +188,7 @@ def test_locked_always_call_kills_bluffs():
     assert sig[nh + names.index("8h7h")] < 0.05
 
 
-@pytest.mark.parametrize("engine", ["fused", "plain", "warp"])
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp", "staged"])
 def test_exploitability_with_rake_matches_oracle(engine):
     cfg = W.small_flop_spot()
     cfg["tree"]["rake_pct"] = 0.05
@@ -210,14 +210,14 @@ def test_root_br_cfv_matches_oracle():
 def test_profile_counts_launches():
     spot = g.Spot(W.small_flop_spot())
     host = g.Solver(spot)
-    for engine in ("fused", "plain", "warp"):
+    for engine in ("fused", "plain", "warp", "staged"):
         gpu = g.GpuSolver(host, engine=engine)
         pr = gpu.iterate_profiled()
         assert pr.launches[0] == 2 and sum(pr.launches) > 10
         assert gpu.iteration == 1
         if engine == "fused":
             assert pr.launches[3] == 0 and pr.launches[4] == 0  # terminals evaluated in place
-        if engine == "warp":
+        if engine in ("warp", "staged"):
             assert pr.launches[3] == 0 and pr.launches[4] > 0  # folds in place, showdowns launched
 
 
@@ -229,7 +229,37 @@ def test_allin_runout_spot_matches_oracle():
         st["bet"] = [{"PotPct": 75.0}, "AllIn"]
         st["raise"] = ["AllIn"]
     cfg["tree"]["effective_stack"] = 120.0
-    for engine in ("fused", "plain", "warp"):
+    for engine in ("fused", "plain", "warp", "staged"):
         for storage in ("f32", "compressed"):
             ospot, osv, spot, host, gpu = _run_pair(cfg, 12, storage=storage, engine=engine)
             _compare(spot, osv, host, "runout/%s/%s" % (engine, storage))
+
+
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp", "staged"])
+def test_locks_match_oracle(engine):
+    """query.rs:700-773 locks on the device path: a frozen root and a
+    range-wide lock one step down play their fixed strategies and are never
+    updated; every other node matches the oracle."""
+    cfg = W.small_flop_spot()
+    ospot = po.Spot(cfg)
+    osv = po.Solver(ospot, prune=False, use_iso=False)
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, use_iso=False)
+    osv.iterate(5)
+    g0 = g.GpuSolver(host, engine=engine)
+    g0.iterate(5)
+    g0.sync_to_cpu(host)
+    g0.close()
+    t = spot.tree()
+    child = int(spot.children()[int(t["child_start"][0])])
+    na1 = int(t["nchild"][child])
+    freqs = [0.4] + [0.6 / (na1 - 1)] * (na1 - 1)
+    assert osv.lock_node([], 0) == host.lock_node([], "freeze") == 0
+    assert osv.lock_node([0], 1, freqs=freqs) == host.lock_node([0], "range", freqs=freqs) == child
+    osv.iterate(12)
+    gpu = g.GpuSolver(host, engine=engine)
+    gpu.iterate(12)
+    gpu.sync_to_cpu(host)
+    _compare(spot, osv, host, "locks/" + engine)
+    eo, eg = osv.exploitability(), gpu.exploitability(host)
+    assert abs(eo - eg) / 60.0 * 100 < EXPL_TOL_PCT, (eo, eg)
