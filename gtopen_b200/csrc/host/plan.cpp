@@ -230,6 +230,23 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
     flatten(edge_l, P.edge, P.edge_span);
     flatten(fold_l, P.fold, P.fold_span);
     flatten(show_l, P.show, P.show_span);
+    // showdowns of a level sorted by river slot and cut into batches of at
+    // most kShowBatch with one slot each: a batch's CTA loads the slot's
+    // tables once for all of them
+    for (size_t l = 0; l < P.show_span.size(); l++) {
+        const Span s = P.show_span[l];
+        auto first = P.show.begin() + s.start;
+        std::stable_sort(first, first + s.count, [](const ShowItem& x, const ShowItem& y) { return x.slot < y.slot; });
+        const uint32_t b0 = (uint32_t)P.show_batch.size();
+        for (uint32_t k = 0; k < s.count;) {
+            const uint32_t slot = P.show[s.start + k].slot;
+            uint32_t e = k;
+            while (e < s.count && e - k < (uint32_t)kShowBatch && P.show[s.start + e].slot == slot) e++;
+            P.show_batch.push_back({s.start + k, e - k, slot, 0});
+            k = e;
+        }
+        P.show_batch_span.push_back({b0, (uint32_t)P.show_batch.size() - b0});
+    }
     flatten(chance_l, P.chance, P.chance_span);
 
     // per-hand card lists (fold evaluator: hands of player q holding card c)

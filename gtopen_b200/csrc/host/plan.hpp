@@ -96,6 +96,11 @@ struct RankEntry {
 };
 
 struct Span { uint32_t start, count; };
+constexpr int kShowBatch = 16;  // showdowns of one river slot evaluated by one CTA
+struct ShowBatch {
+    uint32_t start, count;  // a run of Plan::show (one level, one slot)
+    uint32_t slot, pad;
+};
 
 // Which terminal children the parent's up-sweep kernel evaluates in place
 // (no slots, no launches of their own).
@@ -118,6 +123,8 @@ struct Plan {
     std::vector<Span> fold_span;
     std::vector<ShowItem> show;
     std::vector<Span> show_span;
+    std::vector<ShowBatch> show_batch;      // per level, runs of same-slot showdowns
+    std::vector<Span> show_batch_span;
     std::vector<ChanceItem> chance;
     std::vector<Span> chance_span;
     std::vector<CardEntry> cards;

@@ -604,4 +604,181 @@ inline size_t staged_show_smem_bytes(int nh_pad, int scr_elems) {
     return 16 + (size_t)nh_pad * 4 + (size_t)scr_elems * sizeof(double);
 }
 
+// ------------------------------------------------- batched showdowns
+// One CTA per batch of up to kShowBatch showdowns of one level that share a
+// river slot: the slot's tables (opponent strength order, per-card position
+// lists, the traverser's rank entries and blocked hands) and the traverser's
+// same-combo map are loaded into shared memory once; each warp then evaluates
+// its share of the batch's showdowns on its own.
+struct ShowTab {  // shared-memory copies of one slot's tables
+    const uint16_t* sidx;  // m opponent hands, ascending strength
+    const uint32_t* coff;  // 53 card-list offsets relative to the slot's first entry
+    const uint16_t* bpos;  // per-card sorted positions (ne entries)
+    const uint8_t* bcard;  // card of each entry
+    const uint16_t* bins;  // nbins + 1 bin starts
+    const RankEntry* rank;  // mp entries
+    const uint16_t* zero;  // nz blocked traverser hands
+    const uint32_t* same;  // traverser same-combo map (nh entries)
+    int m, nbins, mp, nz;
+};
+struct ShowTabLayout {  // byte offsets of the tables inside the table region
+    unsigned sidx, coff, bpos, bcard, bins, rank, zero, same, total;
+};
+__host__ __device__ inline unsigned r16u(unsigned b) { return (b + 15u) & ~15u; }
+__host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad, int max_bins) {
+    ShowTabLayout L;
+    unsigned o = 0;
+    L.sidx = o;
+    o += r16u(2u * nh_pad);
+    L.coff = o;
+    o += r16u(53u * 4u);
+    L.bpos = o;
+    o += r16u(4u * nh_pad);
+    L.bcard = o;
+    o += r16u(2u * nh_pad);
+    L.bins = o;
+    o += r16u(2u * (max_bins + 1));
+    L.rank = o;
+    o += r16u(16u * nh_pad);
+    L.zero = o;
+    o += r16u(2u * nh_pad);
+    L.same = o;
+    o += r16u(4u * nh_pad);
+    L.total = o;
+    return L;
+}
+
+// Slot tables of a batch into shared memory (all threads of the CTA).
+__device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char* tabs, const ShowTabLayout& TL,
+                              ShowTab& tb) {
+    const int o = 1 - p;
+    tb.m = (int)d.sorted_cnt[o][slot];
+    const uint32_t* coff_g = d.ccard_off[o] + (size_t)slot * 53;
+    const uint32_t c0 = coff_g[0];
+    const uint32_t ne = coff_g[52] - c0;
+    const uint32_t bo = d.bin_off[o][slot];
+    tb.nbins = (int)(d.bin_off[o][slot + 1] - bo) - 1;
+    tb.mp = (int)d.rank_cnt[p][slot];
+    const uint32_t z0 = d.zero_off[p][slot];
+    tb.nz = (int)(d.zero_off[p][slot + 1] - z0);
+    uint16_t* t_sidx = (uint16_t*)(tabs + TL.sidx);
+    uint32_t* t_coff = (uint32_t*)(tabs + TL.coff);
+    uint16_t* t_bpos = (uint16_t*)(tabs + TL.bpos);
+    uint8_t* t_bcard = (uint8_t*)(tabs + TL.bcard);
+    uint16_t* t_bins = (uint16_t*)(tabs + TL.bins);
+    RankEntry* t_rank = (RankEntry*)(tabs + TL.rank);
+    uint16_t* t_zero = (uint16_t*)(tabs + TL.zero);
+    uint32_t* t_same = (uint32_t*)(tabs + TL.same);
+    const uint16_t* g_sidx = d.sorted_idx[o] + d.sorted_off[o][slot];
+    for (int k = threadIdx.x; k < tb.m; k += blockDim.x) t_sidx[k] = g_sidx[k];
+    if (threadIdx.x < 53) t_coff[threadIdx.x] = coff_g[threadIdx.x] - c0;
+    for (uint32_t k = threadIdx.x; k < ne; k += blockDim.x) {
+        t_bpos[k] = d.ccard_pos[o][c0 + k];
+        t_bcard[k] = d.ccard_card[o][c0 + k];
+    }
+    for (int k = threadIdx.x; k <= tb.nbins; k += blockDim.x) t_bins[k] = d.bin_start[o][bo + k];
+    const RankEntry* g_rank = d.rank[p] + d.rank_off[p][slot];
+    for (int k = threadIdx.x; k < tb.mp; k += blockDim.x) t_rank[k] = g_rank[k];
+    for (int k = threadIdx.x; k < tb.nz; k += blockDim.x) t_zero[k] = d.zero_idx[p][z0 + k];
+    for (int k = threadIdx.x; k < d.nh[p]; k += blockDim.x) t_same[k] = d.same[p][k];
+    tb.sidx = t_sidx;
+    tb.coff = t_coff;
+    tb.bpos = t_bpos;
+    tb.bcard = t_bcard;
+    tb.bins = t_bins;
+    tb.rank = t_rank;
+    tb.zero = t_zero;
+    tb.same = t_same;
+}
+
+// One showdown evaluated by one warp (game.rs:501-577 with the rank tables):
+// R = opponent reach in strength order (gathered from HBM), P = its exclusive
+// prefix (lanes scan contiguous chunks, then a shuffle scan of the chunk
+// totals), Q = per-card prefixes (a lane per card, summing the card's list in
+// strength order, as the reference's running card sums do), then one rank
+// entry per lane.  No block barriers: the warp synchronises itself.
+__device__ void warp_showdown(const ShowTab& tb, const float* ro, float win, float lose, float tie, float* out,
+                              float* R, double* P, double* Q, double* S) {
+    const int lane = threadIdx.x & 31;
+    const int m = tb.m;
+    for (int k = lane; k < m; k += 32) R[k] = ro[tb.sidx[k]];
+    __syncwarp();
+    // P: exclusive prefix of R, P[m] = total
+    const int chunk = (m + 31) / 32;
+    const int lo = min(lane * chunk, m), hi = min(lo + chunk, m);
+    double local = 0.0;
+    for (int k = lo; k < hi; k++) local += (double)R[k];
+    double incl = local;
+#pragma unroll
+    for (int x = 1; x < 32; x <<= 1) {
+        const double y = __shfl_up_sync(0xffffffffu, incl, x);
+        if (lane >= x) incl += y;
+    }
+    double run = incl - local;
+    for (int k = lo; k < hi; k++) {
+        P[k] = run;
+        run += (double)R[k];
+    }
+    if (lane == 31) P[m] = incl;
+    // Q: per-card prefixes; Q[coff[c] + c] = 0 and S[c] = the card's total
+    for (int c = lane; c < 52; c += 32) {
+        const uint32_t b = tb.coff[c], e = tb.coff[c + 1];
+        double s = 0.0;
+        Q[b + c] = 0.0;
+        for (uint32_t t = b; t < e; t++) {
+            s += (double)R[tb.bpos[t]];
+            Q[t + c + 1] = s;
+        }
+        S[c] = s;
+    }
+    __syncwarp();
+    const double total = P[m];
+    for (int k = lane; k < tb.mp; k += 32) {
+        const RankEntry e = tb.rank[k];
+        const int a1 = e.cards & 0xFF, a2 = e.cards >> 8;
+        const float lower = (float)(P[e.lb] - Q[e.q1lo] - Q[e.q2lo]);
+        const float higher = (float)((total - P[e.ub]) - (S[a1] - Q[e.q1hi]) - (S[a2] - Q[e.q2hi]));
+        const uint32_t sm = tb.same[e.idx];
+        const float same_r = sm != kSentinel ? ro[sm] : 0.0f;
+        const float valid = (float)(total - S[a1] - S[a2]) + same_r;
+        const float tied = valid - lower - higher;
+        out[e.idx] = win * lower + lose * higher + tie * tied;
+    }
+    for (int z = lane; z < tb.nz; z += 32) out[tb.zero[z]] = 0.0f;
+    __syncwarp();
+}
+// Per-warp scratch of warp_showdown for m <= msort (bytes, 16-aligned).
+__host__ __device__ inline unsigned warp_show_scratch_bytes(int msort) {
+    return r16u(4u * (unsigned)msort) + (3u * (unsigned)msort + 105u) * 8u;
+}
+constexpr int kShowWarps = 4;
+inline size_t show_warp_smem_bytes(int nh_pad, int msort, int max_bins) {
+    return (size_t)show_tab_layout(nh_pad, max_bins).total + (size_t)kShowWarps * warp_show_scratch_bytes(msort);
+}
+
+// A batch (one level, one slot) per CTA of kShowWarps warps: the tables are
+// loaded once, then each warp evaluates every kShowWarps-th showdown.  The
+// opponent reach is read from HBM by the gather itself (one pass, L1-cached).
+__global__ void __launch_bounds__(kShowWarps * 32) ks_show_warp(Dev d, const ShowItem* items, const ShowBatch* batches,
+                                                                 int p, int max_bins, int msort) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    const ShowBatch bt = batches[blockIdx.x];
+    const int o = 1 - p;
+    const ShowTabLayout TL = show_tab_layout(d.nh_pad, max_bins);
+    ShowTab tb;
+    load_show_tab(d, p, bt.slot, sm, TL, tb);
+    __syncthreads();
+    const int w = threadIdx.x >> 5;
+    unsigned char* ws = sm + TL.total + (size_t)w * warp_show_scratch_bytes(msort);
+    float* R = (float*)ws;
+    double* P = (double*)(ws + r16u(4u * (unsigned)msort));
+    double* Q = P + msort + 1;
+    double* S = Q + 2 * msort + 52;
+    for (int j = w; j < (int)bt.count; j += kShowWarps) {
+        const ShowItem s = items[bt.start + j];
+        const float* ro = d.reach[o] + (size_t)s.rs[o] * d.rstr[o];
+        warp_showdown(tb, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, R, P, Q, S);
+    }
+}
+
 }  // namespace gtob

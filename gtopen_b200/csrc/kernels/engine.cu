@@ -87,6 +87,7 @@ struct EngineImpl {
     EdgeItem* edge = nullptr;
     FoldItem* fold = nullptr;
     ShowItem* show = nullptr;
+    ShowBatch* show_batch = nullptr;
     ChanceItem* chance = nullptr;
     XNode* xnodes[2] = {nullptr, nullptr};
     std::vector<XNode> hx[2];
@@ -98,6 +99,7 @@ struct EngineImpl {
     size_t act_smem = 0;     // fused up-action dynamic smem
     size_t warp_smem = 0;    // warp up-action dynamic smem (one staged reach per warp)
     size_t st_up_smem = 0, st_down_smem = 0, st_show_smem = 0;  // staged kernels
+    size_t show_batch_smem = 0;                                   // batched showdowns
     size_t chance_smem = 0;  // runout chance dynamic smem
     cudaGraphExec_t g_iter = nullptr;
     cudaGraphExec_t g_eval[2] = {nullptr, nullptr};
@@ -290,8 +292,13 @@ struct EngineImpl {
             const Span ss = plan.show_span[l];
             if (ss.count)
                 timed(pr, 4, [&] {
-                    if (staged) ks_showdown<<<ss.count, kThreads, st_show_smem, stream>>>(d, show + ss.start, p);
-                    else k_showdown<<<ss.count, kThreads, show_smem, stream>>>(d, show + ss.start, p);
+                    if (staged) {
+                        const Span sb = plan.show_batch_span[l];
+                        ks_show_warp<<<sb.count, kShowWarps * 32, show_batch_smem, stream>>>(
+                            d, show, show_batch + sb.start, p, (int)plan.max_bins, (int)plan.max_sorted);
+                    } else {
+                        k_showdown<<<ss.count, kThreads, show_smem, stream>>>(d, show + ss.start, p);
+                    }
                 });
             const Span sc = plan.chance_span[l];
             if (sc.count) timed(pr, 5, [&] { launch_chance(sc, p); });
@@ -422,6 +429,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     E.edge = dupload(P.edge, O, &B);
     E.fold = dupload(P.fold, O, &B);
     E.show = dupload(P.show, O, &B);
+    E.show_batch = dupload(P.show_batch, O, &B);
     E.chance = dupload(P.chance, O, &B);
     const size_t tsz = E.term64 ? sizeof(double) : sizeof(float);
     E.show_smem = (size_t)d.scr_elems * sizeof(double);
@@ -438,6 +446,8 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
         set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
         set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
         set_smem((const void*)ks_showdown, E.st_show_smem);
+        E.show_batch_smem = show_warp_smem_bytes(d.nh_pad, (int)P.max_sorted, (int)P.max_bins);
+        set_smem((const void*)ks_show_warp, E.show_batch_smem);
     }
     if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
