@@ -255,23 +255,20 @@ __device__ __forceinline__ float s_block_max(float v, float* sh) {
 }
 
 // Fold summary of a staged opponent reach vector (game.rs:478-485): total
-// and per-card sums in f64.  Each warp owns cards w, w + 4, ...; lanes split
-// a card's list (<= 51 hands) into two 32-lane chunks.
+// and per-card sums in f64.  Threads 0..51 each sum one card's hand list in
+// hand order (the reference's order); the total is a fixed-tree block sum.
 __device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, double* s_red) {
     const int nho = d.nh[o];
     double t = 0.0;
     for (int j = threadIdx.x; j < nho; j += kSThreads) t += (double)ro[j];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int c = warp; c < 52; c += kSWarps) {
+    if (threadIdx.x < 52) {
+        const int c = threadIdx.x;
         const uint32_t b = d.hcard_off[o][c], e = d.hcard_off[o][c + 1];
+        const uint16_t* idx = d.hcard_idx[o];
         double s = 0.0;
-#pragma unroll
-        for (int h = 0; h < 2; h++) {
-            const uint32_t k = b + lane + 32 * h;
-            s += k < e ? (double)ro[d.hcard_idx[o][k]] : 0.0;
-        }
-        s = warp_sum(s);
-        if (lane == 0) S[c] = s;
+        for (uint32_t k = b; k < e; k++) s += (double)ro[idx[k]];
+        S[c] = s;
     }
     t = warp_sum(t);
     if (lane == 0) s_red[warp] = t;
@@ -441,10 +438,13 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
             __syncthreads();
         }
         ftotal = s_fold_sums(d, o, ro, s_S, s_dred);
+        // the fold child's values go where a staged child's cfv would be
+        for (int i = threadIdx.x; i < nh; i += kSThreads)
+            cv[fk * vstride + i] = fold_value(d, p, i, ro, ftotal, s_S, famount);
         __syncthreads();
     }
     float* out = d.cfv + (size_t)it.cslot * d.nh_max;
-#define CHILD_V(k, i) ((k) == fk ? fold_value(d, p, (i), ro, ftotal, s_S, famount) : cv[(k) * vstride + (i)])
+#define CHILD_V(k, i) (cv[(k) * vstride + (i)])
     if (!mine) {  // opponent node: sum of children
         for (int i = threadIdx.x; i < nh; i += kSThreads) {
             float acc = 0.0f;
@@ -608,8 +608,8 @@ inline size_t staged_show_smem_bytes(int nh_pad, int scr_elems) {
 // One CTA per batch of up to kShowBatch showdowns of one level that share a
 // river slot: the slot's tables (opponent strength order, per-card position
 // lists, the traverser's rank entries and blocked hands) and the traverser's
-// same-combo map are loaded into shared memory once; each warp then evaluates
-// its share of the batch's showdowns on its own.
+// same-combo map are loaded into shared memory once, and the showdowns'
+// opponent reach vectors stream through two bulk-copy buffers.
 struct ShowTab {  // shared-memory copies of one slot's tables
     const uint16_t* sidx;  // m opponent hands, ascending strength
     const uint32_t* coff;  // 53 card-list offsets relative to the slot's first entry
@@ -691,21 +691,23 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
     tb.same = t_same;
 }
 
-// One showdown evaluated by one warp (game.rs:501-577 with the rank tables):
-// R = opponent reach in strength order (gathered from HBM), P = its exclusive
-// prefix (lanes scan contiguous chunks, then a shuffle scan of the chunk
-// totals), Q = per-card prefixes (a lane per card, summing the card's list in
-// strength order, as the reference's running card sums do), then one rank
-// entry per lane.  No block barriers: the warp synchronises itself.
-__device__ void warp_showdown(const ShowTab& tb, const float* ro, float win, float lose, float tie, float* out,
-                              float* R, double* P, double* Q, double* S) {
-    const int lane = threadIdx.x & 31;
+constexpr int kShowThreads = 128;
+constexpr int kShowCtaWarps = kShowThreads / 32;
+
+// One showdown evaluated by the CTA (game.rs:501-577 with the rank tables):
+// R = opponent reach in strength order, P = its exclusive prefix (each
+// thread sums a contiguous chunk, then a two-level shuffle scan), Q = per-card
+// prefixes (threads 0..51 each run one card's list in strength order, as the
+// reference's running card sums do), then the rank entries.
+__device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, float lose, float tie, float* out,
+                             float* R, double* P, double* Q, double* S, double* s_w) {
     const int m = tb.m;
-    for (int k = lane; k < m; k += 32) R[k] = ro[tb.sidx[k]];
-    __syncwarp();
-    // P: exclusive prefix of R, P[m] = total
-    const int chunk = (m + 31) / 32;
-    const int lo = min(lane * chunk, m), hi = min(lo + chunk, m);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < m; k += kShowThreads) R[k] = ro[tb.sidx[k]];
+    __syncthreads();
+    // P
+    const int chunk = (m + kShowThreads - 1) / kShowThreads;
+    const int lo = min((int)threadIdx.x * chunk, m), hi = min(lo + chunk, m);
     double local = 0.0;
     for (int k = lo; k < hi; k++) local += (double)R[k];
     double incl = local;
@@ -714,26 +716,33 @@ __device__ void warp_showdown(const ShowTab& tb, const float* ro, float win, flo
         const double y = __shfl_up_sync(0xffffffffu, incl, x);
         if (lane >= x) incl += y;
     }
-    double run = incl - local;
+    if (lane == 31) s_w[warp] = incl;
+    // Q (threads 0..51), independent of P
+    if (threadIdx.x < 52) {
+        const int c = threadIdx.x;
+        const uint32_t b = tb.coff[c], e = tb.coff[c + 1];
+        double q = 0.0;
+        Q[b + c] = 0.0;
+        for (uint32_t t = b; t < e; t++) {
+            q += (double)R[tb.bpos[t]];
+            Q[t + c + 1] = q;
+        }
+        S[c] = q;
+    }
+    __syncthreads();
+    double wbase = 0.0;
+#pragma unroll
+    for (int k = 0; k < kShowCtaWarps; k++)
+        if (k < warp) wbase += s_w[k];
+    double run = wbase + (incl - local);
     for (int k = lo; k < hi; k++) {
         P[k] = run;
         run += (double)R[k];
     }
-    if (lane == 31) P[m] = incl;
-    // Q: per-card prefixes; Q[coff[c] + c] = 0 and S[c] = the card's total
-    for (int c = lane; c < 52; c += 32) {
-        const uint32_t b = tb.coff[c], e = tb.coff[c + 1];
-        double s = 0.0;
-        Q[b + c] = 0.0;
-        for (uint32_t t = b; t < e; t++) {
-            s += (double)R[tb.bpos[t]];
-            Q[t + c + 1] = s;
-        }
-        S[c] = s;
-    }
-    __syncwarp();
+    if (threadIdx.x == kShowThreads - 1) P[m] = run;
+    __syncthreads();
     const double total = P[m];
-    for (int k = lane; k < tb.mp; k += 32) {
+    for (int k = threadIdx.x; k < tb.mp; k += kShowThreads) {
         const RankEntry e = tb.rank[k];
         const int a1 = e.cards & 0xFF, a2 = e.cards >> 8;
         const float lower = (float)(P[e.lb] - Q[e.q1lo] - Q[e.q2lo]);
@@ -744,40 +753,83 @@ __device__ void warp_showdown(const ShowTab& tb, const float* ro, float win, flo
         const float tied = valid - lower - higher;
         out[e.idx] = win * lower + lose * higher + tie * tied;
     }
-    for (int z = lane; z < tb.nz; z += 32) out[tb.zero[z]] = 0.0f;
-    __syncwarp();
+    for (int z = threadIdx.x; z < tb.nz; z += kShowThreads) out[tb.zero[z]] = 0.0f;
+    __syncthreads();
 }
-// Per-warp scratch of warp_showdown for m <= msort (bytes, 16-aligned).
-__host__ __device__ inline unsigned warp_show_scratch_bytes(int msort) {
-    return r16u(4u * (unsigned)msort) + (3u * (unsigned)msort + 105u) * 8u;
+// Shared memory of ks_show_cta: two barriers, two reach buffers, R (floats),
+// P/Q/S (doubles), then the slot tables.
+__host__ __device__ inline unsigned show_cta_scratch_bytes(int nh_pad, int msort) {
+    return 32u + 2u * 4u * (unsigned)nh_pad + r16u(4u * (unsigned)msort) + r16u((3u * (unsigned)msort + 105u) * 8u);
 }
-constexpr int kShowWarps = 4;
-inline size_t show_warp_smem_bytes(int nh_pad, int msort, int max_bins) {
-    return (size_t)show_tab_layout(nh_pad, max_bins).total + (size_t)kShowWarps * warp_show_scratch_bytes(msort);
+inline size_t show_cta_smem_bytes(int nh_pad, int msort, int max_bins) {
+    return (size_t)show_cta_scratch_bytes(nh_pad, msort) + show_tab_layout(nh_pad, max_bins).total;
 }
 
-// A batch (one level, one slot) per CTA of kShowWarps warps: the tables are
-// loaded once, then each warp evaluates every kShowWarps-th showdown.  The
-// opponent reach is read from HBM by the gather itself (one pass, L1-cached).
-__global__ void __launch_bounds__(kShowWarps * 32) ks_show_warp(Dev d, const ShowItem* items, const ShowBatch* batches,
-                                                                 int p, int max_bins, int msort) {
+// A batch (one level, one slot) per CTA: tables loaded once; the batch's
+// opponent reach vectors stream through two bulk-copy buffers, the next one
+// landing while the current one is evaluated.
+__global__ void __launch_bounds__(kShowThreads) ks_show_cta(Dev d, const ShowItem* items, const ShowBatch* batches,
+                                                            int p, int max_bins, int msort) {
     extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ double s_w[kShowCtaWarps];
+    __shared__ int s_flag;
+    __shared__ ShowItem s_it[kShowBatch];
     const ShowBatch bt = batches[blockIdx.x];
     const int o = 1 - p;
-    const ShowTabLayout TL = show_tab_layout(d.nh_pad, max_bins);
-    ShowTab tb;
-    load_show_tab(d, p, bt.slot, sm, TL, tb);
-    __syncthreads();
-    const int w = threadIdx.x >> 5;
-    unsigned char* ws = sm + TL.total + (size_t)w * warp_show_scratch_bytes(msort);
-    float* R = (float*)ws;
-    double* P = (double*)(ws + r16u(4u * (unsigned)msort));
+    const int n = (int)bt.count;
+    uint64_t* bars = (uint64_t*)sm;
+    float* rbuf = (float*)(sm + 32);
+    float* R = rbuf + 2 * d.nh_pad;
+    double* P = (double*)((unsigned char*)R + r16u(4u * (unsigned)msort));
     double* Q = P + msort + 1;
     double* S = Q + 2 * msort + 52;
-    for (int j = w; j < (int)bt.count; j += kShowWarps) {
-        const ShowItem s = items[bt.start + j];
-        const float* ro = d.reach[o] + (size_t)s.rs[o] * d.rstr[o];
-        warp_showdown(tb, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, R, P, Q, S);
+    unsigned char* tabs = sm + show_cta_scratch_bytes(d.nh_pad, msort);
+    const ShowTabLayout TL = show_tab_layout(d.nh_pad, max_bins);
+    if (threadIdx.x < n) s_it[threadIdx.x] = items[bt.start + threadIdx.x];
+    ShowTab tb;
+    load_show_tab(d, p, bt.slot, tabs, TL, tb);
+    const unsigned rbytes = round16((unsigned)d.nh[o] * 4u);
+    if (threadIdx.x == 0) {
+        s_flag = 0;
+        mbar_init(&bars[0], 1);
+        mbar_init(&bars[1], 1);
+    }
+    __syncthreads();  // items, tables and barriers visible
+    auto issue = [&](int j) {  // thread 0: item j's reach into buffer j & 1
+        float* dst = rbuf + (size_t)(j & 1) * d.nh_pad;
+        const float* src = d.reach[o] + (size_t)s_it[j].rs[o] * d.rstr[o];
+        if ((((uintptr_t)dst | (uintptr_t)src) & 15u) != 0) {
+            s_flag = 1;
+            atomicOr(d.err, 2u);
+            mbar_expect_tx(&bars[j & 1], 0);  // completes the phase with nothing in flight
+            return;
+        }
+        mbar_expect_tx(&bars[j & 1], rbytes);
+        bulk_load(dst, src, rbytes, &bars[j & 1]);
+    };
+    if (threadIdx.x == 0) {
+        issue(0);
+        if (n > 1) issue(1);
+    }
+    for (int j = 0; j < n; j++) {
+        const bool ok = mbar_wait(&bars[j & 1], (unsigned)(j >> 1) & 1u);
+        if (__syncthreads_or(!ok) || s_flag) {
+            if (threadIdx.x == 0) {
+                if (!ok) atomicOr(d.err, 1u);
+                // bounded drain of the copies still in flight (this one and the next)
+                mbar_wait(&bars[j & 1], (unsigned)(j >> 1) & 1u);
+                if (j + 1 < n) mbar_wait(&bars[(j + 1) & 1], (unsigned)((j + 1) >> 1) & 1u);
+            }
+            return;
+        }
+        const ShowItem& s = s_it[j];
+        const float* ro = rbuf + (size_t)(j & 1) * d.nh_pad;
+        cta_showdown(tb, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, R, P, Q, S, s_w);
+        // buffer j & 1 is free (the evaluation ends with a barrier): order its
+        // generic reads before the next bulk write into it, then refill it
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (threadIdx.x == 0 && j + 2 < n) issue(j + 2);
     }
 }
 

@@ -294,7 +294,7 @@ struct EngineImpl {
                 timed(pr, 4, [&] {
                     if (staged) {
                         const Span sb = plan.show_batch_span[l];
-                        ks_show_warp<<<sb.count, kShowWarps * 32, show_batch_smem, stream>>>(
+                        ks_show_cta<<<sb.count, kShowThreads, show_batch_smem, stream>>>(
                             d, show, show_batch + sb.start, p, (int)plan.max_bins, (int)plan.max_sorted);
                     } else {
                         k_showdown<<<ss.count, kThreads, show_smem, stream>>>(d, show + ss.start, p);
@@ -446,8 +446,8 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
         set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
         set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
         set_smem((const void*)ks_showdown, E.st_show_smem);
-        E.show_batch_smem = show_warp_smem_bytes(d.nh_pad, (int)P.max_sorted, (int)P.max_bins);
-        set_smem((const void*)ks_show_warp, E.show_batch_smem);
+        E.show_batch_smem = show_cta_smem_bytes(d.nh_pad, (int)P.max_sorted, (int)P.max_bins);
+        set_smem((const void*)ks_show_cta, E.show_batch_smem);
     }
     if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
