@@ -321,7 +321,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="flop", choices=["flop", "turn", "river", "bench_spot"])
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32"])
-    ap.add_argument("--engine", default="fused", choices=["fused", "plain", "warp", "fused32", "staged"])
+    ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=1)

@@ -340,13 +340,13 @@ class Solver:
 class GpuSolver:
     """gpu/mod.rs GpuSolver: device buffers, CUDA-graph iterations, BR checks, syncs."""
 
-    def __init__(self, solver, device_format=None, engine="fused"):
-        """engine: "fused" (terminals evaluated inside their parents' kernels,
-        f64 terminal sums), "plain" (one launch per node kind and level, f64
-        terminal sums), "fused32" (fused, f32 terminal sums), "warp" (one
-        warp per action node, fold children evaluated by that warp) or
-        "staged" (one CTA per node, its data staged in shared memory by bulk
-        copies)."""
+    def __init__(self, solver, device_format=None, engine="staged"):
+        """engine: "staged" (default: one CTA per node, its data staged in
+        shared memory by bulk copies; showdowns batched by river board),
+        "fused" (terminals evaluated inside their parents' kernels, f64
+        terminal sums), "plain" (one launch per node kind and level, f64
+        terminal sums), "fused32" (fused, f32 terminal sums) or "warp" (one
+        warp per action node, fold children evaluated by that warp)."""
         h = C.c_void_p()
         eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}[engine]
         _check(lib().gtob_gpu_new_ex(solver._h, DEVICE_FORMAT[device_format], eng, C.byref(h)))

@@ -266,7 +266,7 @@ int gtob_load(const char* path, int storage, gtob_solver** out) {
     API_END
 }
 
-int gtob_gpu_new(const gtob_solver* v, int fmt, gtob_gpu** out) { return gtob_gpu_new_ex(v, fmt, GTOB_ENGINE_FUSED, out); }
+int gtob_gpu_new(const gtob_solver* v, int fmt, gtob_gpu** out) { return gtob_gpu_new_ex(v, fmt, GTOB_ENGINE_STAGED, out); }
 int gtob_gpu_new_ex(const gtob_solver* v, int fmt, int engine, gtob_gpu** out) {
     REQUIRE(v && out && fmt >= -1 && fmt <= 1 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
     *out = nullptr;

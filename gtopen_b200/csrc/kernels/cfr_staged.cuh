@@ -414,15 +414,16 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
         for (int k = 0; k < kSKA; k++)
             if (k < na && k != fk) cl.add(cv + k * vstride, d.cfv + (size_t)cs[k] * d.nh_max, round16((unsigned)nh * 4u));
     }
-    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
-
-    float sig[kSKA];
-    // scales of the actor's node (16-bit arenas)
-    float kr = 0.0f, kp = 0.0f;
+    // scales of the actor's node (16-bit arenas), loaded while the copies fly
+    float kr = 0.0f, kp = 0.0f, sscale = 0.0f;
     if (FMT != kDevF32 && loff < 0) {
         kr = ar.rscale[a][it.sidx] / 32767.0f;
         if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
+        if (mine) sscale = ar.sscale[a][it.sidx];
     }
+    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
+
+    float sig[kSKA];
     double ftotal = 0.0;
     if (fk >= 0) {
         if (a == o) {  // the opponent folds with probability sigma_o[fk]
@@ -521,15 +522,65 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
         if (use_pred) store_block((unsigned char*)ar.pred[p] + it.aoff * esz, b_pred, blk);
         return;
     }
-    // 16-bit arenas (cfr.rs:350-407): pass 1 finds the node's new maxima,
-    // pass 2 recomputes from the (unchanged) staged quants and requantises in
-    // place; the blocks then go back to HBM.
+    // 16-bit arenas (cfr.rs:350-407).
     int16_t* RQ = (int16_t*)b_reg;
     uint16_t* SQ = (uint16_t*)b_str;
     int16_t* PQ = (int16_t*)b_pred;
-    const float kss = ar.sscale[p][it.sidx] / 65535.0f * ds;
+    const float kss = sscale / 65535.0f * ds;
     float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
-    for (int pass = 0; pass < 2; pass++) {
+    if (!use_pred) {
+        // Pass 1 computes every entry's new regret and strategy sum and the
+        // node's maxima, keeping the f32 values in place of what it consumed:
+        // the new regret where the child's value was, the new strategy sum's
+        // bits split over the entry's two old 16-bit quants (each entry is
+        // read and rewritten by the thread that owns its hand).  Pass 2 only
+        // requantises.
+        uint16_t* SQ_lo = (uint16_t*)b_reg;
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            s_regret_sigma<FMT>(b_reg, nullptr, kr, kp, na, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float r_p = rp[i];
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const int16_t qv = RQ[b + k];
+                    const float nr = (float)qv * kr * (qv > 0 ? pos : neg) + (v[k] - o_);
+                    const float ns = (float)SQ[b + k] * kss + r_p * sig[k];
+                    rmax = fmaxf(rmax, fabsf(nr));
+                    smax = fmaxf(smax, ns);
+                    cv[k * vstride + i] = nr;
+                    const uint32_t bits = __float_as_uint(ns);
+                    SQ_lo[b + k] = (uint16_t)(bits & 0xFFFFu);
+                    SQ[b + k] = (uint16_t)(bits >> 16);
+                }
+            out[i] = o_;
+        }
+        rmax = s_block_max(rmax, s_red);
+        smax = s_block_max(smax, s_red + kSWarps);
+        const float rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
+        const float sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const float nr = cv[k * vstride + i];
+                    const float ns = __uint_as_float((uint32_t)SQ_lo[b + k] | ((uint32_t)SQ[b + k] << 16));
+                    RQ[b + k] = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
+                    SQ[b + k] = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
+                }
+        }
+    }
+    // PCFR+ (predictions too): pass 1 finds the maxima, pass 2 recomputes
+    // from the unchanged staged quants and requantises in place.
+    for (int pass = use_pred ? 0 : 2; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
         if (pass == 1) {
             rmax = s_block_max(rmax, s_red);
@@ -723,7 +774,18 @@ __device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, floa
         const uint32_t b = tb.coff[c], e = tb.coff[c + 1];
         double q = 0.0;
         Q[b + c] = 0.0;
-        for (uint32_t t = b; t < e; t++) {
+        uint32_t t = b;
+        for (; t + 4 <= e; t += 4) {  // loads first, then the running sum in order
+            float r[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) r[u] = R[tb.bpos[t + u]];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                q += (double)r[u];
+                Q[t + u + c + 1] = q;
+            }
+        }
+        for (; t < e; t++) {
             q += (double)R[tb.bpos[t]];
             Q[t + c + 1] = q;
         }

@@ -148,12 +148,12 @@ int gtob_load(const char* path, int storage, gtob_solver** out);
 /* Device for later gtob_gpu_new calls on this thread (the reference always
  * opens device 0, gpu/mod.rs:152; one process per GPU sets its own). */
 int gtob_set_device(int device);
-/* GpuSolver::new (gpu/mod.rs:146); device_format GTOB_DEVICE_* */
+/* GpuSolver::new (gpu/mod.rs:146) with the staged engine; device_format GTOB_DEVICE_* */
 int gtob_gpu_new(const gtob_solver* solver, int device_format, gtob_gpu** out);
-/* GpuSolver::new with the engine choice: GTOB_ENGINE_FUSED (terminals
- * evaluated inside their parents' kernels, the default), GTOB_ENGINE_PLAIN
- * (one launch per node kind and level, the reference's kernel split),
- * GTOB_ENGINE_FUSED_F32, GTOB_ENGINE_WARP or GTOB_ENGINE_STAGED. */
+/* GpuSolver::new with the engine choice: GTOB_ENGINE_STAGED (the default of
+ * gtob_gpu_new), GTOB_ENGINE_FUSED (terminals evaluated inside their parents'
+ * kernels), GTOB_ENGINE_PLAIN (one launch per node kind and level, the
+ * reference's kernel split), GTOB_ENGINE_FUSED_F32 or GTOB_ENGINE_WARP. */
 int gtob_gpu_new_ex(const gtob_solver* solver, int device_format, int engine, gtob_gpu** out);
 void gtob_gpu_free(gtob_gpu* gpu);
 /* GpuSolver::iterate (gpu/mod.rs:304), n times */
