@@ -238,11 +238,18 @@ def run_ours(args, world, rank, local):
         barrier(world)
         t = time.perf_counter()
         gpu2 = g.GpuSolver(host, engine=args.engine)
+        t_new = time.perf_counter()
         gpu2.iterate(args.steps)
+        gpu2.synchronize()
+        t_it = time.perf_counter()
         e = gpu2.exploitability(host)
+        t_ex = time.perf_counter()
         gpu2.sync_to_cpu(host)
         gpu2.synchronize()
-        dt = time.perf_counter() - t
+        t_end = time.perf_counter()
+        dt = t_end - t
+        split = {"new_s": t_new - t, "iterate_s": t_it - t_new, "exploitability_s": t_ex - t_it,
+                 "sync_to_cpu_s": t_end - t_ex}
         dt_max = allmax(dt, world)
         b = 2 if args.storage != "f32" else 4
         arena_bytes = 2 * (spot.data_size[0] + spot.data_size[1]) * b
@@ -250,6 +257,7 @@ def run_ours(args, world, rank, local):
                "h2d_bytes_per_step": int(arena_bytes / args.steps),
                "d2h_bytes_per_step": int((arena_bytes + 16) / args.steps),
                "includes": "GpuSolver::new upload, %d iterations, 1 exploitability check, sync_to_cpu" % args.steps,
+               "split": {k: round(v, 3) for k, v in split.items()},
                "exploitability_pct_pot": e / cfg["tree"]["starting_pot"] * 100}
         gpu2.close()
 

@@ -63,6 +63,9 @@ struct Dev {
     unsigned* iter;
     double* dot;  // root dot products
     unsigned* err;  // device error bits (bounded waits that gave up, bad copies)
+    // staged engine extras
+    const uint32_t* hinfo[2];   // per hand: c1 | c2 << 6 | same << 16 (0xFFFF: no same combo)
+    const uint16_t* hcard52[2]; // per card: the hands holding it, 52 slots, 0xFFFF after the last
 };
 struct Arenas {
     void* reg[2];

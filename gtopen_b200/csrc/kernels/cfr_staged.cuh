@@ -25,6 +25,19 @@ constexpr int kSWarps = kSThreads / 32;
 constexpr int kSKA = 4;                                // staged kernels take nodes with at most 4 actions
 constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s
 
+// One action node as the staged kernels read it: everything its copies need
+// in one 80-byte record (one load round trip per node).
+struct SNode {
+    uint64_t aoff;             // arena offset (elements) in the actor's arena
+    uint32_t cslot, rslot, oslot, sidx;
+    uint32_t cs[kSKA];         // child cfv slots (kNoSlot: the fold child)
+    uint32_t rs[kSKA];         // child reach slots of the actor (down sweep; kNoSlot: none)
+    uint32_t actor, na, fk;    // fk: the fold child's index, kNoSlot if none
+    uint32_t folder;           // the folding player of the fold child
+    float twin, tlose;         // fold payoffs
+};
+static_assert(sizeof(SNode) == 80, "SNode layout");
+
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
     unsigned long long t;
@@ -63,43 +76,13 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, unsigned b
                  : "memory");
 }
 
-// Up to 12 copies per node, described by thread 0 and issued together.
-struct CopyList {
-    int n = 0;
-    unsigned total = 0;
-    bool bad = false;
-    void* dst[12];
-    const void* src[12];
-    unsigned bytes[12];
-    __device__ void add(void* d, const void* s, unsigned b) {
-        if (b == 0) return;
-        if ((((uintptr_t)d | (uintptr_t)s | (uintptr_t)b) & 15u) != 0 || n == 12) {
-            bad = true;
-            return;
-        }
-        dst[n] = d;
-        src[n] = s;
-        bytes[n] = b;
-        total += b;
-        n++;
-    }
-};
 __device__ __forceinline__ unsigned round16(unsigned b) { return (b + 15u) & ~15u; }
 
-// Every thread of the CTA calls this once; thread 0 (which initialised bar and
-// filled cl) issues the copies, then all wait.  Returns false, after the
-// error handling described at the top, when the CTA must end.
-__device__ bool stage_and_wait(const Dev& d, uint64_t* bar, const CopyList& cl, int* s_flag) {
-    if (threadIdx.x == 0) {
-        *s_flag = 0;
-        if (cl.bad) {
-            *s_flag = 1;
-            atomicOr(d.err, 2u);
-        } else {
-            mbar_expect_tx(bar, cl.total);
-            for (int k = 0; k < cl.n; k++) bulk_load(cl.dst[k], cl.src[k], cl.bytes[k], bar);
-        }
-    }
+// After thread 0 initialised bar and issued the CTA's copies on it (setting
+// *s_flag to 1 instead when it refused one as misaligned), every thread
+// waits.  Returns false, after the error handling described at the top, when
+// the CTA must end.
+__device__ bool wait_staged(const Dev& d, uint64_t* bar, int* s_flag) {
     __syncthreads();
     if (*s_flag) return false;
     const bool ok = mbar_wait(bar, 0);
@@ -264,10 +247,17 @@ __device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, d
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (threadIdx.x < 52) {
         const int c = threadIdx.x;
-        const uint32_t b = d.hcard_off[o][c], e = d.hcard_off[o][c + 1];
-        const uint16_t* idx = d.hcard_idx[o];
+        const uint16_t* idx = d.hcard52[o] + c * 52;
         double s = 0.0;
-        for (uint32_t k = b; k < e; k++) s += (double)ro[idx[k]];
+        for (int k = 0; k < 52; k += 4) {  // index loads first, then the sum in hand order
+            uint16_t x[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) x[u] = idx[k + u];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+                if (x[u] != 0xFFFFu) s += (double)ro[x[u]];
+            if (x[3] == 0xFFFFu) break;
+        }
         S[c] = s;
     }
     t = warp_sum(t);
@@ -279,39 +269,41 @@ __device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, d
     return total;
 }
 
-// Shared-memory layout of the staged action kernels (bytes).
+// Shared-memory layout of the staged action kernels (bytes): the regret,
+// strategy-sum and (PCFR+ only) prediction blocks, the opponent and own
+// reach vectors, then kSKA child value vectors.
 struct SLayout {
-    unsigned cap, vec;  // arena block capacity; one hand vector (nh_pad floats)
-    __device__ SLayout(const Dev& d, int esz)
-        : cap(round16((unsigned)(kSKA * d.nh_pad * esz))), vec((unsigned)d.nh_pad * 4u) {}
+    unsigned cap, vec, nblk;  // arena block capacity; one hand vector; blocks staged
+    __device__ SLayout(const Dev& d, int esz, bool pred)
+        : cap(round16((unsigned)(kSKA * d.nh_pad * esz))), vec((unsigned)d.nh_pad * 4u), nblk(pred ? 3u : 2u) {}
     __device__ unsigned reg() const { return 16; }
     __device__ unsigned str() const { return 16 + cap; }
     __device__ unsigned pred() const { return 16 + 2 * cap; }
-    __device__ unsigned ro() const { return 16 + 3 * cap; }
-    __device__ unsigned rp() const { return 16 + 3 * cap + vec; }
-    __device__ unsigned cv() const { return 16 + 3 * cap + 2 * vec; }
+    __device__ unsigned ro() const { return 16 + nblk * cap; }
+    __device__ unsigned rp() const { return 16 + nblk * cap + vec; }
+    __device__ unsigned cv() const { return 16 + nblk * cap + 2 * vec; }
 };
 // Host twins of SLayout's extent: the up kernel uses every region, the down
 // kernel the blocks and one reach vector.
-inline size_t staged_smem_bytes(int nh_pad, int esz) {
+inline size_t staged_smem_bytes(int nh_pad, int esz, bool pred) {
     const size_t cap = ((size_t)kSKA * nh_pad * esz + 15) & ~(size_t)15;
-    return 16 + 3 * cap + (2 + kSKA) * (size_t)nh_pad * 4;
+    return 16 + (pred ? 3 : 2) * cap + (2 + kSKA) * (size_t)nh_pad * 4;
 }
-inline size_t staged_down_smem_bytes(int nh_pad, int esz) {
+inline size_t staged_down_smem_bytes(int nh_pad, int esz, bool pred) {
     const size_t cap = ((size_t)kSKA * nh_pad * esz + 15) & ~(size_t)15;
-    return 16 + 3 * cap + (size_t)nh_pad * 4;
+    return 16 + (pred ? 3 : 2) * cap + (size_t)nh_pad * 4;
 }
 
 // Down sweep, one node per CTA: staged sigma source and parent reach; child
 // reach vectors written with coalesced stores (cfr.rs:469-531 push-down).
 template <int FMT>
-__global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const ActItem* items, int mode) {
+__global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const SNode* nodes, int mode) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ int s_flag;
-    const ActItem it = items[blockIdx.x];
+    const SNode it = nodes[blockIdx.x];
     const int a = (int)it.actor, na = (int)it.na, nh = d.nh[a];
     const int esz = FMT == kDevF32 ? 4 : 2;
-    const SLayout L(d, esz);
+    const SLayout L(d, esz, ar.pred[0] != nullptr);
     uint64_t* bar = (uint64_t*)sm;
     unsigned char* b_reg = sm + L.reg();
     unsigned char* b_str = sm + L.str();
@@ -320,35 +312,38 @@ __global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const Act
     const long long loff = d.lock_off[a][it.sidx];
     const bool has_pred = ar.pred[a] != nullptr;
     const unsigned blk = round16((unsigned)(na * nh * esz));
-    CopyList cl;  // filled and issued by thread 0 only
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
-        if (loff < 0) {
-            if (mode == 0) {
-                cl.add(b_reg, (const unsigned char*)ar.reg[a] + it.aoff * esz, blk);
-                if (has_pred) cl.add(b_pred, (const unsigned char*)ar.pred[a] + it.aoff * esz, blk);
-            } else {
-                cl.add(b_str, (const unsigned char*)ar.str[a] + it.aoff * esz, blk);
-            }
+        const bool u_reg = loff < 0 && mode == 0, u_pred = u_reg && has_pred, u_str = loff < 0 && mode != 0;
+        const unsigned char* g_reg = (const unsigned char*)ar.reg[a] + it.aoff * esz;
+        const unsigned char* g_str = (const unsigned char*)ar.str[a] + it.aoff * esz;
+        const unsigned char* g_pred = u_pred ? (const unsigned char*)ar.pred[a] + it.aoff * esz : nullptr;
+        const float* g_pr = d.reach[a] + (size_t)it.rslot * d.rstr[a];
+        const unsigned vb = round16((unsigned)nh * 4u);
+        s_flag = ((uintptr_t)g_reg | (uintptr_t)g_str | (uintptr_t)g_pred | (uintptr_t)g_pr) & 15u ? 1 : 0;
+        if (s_flag) {
+            atomicOr(d.err, 2u);
+        } else {
+            mbar_expect_tx(bar, (u_reg ? blk : 0u) + (u_pred ? blk : 0u) + (u_str ? blk : 0u) + vb);
+            if (u_reg) bulk_load(b_reg, g_reg, blk, bar);
+            if (u_pred) bulk_load(b_pred, g_pred, blk, bar);
+            if (u_str) bulk_load(b_str, g_str, blk, bar);
+            bulk_load(pr, g_pr, vb, bar);
         }
-        cl.add(pr, d.reach[a] + (size_t)it.rslot * d.rstr[a], round16((unsigned)nh * 4u));
     }
-    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
-    uint32_t rs[kSKA];
-#pragma unroll
-    for (int k = 0; k < kSKA; k++) rs[k] = k < na ? d.crefs[it.cref + k].rslot : kNoSlot;
     float kr = 0.0f, kp = 0.0f;
     if (FMT != kDevF32 && mode == 0 && loff < 0) {
         kr = ar.rscale[a][it.sidx] / 32767.0f;
         if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
     }
+    if (!wait_staged(d, bar, &s_flag)) return;
     float sig[kSKA];
     for (int i = threadIdx.x; i < nh; i += kSThreads) {
         s_node_sigma<FMT>(d, loff, a, i, mode, b_reg, has_pred ? b_pred : nullptr, b_str, kr, kp, na, sig);
         const float p = pr[i];
 #pragma unroll
         for (int k = 0; k < kSKA; k++)
-            if (k < na && rs[k] != kNoSlot) d.reach[a][(size_t)rs[k] * d.rstr[a] + i] = p * sig[k];
+            if (k < na && it.rs[k] != kNoSlot) d.reach[a][(size_t)it.rs[k] * d.rstr[a] + i] = p * sig[k];
     }
 }
 
@@ -357,16 +352,16 @@ __global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const Act
 // The node's fold child, if any, is evaluated here from the staged opponent
 // reach; every other child's cfv is staged from its slot.
 template <int FMT, int EVAL>
-__global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActItem* items, int p, int mode) {
+__global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode* nodes, int p, int mode) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ int s_flag;
     __shared__ double s_S[52];
     __shared__ double s_dred[kSWarps];
     __shared__ float s_red[3 * kSWarps];
-    const ActItem it = items[blockIdx.x];
+    const SNode it = nodes[blockIdx.x];
     const int a = (int)it.actor, na = (int)it.na, o = 1 - p, nh = d.nh[p], nho = d.nh[o];
     const int esz = FMT == kDevF32 ? 4 : 2;
-    const SLayout L(d, esz);
+    const SLayout L(d, esz, ar.pred[0] != nullptr);
     uint64_t* bar = (uint64_t*)sm;
     unsigned char* b_reg = sm + L.reg();
     unsigned char* b_str = sm + L.str();
@@ -375,23 +370,8 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
     float* rp = (float*)(sm + L.rp());
     float* cv = (float*)(sm + L.cv());
     const int vstride = d.nh_pad;
-
-    uint32_t cs[kSKA];
-    int fk = -1;
-    float famount = 0.0f;
-#pragma unroll
-    for (int k = 0; k < kSKA; k++) {
-        cs[k] = kNoSlot;
-        if (k < na) {
-            const ChildRef c = d.crefs[it.cref + k];
-            cs[k] = c.cslot;
-            if (c.kind == kChildFold) {
-                fk = k;
-                const TermInfo tm = d.terms[c.term];
-                famount = (int)tm.aux == p ? tm.tlose : tm.twin;
-            }
-        }
-    }
+    const int fk = it.fk == kNoSlot ? -1 : (int)it.fk;
+    const float famount = (int)it.folder == p ? it.tlose : it.twin;
     const long long loff = d.lock_off[a][it.sidx];
     const bool mine = a == p;
     const bool has_pred = ar.pred[a] != nullptr;
@@ -401,18 +381,39 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
     const bool use_pred = use_reg && has_pred;
     const bool use_rp = mine && !EVAL && loff < 0;
     const unsigned blk = round16((unsigned)(na * d.nh[a] * esz));
-    CopyList cl;  // filled and issued by thread 0 only
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
-        if (use_reg) cl.add(b_reg, (const unsigned char*)ar.reg[a] + it.aoff * esz, blk);
-        if (use_str) cl.add(b_str, (const unsigned char*)ar.str[a] + it.aoff * esz, blk);
-        if (use_pred) cl.add(b_pred, (const unsigned char*)ar.pred[a] + it.aoff * esz, blk);
-        if (use_rp) cl.add(rp, d.reach[p] + (size_t)it.rslot * d.rstr[p], round16((unsigned)nh * 4u));
-        if (fk >= 0)
-            cl.add(ro, d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * d.rstr[o], round16((unsigned)nho * 4u));
+        const unsigned vb = round16((unsigned)nh * 4u), vbo = round16((unsigned)nho * 4u);
+        const unsigned char* g_reg = (const unsigned char*)ar.reg[a] + it.aoff * esz;
+        const unsigned char* g_str = (const unsigned char*)ar.str[a] + it.aoff * esz;
+        const unsigned char* g_pred = use_pred ? (const unsigned char*)ar.pred[a] + it.aoff * esz : nullptr;
+        const float* g_rp = d.reach[p] + (size_t)it.rslot * d.rstr[p];
+        const float* g_ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * d.rstr[o];
+        unsigned total = (use_reg ? blk : 0u) + (use_str ? blk : 0u) + (use_pred ? blk : 0u) + (use_rp ? vb : 0u) +
+                         (fk >= 0 ? vbo : 0u);
+        uintptr_t bad = (uintptr_t)g_reg | (uintptr_t)g_str | (uintptr_t)g_pred;
+        if (use_rp) bad |= (uintptr_t)g_rp;
+        if (fk >= 0) bad |= (uintptr_t)g_ro;
 #pragma unroll
         for (int k = 0; k < kSKA; k++)
-            if (k < na && k != fk) cl.add(cv + k * vstride, d.cfv + (size_t)cs[k] * d.nh_max, round16((unsigned)nh * 4u));
+            if (k < na && k != fk) {
+                total += vb;
+                bad |= (uintptr_t)(d.cfv + (size_t)it.cs[k] * d.nh_max);
+            }
+        s_flag = (bad & 15u) ? 1 : 0;
+        if (s_flag) {
+            atomicOr(d.err, 2u);
+        } else {
+            mbar_expect_tx(bar, total);
+            if (use_reg) bulk_load(b_reg, g_reg, blk, bar);
+            if (use_str) bulk_load(b_str, g_str, blk, bar);
+            if (use_pred) bulk_load(b_pred, g_pred, blk, bar);
+            if (use_rp) bulk_load(rp, g_rp, vb, bar);
+            if (fk >= 0) bulk_load(ro, g_ro, vbo, bar);
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na && k != fk) bulk_load(cv + k * vstride, d.cfv + (size_t)it.cs[k] * d.nh_max, vb, bar);
+        }
     }
     // scales of the actor's node (16-bit arenas), loaded while the copies fly
     float kr = 0.0f, kp = 0.0f, sscale = 0.0f;
@@ -421,7 +422,7 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
         if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
         if (mine) sscale = ar.sscale[a][it.sidx];
     }
-    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
+    if (!wait_staged(d, bar, &s_flag)) return;
 
     float sig[kSKA];
     double ftotal = 0.0;
@@ -440,8 +441,14 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
         }
         ftotal = s_fold_sums(d, o, ro, s_S, s_dred);
         // the fold child's values go where a staged child's cfv would be
-        for (int i = threadIdx.x; i < nh; i += kSThreads)
-            cv[fk * vstride + i] = fold_value(d, p, i, ro, ftotal, s_S, famount);
+        // (fold_value of cfr_kernels.cuh with the hand's cards and same combo
+        // packed in one word)
+        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+            const uint32_t h = d.hinfo[p][i];
+            const uint32_t sm_ = h >> 16;
+            const float same_r = sm_ != 0xFFFFu ? ro[sm_] : 0.0f;
+            cv[fk * vstride + i] = famount * ((float)(ftotal - s_S[h & 63u] - s_S[(h >> 6) & 63u]) + same_r);
+        }
         __syncthreads();
     }
     float* out = d.cfv + (size_t)it.cslot * d.nh_max;
@@ -630,29 +637,6 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const ActIt
         ar.sscale[p][it.sidx] = (smax > 0.0f && isfinite(smax)) ? smax : 0.0f;
         if (use_pred) ar.pscale[p][it.sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
     }
-}
-
-// Showdown terminal with its opponent reach staged in shared memory (the
-// gather by strength order then reads shared memory, not HBM).
-__global__ void __launch_bounds__(kThreads) ks_showdown(Dev d, const ShowItem* items, int p) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ double s_w[kWarps];
-    __shared__ int s_flag;
-    const ShowItem s = items[blockIdx.x];
-    const int o = 1 - p;
-    uint64_t* bar = (uint64_t*)sm;
-    float* ro = (float*)(sm + 16);
-    double* scr = (double*)(sm + 16 + (size_t)d.nh_pad * 4);
-    CopyList cl;  // filled and issued by thread 0 only
-    if (threadIdx.x == 0) {
-        mbar_init(bar, 1);
-        cl.add(ro, d.reach[o] + (size_t)s.rs[o] * d.rstr[o], round16((unsigned)d.nh[o] * 4u));
-    }
-    if (!stage_and_wait(d, bar, cl, &s_flag)) return;
-    eval_showdown<double>(d, p, s.slot, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, scr, s_w);
-}
-inline size_t staged_show_smem_bytes(int nh_pad, int scr_elems) {
-    return 16 + (size_t)nh_pad * 4 + (size_t)scr_elems * sizeof(double);
 }
 
 // ------------------------------------------------- batched showdowns

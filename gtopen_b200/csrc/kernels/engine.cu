@@ -98,7 +98,8 @@ struct EngineImpl {
     size_t show_smem = 0;    // plain showdown kernel (f64 scratch)
     size_t act_smem = 0;     // fused up-action dynamic smem
     size_t warp_smem = 0;    // warp up-action dynamic smem (one staged reach per warp)
-    size_t st_up_smem = 0, st_down_smem = 0, st_show_smem = 0;  // staged kernels
+    size_t st_up_smem = 0, st_down_smem = 0;  // staged kernels
+    SNode* snodes = nullptr;                   // staged node records (same order as act)
     size_t show_batch_smem = 0;                                   // batched showdowns
     size_t chance_smem = 0;  // runout chance dynamic smem
     cudaGraphExec_t g_iter = nullptr;
@@ -188,7 +189,7 @@ struct EngineImpl {
     template <int FMT, int KA>
     void down_action(const Span& sa, int mode) {
         if (staged) {
-            ks_down<FMT><<<sa.count, kSThreads, st_down_smem, stream>>>(d, ar, act + sa.start, mode);
+            ks_down<FMT><<<sa.count, kSThreads, st_down_smem, stream>>>(d, ar, snodes + sa.start, mode);
         } else if (warp) {
             const unsigned grid = (sa.count + kWarps - 1) / kWarps;
             kw_down_action<FMT, KA><<<grid, kThreads, 0, stream>>>(d, ar, act + sa.start, (int)sa.count, mode);
@@ -210,7 +211,7 @@ struct EngineImpl {
     }
     void launch_up_action(const Span& sa, int p, int eval) {
         if (staged) {
-            const ActItem* it = act + sa.start;
+            const SNode* it = snodes + sa.start;
             if (fmt == kFmtF32) {
                 if (eval < 0) ks_up<kDevF32, 0><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, 0);
                 else ks_up<kDevF32, 1><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, eval);
@@ -435,17 +436,59 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     E.show_smem = (size_t)d.scr_elems * sizeof(double);
     if (E.warp) E.warp_smem = (size_t)kWarps * d.nh_pad * sizeof(float);
     if (E.staged) {
+        // node records, packed hand words, fixed-stride card lists
+        std::vector<SNode> sn(P.act.size());
+        for (size_t k = 0; k < P.act.size(); k++) {
+            const ActItem& a = P.act[k];
+            SNode& x = sn[k];
+            std::memset(&x, 0, sizeof(x));
+            x.aoff = a.aoff;
+            x.cslot = a.cslot;
+            x.rslot = a.rslot;
+            x.oslot = a.oslot;
+            x.sidx = a.sidx;
+            x.actor = a.actor;
+            x.na = a.na;
+            x.fk = kNoSlot;
+            for (uint32_t c = 0; c < (uint32_t)kSKA; c++) {
+                x.cs[c] = kNoSlot;
+                x.rs[c] = kNoSlot;
+                if (c >= a.na) continue;
+                const ChildRef& r = P.crefs[a.cref + c];
+                x.cs[c] = r.cslot;
+                x.rs[c] = r.rslot;
+                if (r.kind == kChildFold) {
+                    const TermInfo& t = P.terms[r.term];
+                    x.fk = c;
+                    x.folder = t.aux;
+                    x.twin = t.twin;
+                    x.tlose = t.tlose;
+                }
+            }
+        }
+        E.snodes = dupload(sn, O, &B);
+        for (int q = 0; q < 2; q++) {
+            const Hands& h = sp.hands[q];
+            std::vector<uint32_t> hi(h.c1.size());
+            for (size_t i = 0; i < hi.size(); i++) {
+                const uint32_t s = sp.same[q][i];
+                hi[i] = (uint32_t)h.c1[i] | (uint32_t)h.c2[i] << 6 | (s == kSentinel ? 0xFFFFu : s) << 16;
+            }
+            d.hinfo[q] = dupload(hi, O, &B);
+            std::vector<uint16_t> h52(52 * 52, 0xFFFF);
+            for (int c = 0; c < 52; c++)
+                for (uint32_t k = P.hcard_off[q][c], j = 0; k < P.hcard_off[q][c + 1]; k++, j++) h52[c * 52 + j] = P.hcard_idx[q][k];
+            d.hcard52[q] = dupload(h52, O, &B);
+        }
         const int esz = E.fmt == kFmtF32 ? 4 : 2;
-        E.st_up_smem = staged_smem_bytes(d.nh_pad, esz);
-        E.st_down_smem = staged_down_smem_bytes(d.nh_pad, esz);
-        E.st_show_smem = staged_show_smem_bytes(d.nh_pad, d.scr_elems);
+        E.st_up_smem = staged_smem_bytes(d.nh_pad, esz, E.pcfr);
+        E.st_down_smem = staged_down_smem_bytes(d.nh_pad, esz, E.pcfr);
         set_smem((const void*)ks_up<kDevF32, 0>, E.st_up_smem);
         set_smem((const void*)ks_up<kDevF32, 1>, E.st_up_smem);
         set_smem((const void*)ks_up<kDevI16, 0>, E.st_up_smem);
         set_smem((const void*)ks_up<kDevI16, 1>, E.st_up_smem);
         set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
         set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
-        set_smem((const void*)ks_showdown, E.st_show_smem);
         E.show_batch_smem = show_cta_smem_bytes(d.nh_pad, (int)P.max_sorted, (int)P.max_bins);
         set_smem((const void*)ks_show_cta, E.show_batch_smem);
     }
