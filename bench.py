@@ -49,6 +49,8 @@ def make_config(name):
     from gtopen_b200 import workloads as W
     if name == "flop":
         return W.flop_spot(g.evaluate7, seed=3)
+    if name == "flop_narrow":  # the flop's board and ranges on a narrow tree (profiling case)
+        return W.flop_spot(g.evaluate7, seed=3, bet=("75", "a"), raise_=("a",), max_raises=2)
     if name == "turn":
         return W.turn_spot(g.evaluate7, seed=2)
     if name == "river":
@@ -192,6 +194,8 @@ def run_reference(args, world, rank):
 def workload_config(args, cfg):
     return {"workload": {"flop": "flop SRP: 3-card board seed 3, OOP top40%/IP top55%, pot 55 stack 975, "
                                  "bets {33,75,a} raises {2.5x,a} max 3 raises",
+                         "flop_narrow": "flop SRP board and ranges (seed 3, 470 v 647) on a narrow tree: "
+                                        "bets {75,a}, raises {a}, max 2 raises (353,409 nodes)",
                          "turn": "turn precision study: 4-card board seed 2, top 50% each, pot 100 stack 300",
                          "river": "river HU: 5-card board seed 1, all 1081 combos each side, pot 100 stack 400",
                          "bench_spot": "reference bench_spot.json (Ks7h2d, 257 v 319)"}[args.workload],
@@ -327,7 +331,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="flop", choices=["flop", "turn", "river", "bench_spot"])
+    ap.add_argument("--workload", default="flop", choices=["flop", "flop_narrow", "turn", "river", "bench_spot"])
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32"])
     ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged"])
     ap.add_argument("--no-e2e", action="store_true")
