@@ -103,6 +103,7 @@ void HostSolver::arena_f32(int which, int p, float* out) const {  // save.rs:76-
         if (t.kind[n] == kAction && t.player[n] == p) a.read(n, t.data_off[n], t.nchild[n] * nh, out + t.data_off[n]);
 }
 void HostSolver::set_arena_f32(int which, int p, const float* in) {
+    arenas_zero = false;
     const Tree& t = spot->tree;
     const size_t nh = spot->hands[p].size();
     Arena& a = pick(*this, which, p);
@@ -140,6 +141,7 @@ void HostSolver::average_strategy(uint32_t node, float* sig) const {
 // -------------------------------------------------- symmetrise (cfr.rs:749-871)
 void HostSolver::ensure_symmetric() {
     if (!sym_dirty || !use_iso || spot->perms.size() < 2) { sym_dirty = false; return; }
+    arenas_zero = false;
     symmetrize(0, nullptr, 0);
     sym_dirty = false;
 }
@@ -474,6 +476,7 @@ std::unique_ptr<HostSolver> HostSolver::load(const std::string& path, int storag
         throw Error(std::string("bad lock section: ") + e.what());
     }
     auto s = std::make_unique<HostSolver>(spot, storage_mode, kDcfr, true);
+    s->arenas_zero = false;
     s->iteration = (uint32_t)it->num;
     for (auto& l : locks) s->locks[l.first] = l.second;
     s->lock_labels = labels;

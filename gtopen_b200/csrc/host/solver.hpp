@@ -49,6 +49,10 @@ struct HostSolver {
     std::map<uint32_t, std::vector<float>> locks;
     std::map<uint32_t, std::string> lock_labels;
     bool sym_dirty = false;
+    // Every arena still holds its initial zeros (nothing has written one since
+    // construction): GpuEngine then skips the upload, the device arenas start
+    // zeroed as well.
+    bool arenas_zero = true;
 
     HostSolver(std::shared_ptr<Spot> s, int storage_mode, int algorithm, bool iso);
     void ensure_preds();

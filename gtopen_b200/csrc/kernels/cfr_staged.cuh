@@ -51,12 +51,15 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
 __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }
+// try_wait with a suspend-time hint: a waiting thread sleeps in the
+// instruction (up to kSuspendNs) instead of spinning and issuing.
+constexpr unsigned kSuspendNs = 100000u;
 __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
     uint32_t ok;
     asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}\n"
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n}\n"
         : "=r"(ok)
-        : "r"(smem_u32(bar)), "r"(parity)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(kSuspendNs)
         : "memory");
     return ok != 0;
 }
@@ -296,12 +299,11 @@ inline size_t staged_down_smem_bytes(int nh_pad, int esz, bool pred) {
 
 // Down sweep, one node per CTA: staged sigma source and parent reach; child
 // reach vectors written with coalesced stores (cfr.rs:469-531 push-down).
-template <int FMT>
-__global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const SNode* nodes, int mode) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ int s_flag;
-    const SNode it = nodes[blockIdx.x];
-    const int a = (int)it.actor, na = (int)it.na, nh = d.nh[a];
+template <int FMT, int NA>
+__device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, const SNode& it, int mode,
+                                             unsigned char* sm, int& s_flag) {
+    const int a = (int)it.actor, nh = d.nh[a];
+    constexpr int na = NA;  // the node's action count, a compile-time constant in this instance
     const int esz = FMT == kDevF32 ? 4 : 2;
     const SLayout L(d, esz, ar.pred[0] != nullptr);
     uint64_t* bar = (uint64_t*)sm;
@@ -346,20 +348,38 @@ __global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const SNo
             if (k < na && it.rs[k] != kNoSlot) d.reach[a][(size_t)it.rs[k] * d.rstr[a] + i] = p * sig[k];
     }
 }
+template <int FMT>
+__global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const SNode* nodes, int mode) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ int s_flag;
+    const SNode it = nodes[blockIdx.x];
+    switch (it.na) {  // uniform per CTA: one specialised body per action count
+        case 1: ks_down_node<FMT, 1>(d, ar, it, mode, sm, s_flag); break;
+        case 2: ks_down_node<FMT, 2>(d, ar, it, mode, sm, s_flag); break;
+        case 3: ks_down_node<FMT, 3>(d, ar, it, mode, sm, s_flag); break;
+        default: ks_down_node<FMT, 4>(d, ar, it, mode, sm, s_flag); break;
+    }
+}
 
 // Up sweep, one node per CTA (cfr.rs:469-531 pull-up, 297-409 update;
 // best_response.rs:69-121, 185-219 for EVAL = 1 with mode 0 BR / 1 average).
 // The node's fold child, if any, is evaluated here from the staged opponent
 // reach; every other child's cfv is staged from its slot.
-template <int FMT, int EVAL>
-__global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode* nodes, int p, int mode) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ int s_flag;
-    __shared__ double s_S[52];
-    __shared__ double s_dred[kSWarps];
-    __shared__ float s_red[3 * kSWarps];
-    const SNode it = nodes[blockIdx.x];
-    const int a = (int)it.actor, na = (int)it.na, o = 1 - p, nh = d.nh[p], nho = d.nh[o];
+struct UpShared {  // static shared memory of ks_up
+    int flag;
+    double S[52];
+    double dred[kSWarps];
+    float red[3 * kSWarps];
+};
+template <int FMT, int EVAL, int NA>
+__device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const SNode& it, int p, int mode,
+                                           unsigned char* sm, UpShared& us) {
+    int& s_flag = us.flag;
+    double* s_S = us.S;
+    double* s_dred = us.dred;
+    float* s_red = us.red;
+    const int a = (int)it.actor, o = 1 - p, nh = d.nh[p], nho = d.nh[o];
+    constexpr int na = NA;  // the node's action count, a compile-time constant in this instance
     const int esz = FMT == kDevF32 ? 4 : 2;
     const SLayout L(d, esz, ar.pred[0] != nullptr);
     uint64_t* bar = (uint64_t*)sm;
@@ -638,6 +658,18 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode
         if (use_pred) ar.pscale[p][it.sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
     }
 }
+template <int FMT, int EVAL>
+__global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode* nodes, int p, int mode) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ UpShared us;
+    const SNode it = nodes[blockIdx.x];
+    switch (it.na) {  // uniform per CTA: one specialised body per action count
+        case 1: ks_up_node<FMT, EVAL, 1>(d, ar, it, p, mode, sm, us); break;
+        case 2: ks_up_node<FMT, EVAL, 2>(d, ar, it, p, mode, sm, us); break;
+        case 3: ks_up_node<FMT, EVAL, 3>(d, ar, it, p, mode, sm, us); break;
+        default: ks_up_node<FMT, EVAL, 4>(d, ar, it, p, mode, sm, us); break;
+    }
+}
 
 // ------------------------------------------------- batched showdowns
 // One CTA per batch of up to kShowBatch showdowns of one level that share a
@@ -649,18 +681,16 @@ struct ShowTab {  // shared-memory copies of one slot's tables
     const uint16_t* sidx;  // m opponent hands, ascending strength
     const uint32_t* coff;  // 53 card-list offsets relative to the slot's first entry
     const uint16_t* bpos;  // per-card sorted positions (ne entries)
-    const uint8_t* bcard;  // card of each entry
-    const uint16_t* bins;  // nbins + 1 bin starts
     const RankEntry* rank;  // mp entries
     const uint16_t* zero;  // nz blocked traverser hands
     const uint32_t* same;  // traverser same-combo map (nh entries)
-    int m, nbins, mp, nz;
+    int m, mp, nz;
 };
 struct ShowTabLayout {  // byte offsets of the tables inside the table region
-    unsigned sidx, coff, bpos, bcard, bins, rank, zero, same, total;
+    unsigned sidx, coff, bpos, rank, zero, same, total;
 };
 __host__ __device__ inline unsigned r16u(unsigned b) { return (b + 15u) & ~15u; }
-__host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad, int max_bins) {
+__host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad) {
     ShowTabLayout L;
     unsigned o = 0;
     L.sidx = o;
@@ -669,10 +699,6 @@ __host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad, int max_bin
     o += r16u(53u * 4u);
     L.bpos = o;
     o += r16u(4u * nh_pad);
-    L.bcard = o;
-    o += r16u(2u * nh_pad);
-    L.bins = o;
-    o += r16u(2u * (max_bins + 1));
     L.rank = o;
     o += r16u(16u * nh_pad);
     L.zero = o;
@@ -691,27 +717,19 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
     const uint32_t* coff_g = d.ccard_off[o] + (size_t)slot * 53;
     const uint32_t c0 = coff_g[0];
     const uint32_t ne = coff_g[52] - c0;
-    const uint32_t bo = d.bin_off[o][slot];
-    tb.nbins = (int)(d.bin_off[o][slot + 1] - bo) - 1;
     tb.mp = (int)d.rank_cnt[p][slot];
     const uint32_t z0 = d.zero_off[p][slot];
     tb.nz = (int)(d.zero_off[p][slot + 1] - z0);
     uint16_t* t_sidx = (uint16_t*)(tabs + TL.sidx);
     uint32_t* t_coff = (uint32_t*)(tabs + TL.coff);
     uint16_t* t_bpos = (uint16_t*)(tabs + TL.bpos);
-    uint8_t* t_bcard = (uint8_t*)(tabs + TL.bcard);
-    uint16_t* t_bins = (uint16_t*)(tabs + TL.bins);
     RankEntry* t_rank = (RankEntry*)(tabs + TL.rank);
     uint16_t* t_zero = (uint16_t*)(tabs + TL.zero);
     uint32_t* t_same = (uint32_t*)(tabs + TL.same);
     const uint16_t* g_sidx = d.sorted_idx[o] + d.sorted_off[o][slot];
     for (int k = threadIdx.x; k < tb.m; k += blockDim.x) t_sidx[k] = g_sidx[k];
     if (threadIdx.x < 53) t_coff[threadIdx.x] = coff_g[threadIdx.x] - c0;
-    for (uint32_t k = threadIdx.x; k < ne; k += blockDim.x) {
-        t_bpos[k] = d.ccard_pos[o][c0 + k];
-        t_bcard[k] = d.ccard_card[o][c0 + k];
-    }
-    for (int k = threadIdx.x; k <= tb.nbins; k += blockDim.x) t_bins[k] = d.bin_start[o][bo + k];
+    for (uint32_t k = threadIdx.x; k < ne; k += blockDim.x) t_bpos[k] = d.ccard_pos[o][c0 + k];
     const RankEntry* g_rank = d.rank[p] + d.rank_off[p][slot];
     for (int k = threadIdx.x; k < tb.mp; k += blockDim.x) t_rank[k] = g_rank[k];
     for (int k = threadIdx.x; k < tb.nz; k += blockDim.x) t_zero[k] = d.zero_idx[p][z0 + k];
@@ -719,29 +737,27 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
     tb.sidx = t_sidx;
     tb.coff = t_coff;
     tb.bpos = t_bpos;
-    tb.bcard = t_bcard;
-    tb.bins = t_bins;
     tb.rank = t_rank;
     tb.zero = t_zero;
     tb.same = t_same;
 }
 
-constexpr int kShowThreads = 128;
-constexpr int kShowCtaWarps = kShowThreads / 32;
+// Showdown CTAs have NT threads: 256 for large hand lists, 128 for small ones.
 
 // One showdown evaluated by the CTA (game.rs:501-577 with the rank tables):
 // R = opponent reach in strength order, P = its exclusive prefix (each
 // thread sums a contiguous chunk, then a two-level shuffle scan), Q = per-card
 // prefixes (threads 0..51 each run one card's list in strength order, as the
 // reference's running card sums do), then the rank entries.
+template <int NT>
 __device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, float lose, float tie, float* out,
                              float* R, double* P, double* Q, double* S, double* s_w) {
     const int m = tb.m;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = threadIdx.x; k < m; k += kShowThreads) R[k] = ro[tb.sidx[k]];
+    for (int k = threadIdx.x; k < m; k += NT) R[k] = ro[tb.sidx[k]];
     __syncthreads();
     // P
-    const int chunk = (m + kShowThreads - 1) / kShowThreads;
+    const int chunk = (m + NT - 1) / NT;
     const int lo = min((int)threadIdx.x * chunk, m), hi = min(lo + chunk, m);
     double local = 0.0;
     for (int k = lo; k < hi; k++) local += (double)R[k];
@@ -778,17 +794,17 @@ __device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, floa
     __syncthreads();
     double wbase = 0.0;
 #pragma unroll
-    for (int k = 0; k < kShowCtaWarps; k++)
+    for (int k = 0; k < (NT / 32); k++)
         if (k < warp) wbase += s_w[k];
     double run = wbase + (incl - local);
     for (int k = lo; k < hi; k++) {
         P[k] = run;
         run += (double)R[k];
     }
-    if (threadIdx.x == kShowThreads - 1) P[m] = run;
+    if (threadIdx.x == NT - 1) P[m] = run;
     __syncthreads();
     const double total = P[m];
-    for (int k = threadIdx.x; k < tb.mp; k += kShowThreads) {
+    for (int k = threadIdx.x; k < tb.mp; k += NT) {
         const RankEntry e = tb.rank[k];
         const int a1 = e.cards & 0xFF, a2 = e.cards >> 8;
         const float lower = (float)(P[e.lb] - Q[e.q1lo] - Q[e.q2lo]);
@@ -799,7 +815,7 @@ __device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, floa
         const float tied = valid - lower - higher;
         out[e.idx] = win * lower + lose * higher + tie * tied;
     }
-    for (int z = threadIdx.x; z < tb.nz; z += kShowThreads) out[tb.zero[z]] = 0.0f;
+    for (int z = threadIdx.x; z < tb.nz; z += NT) out[tb.zero[z]] = 0.0f;
     __syncthreads();
 }
 // Shared memory of ks_show_cta: two barriers, two reach buffers, R (floats),
@@ -807,17 +823,18 @@ __device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, floa
 __host__ __device__ inline unsigned show_cta_scratch_bytes(int nh_pad, int msort) {
     return 32u + 2u * 4u * (unsigned)nh_pad + r16u(4u * (unsigned)msort) + r16u((3u * (unsigned)msort + 105u) * 8u);
 }
-inline size_t show_cta_smem_bytes(int nh_pad, int msort, int max_bins) {
-    return (size_t)show_cta_scratch_bytes(nh_pad, msort) + show_tab_layout(nh_pad, max_bins).total;
+inline size_t show_cta_smem_bytes(int nh_pad, int msort) {
+    return (size_t)show_cta_scratch_bytes(nh_pad, msort) + show_tab_layout(nh_pad).total;
 }
 
 // A batch (one level, one slot) per CTA: tables loaded once; the batch's
 // opponent reach vectors stream through two bulk-copy buffers, the next one
 // landing while the current one is evaluated.
-__global__ void __launch_bounds__(kShowThreads) ks_show_cta(Dev d, const ShowItem* items, const ShowBatch* batches,
-                                                            int p, int max_bins, int msort) {
+template <int NT>
+__global__ void __launch_bounds__(NT) ks_show_cta(Dev d, const ShowItem* items, const ShowBatch* batches,
+                                                            int p, int msort) {
     extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ double s_w[kShowCtaWarps];
+    __shared__ double s_w[(NT / 32)];
     __shared__ int s_flag;
     __shared__ ShowItem s_it[kShowBatch];
     const ShowBatch bt = batches[blockIdx.x];
@@ -830,7 +847,7 @@ __global__ void __launch_bounds__(kShowThreads) ks_show_cta(Dev d, const ShowIte
     double* Q = P + msort + 1;
     double* S = Q + 2 * msort + 52;
     unsigned char* tabs = sm + show_cta_scratch_bytes(d.nh_pad, msort);
-    const ShowTabLayout TL = show_tab_layout(d.nh_pad, max_bins);
+    const ShowTabLayout TL = show_tab_layout(d.nh_pad);
     if (threadIdx.x < n) s_it[threadIdx.x] = items[bt.start + threadIdx.x];
     ShowTab tb;
     load_show_tab(d, p, bt.slot, tabs, TL, tb);
@@ -870,7 +887,7 @@ __global__ void __launch_bounds__(kShowThreads) ks_show_cta(Dev d, const ShowIte
         }
         const ShowItem& s = s_it[j];
         const float* ro = rbuf + (size_t)(j & 1) * d.nh_pad;
-        cta_showdown(tb, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, R, P, Q, S, s_w);
+        cta_showdown<NT>(tb, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, R, P, Q, S, s_w);
         // buffer j & 1 is free (the evaluation ends with a barrier): order its
         // generic reads before the next bulk write into it, then refill it
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

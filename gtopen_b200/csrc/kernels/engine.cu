@@ -295,8 +295,12 @@ struct EngineImpl {
                 timed(pr, 4, [&] {
                     if (staged) {
                         const Span sb = plan.show_batch_span[l];
-                        ks_show_cta<<<sb.count, kShowThreads, show_batch_smem, stream>>>(
-                            d, show, show_batch + sb.start, p, (int)plan.max_bins, (int)plan.max_sorted);
+                        if (plan.max_sorted > 384)
+                            ks_show_cta<256><<<sb.count, 256, show_batch_smem, stream>>>(
+                                d, show, show_batch + sb.start, p, (int)plan.max_sorted);
+                        else
+                            ks_show_cta<128><<<sb.count, 128, show_batch_smem, stream>>>(
+                                d, show, show_batch + sb.start, p, (int)plan.max_sorted);
                     } else {
                         k_showdown<<<ss.count, kThreads, show_smem, stream>>>(d, show + ss.start, p);
                     }
@@ -489,8 +493,9 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
         set_smem((const void*)ks_up<kDevI16, 1>, E.st_up_smem);
         set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
         set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
-        E.show_batch_smem = show_cta_smem_bytes(d.nh_pad, (int)P.max_sorted, (int)P.max_bins);
-        set_smem((const void*)ks_show_cta, E.show_batch_smem);
+        E.show_batch_smem = show_cta_smem_bytes(d.nh_pad, (int)P.max_sorted);
+        set_smem((const void*)ks_show_cta<128>, E.show_batch_smem);
+        set_smem((const void*)ks_show_cta<256>, E.show_batch_smem);
     }
     if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
@@ -533,9 +538,10 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     CK(cudaMallocHost(&E.pinned, E.staging_len * sizeof(float)));
     CK(cudaMallocHost(&E.h_dot, 4 * sizeof(double)));
 
-    // upload arenas: quants directly when host and device are both 16-bit, else via f32 (+ encode)
-    std::vector<float> img(E.staging_len);
-    for (int q = 0; q < 2; q++) {
+    // upload arenas: quants directly when host and device are both 16-bit, else via f32 (+ encode);
+    // nothing to upload while the host arenas are still all zero (so are the device's)
+    std::vector<float> img(host.arenas_zero ? 0 : E.staging_len);
+    for (int q = 0; q < 2 && !host.arenas_zero; q++) {
         const int nh = P.nh[q];
         const unsigned nb = (unsigned)P.n_anodes[q];
         if (!nb) continue;
@@ -788,6 +794,7 @@ void GpuEngine::sync_to_cpu(HostSolver& host, bool strategy_only) {  // gpu/mod.
         }
     }
     host.iteration = E.iteration;
+    host.arenas_zero = false;
     if (E.plan.iso_active) host.sym_dirty = true;
 }
 
