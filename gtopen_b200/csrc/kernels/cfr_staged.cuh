@@ -275,27 +275,38 @@ __device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, d
 // Shared-memory layout of the staged action kernels (bytes): the regret,
 // strategy-sum and (PCFR+ only) prediction blocks, the opponent and own
 // reach vectors, then kSKA child value vectors.
+// Three layouts: the down kernel (one sigma-source block -- regrets or, in
+// evaluation sweeps, strategy sums -- the predictions for PCFR+, the parent
+// reach), the up kernel on the traverser's nodes (regret, strategy-sum and
+// prediction blocks, opponent and own reach, child values) and the up kernel
+// on the opponent's nodes (one sigma-source block for the fold child, the
+// predictions, the opponent reach, child values).
+enum SKind { kSDown = 0, kSUpMine = 1, kSUpOpp = 2 };
 struct SLayout {
-    unsigned cap, vec, nblk;  // arena block capacity; one hand vector; blocks staged
-    __device__ SLayout(const Dev& d, int esz, bool pred)
-        : cap(round16((unsigned)(kSKA * d.nh_pad * esz))), vec((unsigned)d.nh_pad * 4u), nblk(pred ? 3u : 2u) {}
-    __device__ unsigned reg() const { return 16; }
-    __device__ unsigned str() const { return 16 + cap; }
-    __device__ unsigned pred() const { return 16 + 2 * cap; }
-    __device__ unsigned ro() const { return 16 + nblk * cap; }
-    __device__ unsigned rp() const { return 16 + nblk * cap + vec; }
-    __device__ unsigned cv() const { return 16 + nblk * cap + 2 * vec; }
+    unsigned cap, vec, o_str, o_pred, o_ro, o_rp, o_cv, total;
+    __host__ __device__ SLayout(int nh_pad, int esz, bool pred, int kind) {
+        cap = ((unsigned)(kSKA * nh_pad * esz) + 15u) & ~15u;
+        vec = (unsigned)nh_pad * 4u;
+        unsigned o = 16 + cap;  // the first block (regrets / sigma source) starts at 16
+        o_str = kind == kSUpMine ? o : 16u;
+        if (kind == kSUpMine) o += cap;
+        o_pred = o;
+        if (pred) o += cap;
+        o_ro = o;
+        o += vec;
+        o_rp = o;
+        if (kind == kSUpMine) o += vec;
+        o_cv = o;
+        if (kind != kSDown) o += (unsigned)kSKA * vec;
+        total = o;
+    }
+    __host__ __device__ unsigned reg() const { return 16; }
+    __host__ __device__ unsigned str() const { return o_str; }
+    __host__ __device__ unsigned pred() const { return o_pred; }
+    __host__ __device__ unsigned ro() const { return o_ro; }
+    __host__ __device__ unsigned rp() const { return o_rp; }
+    __host__ __device__ unsigned cv() const { return o_cv; }
 };
-// Host twins of SLayout's extent: the up kernel uses every region, the down
-// kernel the blocks and one reach vector.
-inline size_t staged_smem_bytes(int nh_pad, int esz, bool pred) {
-    const size_t cap = ((size_t)kSKA * nh_pad * esz + 15) & ~(size_t)15;
-    return 16 + (pred ? 3 : 2) * cap + (2 + kSKA) * (size_t)nh_pad * 4;
-}
-inline size_t staged_down_smem_bytes(int nh_pad, int esz, bool pred) {
-    const size_t cap = ((size_t)kSKA * nh_pad * esz + 15) & ~(size_t)15;
-    return 16 + (pred ? 3 : 2) * cap + (size_t)nh_pad * 4;
-}
 
 // Down sweep, one node per CTA: staged sigma source and parent reach; child
 // reach vectors written with coalesced stores (cfr.rs:469-531 push-down).
@@ -305,7 +316,7 @@ __device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, con
     const int a = (int)it.actor, nh = d.nh[a];
     constexpr int na = NA;  // the node's action count, a compile-time constant in this instance
     const int esz = FMT == kDevF32 ? 4 : 2;
-    const SLayout L(d, esz, ar.pred[0] != nullptr);
+    const SLayout L(d.nh_pad, esz, ar.pred[0] != nullptr, kSDown);
     uint64_t* bar = (uint64_t*)sm;
     unsigned char* b_reg = sm + L.reg();
     unsigned char* b_str = sm + L.str();
@@ -371,7 +382,7 @@ struct UpShared {  // static shared memory of ks_up
     double dred[kSWarps];
     float red[3 * kSWarps];
 };
-template <int FMT, int EVAL, int NA>
+template <int FMT, int EVAL, int NA, bool MINE>
 __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const SNode& it, int p, int mode,
                                            unsigned char* sm, UpShared& us) {
     int& s_flag = us.flag;
@@ -381,7 +392,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     const int a = (int)it.actor, o = 1 - p, nh = d.nh[p], nho = d.nh[o];
     constexpr int na = NA;  // the node's action count, a compile-time constant in this instance
     const int esz = FMT == kDevF32 ? 4 : 2;
-    const SLayout L(d, esz, ar.pred[0] != nullptr);
+    const SLayout L(d.nh_pad, esz, ar.pred[0] != nullptr, MINE ? kSUpMine : kSUpOpp);
     uint64_t* bar = (uint64_t*)sm;
     unsigned char* b_reg = sm + L.reg();
     unsigned char* b_str = sm + L.str();
@@ -393,7 +404,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     const int fk = it.fk == kNoSlot ? -1 : (int)it.fk;
     const float famount = (int)it.folder == p ? it.tlose : it.twin;
     const long long loff = d.lock_off[a][it.sidx];
-    const bool mine = a == p;
+    constexpr bool mine = MINE;  // a launch holds one actor's nodes: a == p iff MINE
     const bool has_pred = ar.pred[a] != nullptr;
     // what the node reads
     const bool use_reg = loff < 0 && !EVAL && (mine || fk >= 0);
@@ -658,16 +669,18 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
         if (use_pred) ar.pscale[p][it.sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
     }
 }
-template <int FMT, int EVAL>
+// MINE: the launch's nodes are the traverser's (the update), else the
+// opponent's (sum of children); a launch never mixes the two.
+template <int FMT, int EVAL, bool MINE>
 __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode* nodes, int p, int mode) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ UpShared us;
     const SNode it = nodes[blockIdx.x];
     switch (it.na) {  // uniform per CTA: one specialised body per action count
-        case 1: ks_up_node<FMT, EVAL, 1>(d, ar, it, p, mode, sm, us); break;
-        case 2: ks_up_node<FMT, EVAL, 2>(d, ar, it, p, mode, sm, us); break;
-        case 3: ks_up_node<FMT, EVAL, 3>(d, ar, it, p, mode, sm, us); break;
-        default: ks_up_node<FMT, EVAL, 4>(d, ar, it, p, mode, sm, us); break;
+        case 1: ks_up_node<FMT, EVAL, 1, MINE>(d, ar, it, p, mode, sm, us); break;
+        case 2: ks_up_node<FMT, EVAL, 2, MINE>(d, ar, it, p, mode, sm, us); break;
+        case 3: ks_up_node<FMT, EVAL, 3, MINE>(d, ar, it, p, mode, sm, us); break;
+        default: ks_up_node<FMT, EVAL, 4, MINE>(d, ar, it, p, mode, sm, us); break;
     }
 }
 

@@ -98,7 +98,7 @@ struct EngineImpl {
     size_t show_smem = 0;    // plain showdown kernel (f64 scratch)
     size_t act_smem = 0;     // fused up-action dynamic smem
     size_t warp_smem = 0;    // warp up-action dynamic smem (one staged reach per warp)
-    size_t st_up_smem = 0, st_down_smem = 0;  // staged kernels
+    size_t st_mine_smem = 0, st_opp_smem = 0, st_down_smem = 0;  // staged kernels
     SNode* snodes = nullptr;                   // staged node records (same order as act)
     size_t show_batch_smem = 0;                                   // batched showdowns
     size_t chance_smem = 0;  // runout chance dynamic smem
@@ -209,18 +209,39 @@ struct EngineImpl {
         set_smem((const void*)kw_up_action<FMT, 0, KA>, bytes);
         set_smem((const void*)kw_up_action<FMT, 1, KA>, bytes);
     }
-    void launch_up_action(const Span& sa, int p, int eval) {
+    template <int FMT, bool MINE>
+    void staged_up(const Span& s, int p, int eval) {
+        if (!s.count) return;
+        const SNode* it = snodes + s.start;
+        const size_t sm = MINE ? st_mine_smem : st_opp_smem;
+        if (eval < 0) ks_up<FMT, 0, MINE><<<s.count, kSThreads, sm, stream>>>(d, ar, it, p, 0);
+        else ks_up<FMT, 1, MINE><<<s.count, kSThreads, sm, stream>>>(d, ar, it, p, eval);
+    }
+    template <int FMT>
+    static void set_staged_smem(size_t mine, size_t opp) {
+        set_smem((const void*)ks_up<FMT, 0, true>, mine);
+        set_smem((const void*)ks_up<FMT, 1, true>, mine);
+        set_smem((const void*)ks_up<FMT, 0, false>, opp);
+        set_smem((const void*)ks_up<FMT, 1, false>, opp);
+    }
+    // Up sweep of one level's action nodes.  The staged engine launches the
+    // traverser's nodes and the opponent's separately (each launch's kernel is
+    // specialised for its side and sized for its shared memory).
+    void launch_up_level(int l, int p, int eval) {
         if (staged) {
-            const SNode* it = snodes + sa.start;
+            const Span mine = plan.act_span_actor[p][l], opp = plan.act_span_actor[1 - p][l];
             if (fmt == kFmtF32) {
-                if (eval < 0) ks_up<kDevF32, 0><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, 0);
-                else ks_up<kDevF32, 1><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, eval);
+                staged_up<kDevF32, true>(mine, p, eval);
+                staged_up<kDevF32, false>(opp, p, eval);
             } else {
-                if (eval < 0) ks_up<kDevI16, 0><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, 0);
-                else ks_up<kDevI16, 1><<<sa.count, kSThreads, st_up_smem, stream>>>(d, ar, it, p, eval);
+                staged_up<kDevI16, true>(mine, p, eval);
+                staged_up<kDevI16, false>(opp, p, eval);
             }
             return;
         }
+        launch_up_action(plan.act_span[l], p, eval);
+    }
+    void launch_up_action(const Span& sa, int p, int eval) {
         if (warp) {
             if (fmt == kFmtF32) {
                 if (wide) warp_up_action<kDevF32, 32>(sa, p, eval);
@@ -308,7 +329,7 @@ struct EngineImpl {
             const Span sc = plan.chance_span[l];
             if (sc.count) timed(pr, 5, [&] { launch_chance(sc, p); });
             const Span sa = plan.act_span[l];
-            if (sa.count) timed(pr, 6, [&] { launch_up_action(sa, p, eval); });
+            if (sa.count) timed(pr, 6, [&] { launch_up_level(l, p, eval); });
         }
         CK(cudaGetLastError());
     }
@@ -485,12 +506,11 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
             d.hcard52[q] = dupload(h52, O, &B);
         }
         const int esz = E.fmt == kFmtF32 ? 4 : 2;
-        E.st_up_smem = staged_smem_bytes(d.nh_pad, esz, E.pcfr);
-        E.st_down_smem = staged_down_smem_bytes(d.nh_pad, esz, E.pcfr);
-        set_smem((const void*)ks_up<kDevF32, 0>, E.st_up_smem);
-        set_smem((const void*)ks_up<kDevF32, 1>, E.st_up_smem);
-        set_smem((const void*)ks_up<kDevI16, 0>, E.st_up_smem);
-        set_smem((const void*)ks_up<kDevI16, 1>, E.st_up_smem);
+        E.st_mine_smem = SLayout(d.nh_pad, esz, E.pcfr, kSUpMine).total;
+        E.st_opp_smem = SLayout(d.nh_pad, esz, E.pcfr, kSUpOpp).total;
+        E.st_down_smem = SLayout(d.nh_pad, esz, E.pcfr, kSDown).total;
+        EngineImpl::set_staged_smem<kDevF32>(E.st_mine_smem, E.st_opp_smem);
+        EngineImpl::set_staged_smem<kDevI16>(E.st_mine_smem, E.st_opp_smem);
         set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
         set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
         E.show_batch_smem = show_cta_smem_bytes(d.nh_pad, (int)P.max_sorted);
