@@ -61,7 +61,7 @@ struct FoldItem {
     uint32_t folder;
     float twin, tlose;
 };
-struct ShowItem {
+struct alignas(16) ShowItem {
     uint32_t cslot;
     uint32_t rs[2];
     uint32_t slot;
@@ -87,7 +87,7 @@ struct CardEntry {  // chance card table (plan.rs:51-61)
 // The per-card prefixes of one board are stored concatenated: card c's
 // segment starts at Q index qbase(c) = ccard_off[c] - ccard_off[0] + c and
 // holds len(c) + 1 exclusive prefix values.
-struct RankEntry {
+struct alignas(16) RankEntry {  // 16-byte aligned: one vector load on the device
     uint16_t idx;         // my hand index
     uint16_t lb, ub;      // #opp hands strictly weaker / not stronger
     uint16_t q1lo, q1hi;  // Q index of the prefix of card c1 over the first lb / ub opp hands

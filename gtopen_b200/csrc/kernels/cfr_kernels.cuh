@@ -77,17 +77,17 @@ struct Arenas {
 };
 
 // ----------------------------------------------------------- small helpers
-__device__ __forceinline__ int16_t sat_i16(float x) {  // Rust `as i16` after round-ties-even
-    if (x != x) return 0;
-    float r = rintf(x);
-    r = fminf(fmaxf(r, -32768.0f), 32767.0f);
-    return (int16_t)r;
+// Rust `as i16` / `as u16` after round_ties_even (store.rs:178, 192): round to
+// nearest even, saturate to the type's range, NaN -> 0.  One cvt.rni.sat each.
+__device__ __forceinline__ int16_t sat_i16(float x) {
+    short r;
+    asm("cvt.rni.sat.s16.f32 %0, %1;" : "=h"(r) : "f"(x));
+    return x != x ? (int16_t)0 : (int16_t)r;
 }
 __device__ __forceinline__ uint16_t sat_u16(float x) {
-    if (x != x) return 0;
-    float r = rintf(x);
-    r = fminf(fmaxf(r, 0.0f), 65535.0f);
-    return (uint16_t)r;
+    unsigned short r;
+    asm("cvt.rni.sat.u16.f32 %0, %1;" : "=h"(r) : "f"(x));
+    return x != x ? (uint16_t)0 : (uint16_t)r;
 }
 __device__ __forceinline__ float block_max(float v, float* sh) {  // order-independent
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));

@@ -27,7 +27,7 @@ constexpr unsigned long long kWaitNs = 2000000000ull;  // 2 s
 
 // One action node as the staged kernels read it: everything its copies need
 // in one 80-byte record (one load round trip per node).
-struct SNode {
+struct alignas(16) SNode {
     uint64_t aoff;             // arena offset (elements) in the actor's arena
     uint32_t cslot, rslot, oslot, sidx;
     uint32_t cs[kSKA];         // child cfv slots (kNoSlot: the fold child)
@@ -142,7 +142,7 @@ __device__ __forceinline__ void s_regret_sigma(const void* reg, const void* pred
                     isum += qv[k];
                 }
             if (isum > 0) {
-                const float inv = 1.0f / (float)isum;
+                const float inv = __frcp_rn((float)isum);  // = 1.0f / x, correctly rounded
 #pragma unroll
                 for (int k = 0; k < kSKA; k++)
                     if (k < na) sig[k] = (float)qv[k] * inv;
@@ -156,7 +156,7 @@ __device__ __forceinline__ void s_regret_sigma(const void* reg, const void* pred
         }
     }
     if (sum > 1e-12f) {
-        const float inv = 1.0f / sum;
+        const float inv = __frcp_rn(sum);
 #pragma unroll
         for (int k = 0; k < kSKA; k++)
             if (k < na) sig[k] = fmaxf(sig[k], 0.0f) * inv;
@@ -201,7 +201,7 @@ __device__ __forceinline__ void s_average_sigma(const void* str, int na, int i, 
                 sum += qv[k];
             }
         if (sum > 0) {
-            const float inv = 1.0f / (float)sum;
+            const float inv = __frcp_rn((float)sum);
 #pragma unroll
             for (int k = 0; k < kSKA; k++)
                 if (k < na) sig[k] = (float)qv[k] * inv;
