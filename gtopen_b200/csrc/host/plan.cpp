@@ -101,7 +101,13 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                     const uint32_t c = t.child(nd, k);
                     if (is_terminal(t.kind[c]) && in_place(t.kind[c])) {
                         uint32_t ti = term_of(c, v.dealt, v.ndealt);
-                        P.crefs.push_back({t.kind[c] == kFold ? kChildFold : kChildShow, kNoSlot, kNoSlot, ti});
+                        // With folds in place but showdowns not (the staged and warp
+                        // engines), a fold child still gets the actor's reach slot: the
+                        // down sweep, which has the actor's strategy at hand, writes the
+                        // folding player's reach there, and the parent's up kernel reads
+                        // it instead of recomputing that strategy.
+                        const uint32_t frs = (t.kind[c] == kFold && !fused) ? (uint32_t)next_r[a]++ : kNoSlot;
+                        P.crefs.push_back({t.kind[c] == kFold ? kChildFold : kChildShow, kNoSlot, frs, ti});
                         it.nterm++;
                         continue;
                     }

@@ -279,19 +279,19 @@ __device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, d
 // evaluation sweeps, strategy sums -- the predictions for PCFR+, the parent
 // reach), the up kernel on the traverser's nodes (regret, strategy-sum and
 // prediction blocks, opponent and own reach, child values) and the up kernel
-// on the opponent's nodes (one sigma-source block for the fold child, the
-// predictions, the opponent reach, child values).
+// on the opponent's nodes (the fold child's reach, child values).
 enum SKind { kSDown = 0, kSUpMine = 1, kSUpOpp = 2 };
 struct SLayout {
     unsigned cap, vec, o_str, o_pred, o_ro, o_rp, o_cv, total;
     __host__ __device__ SLayout(int nh_pad, int esz, bool pred, int kind) {
         cap = ((unsigned)(kSKA * nh_pad * esz) + 15u) & ~15u;
         vec = (unsigned)nh_pad * 4u;
-        unsigned o = 16 + cap;  // the first block (regrets / sigma source) starts at 16
+        unsigned o = 16;
+        if (kind != kSUpOpp) o += cap;  // the first block (regrets / sigma source) starts at 16
         o_str = kind == kSUpMine ? o : 16u;
         if (kind == kSUpMine) o += cap;
         o_pred = o;
-        if (pred) o += cap;
+        if (pred && kind != kSUpOpp) o += cap;
         o_ro = o;
         o += vec;
         o_rp = o;
@@ -406,9 +406,10 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     const long long loff = d.lock_off[a][it.sidx];
     constexpr bool mine = MINE;  // a launch holds one actor's nodes: a == p iff MINE
     const bool has_pred = ar.pred[a] != nullptr;
-    // what the node reads
-    const bool use_reg = loff < 0 && !EVAL && (mine || fk >= 0);
-    const bool use_str = loff < 0 && (EVAL ? (mine ? mode == 1 : fk >= 0) : mine);
+    // what the node reads (an opponent node's fold child comes with the
+    // folding player's reach, written by the down sweep: no strategy needed)
+    const bool use_reg = loff < 0 && !EVAL && mine;
+    const bool use_str = loff < 0 && (EVAL ? (mine && mode == 1) : mine);
     const bool use_pred = use_reg && has_pred;
     const bool use_rp = mine && !EVAL && loff < 0;
     const unsigned blk = round16((unsigned)(na * d.nh[a] * esz));
@@ -419,7 +420,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
         const unsigned char* g_str = (const unsigned char*)ar.str[a] + it.aoff * esz;
         const unsigned char* g_pred = use_pred ? (const unsigned char*)ar.pred[a] + it.aoff * esz : nullptr;
         const float* g_rp = d.reach[p] + (size_t)it.rslot * d.rstr[p];
-        const float* g_ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * d.rstr[o];
+        const float* g_ro = d.reach[o] + (size_t)(mine ? it.oslot : it.rs[fk >= 0 ? fk : 0]) * d.rstr[o];
         unsigned total = (use_reg ? blk : 0u) + (use_str ? blk : 0u) + (use_pred ? blk : 0u) + (use_rp ? vb : 0u) +
                          (fk >= 0 ? vbo : 0u);
         uintptr_t bad = (uintptr_t)g_reg | (uintptr_t)g_str | (uintptr_t)g_pred;
@@ -448,28 +449,16 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     }
     // scales of the actor's node (16-bit arenas), loaded while the copies fly
     float kr = 0.0f, kp = 0.0f, sscale = 0.0f;
-    if (FMT != kDevF32 && loff < 0) {
+    if (FMT != kDevF32 && loff < 0 && mine) {
         kr = ar.rscale[a][it.sidx] / 32767.0f;
         if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
-        if (mine) sscale = ar.sscale[a][it.sidx];
+        sscale = ar.sscale[a][it.sidx];
     }
     if (!wait_staged(d, bar, &s_flag)) return;
 
     float sig[kSKA];
     double ftotal = 0.0;
     if (fk >= 0) {
-        if (a == o) {  // the opponent folds with probability sigma_o[fk]
-            for (int j = threadIdx.x; j < nho; j += kSThreads) {
-                s_node_sigma<FMT>(d, loff, a, j, EVAL ? 1 : 0, b_reg, use_pred ? b_pred : nullptr, b_str, kr, kp, na,
-                                  sig);
-                float sf = 0.0f;
-#pragma unroll
-                for (int k = 0; k < kSKA; k++)
-                    if (k == fk) sf = sig[k];
-                ro[j] = ro[j] * sf;
-            }
-            __syncthreads();
-        }
         ftotal = s_fold_sums(d, o, ro, s_S, s_dred);
         // the fold child's values go where a staged child's cfv would be
         // (fold_value of cfr_kernels.cuh with the hand's cards and same combo

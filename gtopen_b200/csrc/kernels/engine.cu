@@ -845,7 +845,7 @@ double GpuEngine::iter_bytes() const {
 }
 
 uint64_t estimate_vram(const Spot& spot) {  // same role as game.rs:365-373, for this engine's layout
-    Plan P = build_plan(spot, true, kFuseAll);
+    Plan P = build_plan(spot, true, kFuseFolds);  // the default (staged) engine's plan
     uint64_t b = P.n_cslots * (uint64_t)P.nh_max * 4 + P.n_rslots[0] * (uint64_t)P.nh[0] * 4 +
                  P.n_rslots[1] * (uint64_t)P.nh[1] * 4;
     b += (P.arena_len[0] + P.arena_len[1]) * 2 * 4;
