@@ -675,21 +675,21 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode
 
 // ------------------------------------------------- batched showdowns
 // One CTA per batch of up to kShowBatch showdowns of one level that share a
-// river slot: the slot's tables (opponent strength order, per-card position
-// lists, the traverser's rank entries and blocked hands) and the traverser's
-// same-combo map are loaded into shared memory once, and the showdowns'
-// opponent reach vectors stream through two bulk-copy buffers.
-struct ShowTab {  // shared-memory copies of one slot's tables
-    const uint16_t* sidx;  // m opponent hands, ascending strength
-    const uint32_t* coff;  // 53 card-list offsets relative to the slot's first entry
-    const uint16_t* bpos;  // per-card sorted positions (ne entries)
-    const RankEntry* rank;  // mp entries
-    const uint16_t* zero;  // nz blocked traverser hands
-    const uint32_t* same;  // traverser same-combo map (nh entries)
+// river slot: the slot's opponent strength order and per-card position lists
+// are loaded into shared memory once (the rank entries are read in place and
+// stay in L1 across the batch), and the showdowns' opponent reach vectors
+// stream through two bulk-copy buffers.
+struct ShowTab {  // one slot's tables: shared-memory copies, or HBM for the last three
+    const uint16_t* sidx;  // m opponent hands, ascending strength (shared)
+    const uint32_t* coff;  // 53 card-list offsets relative to the slot's first entry (shared)
+    const uint16_t* bpos;  // per-card sorted positions, ne entries (shared)
+    const RankEntry* rank;  // mp entries (global, L1-resident across the batch)
+    const uint16_t* zero;  // nz blocked traverser hands (global)
+    const uint32_t* same;  // traverser same-combo map, nh entries (global)
     int m, mp, nz;
 };
 struct ShowTabLayout {  // byte offsets of the tables inside the table region
-    unsigned sidx, coff, bpos, rank, zero, same, total;
+    unsigned sidx, coff, bpos, total;
 };
 __host__ __device__ inline unsigned r16u(unsigned b) { return (b + 15u) & ~15u; }
 __host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad) {
@@ -700,12 +700,6 @@ __host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad) {
     L.coff = o;
     o += r16u(53u * 4u);
     L.bpos = o;
-    o += r16u(4u * nh_pad);
-    L.rank = o;
-    o += r16u(16u * nh_pad);
-    L.zero = o;
-    o += r16u(2u * nh_pad);
-    L.same = o;
     o += r16u(4u * nh_pad);
     L.total = o;
     return L;
@@ -725,23 +719,18 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
     uint16_t* t_sidx = (uint16_t*)(tabs + TL.sidx);
     uint32_t* t_coff = (uint32_t*)(tabs + TL.coff);
     uint16_t* t_bpos = (uint16_t*)(tabs + TL.bpos);
-    RankEntry* t_rank = (RankEntry*)(tabs + TL.rank);
-    uint16_t* t_zero = (uint16_t*)(tabs + TL.zero);
-    uint32_t* t_same = (uint32_t*)(tabs + TL.same);
     const uint16_t* g_sidx = d.sorted_idx[o] + d.sorted_off[o][slot];
     for (int k = threadIdx.x; k < tb.m; k += blockDim.x) t_sidx[k] = g_sidx[k];
     if (threadIdx.x < 53) t_coff[threadIdx.x] = coff_g[threadIdx.x] - c0;
     for (uint32_t k = threadIdx.x; k < ne; k += blockDim.x) t_bpos[k] = d.ccard_pos[o][c0 + k];
-    const RankEntry* g_rank = d.rank[p] + d.rank_off[p][slot];
-    for (int k = threadIdx.x; k < tb.mp; k += blockDim.x) t_rank[k] = g_rank[k];
-    for (int k = threadIdx.x; k < tb.nz; k += blockDim.x) t_zero[k] = d.zero_idx[p][z0 + k];
-    for (int k = threadIdx.x; k < d.nh[p]; k += blockDim.x) t_same[k] = d.same[p][k];
     tb.sidx = t_sidx;
     tb.coff = t_coff;
     tb.bpos = t_bpos;
-    tb.rank = t_rank;
-    tb.zero = t_zero;
-    tb.same = t_same;
+    // read in place (L1-resident across the batch): keeps the CTA's shared
+    // memory small, so more batches run per SM
+    tb.rank = d.rank[p] + d.rank_off[p][slot];
+    tb.zero = d.zero_idx[p] + z0;
+    tb.same = d.same[p];
 }
 
 // Showdown CTAs have NT threads: 256 for large hand lists, 128 for small ones.
