@@ -736,31 +736,33 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
 // Showdown CTAs have NT threads: 256 for large hand lists, 128 for small ones.
 
 // One showdown evaluated by the CTA (game.rs:501-577 with the rank tables):
-// R = opponent reach in strength order, P = its exclusive prefix (each
-// thread sums a contiguous chunk, then a two-level shuffle scan), Q = per-card
+// R = opponent reach in strength order; then, at the same time, Q = per-card
 // prefixes (threads 0..51 each run one card's list in strength order, as the
-// reference's running card sums do), then the rank entries.
+// reference's running card sums do) and P = R's exclusive prefix (threads
+// 64..NT-1: contiguous chunks, a shuffle scan, the warp totals); then the rank
+// entries.
 template <int NT>
 __device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, float lose, float tie, float* out,
                              float* R, double* P, double* Q, double* S, double* s_w) {
+    constexpr int kPT = NT - 64;  // P threads
     const int m = tb.m;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < m; k += NT) R[k] = ro[tb.sidx[k]];
     __syncthreads();
-    // P
-    const int chunk = (m + NT - 1) / NT;
-    const int lo = min((int)threadIdx.x * chunk, m), hi = min(lo + chunk, m);
-    double local = 0.0;
-    for (int k = lo; k < hi; k++) local += (double)R[k];
-    double incl = local;
+    const int pt = (int)threadIdx.x - 64, pw = warp - 2;
+    const int chunk = (m + kPT - 1) / kPT;
+    const int lo = pt >= 0 ? min(pt * chunk, m) : 0, hi = pt >= 0 ? min(lo + chunk, m) : 0;
+    double local = 0.0, incl = 0.0;
+    if (pt >= 0) {
+        for (int k = lo; k < hi; k++) local += (double)R[k];
+        incl = local;
 #pragma unroll
-    for (int x = 1; x < 32; x <<= 1) {
-        const double y = __shfl_up_sync(0xffffffffu, incl, x);
-        if (lane >= x) incl += y;
-    }
-    if (lane == 31) s_w[warp] = incl;
-    // Q (threads 0..51), independent of P
-    if (threadIdx.x < 52) {
+        for (int x = 1; x < 32; x <<= 1) {
+            const double y = __shfl_up_sync(0xffffffffu, incl, x);
+            if (lane >= x) incl += y;
+        }
+        if (lane == 31) s_w[pw] = incl;
+    } else if (threadIdx.x < 52) {
         const int c = threadIdx.x;
         const uint32_t b = tb.coff[c], e = tb.coff[c + 1];
         double q = 0.0;
@@ -783,16 +785,18 @@ __device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, floa
         S[c] = q;
     }
     __syncthreads();
-    double wbase = 0.0;
+    if (pt >= 0) {
+        double wbase = 0.0;
 #pragma unroll
-    for (int k = 0; k < (NT / 32); k++)
-        if (k < warp) wbase += s_w[k];
-    double run = wbase + (incl - local);
-    for (int k = lo; k < hi; k++) {
-        P[k] = run;
-        run += (double)R[k];
+        for (int k = 0; k < kPT / 32; k++)
+            if (k < pw) wbase += s_w[k];
+        double run = wbase + (incl - local);
+        for (int k = lo; k < hi; k++) {
+            P[k] = run;
+            run += (double)R[k];
+        }
+        if (threadIdx.x == NT - 1) P[m] = run;
     }
-    if (threadIdx.x == NT - 1) P[m] = run;
     __syncthreads();
     const double total = P[m];
     for (int k = threadIdx.x; k < tb.mp; k += NT) {
