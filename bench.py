@@ -150,6 +150,15 @@ def barrier(world):
         dist.barrier()
 
 
+# --storage: compressed = i16/u16 host and device arenas (the reference CLI
+# default); f32; fp8 = f32 host arenas, FP8 E4M3 device arenas (precision study)
+HOST_STORAGE = {"compressed": "compressed", "f32": "f32", "fp8": "f32"}
+DEVICE_FORMAT = {"compressed": None, "f32": None, "fp8": "fp8"}
+DTYPE = {"compressed": "i16", "f32": "f32", "fp8": "fp8_e4m3"}
+ARENA_DESC = {"compressed": "i16/u16 per-node scale", "f32": "f32", "fp8": "FP8 E4M3 per-node scale"}
+HOST_BYTES = {"compressed": 2, "f32": 4, "fp8": 4}
+
+
 def cpu_baseline(cfg, storage, steps, threads=None):
     """The oracle (reference CPU engine restated, pruning on) on the host cores."""
     from oracle import pyoracle as po
@@ -158,7 +167,8 @@ def cpu_baseline(cfg, storage, steps, threads=None):
     t0 = time.perf_counter()
     spot = po.Spot(cfg)
     build_s = time.perf_counter() - t0
-    sv = po.Solver(spot, compressed=storage != "f32", algo="dcfr", use_iso=True, prune=True)
+    sv = po.Solver(spot, compressed=storage == "compressed", fp8=storage == "fp8", algo="dcfr", use_iso=True,
+                   prune=True)
     times = []
     for _ in range(steps):
         t = time.perf_counter()
@@ -181,7 +191,7 @@ def run_reference(args, world, rank):
         "impl": "reference", "metric": "CFR iterations/s (time-to-0.3%-pot exploitability & HBM GB/s vs peak)",
         "value": value, "unit": "iter/s", "n_gpus": args.gpus, "steps": len(timed), "warmup": w,
         "ms_per_step": 1000.0 * total / len(timed), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "i16" if args.storage != "f32" else "f32", "data": "synthetic (seeded spot)",
+        "vs_baseline": None, "dtype": DTYPE[args.storage], "data": "synthetic (seeded spot)",
         "config": workload_config(args, cfg),
         "cpu_baseline": {"value": value, "unit": "iter/s", "cores": r["cores"], "kind": "port",
                          "sample": "%d full DCFR iterations of the workload on the CPU oracle "
@@ -199,7 +209,7 @@ def workload_config(args, cfg):
                          "turn": "turn precision study: 4-card board seed 2, top 50% each, pot 100 stack 300",
                          "river": "river HU: 5-card board seed 1, all 1081 combos each side, pot 100 stack 400",
                          "bench_spot": "reference bench_spot.json (Ks7h2d, 257 v 319)"}[args.workload],
-            "board": cfg["board"], "arenas": "i16/u16 per-node scale" if args.storage != "f32" else "f32",
+            "board": cfg["board"], "arenas": ARENA_DESC[args.storage],
             "algo": "DCFR alpha 1.5 beta 0 gamma 2, alternating", "l2": "inputs larger than L2 (arenas GB-sized)",
             "parallelism": "replica per GPU (weak scaling)", "engine": getattr(args, "engine", "fused")}
 
@@ -210,9 +220,9 @@ def run_ours(args, world, rank, local):
     cfg = make_config(args.workload)
     t0 = time.perf_counter()
     spot = g.Spot(cfg)
-    host = g.Solver(spot, storage=args.storage, algo="dcfr", use_iso=True)
+    host = g.Solver(spot, storage=HOST_STORAGE[args.storage], algo="dcfr", use_iso=True)
     build_s = time.perf_counter() - t0
-    gpu = g.GpuSolver(host, engine=args.engine)
+    gpu = g.GpuSolver(host, device_format=DEVICE_FORMAT[args.storage], engine=args.engine)
     info = gpu.info()
     gpu.iterate(args.warmup)
     gpu.synchronize()
@@ -241,7 +251,7 @@ def run_ours(args, world, rank, local):
     if not args.no_e2e:
         barrier(world)
         t = time.perf_counter()
-        gpu2 = g.GpuSolver(host, engine=args.engine)
+        gpu2 = g.GpuSolver(host, device_format=DEVICE_FORMAT[args.storage], engine=args.engine)
         t_new = time.perf_counter()
         gpu2.iterate(args.steps)
         gpu2.synchronize()
@@ -255,7 +265,7 @@ def run_ours(args, world, rank, local):
         split = {"new_s": t_new - t, "iterate_s": t_it - t_new, "exploitability_s": t_ex - t_it,
                  "sync_to_cpu_s": t_end - t_ex}
         dt_max = allmax(dt, world)
-        b = 2 if args.storage != "f32" else 4
+        b = HOST_BYTES[args.storage]
         arena_bytes = 2 * (spot.data_size[0] + spot.data_size[1]) * b
         e2e = {"value": world * args.steps / dt_max, "unit": "iter/s",
                "h2d_bytes_per_step": int(arena_bytes / args.steps),
@@ -283,7 +293,7 @@ def run_ours(args, world, rank, local):
         "metric": "CFR iterations/s (time-to-0.3%-pot exploitability & HBM GB/s vs peak)",
         "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "i16" if args.storage != "f32" else "f32", "data": "synthetic (seeded spot)",
+        "dtype": DTYPE[args.storage], "data": "synthetic (seeded spot)",
         "config": workload_config(args, cfg),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
@@ -307,9 +317,9 @@ def run_ours(args, world, rank, local):
 
 def time_to_target(g, cfg, args):
     spot = g.Spot(cfg)
-    host = g.Solver(spot, storage=args.storage, algo="dcfr", use_iso=True)
+    host = g.Solver(spot, storage=HOST_STORAGE[args.storage], algo="dcfr", use_iso=True)
     t = time.perf_counter()
-    gpu = g.GpuSolver(host, engine=args.engine)
+    gpu = g.GpuSolver(host, device_format=DEVICE_FORMAT[args.storage], engine=args.engine)
     pot = cfg["tree"]["starting_pot"]
     pct = None
     while gpu.iteration < args.ttt_max:
@@ -332,7 +342,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="flop", choices=["flop", "flop_narrow", "turn", "river", "bench_spot"])
-    ap.add_argument("--storage", default="compressed", choices=["compressed", "f32"])
+    ap.add_argument("--storage", default="compressed", choices=["compressed", "f32", "fp8"])
     ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")

@@ -268,7 +268,7 @@ int gtob_load(const char* path, int storage, gtob_solver** out) {
 
 int gtob_gpu_new(const gtob_solver* v, int fmt, gtob_gpu** out) { return gtob_gpu_new_ex(v, fmt, GTOB_ENGINE_STAGED, out); }
 int gtob_gpu_new_ex(const gtob_solver* v, int fmt, int engine, gtob_gpu** out) {
-    REQUIRE(v && out && fmt >= -1 && fmt <= 1 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+    REQUIRE(v && out && fmt >= -1 && fmt <= 2 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
     *out = nullptr;
     API_BEGIN
     *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt, engine)};

@@ -9,6 +9,7 @@
 // the reference GPU kernels (gpu/kernels.cu:117-266) to halve the shared
 // memory and instruction count of the scans.
 #pragma once
+#include <cuda_fp8.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -18,7 +19,7 @@
 
 namespace gtob {
 
-enum ArenaFormatDev { kDevF32 = 0, kDevI16 = 1 };
+enum ArenaFormatDev { kDevF32 = 0, kDevI16 = 1, kDevFP8 = 2 };
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
@@ -77,6 +78,15 @@ struct Arenas {
 };
 
 // ----------------------------------------------------------- small helpers
+// FP8 E4M3 arena values (the precision-study format): cvt with satfinite --
+// round to nearest even, saturate to +-448 -- and the exact widening back.
+__device__ __forceinline__ uint8_t f32_to_e4m3(float x) {
+    return (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3);
+}
+__device__ __forceinline__ float e4m3_to_f32(uint8_t q) {
+    return __half2float(__half(__nv_cvt_fp8_to_halfraw((__nv_fp8_storage_t)q, __NV_E4M3)));
+}
+
 // Rust `as i16` / `as u16` after round_ties_even (store.rs:178, 192): round to
 // nearest even, saturate to the type's range, NaN -> 0.  One cvt.rni.sat each.
 __device__ __forceinline__ int16_t sat_i16(float x) {
@@ -1082,6 +1092,35 @@ __global__ void __launch_bounds__(kThreads) k_encode(const float* host, void* de
         else ((int16_t*)dev)[di] = ok ? sat_i16(v * kq) : (int16_t)0;
     }
     if (threadIdx.x == 0) scale[x.sidx] = ok ? m : 0.0f;
+}
+// The FP8 twins of k_encode / k_decode_to_host: v * (448 / max) per node and
+// back, max kept as the node's scale (strategy sums clamped at 0).
+__global__ void __launch_bounds__(kThreads) k_encode_fp8(const float* host, uint8_t* dev, float* scale, const XNode* xs,
+                                                         int nh, int is_unsigned) {
+    __shared__ float s_max[kWarps];
+    const XNode x = xs[blockIdx.x];
+    const size_t n = (size_t)x.na * nh;
+    float m = 0.0f;
+    for (size_t t = threadIdx.x; t < n; t += blockDim.x) {
+        const float v = host[x.host_off + t];
+        m = is_unsigned ? fmaxf(m, v) : fmaxf(m, fabsf(v));
+    }
+    m = block_max(m, s_max);
+    const bool ok = m > 0.0f && isfinite(m);
+    const float kq = ok ? 448.0f / m : 0.0f;
+    for (size_t t = threadIdx.x; t < n; t += blockDim.x) {
+        const size_t k = t / nh, i = t % nh;
+        const float v = host[x.host_off + t];
+        dev[x.dev_off + i * x.na + k] = ok ? f32_to_e4m3(is_unsigned ? fmaxf(v, 0.0f) * kq : v * kq) : (uint8_t)0;
+    }
+    if (threadIdx.x == 0) scale[x.sidx] = ok ? m : 0.0f;
+}
+__global__ void k_decode_fp8_to_host(const uint8_t* dev, const float* scale, float* host, const XNode* xs, int nh) {
+    const XNode x = xs[blockIdx.x];
+    const float kq = scale[x.sidx] / 448.0f;
+    for (int i = threadIdx.x; i < nh; i += blockDim.x)
+        for (uint32_t k = 0; k < x.na; k++)
+            host[x.host_off + (size_t)k * nh + i] = e4m3_to_f32(dev[x.dev_off + (size_t)i * x.na + k]) * kq;
 }
 
 }  // namespace gtob

@@ -122,6 +122,19 @@ __device__ __forceinline__ void s_regret_sigma(const void* reg, const void* pred
                 sig[k] = v;
                 sum += fmaxf(v, 0.0f);
             }
+    } else if (FMT == kDevFP8) {
+        // FP8: regret matching on the stored values before scaling (one scale
+        // per node cancels); PCFR+ predictions decoded with their scales
+        const uint8_t* q = (const uint8_t*)reg + base;
+        const uint8_t* qp = (const uint8_t*)pred;
+#pragma unroll
+        for (int k = 0; k < kSKA; k++)
+            if (k < na) {
+                const float v = qp ? fmaxf(e4m3_to_f32(q[k]), 0.0f) * kr + e4m3_to_f32(qp[base + k]) * kp
+                                   : e4m3_to_f32(q[k]);
+                sig[k] = v;
+                sum += fmaxf(v, 0.0f);
+            }
     } else {
         const int16_t* q = (const int16_t*)reg + base;
         if (pred) {
@@ -170,14 +183,14 @@ __device__ __forceinline__ void s_regret_sigma(const void* reg, const void* pred
 template <int FMT>
 __device__ __forceinline__ void s_average_sigma(const void* str, int na, int i, float (&sig)[kSKA]) {
     const int base = i * na;
-    if (FMT == kDevF32) {
-        const float* s = (const float*)str + base;
+    if (FMT == kDevF32 || FMT == kDevFP8) {  // FP8: the f32 rule on the stored values (the scale cancels)
         double sum = 0.0;
         float v[kSKA];
 #pragma unroll
         for (int k = 0; k < kSKA; k++)
             if (k < na) {
-                v[k] = fmaxf(s[k], 0.0f);
+                v[k] = FMT == kDevF32 ? fmaxf(((const float*)str)[base + k], 0.0f)
+                                      : fmaxf(e4m3_to_f32(((const uint8_t*)str)[base + k]), 0.0f);
                 sum += (double)v[k];
             }
         if (sum > 1e-12) {
@@ -308,6 +321,31 @@ struct SLayout {
     __host__ __device__ unsigned cv() const { return o_cv; }
 };
 
+// The two quantised arena formats: 16-bit (store.rs: i16 regrets, u16
+// strategy sums) and FP8 E4M3 (both signed 8-bit), each with a per-node scale
+// = the block's max magnitude, stored as value * (kR or kS) / scale.
+template <int FMT>
+struct QT {
+    using R = int16_t;
+    using S = uint16_t;
+    static constexpr float kR = 32767.0f, kS = 65535.0f;
+    __device__ static float dr(R q) { return (float)q; }
+    __device__ static float ds(S q) { return (float)q; }
+    __device__ static R er(float x) { return sat_i16(x); }
+    __device__ static S es(float x) { return sat_u16(x); }
+};
+template <>
+struct QT<kDevFP8> {
+    using R = uint8_t;
+    using S = uint8_t;
+    static constexpr float kR = 448.0f, kS = 448.0f;
+    __device__ static float dr(R q) { return e4m3_to_f32(q); }
+    __device__ static float ds(S q) { return e4m3_to_f32(q); }
+    __device__ static R er(float x) { return f32_to_e4m3(x); }
+    __device__ static S es(float x) { return f32_to_e4m3(x); }
+};
+__host__ __device__ constexpr int fmt_bytes(int fmt) { return fmt == kDevF32 ? 4 : fmt == kDevFP8 ? 1 : 2; }
+
 // Down sweep, one node per CTA: staged sigma source and parent reach; child
 // reach vectors written with coalesced stores (cfr.rs:469-531 push-down).
 template <int FMT, int NA>
@@ -315,7 +353,7 @@ __device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, con
                                              unsigned char* sm, int& s_flag) {
     const int a = (int)it.actor, nh = d.nh[a];
     constexpr int na = NA;  // the node's action count, a compile-time constant in this instance
-    const int esz = FMT == kDevF32 ? 4 : 2;
+    const int esz = fmt_bytes(FMT);
     const SLayout L(d.nh_pad, esz, ar.pred[0] != nullptr, kSDown);
     uint64_t* bar = (uint64_t*)sm;
     unsigned char* b_reg = sm + L.reg();
@@ -346,8 +384,8 @@ __device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, con
     }
     float kr = 0.0f, kp = 0.0f;
     if (FMT != kDevF32 && mode == 0 && loff < 0) {
-        kr = ar.rscale[a][it.sidx] / 32767.0f;
-        if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
+        kr = ar.rscale[a][it.sidx] / QT<FMT>::kR;
+        if (has_pred) kp = ar.pscale[a][it.sidx] / QT<FMT>::kR;
     }
     if (!wait_staged(d, bar, &s_flag)) return;
     float sig[kSKA];
@@ -391,7 +429,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     float* s_red = us.red;
     const int a = (int)it.actor, o = 1 - p, nh = d.nh[p], nho = d.nh[o];
     constexpr int na = NA;  // the node's action count, a compile-time constant in this instance
-    const int esz = FMT == kDevF32 ? 4 : 2;
+    const int esz = fmt_bytes(FMT);
     const SLayout L(d.nh_pad, esz, ar.pred[0] != nullptr, MINE ? kSUpMine : kSUpOpp);
     uint64_t* bar = (uint64_t*)sm;
     unsigned char* b_reg = sm + L.reg();
@@ -450,8 +488,8 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     // scales of the actor's node (16-bit arenas), loaded while the copies fly
     float kr = 0.0f, kp = 0.0f, sscale = 0.0f;
     if (FMT != kDevF32 && loff < 0 && mine) {
-        kr = ar.rscale[a][it.sidx] / 32767.0f;
-        if (has_pred) kp = ar.pscale[a][it.sidx] / 32767.0f;
+        kr = ar.rscale[a][it.sidx] / QT<FMT>::kR;
+        if (has_pred) kp = ar.pscale[a][it.sidx] / QT<FMT>::kR;
         sscale = ar.sscale[a][it.sidx];
     }
     if (!wait_staged(d, bar, &s_flag)) return;
@@ -549,13 +587,14 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
         if (use_pred) store_block((unsigned char*)ar.pred[p] + it.aoff * esz, b_pred, blk);
         return;
     }
-    // 16-bit arenas (cfr.rs:350-407).
-    int16_t* RQ = (int16_t*)b_reg;
-    uint16_t* SQ = (uint16_t*)b_str;
-    int16_t* PQ = (int16_t*)b_pred;
-    const float kss = sscale / 65535.0f * ds;
+    // Quantised arenas (cfr.rs:350-407): 16-bit, or FP8 with the same steps.
+    using Q = QT<FMT == kDevFP8 ? kDevFP8 : kDevI16>;
+    const float kss = sscale / Q::kS * ds;
     float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
-    if (!use_pred) {
+    const bool one_pass = FMT == kDevI16 && !use_pred;
+    if (one_pass) {
+        int16_t* RQ = (int16_t*)b_reg;
+        uint16_t* SQ = (uint16_t*)b_str;
         // Pass 1 computes every entry's new regret and strategy sum and the
         // node's maxima, keeping the f32 values in place of what it consumed:
         // the new regret where the child's value was, the new strategy sum's
@@ -605,17 +644,21 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
                 }
         }
     }
-    // PCFR+ (predictions too): pass 1 finds the maxima, pass 2 recomputes
-    // from the unchanged staged quants and requantises in place.
-    for (int pass = use_pred ? 0 : 2; pass < 2; pass++) {
+    // Otherwise (PCFR+ predictions, or FP8, whose quants leave no room for
+    // the f32 values): pass 1 finds the maxima, pass 2 recomputes from the
+    // unchanged staged quants and requantises in place.
+    typename Q::R* RQ = (typename Q::R*)b_reg;
+    typename Q::S* SQ = (typename Q::S*)b_str;
+    typename Q::R* PQ = (typename Q::R*)b_pred;
+    for (int pass = one_pass ? 2 : 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
         if (pass == 1) {
             rmax = s_block_max(rmax, s_red);
             smax = s_block_max(smax, s_red + kSWarps);
             if (use_pred) pmax = s_block_max(pmax, s_red + 2 * kSWarps);
-            rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
-            sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
-            pk = (pmax > 0.0f && isfinite(pmax)) ? 32767.0f / pmax : 0.0f;
+            rk = (rmax > 0.0f && isfinite(rmax)) ? Q::kR / rmax : 0.0f;
+            sk = (smax > 0.0f && isfinite(smax)) ? Q::kS / smax : 0.0f;
+            pk = (pmax > 0.0f && isfinite(pmax)) ? Q::kR / pmax : 0.0f;
         }
         for (int i = threadIdx.x; i < nh; i += kSThreads) {
             s_regret_sigma<FMT>(b_reg, predp, kr, kp, na, i, sig);
@@ -631,17 +674,17 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
 #pragma unroll
             for (int k = 0; k < kSKA; k++)
                 if (k < na) {
-                    const int16_t qv = RQ[b + k];
-                    const float nr = (float)qv * kr * (qv > 0 ? pos : neg) + (v[k] - o_);
-                    const float ns = (float)SQ[b + k] * kss + r_p * sig[k];
+                    const float dv = Q::dr(RQ[b + k]);  // the discount follows the stored sign
+                    const float nr = dv * kr * (dv > 0.0f ? pos : neg) + (v[k] - o_);
+                    const float ns = Q::ds(SQ[b + k]) * kss + r_p * sig[k];
                     if (pass == 0) {
                         rmax = fmaxf(rmax, fabsf(nr));
                         smax = fmaxf(smax, ns);
                         if (use_pred) pmax = fmaxf(pmax, fabsf(v[k] - o_));
                     } else {
-                        RQ[b + k] = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
-                        SQ[b + k] = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
-                        if (use_pred) PQ[b + k] = pk > 0.0f ? sat_i16((v[k] - o_) * pk) : (int16_t)0;
+                        RQ[b + k] = rk > 0.0f ? Q::er(nr * rk) : (typename Q::R)0;
+                        SQ[b + k] = sk > 0.0f ? Q::es(fmaxf(ns, 0.0f) * sk) : (typename Q::S)0;
+                        if (use_pred) PQ[b + k] = pk > 0.0f ? Q::er((v[k] - o_) * pk) : (typename Q::R)0;
                     }
                 }
             if (pass == 1) out[i] = o_;

@@ -233,6 +233,9 @@ struct EngineImpl {
             if (fmt == kFmtF32) {
                 staged_up<kDevF32, true>(mine, p, eval);
                 staged_up<kDevF32, false>(opp, p, eval);
+            } else if (fmt == kFmtFP8) {
+                staged_up<kDevFP8, true>(mine, p, eval);
+                staged_up<kDevFP8, false>(opp, p, eval);
             } else {
                 staged_up<kDevI16, true>(mine, p, eval);
                 staged_up<kDevI16, false>(opp, p, eval);
@@ -261,6 +264,10 @@ struct EngineImpl {
         }
     }
     void launch_down_action(const Span& sa, int mode) {
+        if (fmt == kFmtFP8) {  // the staged engine only
+            ks_down<kDevFP8><<<sa.count, kSThreads, st_down_smem, stream>>>(d, ar, snodes + sa.start, mode);
+            return;
+        }
         if (fmt == kFmtF32) {
             if (wide) down_action<kDevF32, 32>(sa, mode);
             else down_action<kDevF32, 8>(sa, mode);
@@ -269,6 +276,7 @@ struct EngineImpl {
             else down_action<kDevI16, 8>(sa, mode);
         }
     }
+
     void launch_chance(const Span& sc, int p) {
         // runout showdowns: f32 sums in the fused engine, f64 in the plain one
         if (plan.fused && !term64) k_chance<float><<<sc.count, kThreads, chance_smem, stream>>>(d, chance + sc.start, p);
@@ -391,13 +399,15 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     E.algo = host.algo;
     E.pcfr = host.algo == kPcfrPlus;
     E.fmt = fmt < 0 ? (host.storage == kStoreF32 ? kFmtF32 : kFmtI16) : fmt;
-    if (E.fmt != kFmtF32 && E.fmt != kFmtI16) throw Error("unknown device arena format");
+    if (E.fmt != kFmtF32 && E.fmt != kFmtI16 && E.fmt != kFmtFP8) throw Error("unknown device arena format");
+    if (E.fmt == kFmtFP8 && engine != kEngineStaged) throw Error("FP8 arenas run on the staged engine only");
     E.iteration = host.iteration;
     E.plan = build_plan(sp, host.use_iso, fuse);
     const Plan& P = E.plan;
     if (P.max_children > 32u) throw Error("an action node with more than 32 actions is not supported on the GPU");
     E.wide = P.max_children > 8u;
     E.staged = engine == kEngineStaged && P.max_children <= (uint32_t)kSKA;
+    if (E.fmt == kFmtFP8 && !E.staged) throw Error("FP8 arenas need nodes of at most 4 actions (the staged kernels)");
     if (P.nh_max > kThreads * kMaxHpt) throw Error("more than 1536 hands per player is not supported on the GPU");
     CK(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
     size_t& B = E.bytes;
@@ -505,7 +515,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
                 for (uint32_t k = P.hcard_off[q][c], j = 0; k < P.hcard_off[q][c + 1]; k++, j++) h52[c * 52 + j] = P.hcard_idx[q][k];
             d.hcard52[q] = dupload(h52, O, &B);
         }
-        const int esz = E.fmt == kFmtF32 ? 4 : 2;
+        const int esz = fmt_bytes(E.fmt);
         E.st_mine_smem = SLayout(d.nh_pad, esz, E.pcfr, kSUpMine).total;
         E.st_opp_smem = SLayout(d.nh_pad, esz, E.pcfr, kSUpOpp).total;
         E.st_down_smem = SLayout(d.nh_pad, esz, E.pcfr, kSDown).total;
@@ -536,13 +546,13 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     EngineImpl::set_warp_smem<kDevI16, 32>(E.warp_smem);
 
     // arenas
-    const size_t esz = E.fmt == kFmtF32 ? 4 : 2;
+    const size_t esz = (size_t)fmt_bytes(E.fmt);
     for (int q = 0; q < 2; q++) {
         const size_t len = P.arena_len[q];
         E.ar.reg[q] = dalloc(len * esz, O, &B);
         E.ar.str[q] = dalloc(len * esz, O, &B);
         E.ar.pred[q] = E.pcfr ? dalloc(len * esz, O, &B) : nullptr;
-        if (E.fmt == kFmtI16) {
+        if (E.fmt != kFmtF32) {
             E.ar.rscale[q] = (float*)dalloc(std::max<uint64_t>(P.n_anodes[q], 1) * 4, O, &B);
             E.ar.sscale[q] = (float*)dalloc(std::max<uint64_t>(P.n_anodes[q], 1) * 4, O, &B);
             E.ar.pscale[q] = E.pcfr ? (float*)dalloc(std::max<uint64_t>(P.n_anodes[q], 1) * 4, O, &B) : nullptr;
@@ -589,7 +599,11 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
                 k_to_dev<float><<<nb, kThreads, 0, E.stream>>>(E.staging, (float*)dst, E.xnodes[q], nh);
             } else {
                 float* dsc = which == kRegrets ? E.ar.rscale[q] : which == kStrategy ? E.ar.sscale[q] : E.ar.pscale[q];
-                k_encode<<<nb, kThreads, 0, E.stream>>>(E.staging, dst, dsc, E.xnodes[q], nh, which == kStrategy);
+                if (E.fmt == kFmtFP8)
+                    k_encode_fp8<<<nb, kThreads, 0, E.stream>>>(E.staging, (uint8_t*)dst, dsc, E.xnodes[q], nh,
+                                                                 which == kStrategy);
+                else
+                    k_encode<<<nb, kThreads, 0, E.stream>>>(E.staging, dst, dsc, E.xnodes[q], nh, which == kStrategy);
             }
             CK(cudaGetLastError());
             CK(cudaStreamSynchronize(E.stream));
@@ -684,6 +698,10 @@ void GpuEngine::export_arena(int which, int p, float* out) {
     if (nb && src) {
         if (E.fmt == kFmtF32) {
             k_to_host<float><<<nb, kThreads, 0, E.stream>>>((const float*)src, E.staging, E.xnodes[p], E.plan.nh[p]);
+        } else if (E.fmt == kFmtFP8) {
+            const float* sc = which == kRegrets ? E.ar.rscale[p] : which == kStrategy ? E.ar.sscale[p] : E.ar.pscale[p];
+            k_decode_fp8_to_host<<<nb, kThreads, 0, E.stream>>>((const uint8_t*)src, sc, E.staging, E.xnodes[p],
+                                                                 E.plan.nh[p]);
         } else if (which == kStrategy) {
             k_decode_to_host<uint16_t><<<nb, kThreads, 0, E.stream>>>((const uint16_t*)src, E.ar.sscale[p], E.staging,
                                                                        E.xnodes[p], E.plan.nh[p], 65535.0f);
@@ -717,6 +735,13 @@ __global__ void k_node_to_scratch(const T* dev, const float* scale, float div, f
         const T v = dev[x.dev_off + (size_t)i * x.na + k];
         dst[(size_t)k * nh + i] = scale ? (float)v * kq : (float)v;
     }
+}
+// FP8 arenas: e4m3 value * (scale / 448), as k_decode_fp8_to_host.
+__global__ void k_node_fp8_to_scratch(const uint8_t* dev, const float* scale, float* dst, XNode x, int nh) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nh) return;
+    const float kq = scale[x.sidx] / 448.0f;
+    for (uint32_t k = 0; k < x.na; k++) dst[(size_t)k * nh + i] = e4m3_to_f32(dev[x.dev_off + (size_t)i * x.na + k]) * kq;
 }
 constexpr int kMaxDevices = 64;
 
@@ -761,6 +786,9 @@ size_t GpuEngine::read_node_static(int which, uint32_t node, float* out, size_t 
     const unsigned grid = (unsigned)((nh + kThreads - 1) / kThreads);
     if (E.fmt == kFmtF32) {
         k_node_to_scratch<float><<<grid, kThreads, 0, E.stream>>>((const float*)src, nullptr, 1.0f, scratch, x, nh);
+    } else if (E.fmt == kFmtFP8) {
+        const float* sc = which == kRegrets ? E.ar.rscale[p] : which == kStrategy ? E.ar.sscale[p] : E.ar.pscale[p];
+        k_node_fp8_to_scratch<<<grid, kThreads, 0, E.stream>>>((const uint8_t*)src, sc, scratch, x, nh);
     } else {
         const float* sc = which == kRegrets ? E.ar.rscale[p] : which == kStrategy ? E.ar.sscale[p] : E.ar.pscale[p];
         if (which == kStrategy)
@@ -837,7 +865,7 @@ double GpuEngine::iter_bytes() const {
     // down sweeps, read+write of the traverser's regrets and sums, one
     // opponent-reach read and one cfv write per terminal per traversal.
     const Plan& P = d_->plan;
-    const double b = d_->fmt == kFmtF32 ? 4.0 : 2.0;
+    const double b = (double)fmt_bytes(d_->fmt);
     const double D = (double)(P.visited_action_elems[0] + P.visited_action_elems[1]);
     double bytes = 2.0 * D * b + 2.0 * D * (b + b) + 2.0 * (double)P.visited_terminals * (P.nh[0] + P.nh[1]) * 4.0;
     if (d_->fmt != kFmtF32) bytes += 8.0 * (double)(P.n_anodes[0] + P.n_anodes[1]) * 2.0;

@@ -11,7 +11,7 @@
 
 namespace gtob {
 
-enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1 };
+enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1, kFmtFP8 = 2 };  // FP8: E4M3 with a per-node scale
 constexpr size_t kNodeScratchElems = 16384;  // 64 KiB of f32: the read_node_static limit
 enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2, kEngineWarp = 3, kEngineStaged = 4 };
 

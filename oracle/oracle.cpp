@@ -1040,28 +1040,83 @@ static void decode_u16(const uint16_t* q, int n, float scale, float* out) {  // 
     for (int i = 0; i < n; i++) out[i] = (float)q[i] * k;
 }
 
-// One arena (store.rs:79-150): f32, or 16-bit quants with a per-node scale.
+// ------------------------------------------------ FP8 (E4M3) arenas
+// Not in the reference: the 8-bit arena format of the precision study.  OCP
+// FP8 E4M3: 1 sign bit, 4 exponent bits (bias 7), 3 mantissa bits, no
+// infinities, S.1111.111 is NaN, the largest finite value is 448.  Encoding
+// rounds to nearest, ties to even, and saturates to +-448 (the device's cvt
+// to e4m3 with satfinite).  A node's block is stored as v * (448 / max|v|)
+// with the max kept as the node's scale, like the 16-bit format.
+static uint8_t f32_to_e4m3(float x) {
+    if (std::isnan(x)) return 0x7F;
+    const uint8_t sign = std::signbit(x) ? 0x80 : 0x00;
+    const float a = std::fabs(x);
+    if (a >= 448.0f) return sign | 0x7E;
+    if (a == 0.0f) return sign;
+    int e2 = 0;
+    std::frexp(a, &e2);
+    int E = e2 - 1;  // a in [2^E, 2^(E+1))
+    if (E < -6) {    // subnormals: m * 2^-9, m in 0..7; 8 is the smallest normal
+        const float m = std::nearbyint(a * 512.0f);
+        return m >= 8.0f ? (uint8_t)(sign | 0x08) : (uint8_t)(sign | (uint8_t)m);
+    }
+    float m = std::nearbyint(std::ldexp(a, 3 - E));  // (8 + M), exact scaling then RNE
+    if (m >= 16.0f) { m = 8.0f; E += 1; }
+    const int ef = E + 7;
+    if (ef > 15 || (ef == 15 && m > 14.0f)) return sign | 0x7E;
+    return (uint8_t)(sign | (ef << 3) | (int)(m - 8.0f));
+}
+static float e4m3_to_f32(uint8_t q) {
+    const int E = (q >> 3) & 15, M = q & 7;
+    float v;
+    if (E == 15 && M == 7) v = NAN;
+    else if (E == 0) v = std::ldexp((float)M, -9);
+    else v = std::ldexp((float)(8 + M), E - 10);
+    return (q & 0x80) ? -v : v;
+}
+static float quantize_fp8(const float* src, int n, float max, bool nonneg, uint8_t* dst) {
+    if (!(max > 0.0f && std::isfinite(max))) { std::fill(dst, dst + n, (uint8_t)0); return 0.0f; }
+    float k = 448.0f / max;
+    for (int i = 0; i < n; i++) dst[i] = f32_to_e4m3(nonneg ? std::fmax(src[i], 0.0f) * k : src[i] * k);
+    return max;
+}
+static float encode_fp8(const float* src, int n, bool nonneg, uint8_t* dst) {
+    float m = 0.0f;
+    for (int i = 0; i < n; i++) m = std::fmax(m, nonneg ? src[i] : std::fabs(src[i]));
+    return quantize_fp8(src, n, m, nonneg, dst);
+}
+static void decode_fp8(const uint8_t* q, int n, float scale, float* out) {
+    float k = scale / 448.0f;
+    for (int i = 0; i < n; i++) out[i] = e4m3_to_f32(q[i]) * k;
+}
+
+// One arena (store.rs:79-150): f32, or 16-bit quants with a per-node scale
+// (or, for the precision study, FP8 E4M3 with a per-node scale).
 struct Store {
-    int kind = 0;  // 0 f32, 1 i16, 2 u16
+    int kind = 0;  // 0 f32, 1 i16, 2 u16, 3 fp8 (signed), 4 fp8 (strategy sums, >= 0)
     std::vector<float> f;
     std::vector<int16_t> qi;
     std::vector<uint16_t> qu;
+    std::vector<uint8_t> q8;
     std::vector<float> scale;
     void init(int k, uint64_t len, size_t nodes) {
         kind = k;
         if (k == 0) f.assign(len, 0.0f);
         else if (k == 1) { qi.assign(len, 0); scale.assign(nodes, 0.0f); }
-        else { qu.assign(len, 0); scale.assign(nodes, 0.0f); }
+        else if (k == 2) { qu.assign(len, 0); scale.assign(nodes, 0.0f); }
+        else { q8.assign(len, 0); scale.assign(nodes, 0.0f); }
     }
     void read_f32(uint32_t node, uint64_t off, int n, float* out) const {
         if (kind == 0) std::memcpy(out, f.data() + off, sizeof(float) * n);
         else if (kind == 1) decode_i16(qi.data() + off, n, scale[node], out);
-        else decode_u16(qu.data() + off, n, scale[node], out);
+        else if (kind == 2) decode_u16(qu.data() + off, n, scale[node], out);
+        else decode_fp8(q8.data() + off, n, scale[node], out);
     }
     void write_f32(uint32_t node, uint64_t off, int n, const float* src) {
         if (kind == 0) std::memcpy(f.data() + off, src, sizeof(float) * n);
         else if (kind == 1) scale[node] = encode_i16(src, n, qi.data() + off);
-        else scale[node] = encode_u16(src, n, qu.data() + off);
+        else if (kind == 2) scale[node] = encode_u16(src, n, qu.data() + off);
+        else scale[node] = encode_fp8(src, n, kind == 4, q8.data() + off);
     }
 };
 
@@ -1126,7 +1181,8 @@ static void regret_match_inplace(float* sig, int na, int nh) {  // cfr.rs:923-94
 
 struct Solver {
     Spot* spot;
-    bool compressed;
+    bool compressed;  // 16-bit (mode 1) or FP8 (mode 2) arenas
+    int mode;         // 0 f32, 1 i16/u16, 2 fp8
     int algo;
     bool use_iso;
     bool prune;
@@ -1137,17 +1193,18 @@ struct Solver {
     std::map<uint32_t, std::vector<float>> locks;
     bool sym_dirty = false;
 
-    Solver(Spot* s, bool comp, int al, bool iso, bool pr) : spot(s), compressed(comp), algo(al), use_iso(iso), prune(pr) {
+    Solver(Spot* s, int storage_mode, int al, bool iso, bool pr)
+        : spot(s), compressed(storage_mode != 0), mode(storage_mode), algo(al), use_iso(iso), prune(pr) {
         size_t nn = s->tree.nodes.size();
         for (int p = 0; p < 2; p++) {
-            regrets[p].init(comp ? 1 : 0, s->tree.data_size[p], nn);
-            strat[p].init(comp ? 2 : 0, s->tree.data_size[p], nn);
+            regrets[p].init(mode == 0 ? 0 : mode == 1 ? 1 : 3, s->tree.data_size[p], nn);
+            strat[p].init(mode == 0 ? 0 : mode == 1 ? 2 : 4, s->tree.data_size[p], nn);
         }
     }
     void ensure_preds() {  // cfr.rs:157-168
         if (have_preds) return;
         size_t nn = spot->tree.nodes.size();
-        for (int p = 0; p < 2; p++) preds[p].init(compressed ? 1 : 0, spot->tree.data_size[p], nn);
+        for (int p = 0; p < 2; p++) preds[p].init(mode == 0 ? 0 : mode == 1 ? 1 : 3, spot->tree.data_size[p], nn);
         have_preds = true;
     }
     int nh(int p) const { return (int)spot->hands[p].size(); }
@@ -1177,6 +1234,20 @@ struct Solver {
             const float* r = R.f.data() + off;
             const float* pr = preds[p].f.data() + off;
             for (int i = 0; i < cnt; i++) sig[i] = std::fmax(r[i], 0.0f) + pr[i];
+            regret_match_inplace(sig, na, h);
+        } else if (R.kind == 3) {
+            // FP8: regret matching on the stored values before scaling (one
+            // scale per node: it cancels), predictions decoded for PCFR+
+            const uint8_t* qr = R.q8.data() + off;
+            if (!pc) {
+                for (int i = 0; i < cnt; i++) sig[i] = e4m3_to_f32(qr[i]);
+                regret_match_inplace(sig, na, h);
+                return;
+            }
+            float kr = R.scale[idx] / 448.0f;
+            const uint8_t* qp = preds[p].q8.data() + off;
+            float kp = preds[p].scale[idx] / 448.0f;
+            for (int i = 0; i < cnt; i++) sig[i] = std::fmax(e4m3_to_f32(qr[i]), 0.0f) * kr + e4m3_to_f32(qp[i]) * kp;
             regret_match_inplace(sig, na, h);
         } else {
             if (!pc) { regret_match_q(R.qi.data() + off, na, h, sig); return; }
@@ -1209,6 +1280,43 @@ struct Solver {
                 float* P = preds[p].f.data() + off;
                 for (int a = 0; a < na; a++)
                     for (int i = 0; i < h; i++) P[a * h + i] = vals[a * h + i] - out[i];
+            }
+            return;
+        }
+        if (mode == 2) {  // FP8, the same steps as the 16-bit branch below
+            uint8_t* rq = regrets[p].q8.data() + off;
+            uint8_t* sq = strat[p].q8.data() + off;
+            float kr = regrets[p].scale[idx] / 448.0f;
+            float kss = strat[p].scale[idx] / 448.0f * d.strat;
+            std::vector<float> rb(cnt), sb(cnt);
+            float rmax = 0.0f, smax = 0.0f;
+            for (int a = 0; a < na; a++) {
+                for (int i = 0; i < h; i++) {
+                    int b = a * h + i;
+                    float dv = e4m3_to_f32(rq[b]);
+                    float dd = dv > 0.0f ? d.pos : d.neg;
+                    float nr = dv * kr * dd + (vals[b] - out[i]);
+                    rb[b] = nr;
+                    rmax = std::fmax(rmax, std::fabs(nr));
+                }
+                for (int i = 0; i < h; i++) {
+                    int b = a * h + i;
+                    float s = e4m3_to_f32(sq[b]) * kss + reach_p[i] * sig[b];
+                    sb[b] = s;
+                    smax = std::fmax(smax, s);
+                }
+            }
+            regrets[p].scale[idx] = quantize_fp8(rb.data(), cnt, rmax, false, rq);
+            strat[p].scale[idx] = quantize_fp8(sb.data(), cnt, smax, true, sq);
+            if (pc) {
+                float pmax = 0.0f;
+                for (int a = 0; a < na; a++)
+                    for (int i = 0; i < h; i++) {
+                        float delta = vals[a * h + i] - out[i];
+                        rb[a * h + i] = delta;
+                        pmax = std::fmax(pmax, std::fabs(delta));
+                    }
+                preds[p].scale[idx] = quantize_fp8(rb.data(), cnt, pmax, false, preds[p].q8.data() + off);
             }
             return;
         }
@@ -1375,6 +1483,19 @@ struct Solver {
                 for (int a = 0; a < na; a++) sum += (double)std::fmax(s[a * h + i], 0.0f);
                 if (sum > 1e-12) {
                     for (int a = 0; a < na; a++) sig[a * h + i] = (float)((double)std::fmax(s[a * h + i], 0.0f) / sum);
+                } else {
+                    float u = 1.0f / (float)na;
+                    for (int a = 0; a < na; a++) sig[a * h + i] = u;
+                }
+            }
+        } else if (S.kind == 4) {  // FP8: the f32 rule on the stored values (the scale cancels)
+            const uint8_t* q = S.q8.data() + n.data_offset;
+            for (int i = 0; i < h; i++) {
+                double sum = 0;
+                for (int a = 0; a < na; a++) sum += (double)std::fmax(e4m3_to_f32(q[a * h + i]), 0.0f);
+                if (sum > 1e-12) {
+                    for (int a = 0; a < na; a++)
+                        sig[a * h + i] = (float)((double)std::fmax(e4m3_to_f32(q[a * h + i]), 0.0f) / sum);
                 } else {
                     float u = 1.0f / (float)na;
                     for (int a = 0; a < na; a++) sig[a * h + i] = u;
@@ -1897,8 +2018,14 @@ void orc_showdown_cfv(const orc_spot* s, int p, const uint8_t* dealt, int nd, co
     for (int i = 0; i < nd; i++) d = d.push(dealt[i]);
     showdown_cfv(s->s->river_get(d), p, s->s->hands[p], s->s->hands[1 - p], ro, s->s->same_combo[p], win, lose, tie, out);
 }
+void orc_fp8_encode(const float* x, int n, uint8_t* out) {
+    for (int i = 0; i < n; i++) out[i] = f32_to_e4m3(x[i]);
+}
+void orc_fp8_decode(const uint8_t* q, int n, float* out) {
+    for (int i = 0; i < n; i++) out[i] = e4m3_to_f32(q[i]);
+}
 orc_solver* orc_solver_new(orc_spot* s, int compressed, int algo, int use_iso, int prune) {
-    return new orc_solver{new Solver(s->s, compressed != 0, algo, use_iso != 0, prune != 0)};
+    return new orc_solver{new Solver(s->s, compressed, algo, use_iso != 0, prune != 0)};
 }
 void orc_solver_free(orc_solver* v) {
     if (v) { delete v->v; delete v; }

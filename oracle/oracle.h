@@ -91,6 +91,10 @@ void orc_showdown_cfv(const orc_spot* s, int p, const uint8_t* dealt, int ndealt
                       float win, float lose, float tie, float* out);
 
 /* solver (cfr.rs / best_response.rs) */
+/* FP8 E4M3 codec of the precision-study arenas (round to nearest even, saturating to +-448) */
+void orc_fp8_encode(const float* x, int n, uint8_t* out);
+void orc_fp8_decode(const uint8_t* q, int n, float* out);
+/* compressed: 0 f32 arenas, 1 i16 regrets / u16 strategy sums (store.rs), 2 FP8 E4M3 (precision study) */
 orc_solver* orc_solver_new(orc_spot* s, int compressed, int algo, int use_iso, int prune);
 void orc_solver_free(orc_solver* v);
 void orc_solver_iterate(orc_solver* v, int n);

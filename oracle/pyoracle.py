@@ -241,9 +241,10 @@ class Solver:
     """The reference CPU engine (cfr.rs); prune=True reproduces it exactly,
     prune=False gives the no-pruning semantics of a level-synchronous sweep."""
 
-    def __init__(self, spot, compressed=False, algo="dcfr", use_iso=True, prune=True):
+    def __init__(self, spot, compressed=False, algo="dcfr", use_iso=True, prune=True, fp8=False):
         self.spot = spot
-        self.h = lib().orc_solver_new(spot.h, int(compressed), ALGOS[algo], int(use_iso), int(prune))
+        mode = 2 if fp8 else int(bool(compressed))
+        self.h = lib().orc_solver_new(spot.h, mode, ALGOS[algo], int(use_iso), int(prune))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -312,6 +313,21 @@ def discounts(algo, t):
     a, b, c = C.c_float(), C.c_float(), C.c_float()
     lib().orc_solver_discounts(ALGOS[algo], int(t), C.byref(a), C.byref(b), C.byref(c))
     return a.value, b.value, c.value
+
+
+def fp8_encode(x):
+    """FP8 E4M3 bytes of float32 values (round to nearest even, saturating)."""
+    a = np.ascontiguousarray(x, np.float32)
+    out = np.zeros(a.size, np.uint8)
+    lib().orc_fp8_encode(ptr(a), a.size, ptr(out))
+    return out
+
+
+def fp8_decode(q):
+    a = np.ascontiguousarray(q, np.uint8)
+    out = np.zeros(a.size, np.float32)
+    lib().orc_fp8_decode(ptr(a), a.size, ptr(out))
+    return out
 
 
 def set_threads(n):

@@ -263,3 +263,35 @@ def test_locks_match_oracle(engine):
     _compare(spot, osv, host, "locks/" + engine)
     eo, eg = osv.exploitability(), gpu.exploitability(host)
     assert abs(eo - eg) / 60.0 * 100 < EXPL_TOL_PCT, (eo, eg)
+
+
+@pytest.mark.parametrize("algo", ["dcfr", "pcfr+"])
+@pytest.mark.parametrize("name,cfg_fn,iters", [
+    ("small_flop", W.small_flop_spot, 15),
+    ("river_1081", W.river_spot, 10),
+])
+def test_fp8_arenas_match_oracle(name, cfg_fn, iters, algo):
+    """FP8 E4M3 device arenas (the precision study; staged engine) against the
+    oracle's FP8 arenas: the same codes in > 99.9% of entries, average
+    strategies within 1e-4, exploitability within 0.01% of the pot."""
+    cfg = cfg_fn()
+    ospot = po.Spot(cfg)
+    osv = po.Solver(ospot, fp8=True, algo=algo, prune=False)
+    osv.iterate(iters)
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, storage="f32", algo=algo)
+    gpu = g.GpuSolver(host, device_format="fp8")
+    gpu.iterate(iters)
+    gpu.sync_to_cpu(host)
+    for which in (0, 1):
+        for p in (0, 1):
+            a, b = osv.arena(which, p), host.arena(which, p)
+            frac = float(np.mean(a == b))
+            assert frac > 0.999, (name, algo, which, p, frac)
+    so = _avg_strategies(spot, lambda p: osv.arena(1, p))
+    sg = _avg_strategies(spot, lambda p: host.arena(1, p))
+    worst = max(float(np.abs(so[n] - sg[n]).max()) for n in so)
+    assert worst < STRAT_TOL, (name, algo, worst)
+    pot = cfg["tree"]["starting_pot"]
+    eo, eg = osv.exploitability(), gpu.exploitability(host)
+    assert abs(eo - eg) / pot * 100 < EXPL_TOL_PCT, (eo, eg)

@@ -238,3 +238,45 @@ def test_fp64_oracle_agrees_with_f32_br():
     sv.iterate(50)
     e32, e64 = sv.exploitability(), sv.exploitability_f64()
     assert abs(e32 - e64) / 60 * 100 < 1e-3, (e32, e64)
+
+
+def test_fp8_codec_matches_e4m3fn():
+    """The oracle's FP8 E4M3 codec (the precision-study arenas): every code
+    decodes like torch's float8_e4m3fn, in-range floats round like it
+    (nearest, ties to even), and out-of-range values saturate to +-448."""
+    import torch
+    dec = po.fp8_decode(np.arange(256, dtype=np.uint8))
+    ref = torch.arange(256, dtype=torch.uint8).view(torch.float8_e4m3fn).float().numpy()
+    assert np.all((dec == ref) | (np.isnan(dec) & np.isnan(ref)))
+    rng = np.random.default_rng(3)
+    x = np.concatenate([rng.standard_normal(100000).astype(np.float32) * s for s in (1e-3, 0.05, 1.0, 30.0, 200.0)])
+    x = np.clip(x, -448.0, 448.0).astype(np.float32)
+    # exact midpoints between neighbouring codes (ties go to the even code)
+    fin = np.sort(np.unique(ref[np.isfinite(ref) & (ref >= 0)]))
+    mids = ((fin[:-1].astype(np.float64) + fin[1:]) / 2).astype(np.float32)
+    x = np.concatenate([x, mids, -mids])
+    q = po.fp8_encode(x)
+    t = torch.from_numpy(x).to(torch.float8_e4m3fn).view(torch.uint8).numpy()
+    assert int((q != t).sum()) == 0
+    big = np.array([448.0, 449.0, 464.0, 1e6, -500.0, np.inf, -np.inf], np.float32)
+    assert list(po.fp8_encode(big)) == [0x7E, 0x7E, 0x7E, 0x7E, 0xFE, 0x7E, 0xFE]
+
+
+def test_fp8_arenas_precision_study():
+    """Precision study (small flop, f64 best response): FP8 E4M3 arenas with a
+    per-node scale and round-to-nearest converge at first, then stall near
+    3.3% of the pot -- increments below the format's 3-bit mantissa no longer
+    change the stored regrets and strategy sums -- where f32 and the 16-bit
+    format keep converging (0.08% and 0.11% after 300 iterations)."""
+    spot = po.Spot(W.small_flop_spot())
+    pot = W.small_flop_spot()["tree"]["starting_pot"]
+    res = {}
+    for name, kw in (("f32", {}), ("i16", {"compressed": True}), ("fp8", {"fp8": True})):
+        sv = po.Solver(spot, prune=False, **kw)
+        sv.iterate(10)
+        first = sv.exploitability_f64() / pot * 100
+        sv.iterate(290)
+        res[name] = (first, sv.exploitability_f64() / pot * 100)
+    assert res["f32"][1] < 0.1 and res["i16"][1] < 0.15
+    assert res["fp8"][1] < res["fp8"][0] and res["fp8"][1] < 4.0
+    assert res["fp8"][1] > 10 * res["f32"][1]  # the stall, as recorded
