@@ -79,6 +79,9 @@ struct EngineImpl {
     bool reach_valid = false;  // reach slots hold the current strategies' reach (see prime)
     uint32_t iteration = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;  // terminals of a captured sweep
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    std::vector<cudaEvent_t> ev_term;  // per level: that level's terminals are done
     std::vector<void*> owned;
     size_t bytes = 0;
     Dev d{};
@@ -115,6 +118,10 @@ struct EngineImpl {
         for (void* p : owned) cudaFree(p);
         if (pinned) cudaFreeHost(pinned);
         if (h_dot) cudaFreeHost(h_dot);
+        for (cudaEvent_t e : ev_term) cudaEventDestroy(e);
+        if (ev_fork) cudaEventDestroy(ev_fork);
+        if (ev_join) cudaEventDestroy(ev_join);
+        if (side) cudaStreamDestroy(side);
         if (stream) cudaStreamDestroy(stream);
     }
 
@@ -316,30 +323,52 @@ struct EngineImpl {
             down(3, 1, pr);
             reach_valid = false;
         }
+        // Terminal kernels (folds and showdowns with slots of their own) read
+        // only reach vectors, so in a captured sweep they run on a second
+        // stream, every level of them, beside the chain of chance and action
+        // levels; the chain waits for level l + 1's terminals before it
+        // consumes them at level l.
+        const bool fork = pr == nullptr && side != nullptr;
+        if (fork) {
+            CK(cudaEventRecord(ev_fork, stream));
+            CK(cudaStreamWaitEvent(side, ev_fork, 0));
+            for (int l = L - 1; l >= 0; l--) {
+                launch_terminals(l, p, side, nullptr);
+                CK(cudaEventRecord(ev_term[l], side));
+            }
+        }
         for (int l = L - 1; l >= 0; l--) {
-            const Span sf = plan.fold_span[l];
-            if (sf.count) timed(pr, 3, [&] { k_fold<<<sf.count, kThreads, 0, stream>>>(d, fold + sf.start, p); });
-            const Span ss = plan.show_span[l];
-            if (ss.count)
-                timed(pr, 4, [&] {
-                    if (staged) {
-                        const Span sb = plan.show_batch_span[l];
-                        if (plan.max_sorted > 384)
-                            ks_show_cta<256><<<sb.count, 256, show_batch_smem, stream>>>(
-                                d, show, show_batch + sb.start, p, (int)plan.max_sorted);
-                        else
-                            ks_show_cta<128><<<sb.count, 128, show_batch_smem, stream>>>(
-                                d, show, show_batch + sb.start, p, (int)plan.max_sorted);
-                    } else {
-                        k_showdown<<<ss.count, kThreads, show_smem, stream>>>(d, show + ss.start, p);
-                    }
-                });
+            if (!fork) launch_terminals(l, p, stream, pr);
+            else if (l + 1 < L) CK(cudaStreamWaitEvent(stream, ev_term[l + 1], 0));
             const Span sc = plan.chance_span[l];
             if (sc.count) timed(pr, 5, [&] { launch_chance(sc, p); });
             const Span sa = plan.act_span[l];
             if (sa.count) timed(pr, 6, [&] { launch_up_level(l, p, eval); });
         }
+        if (fork) {
+            CK(cudaEventRecord(ev_join, side));
+            CK(cudaStreamWaitEvent(stream, ev_join, 0));
+        }
         CK(cudaGetLastError());
+    }
+    void launch_terminals(int l, int p, cudaStream_t st, Profile* pr) {
+        const Span sf = plan.fold_span[l];
+        if (sf.count) timed(pr, 3, [&] { k_fold<<<sf.count, kThreads, 0, st>>>(d, fold + sf.start, p); });
+        const Span ss = plan.show_span[l];
+        if (ss.count)
+            timed(pr, 4, [&] {
+                if (staged) {
+                    const Span sb = plan.show_batch_span[l];
+                    if (plan.max_sorted > 384)
+                        ks_show_cta<256><<<sb.count, 256, show_batch_smem, st>>>(d, show, show_batch + sb.start, p,
+                                                                                  (int)plan.max_sorted);
+                    else
+                        ks_show_cta<128><<<sb.count, 128, show_batch_smem, st>>>(d, show, show_batch + sb.start, p,
+                                                                                  (int)plan.max_sorted);
+                } else {
+                    k_showdown<<<ss.count, kThreads, show_smem, st>>>(d, show + ss.start, p);
+                }
+            });
     }
     void record_iteration() {
         k_begin_iteration<<<1, 1, 0, stream>>>(d.iter, d.disc, algo);
@@ -410,6 +439,11 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     if (E.fmt == kFmtFP8 && !E.staged) throw Error("FP8 arenas need nodes of at most 4 actions (the staged kernels)");
     if (P.nh_max > kThreads * kMaxHpt) throw Error("more than 1536 hands per player is not supported on the GPU");
     CK(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&E.side, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&E.ev_fork, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&E.ev_join, cudaEventDisableTiming));
+    E.ev_term.resize(std::max(P.num_levels, 1));
+    for (auto& e : E.ev_term) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     size_t& B = E.bytes;
     auto& O = E.owned;
     Dev& d = E.d;
