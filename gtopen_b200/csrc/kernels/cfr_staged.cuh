@@ -778,113 +778,149 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
 
 // Showdown CTAs have NT threads: 256 for large hand lists, 128 for small ones.
 
-// One showdown evaluated by the CTA (game.rs:501-577 with the rank tables):
-// R = opponent reach in strength order; then, at the same time, Q = per-card
-// prefixes (threads 0..51 each run one card's list in strength order, as the
-// reference's running card sums do) and P = R's exclusive prefix (threads
-// 64..NT-1: contiguous chunks, a shuffle scan, the warp totals); then the rank
-// entries.
+// ------------------------------------------- showdowns two at a time
+// Two showdowns of one batch evaluated together by the CTA (game.rs:501-577
+// with the rank tables): they share the board's tables, so every index load,
+// rank-entry decode and address computation is done once for both, and the
+// two reach / prefix values travel as pairs (float2 / double2) in one
+// shared-memory access.  Per showdown: R = opponent reach in strength order;
+// then, at the same time, Q = per-card prefixes (threads 0..51 each run one
+// card's list in strength order, as the reference's running card sums do) and
+// P = R's exclusive prefix (threads 64..NT-1: contiguous chunks, a shuffle
+// scan, the warp totals); then the rank entries.
 template <int NT>
-__device__ void cta_showdown(const ShowTab& tb, const float* ro, float win, float lose, float tie, float* out,
-                             float* R, double* P, double* Q, double* S, double* s_w) {
+__device__ void cta_showdown2(const ShowTab& tb, const float* roA, const float* roB, const ShowItem& ia,
+                              const ShowItem& ib, float* outA, float* outB, float2* R, double2* P, double2* Q,
+                              double2* S, double2* s_w) {
     constexpr int kPT = NT - 64;  // P threads
     const int m = tb.m;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = threadIdx.x; k < m; k += NT) R[k] = ro[tb.sidx[k]];
+    for (int k = threadIdx.x; k < m; k += NT) {
+        const int h = tb.sidx[k];
+        R[k] = make_float2(roA[h], roB[h]);
+    }
     __syncthreads();
     const int pt = (int)threadIdx.x - 64, pw = warp - 2;
     const int chunk = (m + kPT - 1) / kPT;
     const int lo = pt >= 0 ? min(pt * chunk, m) : 0, hi = pt >= 0 ? min(lo + chunk, m) : 0;
-    double local = 0.0, incl = 0.0;
+    double lx = 0.0, ly = 0.0, ix = 0.0, iy = 0.0;
     if (pt >= 0) {
-        for (int k = lo; k < hi; k++) local += (double)R[k];
-        incl = local;
+        for (int k = lo; k < hi; k++) {
+            const float2 r = R[k];
+            lx += (double)r.x;
+            ly += (double)r.y;
+        }
+        ix = lx;
+        iy = ly;
 #pragma unroll
         for (int x = 1; x < 32; x <<= 1) {
-            const double y = __shfl_up_sync(0xffffffffu, incl, x);
-            if (lane >= x) incl += y;
+            const double yx = __shfl_up_sync(0xffffffffu, ix, x);
+            const double yy = __shfl_up_sync(0xffffffffu, iy, x);
+            if (lane >= x) {
+                ix += yx;
+                iy += yy;
+            }
         }
-        if (lane == 31) s_w[pw] = incl;
+        if (lane == 31) s_w[pw] = make_double2(ix, iy);
     } else if (threadIdx.x < 52) {
         const int c = threadIdx.x;
         const uint32_t b = tb.coff[c], e = tb.coff[c + 1];
-        double q = 0.0;
-        Q[b + c] = 0.0;
+        double qx = 0.0, qy = 0.0;
+        Q[b + c] = make_double2(0.0, 0.0);
         uint32_t t = b;
-        for (; t + 4 <= e; t += 4) {  // loads first, then the running sum in order
-            float r[4];
+        for (; t + 4 <= e; t += 4) {
+            float2 r[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) r[u] = R[tb.bpos[t + u]];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
-                q += (double)r[u];
-                Q[t + u + c + 1] = q;
+                qx += (double)r[u].x;
+                qy += (double)r[u].y;
+                Q[t + u + c + 1] = make_double2(qx, qy);
             }
         }
         for (; t < e; t++) {
-            q += (double)R[tb.bpos[t]];
-            Q[t + c + 1] = q;
+            const float2 r = R[tb.bpos[t]];
+            qx += (double)r.x;
+            qy += (double)r.y;
+            Q[t + c + 1] = make_double2(qx, qy);
         }
-        S[c] = q;
+        S[c] = make_double2(qx, qy);
     }
     __syncthreads();
     if (pt >= 0) {
-        double wbase = 0.0;
+        double wx = 0.0, wy = 0.0;
 #pragma unroll
         for (int k = 0; k < kPT / 32; k++)
-            if (k < pw) wbase += s_w[k];
-        double run = wbase + (incl - local);
+            if (k < pw) {
+                wx += s_w[k].x;
+                wy += s_w[k].y;
+            }
+        double rx = wx + (ix - lx), ry = wy + (iy - ly);
         for (int k = lo; k < hi; k++) {
-            P[k] = run;
-            run += (double)R[k];
+            P[k] = make_double2(rx, ry);
+            const float2 r = R[k];
+            rx += (double)r.x;
+            ry += (double)r.y;
         }
-        if (threadIdx.x == NT - 1) P[m] = run;
+        if (threadIdx.x == NT - 1) P[m] = make_double2(rx, ry);
     }
     __syncthreads();
-    const double total = P[m];
+    const double2 total = P[m];
     for (int k = threadIdx.x; k < tb.mp; k += NT) {
         const RankEntry e = tb.rank[k];
         const int a1 = e.cards & 0xFF, a2 = e.cards >> 8;
-        const float lower = (float)(P[e.lb] - Q[e.q1lo] - Q[e.q2lo]);
-        const float higher = (float)((total - P[e.ub]) - (S[a1] - Q[e.q1hi]) - (S[a2] - Q[e.q2hi]));
+        const double2 plb = P[e.lb], pub = P[e.ub], q1lo = Q[e.q1lo], q2lo = Q[e.q2lo], q1hi = Q[e.q1hi],
+                      q2hi = Q[e.q2hi], s1 = S[a1], s2 = S[a2];
         const uint32_t sm = tb.same[e.idx];
-        const float same_r = sm != kSentinel ? ro[sm] : 0.0f;
-        const float valid = (float)(total - S[a1] - S[a2]) + same_r;
-        const float tied = valid - lower - higher;
-        out[e.idx] = win * lower + lose * higher + tie * tied;
+        {
+            const float lower = (float)(plb.x - q1lo.x - q2lo.x);
+            const float higher = (float)((total.x - pub.x) - (s1.x - q1hi.x) - (s2.x - q2hi.x));
+            const float same_r = sm != kSentinel ? roA[sm] : 0.0f;
+            const float valid = (float)(total.x - s1.x - s2.x) + same_r;
+            const float tied = valid - lower - higher;
+            outA[e.idx] = ia.twin * lower + ia.tlose * higher + ia.ttie * tied;
+        }
+        if (outB) {
+            const float lower = (float)(plb.y - q1lo.y - q2lo.y);
+            const float higher = (float)((total.y - pub.y) - (s1.y - q1hi.y) - (s2.y - q2hi.y));
+            const float same_r = sm != kSentinel ? roB[sm] : 0.0f;
+            const float valid = (float)(total.y - s1.y - s2.y) + same_r;
+            const float tied = valid - lower - higher;
+            outB[e.idx] = ib.twin * lower + ib.tlose * higher + ib.ttie * tied;
+        }
     }
-    for (int z = threadIdx.x; z < tb.nz; z += NT) out[tb.zero[z]] = 0.0f;
+    for (int z = threadIdx.x; z < tb.nz; z += NT) {
+        outA[tb.zero[z]] = 0.0f;
+        if (outB) outB[tb.zero[z]] = 0.0f;
+    }
     __syncthreads();
 }
-// Shared memory of ks_show_cta: two barriers, two reach buffers, R (floats),
-// P/Q/S (doubles), then the slot tables.
-__host__ __device__ inline unsigned show_cta_scratch_bytes(int nh_pad, int msort) {
-    return 32u + 2u * 4u * (unsigned)nh_pad + r16u(4u * (unsigned)msort) + r16u((3u * (unsigned)msort + 105u) * 8u);
+// Shared memory of ks_show_pair: two barriers, four reach buffers (two
+// stages of a pair), R pairs, P/Q/S pairs, then the slot tables.
+__host__ __device__ inline unsigned show_pair_scratch_bytes(int nh_pad, int msort) {
+    return 32u + 4u * 4u * (unsigned)nh_pad + r16u(8u * (unsigned)msort) + (3u * (unsigned)msort + 105u) * 16u;
 }
-inline size_t show_cta_smem_bytes(int nh_pad, int msort) {
-    return (size_t)show_cta_scratch_bytes(nh_pad, msort) + show_tab_layout(nh_pad).total;
+inline size_t show_pair_smem_bytes(int nh_pad, int msort) {
+    return (size_t)show_pair_scratch_bytes(nh_pad, msort) + show_tab_layout(nh_pad).total;
 }
-
-// A batch (one level, one slot) per CTA: tables loaded once; the batch's
-// opponent reach vectors stream through two bulk-copy buffers, the next one
-// landing while the current one is evaluated.
 template <int NT>
-__global__ void __launch_bounds__(NT) ks_show_cta(Dev d, const ShowItem* items, const ShowBatch* batches,
-                                                            int p, int msort) {
+__global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items, const ShowBatch* batches, int p,
+                                                    int msort) {
     extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ double s_w[(NT / 32)];
+    __shared__ double2 s_w[NT / 32];
     __shared__ int s_flag;
     __shared__ ShowItem s_it[kShowBatch];
     const ShowBatch bt = batches[blockIdx.x];
     const int o = 1 - p;
-    const int n = (int)bt.count;
+    const int n = (int)bt.count, npairs = (n + 1) / 2;
     uint64_t* bars = (uint64_t*)sm;
     float* rbuf = (float*)(sm + 32);
-    float* R = rbuf + 2 * d.nh_pad;
-    double* P = (double*)((unsigned char*)R + r16u(4u * (unsigned)msort));
-    double* Q = P + msort + 1;
-    double* S = Q + 2 * msort + 52;
-    unsigned char* tabs = sm + show_cta_scratch_bytes(d.nh_pad, msort);
+    float2* R = (float2*)(rbuf + 4 * d.nh_pad);
+    double2* P = (double2*)((unsigned char*)R + r16u(8u * (unsigned)msort));
+    double2* Q = P + msort + 1;
+    double2* S = Q + 2 * msort + 52;
+    unsigned char* tabs = sm + show_pair_scratch_bytes(d.nh_pad, msort);
     const ShowTabLayout TL = show_tab_layout(d.nh_pad);
     if (threadIdx.x < n) s_it[threadIdx.x] = items[bt.start + threadIdx.x];
     ShowTab tb;
@@ -896,41 +932,51 @@ __global__ void __launch_bounds__(NT) ks_show_cta(Dev d, const ShowItem* items, 
         mbar_init(&bars[1], 1);
     }
     __syncthreads();  // items, tables and barriers visible
-    auto issue = [&](int j) {  // thread 0: item j's reach into buffer j & 1
-        float* dst = rbuf + (size_t)(j & 1) * d.nh_pad;
-        const float* src = d.reach[o] + (size_t)s_it[j].rs[o] * d.rstr[o];
-        if ((((uintptr_t)dst | (uintptr_t)src) & 15u) != 0) {
+    auto issue = [&](int q) {  // thread 0: pair q's reach vectors into stage q & 1
+        const int st = q & 1, j0 = 2 * q, cnt = j0 + 1 < n ? 2 : 1;
+        bool bad = false;
+        for (int u = 0; u < cnt; u++) {
+            const float* src = d.reach[o] + (size_t)s_it[j0 + u].rs[o] * d.rstr[o];
+            bad = bad || ((((uintptr_t)(rbuf + (size_t)(2 * st + u) * d.nh_pad)) | (uintptr_t)src) & 15u) != 0;
+        }
+        if (bad) {
             s_flag = 1;
             atomicOr(d.err, 2u);
-            mbar_expect_tx(&bars[j & 1], 0);  // completes the phase with nothing in flight
+            mbar_expect_tx(&bars[st], 0);  // completes the phase with nothing in flight
             return;
         }
-        mbar_expect_tx(&bars[j & 1], rbytes);
-        bulk_load(dst, src, rbytes, &bars[j & 1]);
+        mbar_expect_tx(&bars[st], rbytes * (unsigned)cnt);
+        for (int u = 0; u < cnt; u++)
+            bulk_load(rbuf + (size_t)(2 * st + u) * d.nh_pad, d.reach[o] + (size_t)s_it[j0 + u].rs[o] * d.rstr[o],
+                      rbytes, &bars[st]);
     };
     if (threadIdx.x == 0) {
         issue(0);
-        if (n > 1) issue(1);
+        if (npairs > 1) issue(1);
     }
-    for (int j = 0; j < n; j++) {
-        const bool ok = mbar_wait(&bars[j & 1], (unsigned)(j >> 1) & 1u);
+    for (int q = 0; q < npairs; q++) {
+        const int st = q & 1;
+        const bool ok = mbar_wait(&bars[st], (unsigned)(q >> 1) & 1u);
         if (__syncthreads_or(!ok) || s_flag) {
             if (threadIdx.x == 0) {
                 if (!ok) atomicOr(d.err, 1u);
-                // bounded drain of the copies still in flight (this one and the next)
-                mbar_wait(&bars[j & 1], (unsigned)(j >> 1) & 1u);
-                if (j + 1 < n) mbar_wait(&bars[(j + 1) & 1], (unsigned)((j + 1) >> 1) & 1u);
+                // bounded drain of the copies still in flight (this pair and the next)
+                mbar_wait(&bars[st], (unsigned)(q >> 1) & 1u);
+                if (q + 1 < npairs) mbar_wait(&bars[st ^ 1], (unsigned)((q + 1) >> 1) & 1u);
             }
             return;
         }
-        const ShowItem& s = s_it[j];
-        const float* ro = rbuf + (size_t)(j & 1) * d.nh_pad;
-        cta_showdown<NT>(tb, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, R, P, Q, S, s_w);
-        // buffer j & 1 is free (the evaluation ends with a barrier): order its
-        // generic reads before the next bulk write into it, then refill it
+        const int j0 = 2 * q;
+        const bool two = j0 + 1 < n;
+        const ShowItem& ia = s_it[j0];
+        const ShowItem& ib = s_it[two ? j0 + 1 : j0];
+        const float* roA = rbuf + (size_t)(2 * st) * d.nh_pad;
+        const float* roB = two ? roA + d.nh_pad : roA;
+        cta_showdown2<NT>(tb, roA, roB, ia, ib, d.cfv + (size_t)ia.cslot * d.nh_max,
+                          two ? d.cfv + (size_t)ib.cslot * d.nh_max : nullptr, R, P, Q, S, s_w);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
-        if (threadIdx.x == 0 && j + 2 < n) issue(j + 2);
+        if (threadIdx.x == 0 && q + 2 < npairs) issue(q + 2);
     }
 }
 

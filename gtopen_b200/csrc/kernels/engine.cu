@@ -103,7 +103,7 @@ struct EngineImpl {
     size_t warp_smem = 0;    // warp up-action dynamic smem (one staged reach per warp)
     size_t st_mine_smem = 0, st_opp_smem = 0, st_down_smem = 0;  // staged kernels
     SNode* snodes = nullptr;                   // staged node records (same order as act)
-    size_t show_batch_smem = 0;                                   // batched showdowns
+    size_t show_pair_smem = 0;                                    // batched showdowns
     size_t chance_smem = 0;  // runout chance dynamic smem
     cudaGraphExec_t g_iter = nullptr;
     cudaGraphExec_t g_eval[2] = {nullptr, nullptr};
@@ -360,10 +360,10 @@ struct EngineImpl {
                 if (staged) {
                     const Span sb = plan.show_batch_span[l];
                     if (plan.max_sorted > 384)
-                        ks_show_cta<256><<<sb.count, 256, show_batch_smem, st>>>(d, show, show_batch + sb.start, p,
+                        ks_show_pair<256><<<sb.count, 256, show_pair_smem, st>>>(d, show, show_batch + sb.start, p,
                                                                                   (int)plan.max_sorted);
                     else
-                        ks_show_cta<128><<<sb.count, 128, show_batch_smem, st>>>(d, show, show_batch + sb.start, p,
+                        ks_show_pair<128><<<sb.count, 128, show_pair_smem, st>>>(d, show, show_batch + sb.start, p,
                                                                                   (int)plan.max_sorted);
                 } else {
                     k_showdown<<<ss.count, kThreads, show_smem, st>>>(d, show + ss.start, p);
@@ -557,9 +557,9 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
         EngineImpl::set_staged_smem<kDevI16>(E.st_mine_smem, E.st_opp_smem);
         set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
         set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
-        E.show_batch_smem = show_cta_smem_bytes(d.nh_pad, (int)P.max_sorted);
-        set_smem((const void*)ks_show_cta<128>, E.show_batch_smem);
-        set_smem((const void*)ks_show_cta<256>, E.show_batch_smem);
+        E.show_pair_smem = show_pair_smem_bytes(d.nh_pad, (int)P.max_sorted);
+        set_smem((const void*)ks_show_pair<128>, E.show_pair_smem);
+        set_smem((const void*)ks_show_pair<256>, E.show_pair_smem);
     }
     if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
