@@ -267,10 +267,13 @@ def run_ours(args, world, rank, local):
         dt_max = allmax(dt, world)
         b = HOST_BYTES[args.storage]
         arena_bytes = 2 * (spot.data_size[0] + spot.data_size[1]) * b
+        up = gpu2.info()["upload_bytes"]
         e2e = {"value": world * args.steps / dt_max, "unit": "iter/s",
-               "h2d_bytes_per_step": int(arena_bytes / args.steps),
+               "h2d_bytes_per_step": int(up / args.steps),
                "d2h_bytes_per_step": int((arena_bytes + 16) / args.steps),
-               "includes": "GpuSolver::new upload, %d iterations, 1 exploitability check, sync_to_cpu" % args.steps,
+               "includes": "GpuSolver::new (plan tables and, when the host solver has any, arenas uploaded; "
+                           "a fresh solver's arenas are all zero and are not copied), %d iterations, "
+                           "1 exploitability check (f64 read back), sync_to_cpu (every arena read back)" % args.steps,
                "split": {k: round(v, 3) for k, v in split.items()},
                "exploitability_pct_pot": e / cfg["tree"]["starting_pot"] * 100}
         gpu2.close()

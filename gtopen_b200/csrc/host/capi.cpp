@@ -335,6 +335,7 @@ int gtob_gpu_info_get(gtob_gpu* g, gtob_gpu_info* o) {
     o->num_river_slots = P.num_slots;
     o->arena_format = g->e->format();
     o->iter_bytes = g->e->iter_bytes();
+    o->upload_bytes = g->e->upload_bytes();
     return GTOB_OK;
 }
 int gtob_gpu_root_cfv(gtob_gpu* g, int p, int mode, float* out) {

@@ -44,6 +44,7 @@ const char* const kKernelNames[7] = {"copy_root", "down_action", "down_chance", 
         if (e_ != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(e_) + " at " #x); \
     } while (0)
 
+static thread_local uint64_t g_uploaded = 0;  // host-to-device bytes of the engine being built
 template <class T>
 static T* dupload(const std::vector<T>& v, std::vector<void*>& owned, size_t* bytes) {
     T* p = nullptr;
@@ -52,6 +53,7 @@ static T* dupload(const std::vector<T>& v, std::vector<void*>& owned, size_t* by
     owned.push_back(p);
     *bytes += n * sizeof(T);
     if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    g_uploaded += v.size() * sizeof(T);
     return p;
 }
 static void* dalloc(size_t bytes, std::vector<void*>& owned, size_t* total) {
@@ -84,6 +86,7 @@ struct EngineImpl {
     std::vector<cudaEvent_t> ev_term;  // per level: that level's terminals are done
     std::vector<void*> owned;
     size_t bytes = 0;
+    uint64_t uploaded = 0;  // host-to-device bytes copied by the constructor
     Dev d{};
     Arenas ar{};
     ActItem* act = nullptr;
@@ -96,7 +99,6 @@ struct EngineImpl {
     std::vector<XNode> hx[2];
     void* lock_buf = nullptr;
     float* staging = nullptr;  // device f32 image of one arena in the reference layout
-    float* pinned = nullptr;
     size_t staging_len = 0;
     size_t show_smem = 0;    // plain showdown kernel (f64 scratch)
     size_t act_smem = 0;     // fused up-action dynamic smem
@@ -116,7 +118,6 @@ struct EngineImpl {
             if (g) cudaGraphExecDestroy(g);
         if (lock_buf) cudaFree(lock_buf);
         for (void* p : owned) cudaFree(p);
-        if (pinned) cudaFreeHost(pinned);
         if (h_dot) cudaFreeHost(h_dot);
         for (cudaEvent_t e : ev_term) cudaEventDestroy(e);
         if (ev_fork) cudaEventDestroy(ev_fork);
@@ -418,6 +419,7 @@ struct EngineImpl {
 GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new EngineImpl()) {
     EngineImpl& E = *d_;
     const Spot& sp = *host.spot;
+    g_uploaded = 0;
     if (engine < kEngineFused || engine > kEngineStaged) throw Error("unknown engine kind");
     const int fuse = engine == kEnginePlain                               ? kFuseNone
                      : (engine == kEngineWarp || engine == kEngineStaged) ? kFuseFolds
@@ -599,12 +601,11 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     }
     E.staging_len = std::max<uint64_t>(std::max(sp.tree.data_size[0], sp.tree.data_size[1]), 1);
     E.staging = (float*)dalloc(E.staging_len * sizeof(float), O, &B);
-    CK(cudaMallocHost(&E.pinned, E.staging_len * sizeof(float)));
     CK(cudaMallocHost(&E.h_dot, 4 * sizeof(double)));
 
     // upload arenas: quants directly when host and device are both 16-bit, else via f32 (+ encode);
     // nothing to upload while the host arenas are still all zero (so are the device's)
-    std::vector<float> img(host.arenas_zero ? 0 : E.staging_len);
+    std::vector<float> img;  // f32 image of one host arena, when one is needed
     for (int q = 0; q < 2 && !host.arenas_zero; q++) {
         const int nh = P.nh[q];
         const unsigned nb = (unsigned)P.n_anodes[q];
@@ -619,6 +620,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
                 const size_t len = sp.tree.data_size[q];
                 if (ha->kind == 1) CK(cudaMemcpy(E.staging, ha->qi.data(), len * 2, cudaMemcpyHostToDevice));
                 else CK(cudaMemcpy(E.staging, ha->qu.data(), len * 2, cudaMemcpyHostToDevice));
+                g_uploaded += len * 2 + P.n_anodes[q] * 4;
                 k_to_dev<uint16_t><<<nb, kThreads, 0, E.stream>>>((const uint16_t*)E.staging, (uint16_t*)dst, E.xnodes[q], nh);
                 std::vector<float> sc(P.n_anodes[q]);
                 for (uint64_t s = 0; s < P.n_anodes[q]; s++) sc[s] = ha->scale[P.anode_id[q][s]];
@@ -627,8 +629,16 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
                 CK(cudaStreamSynchronize(E.stream));
                 continue;
             }
-            host.arena_f32(which, q, img.data());
-            CK(cudaMemcpy(E.staging, img.data(), sp.tree.data_size[q] * 4, cudaMemcpyHostToDevice));
+            const float* src32;
+            if (ha->kind == 0) {  // f32 host arena: already the image
+                src32 = ha->f.data();
+            } else {
+                img.resize(E.staging_len);
+                host.arena_f32(which, q, img.data());
+                src32 = img.data();
+            }
+            CK(cudaMemcpy(E.staging, src32, sp.tree.data_size[q] * 4, cudaMemcpyHostToDevice));
+            g_uploaded += sp.tree.data_size[q] * 4;
             if (E.fmt == kFmtF32) {
                 k_to_dev<float><<<nb, kThreads, 0, E.stream>>>(E.staging, (float*)dst, E.xnodes[q], nh);
             } else {
@@ -645,9 +655,11 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     }
     E.upload_locks(host);
     CK(cudaStreamSynchronize(E.stream));
+    E.uploaded = g_uploaded;
 }
 
 GpuEngine::~GpuEngine() = default;
+uint64_t GpuEngine::upload_bytes() const { return d_->uploaded; }
 
 void GpuEngine::iterate(int n) {
     EngineImpl& E = *d_;
@@ -850,28 +862,41 @@ void GpuEngine::sync_to_cpu(HostSolver& host, bool strategy_only) {  // gpu/mod.
             const unsigned nb = (unsigned)E.plan.n_anodes[p];
             if (!nb) continue;
             void* src = which == kRegrets ? E.ar.reg[p] : which == kStrategy ? E.ar.str[p] : E.ar.pred[p];
+            // Without suit isomorphism every action node is on the device, so the
+            // reference-layout image is the whole host arena and lands there
+            // directly; otherwise it goes through a temporary and only the
+            // device's nodes are copied (the symmetric branches keep theirs).
+            const bool whole = !E.plan.iso_active;
             if (E.fmt == kFmtI16 && ha.kind != 0) {
                 // 16-bit on both sides: quants and scales move exactly
                 k_to_host<uint16_t><<<nb, kThreads, 0, E.stream>>>((const uint16_t*)src, (uint16_t*)E.staging, E.xnodes[p], nh);
-                CK(cudaMemcpyAsync(E.pinned, E.staging, t.data_size[p] * 2, cudaMemcpyDeviceToHost, E.stream));
                 std::vector<float> sc(E.plan.n_anodes[p]);
                 const float* dsc = which == kRegrets ? E.ar.rscale[p] : which == kStrategy ? E.ar.sscale[p] : E.ar.pscale[p];
                 CK(cudaMemcpyAsync(sc.data(), dsc, sc.size() * 4, cudaMemcpyDeviceToHost, E.stream));
+                uint16_t* harena = ha.kind == 1 ? (uint16_t*)ha.qi.data() : ha.qu.data();
+                std::vector<uint16_t> tmp(whole ? 0 : t.data_size[p]);
+                CK(cudaMemcpyAsync(whole ? harena : tmp.data(), E.staging, t.data_size[p] * 2, cudaMemcpyDeviceToHost,
+                                   E.stream));
                 CK(cudaStreamSynchronize(E.stream));
-                const uint16_t* q = (const uint16_t*)E.pinned;
                 for (uint64_t s = 0; s < E.plan.n_anodes[p]; s++) {
                     const uint32_t nd = E.plan.anode_id[p][s];
-                    const size_t off = t.data_off[nd], cnt = (size_t)t.nchild[nd] * nh;
-                    if (ha.kind == 1) std::memcpy(ha.qi.data() + off, q + off, cnt * 2);
-                    else std::memcpy(ha.qu.data() + off, q + off, cnt * 2);
+                    if (!whole) {
+                        const size_t off = t.data_off[nd], cnt = (size_t)t.nchild[nd] * nh;
+                        std::memcpy(harena + off, tmp.data() + off, cnt * 2);
+                    }
                     ha.scale[nd] = sc[s];
                 }
                 continue;
             }
-            export_arena(which, p, E.pinned);
+            if (whole && ha.kind == 0) {
+                export_arena(which, p, ha.f.data());
+                continue;
+            }
+            std::vector<float> img(t.data_size[p]);
+            export_arena(which, p, img.data());
             for (uint64_t s = 0; s < E.plan.n_anodes[p]; s++) {
                 const uint32_t nd = E.plan.anode_id[p][s];
-                ha.write(nd, t.data_off[nd], (size_t)t.nchild[nd] * nh, E.pinned + t.data_off[nd]);
+                ha.write(nd, t.data_off[nd], (size_t)t.nchild[nd] * nh, img.data() + t.data_off[nd]);
             }
         }
     }

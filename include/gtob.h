@@ -82,6 +82,7 @@ typedef struct {
     uint32_t num_river_slots;
     int32_t arena_format;
     double iter_bytes; /* algorithmic bytes of one CFR iteration */
+    uint64_t upload_bytes; /* host-to-device bytes copied by gtob_gpu_new (plan tables, arenas) */
 } gtob_gpu_info;
 
 /* Thread-local message of the last failed call (Result::Err text). */
