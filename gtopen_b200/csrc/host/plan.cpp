@@ -15,13 +15,20 @@ struct Visit {
     int ndealt;
     uint32_t cslot;
     uint32_t rs[2];
+    uint32_t slot;  // river slot once the board is complete, else kNoSlot
 };
 template <class T>
 void flatten(std::vector<std::vector<std::pair<uint32_t, T>>>& by_level, std::vector<T>& flat, std::vector<Span>& span) {
+    size_t total = 0;
+    for (auto& lst : by_level) total += lst.size();
+    flat.reserve(total);
+    auto by_node = [](const auto& a, const auto& b) { return a.first < b.first; };
     for (auto& lst : by_level) {
-        std::sort(lst.begin(), lst.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        // the traversal visits a level's nodes in node order already; sort only if not
+        if (!std::is_sorted(lst.begin(), lst.end(), by_node)) std::sort(lst.begin(), lst.end(), by_node);
         span.push_back({(uint32_t)flat.size(), (uint32_t)lst.size()});
         for (auto& x : lst) flat.push_back(x.second);
+        std::vector<std::pair<uint32_t, T>>().swap(lst);
     }
 }
 bool is_terminal(uint8_t k) { return k == kFold || k == kShowdown; }
@@ -73,10 +80,21 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
         return (uint32_t)(P.terms.size() - 1);
     };
     std::vector<uint8_t> visited(n, 0);
+    {  // capacity for the flat tables (no regrowth during the traversal)
+        size_t nchild = 0, nterm = 0;
+        for (size_t i = 0; i < n; i++) {
+            if (t.kind[i] == kAction) nchild += t.nchild[i];
+            else if (is_terminal(t.kind[i])) nterm++;
+        }
+        P.crefs.reserve(nchild);
+        P.terms.reserve(nterm);
+    }
 
     uint64_t next_c = 1, next_r[2] = {1, 1};
     std::vector<Visit> stack;
-    stack.push_back({0, 0, {0, 0}, 0, 0, {0, 0}});
+    const bool full_board = sp.board.size() == 5;
+    stack.push_back({0, 0, {0, 0}, 0, 0, {0, 0}, full_board ? river_slot(nullptr, 0) : kNoSlot});
+    Visit kids[256];  // children of the node being visited (nchild is a u8)
     while (!stack.empty()) {
         Visit v = stack.back();
         stack.pop_back();
@@ -96,7 +114,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                 it.na = (uint32_t)na;
                 it.cref = (uint32_t)P.crefs.size();
                 P.max_children = std::max<uint32_t>(P.max_children, (uint32_t)na);
-                std::vector<Visit> kids;
+                int nkids = 0;
                 for (int k = 0; k < na; k++) {
                     const uint32_t c = t.child(nd, k);
                     if (is_terminal(t.kind[c]) && in_place(t.kind[c])) {
@@ -117,10 +135,10 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                     cv.cslot = (uint32_t)next_c++;
                     cv.rs[a] = (uint32_t)next_r[a]++;
                     P.crefs.push_back({kChildNode, cv.cslot, cv.rs[a], kNoSlot});
-                    kids.push_back(cv);
+                    kids[nkids++] = cv;
                 }
                 act_l[v.level].push_back({nd, it});
-                for (auto k = kids.rbegin(); k != kids.rend(); ++k) stack.push_back(*k);
+                for (int k = nkids - 1; k >= 0; k--) stack.push_back(kids[k]);
                 break;
             }
             case kChance: {
@@ -146,7 +164,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                 ci.inv = 1.0f / (float)(46 - (int)t.street[nd]);
                 ci.rs[0] = v.rs[0];
                 ci.rs[1] = v.rs[1];
-                std::vector<Visit> kids;
+                int nkids = 0;
                 for (auto& x : cr) {
                     if (x.card != x.rep) continue;
                     const uint32_t c = t.children[t.child_start[nd] + x.card];
@@ -163,6 +181,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                     cv.dealt[0] = d2[0];
                     cv.dealt[1] = d2[1];
                     cv.ndealt = v.ndealt + 1;
+                    cv.slot = sp.board.size() + (size_t)cv.ndealt == 5 ? river_slot(cv.dealt, cv.ndealt) : kNoSlot;
                     cv.cslot = (uint32_t)next_c++;
                     cv.rs[0] = (uint32_t)next_r[0]++;
                     cv.rs[1] = (uint32_t)next_r[1]++;
@@ -170,7 +189,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                     rep_term[x.card] = kNoSlot;
                     EdgeItem e{{v.rs[0], v.rs[1]}, {cv.rs[0], cv.rs[1]}, x.card, 0};
                     edge_l[v.level].push_back({c, e});
-                    kids.push_back(cv);
+                    kids[nkids++] = cv;
                 }
                 ci.cc_start = (uint32_t)P.cards.size();
                 ci.cc_count = (uint32_t)cr.size();
@@ -180,7 +199,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                     if (rep_term[x.rep] != kNoSlot) ci.nterm++;
                 }
                 chance_l[v.level].push_back({nd, ci});
-                for (auto k = kids.rbegin(); k != kids.rend(); ++k) stack.push_back(*k);
+                for (int k = nkids - 1; k >= 0; k--) stack.push_back(kids[k]);
                 break;
             }
             case kFold: {
@@ -190,8 +209,8 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
                 break;
             }
             default: {
-                ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, river_slot(v.dealt, v.ndealt), (float)t.twin[nd],
-                            (float)t.tlose[nd], (float)t.ttie[nd], 0};
+                ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, v.slot != kNoSlot ? v.slot : river_slot(v.dealt, v.ndealt),
+                            (float)t.twin[nd], (float)t.tlose[nd], (float)t.ttie[nd], 0};
                 show_l[v.level].push_back({nd, si});
                 P.visited_terminals++;
                 break;
@@ -242,7 +261,14 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
     for (size_t l = 0; l < P.show_span.size(); l++) {
         const Span s = P.show_span[l];
         auto first = P.show.begin() + s.start;
-        std::stable_sort(first, first + s.count, [](const ShowItem& x, const ShowItem& y) { return x.slot < y.slot; });
+        {  // stable counting sort by slot
+            std::vector<uint32_t> cnt(P.slot_key.size() + 1, 0);
+            for (uint32_t k = 0; k < s.count; k++) cnt[first[k].slot + 1]++;
+            for (size_t k = 1; k < cnt.size(); k++) cnt[k] += cnt[k - 1];
+            std::vector<ShowItem> tmp(s.count);
+            for (uint32_t k = 0; k < s.count; k++) tmp[cnt[first[k].slot]++] = first[k];
+            std::copy(tmp.begin(), tmp.end(), first);
+        }
         const uint32_t b0 = (uint32_t)P.show_batch.size();
         for (uint32_t k = 0; k < s.count;) {
             const uint32_t slot = P.show[s.start + k].slot;
