@@ -12,9 +12,9 @@ hands) for 100 iterations on the GPU engine, exploitability every 10:
   CPU engines by 0.22%;
 * against the reference's own GPU run (bench/gpu_f32_dcfr.log, recorded in
   the same fixture): that engine is unpruned too but sums terminals in f32 and
-  divides in regret matching, and its trajectory drifts from the f64 one by up
-  to 0.22% of the pot (iteration 30) before the two meet again (0.04% at 100),
-  so the bar there is 0.25%.
+  divides in regret matching, and its trajectory differs from the f64 one by
+  0.82% of the pot at iteration 10, 0.22% at 30 and under 0.05% from 50 on, so
+  the bar there is 1% of the pot to iteration 30 and 0.1% after.
 """
 import json
 import os
@@ -50,4 +50,4 @@ def test_bench_spot_trajectory(storage, mode, engine):
         assert abs(a - b) / pot * 100 < (0.01 if it <= 50 else 0.1), (it, a, b)
     if storage == "f32":
         for it, a, b in zip(gold["iters"], ours, gold["reference_gpu_f32_dcfr"]):
-            assert abs(a - b) / pot * 100 < 0.25, (it, a, b)
+            assert abs(a - b) / pot * 100 < (1.0 if it <= 30 else 0.1), (it, a, b)
