@@ -242,39 +242,54 @@ __device__ __forceinline__ void s_node_sigma(const Dev& d, long long loff, int a
     }
 }
 
-__device__ __forceinline__ float s_block_max(float v, float* sh) {
-    v = warp_max(v);
+// Block maxima of three values behind one barrier (sh: 3 * kSWarps floats,
+// written once per CTA).
+__device__ __forceinline__ void s_block_max3(float& a, float& b, float& c, float* sh) {
+    a = warp_max(a);
+    b = warp_max(b);
+    c = warp_max(c);
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5] = a;
+        sh[kSWarps + (threadIdx.x >> 5)] = b;
+        sh[2 * kSWarps + (threadIdx.x >> 5)] = c;
+    }
     __syncthreads();
-    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
-    __syncthreads();
-    float m = sh[0];
+    a = sh[0];
+    b = sh[kSWarps];
+    c = sh[2 * kSWarps];
 #pragma unroll
-    for (int k = 1; k < kSWarps; k++) m = fmaxf(m, sh[k]);
-    return m;
+    for (int k = 1; k < kSWarps; k++) {
+        a = fmaxf(a, sh[k]);
+        b = fmaxf(b, sh[kSWarps + k]);
+        c = fmaxf(c, sh[2 * kSWarps + k]);
+    }
 }
 
 // Fold summary of a staged opponent reach vector (game.rs:478-485): total
-// and per-card sums in f64.  Threads 0..51 each sum one card's hand list in
-// hand order (the reference's order); the total is a fixed-tree block sum.
+// and per-card sums in f64, each a fixed-order sum.  Threads 2c and 2c+1 sum
+// the even and odd entries of card c's hand list (ascending hand index; the
+// list ends at the first 0xFFFF) and add the two halves; the total is a
+// fixed-tree block sum.
 __device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, double* s_red) {
     const int nho = d.nh[o];
     double t = 0.0;
     for (int j = threadIdx.x; j < nho; j += kSThreads) t += (double)ro[j];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x < 52) {
-        const int c = threadIdx.x;
-        const uint16_t* idx = d.hcard52[o] + c * 52;
+    if (threadIdx.x < 104) {  // warps 0..3, whole lane pairs
+        const int c = threadIdx.x >> 1, par = threadIdx.x & 1;
+        const uint16_t* idx = d.hcard52[o] + c * 52 + par;
         double s = 0.0;
-        for (int k = 0; k < 52; k += 4) {  // index loads first, then the sum in hand order
+        for (int k = 0; k + par < 52; k += 8) {  // index loads first, then the sums
             uint16_t x[4];
 #pragma unroll
-            for (int u = 0; u < 4; u++) x[u] = idx[k + u];
+            for (int u = 0; u < 4; u++) x[u] = k + 2 * u + par < 52 ? idx[k + 2 * u] : (uint16_t)0xFFFFu;
 #pragma unroll
             for (int u = 0; u < 4; u++)
                 if (x[u] != 0xFFFFu) s += (double)ro[x[u]];
             if (x[3] == 0xFFFFu) break;
         }
-        S[c] = s;
+        s += __shfl_xor_sync(0xffffffffu >> (threadIdx.x >= 96 ? 24 : 0), s, 1);
+        if (par == 0) S[c] = s;
     }
     t = warp_sum(t);
     if (lane == 0) s_red[warp] = t;
@@ -360,12 +375,13 @@ __device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, con
     unsigned char* b_str = sm + L.str();
     unsigned char* b_pred = sm + L.pred();
     float* pr = (float*)(sm + L.ro());
-    const long long loff = d.lock_off[a][it.sidx];
     const bool has_pred = ar.pred[a] != nullptr;
     const unsigned blk = round16((unsigned)(na * nh * esz));
     if (threadIdx.x == 0) {
+        // the sigma source is staged before the lock table is read (a locked
+        // node's block is staged and not used)
         mbar_init(bar, 1);
-        const bool u_reg = loff < 0 && mode == 0, u_pred = u_reg && has_pred, u_str = loff < 0 && mode != 0;
+        const bool u_reg = mode == 0, u_pred = u_reg && has_pred, u_str = mode != 0;
         const unsigned char* g_reg = (const unsigned char*)ar.reg[a] + it.aoff * esz;
         const unsigned char* g_str = (const unsigned char*)ar.str[a] + it.aoff * esz;
         const unsigned char* g_pred = u_pred ? (const unsigned char*)ar.pred[a] + it.aoff * esz : nullptr;
@@ -382,6 +398,7 @@ __device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, con
             bulk_load(pr, g_pr, vb, bar);
         }
     }
+    const long long loff = d.lock_off[a][it.sidx];
     float kr = 0.0f, kp = 0.0f;
     if (FMT != kDevF32 && mode == 0 && loff < 0) {
         kr = ar.rscale[a][it.sidx] / QT<FMT>::kR;
@@ -441,15 +458,16 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     const int vstride = d.nh_pad;
     const int fk = it.fk == kNoSlot ? -1 : (int)it.fk;
     const float famount = (int)it.folder == p ? it.tlose : it.twin;
-    const long long loff = d.lock_off[a][it.sidx];
     constexpr bool mine = MINE;  // a launch holds one actor's nodes: a == p iff MINE
     const bool has_pred = ar.pred[a] != nullptr;
     // what the node reads (an opponent node's fold child comes with the
-    // folding player's reach, written by the down sweep: no strategy needed)
-    const bool use_reg = loff < 0 && !EVAL && mine;
-    const bool use_str = loff < 0 && (EVAL ? (mine && mode == 1) : mine);
+    // folding player's reach, written by the down sweep: no strategy needed).
+    // The blocks are staged before the lock table is read; a locked node's
+    // are staged and not used.
+    const bool use_reg = !EVAL && mine;
+    const bool use_str = EVAL ? (mine && mode == 1) : mine;
     const bool use_pred = use_reg && has_pred;
-    const bool use_rp = mine && !EVAL && loff < 0;
+    const bool use_rp = mine && !EVAL;
     const unsigned blk = round16((unsigned)(na * d.nh[a] * esz));
     if (threadIdx.x == 0) {
         mbar_init(bar, 1);
@@ -485,7 +503,9 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
                 if (k < na && k != fk) bulk_load(cv + k * vstride, d.cfv + (size_t)it.cs[k] * d.nh_max, vb, bar);
         }
     }
-    // scales of the actor's node (16-bit arenas), loaded while the copies fly
+    // lock and scales of the actor's node (16-bit arenas), loaded while the
+    // copies fly
+    const long long loff = d.lock_off[a][it.sidx];
     float kr = 0.0f, kp = 0.0f, sscale = 0.0f;
     if (FMT != kDevF32 && loff < 0 && mine) {
         kr = ar.rscale[a][it.sidx] / QT<FMT>::kR;
@@ -628,8 +648,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
                 }
             out[i] = o_;
         }
-        rmax = s_block_max(rmax, s_red);
-        smax = s_block_max(smax, s_red + kSWarps);
+        s_block_max3(rmax, smax, pmax, s_red);
         const float rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
         const float sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
         for (int i = threadIdx.x; i < nh; i += kSThreads) {
@@ -653,9 +672,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     for (int pass = one_pass ? 2 : 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
         if (pass == 1) {
-            rmax = s_block_max(rmax, s_red);
-            smax = s_block_max(smax, s_red + kSWarps);
-            if (use_pred) pmax = s_block_max(pmax, s_red + 2 * kSWarps);
+            s_block_max3(rmax, smax, pmax, s_red);
             rk = (rmax > 0.0f && isfinite(rmax)) ? Q::kR / rmax : 0.0f;
             sk = (smax > 0.0f && isfinite(smax)) ? Q::kS / smax : 0.0f;
             pk = (pmax > 0.0f && isfinite(pmax)) ? Q::kR / pmax : 0.0f;
