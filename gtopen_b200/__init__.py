@@ -114,6 +114,8 @@ def lib():
         "gtob_gpu_export_arena": (I, [P, I, I, P]),
         "gtob_gpu_read_node_static": (I, [P, I, C.c_uint32, P, C.c_uint64, P]),
         "gtob_gpu_discounts": (I, [P, P]),
+        "gtob_gpu_save": (I, [P, P, C.c_char_p]),
+        "gtob_gpu_load": (I, [C.c_char_p, I, I, I, C.POINTER(P), C.POINTER(P)]),
         "gtob_set_device": (I, [I]),
         "gtob_gpu_time_iterations": (I, [P, I, C.POINTER(D)]),
     }
@@ -416,6 +418,30 @@ class GpuSolver:
         _check(lib().gtob_gpu_read_node_static(self._h, int(which), int(node), _ptr(out), out.size,
                                                C.byref(written)))
         return out[:written.value]
+
+    def save(self, path, solver=None):
+        """.gto written from the device arenas (config and locks from the host
+        solver): the file sync_to_cpu + ensure_symmetric + Solver.save would
+        give an f32 host solver, without a host arena copy."""
+        _check(lib().gtob_gpu_save(self._h, (solver or self.solver)._h, os.fspath(path).encode()))
+
+    @staticmethod
+    def load(path, storage="f32", device_format=None, engine="staged"):
+        """Solver.load + GpuSolver with the arenas streamed from the file into
+        device memory.  Returns (solver, gpu); the host solver holds only the
+        blocks the device does not, the rest after gpu.sync_to_cpu()."""
+        sh, gh = C.c_void_p(), C.c_void_p()
+        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}[engine]
+        _check(lib().gtob_gpu_load(os.fspath(path).encode(), STORAGE[storage], DEVICE_FORMAT[device_format], eng,
+                                   C.byref(sh), C.byref(gh)))
+        with open(path, "rb") as f:
+            f.read(10)
+            header = json.loads(f.readline())
+        solver = Solver(Spot(header["config"], lenient=True), storage=storage, _handle=sh)
+        gpu = GpuSolver.__new__(GpuSolver)
+        gpu._h = gh
+        gpu.solver = solver
+        return solver, gpu
 
     def discounts(self):
         out = np.zeros(3, np.float32)

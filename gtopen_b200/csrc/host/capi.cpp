@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <fstream>
 #include <memory>
 #include <string>
 
@@ -266,6 +267,27 @@ int gtob_load(const char* path, int storage, gtob_solver** out) {
     API_END
 }
 
+int gtob_gpu_save(gtob_gpu* g, const gtob_solver* v, const char* path) {
+    REQUIRE(g && v && path);
+    API_BEGIN
+    g->e->save(*v->v, path);
+    API_END
+}
+int gtob_gpu_load(const char* path, int storage, int fmt, int engine, gtob_solver** solver_out, gtob_gpu** gpu_out) {
+    REQUIRE(path && solver_out && gpu_out && (storage == 0 || storage == 1) && fmt >= -1 && fmt <= 2 &&
+            engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+    *solver_out = nullptr;
+    *gpu_out = nullptr;
+    API_BEGIN
+    std::ifstream in(path, std::ios::binary);
+    if (!in) throw Error(std::string("cannot open ") + path);
+    auto host = HostSolver::load_header(in, storage);
+    auto eng = std::make_unique<GpuEngine>(*host, fmt, engine);
+    eng->load_arenas(in, *host);
+    *solver_out = new gtob_solver{std::move(host)};
+    *gpu_out = new gtob_gpu{std::move(eng)};
+    API_END
+}
 int gtob_gpu_new(const gtob_solver* v, int fmt, gtob_gpu** out) { return gtob_gpu_new_ex(v, fmt, GTOB_ENGINE_STAGED, out); }
 int gtob_gpu_new_ex(const gtob_solver* v, int fmt, int engine, gtob_gpu** out) {
     REQUIRE(v && out && fmt >= -1 && fmt <= 2 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);

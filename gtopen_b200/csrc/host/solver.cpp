@@ -142,13 +142,18 @@ void HostSolver::average_strategy(uint32_t node, float* sig) const {
 void HostSolver::ensure_symmetric() {
     if (!sym_dirty || !use_iso || spot->perms.size() < 2) { sym_dirty = false; return; }
     arenas_zero = false;
-    symmetrize(0, nullptr, 0);
+    sym_walk(0, nullptr, 0, [&](uint32_t src, uint32_t dst, int k) { copy_branch(src, dst, k); });
     sym_dirty = false;
 }
-void HostSolver::symmetrize(uint32_t node, const uint8_t* dealt, int nd) {
+// The branch copies of ensure_symmetric in its order (cfr.rs:749-800): below
+// every chance node, the representative children first (recursively), then
+// each non-representative child from its representative with the first
+// permutation that maps the card onto it.
+void HostSolver::sym_walk(uint32_t node, const uint8_t* dealt, int nd,
+                          const std::function<void(uint32_t, uint32_t, int)>& on_branch) const {
     const Tree& t = spot->tree;
     if (t.kind[node] == kAction) {
-        for (int a = 0; a < t.nchild[node]; a++) symmetrize(t.child(node, a), dealt, nd);
+        for (int a = 0; a < t.nchild[node]; a++) sym_walk(t.child(node, a), dealt, nd, on_branch);
         return;
     }
     if (t.kind[node] != kChance) return;
@@ -171,38 +176,54 @@ void HostSolver::symmetrize(uint32_t node, const uint8_t* dealt, int nd) {
     for (auto& o : orbit)
         if (o.c == o.rep) {
             d2[nd] = o.c;
-            symmetrize(t.children[t.child_start[node] + o.c], d2, nd + 1);
+            sym_walk(t.children[t.child_start[node] + o.c], d2, nd + 1, on_branch);
         }
     for (auto& o : orbit)
-        if (o.c != o.rep) copy_branch(t.children[t.child_start[node] + o.rep], t.children[t.child_start[node] + o.c], o.k);
+        if (o.c != o.rep) on_branch(t.children[t.child_start[node] + o.rep], t.children[t.child_start[node] + o.c], o.k);
+}
+// The action-node pairs of one branch copy, parent before children
+// (cfr.rs:806-871).
+void HostSolver::branch_walk(uint32_t src, uint32_t dst, int k, const std::function<void(uint32_t, uint32_t)>& on_action) const {
+    const Tree& t = spot->tree;
+    if (t.kind[src] == kAction) {
+        on_action(src, dst);
+        for (int a = 0; a < t.nchild[src]; a++) branch_walk(t.child(src, a), t.child(dst, a), k, on_action);
+    } else if (t.kind[src] == kChance) {
+        for (int x = 0; x < 52; x++) {
+            uint32_t dc = t.children[t.child_start[dst] + x];
+            if (dc == kSentinel) continue;
+            uint8_t sx = card_permute((uint8_t)x, spot->perms[k]);
+            branch_walk(t.children[t.child_start[src] + sx], dc, k, on_action);
+        }
+    }
 }
 void HostSolver::copy_branch(uint32_t src, uint32_t dst, int k) {
     const Tree& t = spot->tree;
-    if (t.kind[src] == kAction) {
-        const int p = t.player[src], na = t.nchild[src];
+    branch_walk(src, dst, k, [&](uint32_t s, uint32_t d) {
+        const int p = t.player[s], na = t.nchild[s];
         const size_t nh = spot->hands[p].size(), cnt = na * nh;
         const auto& tbl = spot->hand_perm[p][k];
-        auto lk = locks.find(src);
+        auto lk = locks.find(s);
         std::vector<float> sr(cnt), ss(cnt), dr(cnt), ds(cnt);
-        regrets[p].read(src, t.data_off[src], cnt, sr.data());
-        strat[p].read(src, t.data_off[src], cnt, ss.data());
+        regrets[p].read(s, t.data_off[s], cnt, sr.data());
+        strat[p].read(s, t.data_off[s], cnt, ss.data());
         for (int a = 0; a < na; a++)
             for (size_t i = 0; i < nh; i++) {
                 size_t j = tbl[i];
                 dr[a * nh + i] = sr[a * nh + j];
                 ds[a * nh + i] = lk != locks.end() ? lk->second[a * nh + j] : ss[a * nh + j];
             }
-        regrets[p].write(dst, t.data_off[dst], cnt, dr.data());
-        strat[p].write(dst, t.data_off[dst], cnt, ds.data());
-        for (int a = 0; a < na; a++) copy_branch(t.child(src, a), t.child(dst, a), k);
-    } else if (t.kind[src] == kChance) {
-        for (int x = 0; x < 52; x++) {
-            uint32_t dc = t.children[t.child_start[dst] + x];
-            if (dc == kSentinel) continue;
-            uint8_t sx = card_permute((uint8_t)x, spot->perms[k]);
-            copy_branch(t.children[t.child_start[src] + sx], dc, k);
-        }
-    }
+        regrets[p].write(d, t.data_off[d], cnt, dr.data());
+        strat[p].write(d, t.data_off[d], cnt, ds.data());
+    });
+}
+std::vector<HostSolver::SymCopy> HostSolver::symmetric_copies() const {
+    std::vector<SymCopy> out;
+    if (!use_iso || spot->perms.size() < 2) return out;
+    sym_walk(0, nullptr, 0, [&](uint32_t src, uint32_t dst, int k) {
+        branch_walk(src, dst, k, [&](uint32_t s, uint32_t d) { out.push_back({s, d, k}); });
+    });
+    return out;
 }
 
 // ------------------------------------------------------- locks (query.rs)
@@ -390,6 +411,22 @@ void validate_locks(const Spot& spot, const std::vector<std::pair<uint32_t, std:
 static const char kMagic[] = "GTOSOLVE2\n";
 
 void HostSolver::save(const std::string& path) const {  // save.rs:92-143
+    std::vector<float> buf;
+    save_stream(path, iteration, [&](int k, FILE* f) {
+        const int p = k % 2, which = k < 2 ? kRegrets : kStrategy;
+        const uint64_t len = spot->tree.data_size[p];
+        buf.resize(len);
+        arena_f32(which, p, buf.data());
+        return write_arena_len(f, len) && fwrite(buf.data(), 4, len, f) == len;
+    });
+}
+bool write_arena_len(FILE* f, uint64_t len) {
+    uint8_t lenb[8];
+    for (int b = 0; b < 8; b++) lenb[b] = (uint8_t)(len >> (8 * b));
+    return fwrite(lenb, 1, 8, f) == 8;
+}
+void HostSolver::save_stream(const std::string& path, uint32_t iter,
+                             const std::function<bool(int, FILE*)>& write_arena) const {
     const std::string tmp = path + ".tmp";
     auto fail = [&](const std::string& m) {
         std::remove(tmp.c_str());
@@ -399,7 +436,7 @@ void HostSolver::save(const std::string& path) const {  // save.rs:92-143
     if (!f) throw Error("cannot create " + tmp + ": " + strerror(errno));
     json::Value h = json::Value::object();
     h.set("config", config_to_json(spot->config));
-    h.set("iteration", json::Value::integer(iteration));
+    h.set("iteration", json::Value::integer(iter));
     json::Value lk = json::Value::array(), lb = json::Value::array();
     for (auto& kv : locks) {
         json::Value e = json::Value::array(), s = json::Value::array();
@@ -418,15 +455,12 @@ void HostSolver::save(const std::string& path) const {  // save.rs:92-143
     h.set("lock_labels", lb);
     std::string hs = json::dump(h);
     bool ok = fwrite(kMagic, 1, 10, f) == 10 && fwrite(hs.data(), 1, hs.size(), f) == hs.size() && fputc('\n', f) != EOF;
-    std::vector<float> buf;
-    for (int k = 0; k < 4 && ok; k++) {
-        const int p = k % 2, which = k < 2 ? kRegrets : kStrategy;
-        const uint64_t len = spot->tree.data_size[p];
-        buf.resize(len);
-        arena_f32(which, p, buf.data());
-        uint8_t lenb[8];
-        for (int b = 0; b < 8; b++) lenb[b] = (uint8_t)(len >> (8 * b));
-        ok = fwrite(lenb, 1, 8, f) == 8 && fwrite(buf.data(), 4, len, f) == len;
+    try {
+        for (int k = 0; k < 4 && ok; k++) ok = write_arena(k, f);
+    } catch (...) {
+        fclose(f);
+        std::remove(tmp.c_str());
+        throw;
     }
     ok = ok && fflush(f) == 0 && fsync(fileno(f)) == 0;
     if (fclose(f) != 0) ok = false;
@@ -437,6 +471,30 @@ void HostSolver::save(const std::string& path) const {  // save.rs:92-143
 std::unique_ptr<HostSolver> HostSolver::load(const std::string& path, int storage_mode) {  // save.rs:149-227
     std::ifstream in(path, std::ios::binary);
     if (!in) throw Error("cannot open " + path);
+    auto s = load_header(in, storage_mode);
+    const Spot* spot = s->spot.get();
+    s->arenas_zero = false;
+    std::vector<float> buf;
+    for (int k = 0; k < 4; k++) {
+        const int p = k % 2;
+        const uint64_t len = read_arena_len(in, spot->tree.data_size[p]);
+        buf.resize(len);
+        if (!in.read((char*)buf.data(), (std::streamsize)(len * 4))) throw Error("truncated arena");
+        s->set_arena_f32(k < 2 ? kRegrets : kStrategy, p, buf.data());
+    }
+    return s;
+}
+uint64_t read_arena_len(std::istream& in, uint64_t expected) {
+    uint8_t lb[8];
+    if (!in.read((char*)lb, 8)) throw Error("truncated arena");
+    uint64_t len = 0;
+    for (int b = 0; b < 8; b++) len |= (uint64_t)lb[b] << (8 * b);
+    if (len != expected)
+        throw Error("arena size mismatch: file " + std::to_string(len) + ", expected " + std::to_string(expected) +
+                    " (tree config changed?)");
+    return len;
+}
+std::unique_ptr<HostSolver> HostSolver::load_header(std::istream& in, int storage_mode) {  // save.rs:149-188
     char magic[10];
     if (!in.read(magic, 10) || std::memcmp(magic, kMagic, 10) != 0) throw Error("not a solver save file");
     std::string hl;
@@ -476,25 +534,10 @@ std::unique_ptr<HostSolver> HostSolver::load(const std::string& path, int storag
         throw Error(std::string("bad lock section: ") + e.what());
     }
     auto s = std::make_unique<HostSolver>(spot, storage_mode, kDcfr, true);
-    s->arenas_zero = false;
     s->iteration = (uint32_t)it->num;
     for (auto& l : locks) s->locks[l.first] = l.second;
     s->lock_labels = labels;
     if (!s->locks.empty()) s->sym_dirty = true;
-    std::vector<float> buf;
-    for (int k = 0; k < 4; k++) {
-        const int p = k % 2;
-        uint8_t lb[8];
-        if (!in.read((char*)lb, 8)) throw Error("truncated arena");
-        uint64_t len = 0;
-        for (int b = 0; b < 8; b++) len |= (uint64_t)lb[b] << (8 * b);
-        if (len != spot->tree.data_size[p])
-            throw Error("arena size mismatch: file " + std::to_string(len) + ", expected " +
-                        std::to_string(spot->tree.data_size[p]) + " (tree config changed?)");
-        buf.resize(len);
-        if (!in.read((char*)buf.data(), (std::streamsize)(len * 4))) throw Error("truncated arena");
-        s->set_arena_f32(k < 2 ? kRegrets : kStrategy, p, buf.data());
-    }
     return s;
 }
 

@@ -5,6 +5,9 @@
 // on the GPU (engine.cu); this object is the source of truth for queries,
 // locks and .gto saves (save.rs).
 #pragma once
+#include <cstdio>
+#include <functional>
+#include <istream>
 #include <map>
 #include <memory>
 #include <string>
@@ -70,14 +73,40 @@ struct HostSolver {
                        const std::vector<std::pair<std::string, std::vector<float>>>& edits, const std::string& label);
     void walk(const std::vector<int>& steps, uint32_t* node, std::vector<float> reach[2]) const;
     std::vector<int> canonical_steps(const std::vector<int>& steps, std::array<uint8_t, 4>* perm) const;
+    // Action-node copies ensure_symmetric makes, in its order: dst's blocks
+    // become src's under hand permutation `perm` (a locked src gives its lock
+    // as the strategy sums).  Empty without suit isomorphism.
+    struct SymCopy {
+        uint32_t src, dst;
+        int perm;
+    };
+    std::vector<SymCopy> symmetric_copies() const;
     // .gto (save.rs)
     void save(const std::string& path) const;
     static std::unique_ptr<HostSolver> load(const std::string& path, int storage_mode);
+    // The save with its arena section written by the caller: header (config,
+    // `iteration`, this solver's locks), then write_arena(k, f) for k = 0..3
+    // (regrets of players 0, 1, strategy sums of players 0, 1), each writing
+    // its little-endian u64 length and f32 data; staged in `path`.tmp and
+    // renamed over `path` once durable (save.rs:92-143).
+    void save_stream(const std::string& path, uint32_t iteration,
+                     const std::function<bool(int, FILE*)>& write_arena) const;
+    // The header half of load (save.rs:149-188): the spot rebuilt from the
+    // saved config (lenient), locks validated, arenas still zero; `in` is left
+    // at the first arena section.
+    static std::unique_ptr<HostSolver> load_header(std::istream& in, int storage_mode);
 
   private:
-    void symmetrize(uint32_t node, const uint8_t* dealt, int nd);
+    void sym_walk(uint32_t node, const uint8_t* dealt, int nd,
+                  const std::function<void(uint32_t, uint32_t, int)>& on_branch) const;
+    void branch_walk(uint32_t src, uint32_t dst, int k, const std::function<void(uint32_t, uint32_t)>& on_action) const;
     void copy_branch(uint32_t src, uint32_t dst, int k);
 };
+
+// One arena section's length field of a .gto: write it, or read it and check
+// it against the tree's arena size.
+bool write_arena_len(FILE* f, uint64_t len);
+uint64_t read_arena_len(std::istream& in, uint64_t expected);
 
 void validate_locks(const Spot& spot, const std::vector<std::pair<uint32_t, std::vector<float>>>& locks);
 void rake_to_target(float* sigma, int na, int nh, const float* reach, const float* target);

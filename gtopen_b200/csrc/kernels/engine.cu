@@ -24,8 +24,11 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <istream>
+#include <map>
 #include <mutex>
 #include <stdexcept>
+#include <unordered_map>
 #include <string>
 #include <vector>
 
@@ -126,6 +129,24 @@ struct EngineImpl {
         if (stream) cudaStreamDestroy(stream);
     }
 
+    // The f32 reference-layout image in `staging` into device arena `which` of
+    // player q (encoded for 16-bit and FP8 arenas, with per-node scales).
+    void encode_staging(int which, int q) {
+        const unsigned nb = (unsigned)plan.n_anodes[q];
+        if (!nb) return;
+        const int nh = plan.nh[q];
+        void* dst = which == kRegrets ? ar.reg[q] : which == kStrategy ? ar.str[q] : ar.pred[q];
+        if (fmt == kFmtF32) {
+            k_to_dev<float><<<nb, kThreads, 0, stream>>>(staging, (float*)dst, xnodes[q], nh);
+        } else {
+            float* dsc = which == kRegrets ? ar.rscale[q] : which == kStrategy ? ar.sscale[q] : ar.pscale[q];
+            if (fmt == kFmtFP8)
+                k_encode_fp8<<<nb, kThreads, 0, stream>>>(staging, (uint8_t*)dst, dsc, xnodes[q], nh, which == kStrategy);
+            else
+                k_encode<<<nb, kThreads, 0, stream>>>(staging, dst, dsc, xnodes[q], nh, which == kStrategy);
+        }
+        CK(cudaGetLastError());
+    }
     void upload_locks(const HostSolver& host) {
         if (lock_buf) {
             CK(cudaStreamSynchronize(stream));
@@ -639,17 +660,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
             }
             CK(cudaMemcpy(E.staging, src32, sp.tree.data_size[q] * 4, cudaMemcpyHostToDevice));
             g_uploaded += sp.tree.data_size[q] * 4;
-            if (E.fmt == kFmtF32) {
-                k_to_dev<float><<<nb, kThreads, 0, E.stream>>>(E.staging, (float*)dst, E.xnodes[q], nh);
-            } else {
-                float* dsc = which == kRegrets ? E.ar.rscale[q] : which == kStrategy ? E.ar.sscale[q] : E.ar.pscale[q];
-                if (E.fmt == kFmtFP8)
-                    k_encode_fp8<<<nb, kThreads, 0, E.stream>>>(E.staging, (uint8_t*)dst, dsc, E.xnodes[q], nh,
-                                                                 which == kStrategy);
-                else
-                    k_encode<<<nb, kThreads, 0, E.stream>>>(E.staging, dst, dsc, E.xnodes[q], nh, which == kStrategy);
-            }
-            CK(cudaGetLastError());
+            E.encode_staging(which, q);
             CK(cudaStreamSynchronize(E.stream));
         }
     }
@@ -736,8 +747,14 @@ void GpuEngine::root_cfv(int p, int mode, float* out) {
 
 void GpuEngine::export_arena(int which, int p, float* out) {
     EngineImpl& E = *d_;
-    const Spot& sp = *E.spot;
-    const size_t len = sp.tree.data_size[p];
+    fill_staging(which, p);
+    CK(cudaMemcpyAsync(out, E.staging, E.spot->tree.data_size[p] * 4, cudaMemcpyDeviceToHost, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+}
+// Device arena `which` of player p decoded into `staging` in the reference
+// layout; nodes the engine does not hold (symmetric branches) are zero.
+void GpuEngine::fill_staging(int which, int p) {
+    EngineImpl& E = *d_;
     CK(cudaMemsetAsync(E.staging, 0, E.staging_len * 4, E.stream));
     const unsigned nb = (unsigned)E.plan.n_anodes[p];
     void* src = which == kRegrets ? E.ar.reg[p] : which == kStrategy ? E.ar.str[p] : E.ar.pred[p];
@@ -758,8 +775,252 @@ void GpuEngine::export_arena(int which, int p, float* out) {
         }
         CK(cudaGetLastError());
     }
-    CK(cudaMemcpyAsync(out, E.staging, len * 4, cudaMemcpyDeviceToHost, E.stream));
+}
+
+// ------------------------------------------------ .gto straight from / to HBM
+// One block of a device save's image: dst <- src gathered through a hand
+// permutation table, action by action (cfr.rs:806-871 copy_branch, with
+// chains of copies composed down to a block in the image or one in the aux
+// buffer: a lock, or a host block the engine does not hold).
+struct SymOp {
+    uint64_t dst, src;  // element offsets: dst in the image, src in the image or the aux buffer
+    uint32_t na, tbl, aux, pad;
+};
+__global__ void k_sym_gather(float* img, const float* aux, const uint16_t* tbls, const SymOp* ops, int nh) {
+    const SymOp op = ops[blockIdx.x];
+    const uint16_t* T = tbls + (size_t)op.tbl * nh;
+    const float* src = op.aux ? aux + op.src : img + op.src;
+    const int n = (int)op.na * nh;
+    for (int e = threadIdx.x; e < n; e += blockDim.x) {
+        const int a = e / nh, i = e - a * nh;
+        img[op.dst + e] = src[(size_t)a * nh + T[i]];
+    }
+}
+
+namespace {
+// Device buffers and pinned host buffers owned for the length of one call.
+struct TempDev {
+    std::vector<void*> bufs;
+    template <class T>
+    T* put(const std::vector<T>& v, cudaStream_t st) {
+        void* p = nullptr;
+        CK(cudaMalloc(&p, std::max<size_t>(v.size(), 1) * sizeof(T)));
+        bufs.push_back(p);
+        if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+        return (T*)p;
+    }
+    ~TempDev() {
+        for (void* p : bufs) cudaFree(p);
+    }
+};
+// Two pinned chunks and their events: the copy of one chunk overlaps the
+// file I/O of the other.
+struct PinnedPair {
+    static constexpr size_t kChunk = size_t(8) << 20;  // floats (32 MiB)
+    float* h[2] = {nullptr, nullptr};
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    PinnedPair() {
+        for (int b = 0; b < 2; b++) {
+            CK(cudaMallocHost(&h[b], kChunk * sizeof(float)));
+            CK(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+        }
+    }
+    ~PinnedPair() {
+        for (int b = 0; b < 2; b++) {
+            if (ev[b]) cudaEventDestroy(ev[b]);
+            if (h[b]) cudaFreeHost(h[b]);
+        }
+    }
+};
+}  // namespace
+
+void GpuEngine::save(const HostSolver& host, const std::string& path) {
+    EngineImpl& E = *d_;
     CK(cudaStreamSynchronize(E.stream));
+    E.check_err();
+    const Spot& sp = *E.spot;
+    const Tree& t = sp.tree;
+    if (host.spot->tree.size() != t.size() || host.spot->tree.data_size[0] != t.data_size[0] ||
+        host.spot->tree.data_size[1] != t.data_size[1])
+        throw Error("invalid argument: the solver is not the one this GPU solver was built from");
+    // The image of each arena, as the host path leaves it (sync_to_cpu, then
+    // ensure_symmetric): the engine's blocks; with suit isomorphism, each
+    // copy of ensure_symmetric in its order, composed with the copy that
+    // produced its source until the source is a block of the image or a lock
+    // (strategy sums); and the host's own values for the blocks neither
+    // writes (children of a chance node for an already dealt card, which no
+    // sweep visits).
+    std::vector<std::vector<uint16_t>> tbl[2];
+    std::map<std::vector<uint16_t>, uint32_t> tid[2];
+    auto intern = [&](int p, std::vector<uint16_t>&& T) {
+        auto it = tid[p].find(T);
+        if (it != tid[p].end()) return it->second;
+        const uint32_t k = (uint32_t)tbl[p].size();
+        tid[p].emplace(T, k);
+        tbl[p].push_back(std::move(T));
+        return k;
+    };
+    for (int p = 0; p < 2; p++) {
+        std::vector<uint16_t> id(E.plan.nh[p]);
+        for (size_t i = 0; i < id.size(); i++) id[i] = (uint16_t)i;
+        intern(p, std::move(id));
+    }
+    struct Src {
+        uint32_t node, tbl;
+        bool lock;
+    };
+    std::vector<SymOp> fill[2][2], copy[2][2];  // [regrets / strategy sums][player]
+    std::vector<float> aux[2];                    // per arena kind: host blocks, then locks
+    if (E.plan.iso_active) {
+        std::unordered_map<uint32_t, Src> rsrc, ssrc;
+        for (const auto& c : host.symmetric_copies()) {
+            const int p = t.player[c.src];
+            const auto& hk = sp.hand_perm[p][c.perm];
+            auto compose = [&](uint32_t base) {
+                const std::vector<uint16_t>& B = tbl[p][base];
+                std::vector<uint16_t> T(hk.size());
+                for (size_t i = 0; i < T.size(); i++) T[i] = B[hk[i]];
+                return intern(p, std::move(T));
+            };
+            auto ri = rsrc.find(c.src);
+            const Src r = ri != rsrc.end() ? ri->second : Src{c.src, 0, false};
+            rsrc[c.dst] = {r.node, compose(r.tbl), false};
+            if (host.locks.count(c.src)) {
+                ssrc[c.dst] = {c.src, compose(0), true};
+            } else {
+                auto si = ssrc.find(c.src);
+                const Src q = si != ssrc.end() ? si->second : Src{c.src, 0, false};
+                ssrc[c.dst] = {q.node, compose(q.tbl), q.lock};
+            }
+        }
+        for (uint32_t nd = 0; nd < t.size(); nd++) {
+            if (t.kind[nd] != kAction || E.plan.node_sidx[nd] >= 0 || rsrc.count(nd)) continue;
+            const int p = t.player[nd];
+            const size_t cnt = (size_t)t.nchild[nd] * E.plan.nh[p];
+            for (int w = 0; w < 2; w++) {
+                const size_t at = aux[w].size();
+                aux[w].resize(at + cnt);
+                (w == 0 ? host.regrets[p] : host.strat[p]).read(nd, t.data_off[nd], cnt, aux[w].data() + at);
+                fill[w][p].push_back({t.data_off[nd], at, t.nchild[nd], 0u, 1u, 0u});
+            }
+        }
+        std::map<uint32_t, uint64_t> lock_at;
+        for (int w = 0; w < 2; w++)
+            for (const auto& kv : w == 0 ? rsrc : ssrc) {
+                const uint32_t dst = kv.first;
+                const Src& sr = kv.second;
+                uint64_t src_off = t.data_off[sr.node];
+                if (sr.lock) {
+                    auto it = lock_at.find(sr.node);
+                    if (it == lock_at.end()) {
+                        const auto& lv = host.locks.at(sr.node);
+                        it = lock_at.emplace(sr.node, (uint64_t)aux[1].size()).first;
+                        aux[1].insert(aux[1].end(), lv.begin(), lv.end());
+                    }
+                    src_off = it->second;
+                }
+                copy[w][t.player[dst]].push_back({t.data_off[dst], src_off, t.nchild[dst], sr.tbl, sr.lock ? 1u : 0u, 0u});
+            }
+    }
+    TempDev tmp;
+    const uint16_t* dtbl[2] = {nullptr, nullptr};
+    for (int p = 0; p < 2; p++) {
+        std::vector<uint16_t> flat;
+        for (const auto& T : tbl[p]) flat.insert(flat.end(), T.begin(), T.end());
+        dtbl[p] = tmp.put(flat, E.stream);
+    }
+    const float* daux[2] = {tmp.put(aux[0], E.stream), tmp.put(aux[1], E.stream)};
+    PinnedPair pin;
+    host.save_stream(path, E.iteration, [&](int k, FILE* f) {
+        const int p = k % 2, w = k < 2 ? 0 : 1;
+        const uint64_t len = t.data_size[p];
+        fill_staging(w == 0 ? kRegrets : kStrategy, p);
+        for (const auto* ops : {&fill[w][p], &copy[w][p]})  // the copies read filled blocks: two launches
+            if (!ops->empty()) {
+                const SymOp* dops = tmp.put(*ops, E.stream);
+                k_sym_gather<<<(unsigned)ops->size(), kThreads, 0, E.stream>>>(E.staging, daux[w], dtbl[p], dops,
+                                                                              E.plan.nh[p]);
+                CK(cudaGetLastError());
+            }
+        if (!write_arena_len(f, len)) return false;
+        const size_t nc = (len + PinnedPair::kChunk - 1) / PinnedPair::kChunk;
+        auto issue = [&](size_t j) {
+            const size_t off = j * PinnedPair::kChunk, cnt = std::min<size_t>(PinnedPair::kChunk, len - off);
+            CK(cudaMemcpyAsync(pin.h[j & 1], E.staging + off, cnt * 4, cudaMemcpyDeviceToHost, E.stream));
+            CK(cudaEventRecord(pin.ev[j & 1], E.stream));
+        };
+        if (nc) issue(0);
+        for (size_t j = 0; j < nc; j++) {
+            if (j + 1 < nc) issue(j + 1);
+            CK(cudaEventSynchronize(pin.ev[j & 1]));
+            const size_t cnt = std::min<size_t>(PinnedPair::kChunk, len - j * PinnedPair::kChunk);
+            if (fwrite(pin.h[j & 1], 4, cnt, f) != cnt) {
+                CK(cudaStreamSynchronize(E.stream));
+                return false;
+            }
+        }
+        return true;
+    });
+    CK(cudaStreamSynchronize(E.stream));
+}
+
+void GpuEngine::load_arenas(std::istream& in, HostSolver& host) {
+    EngineImpl& E = *d_;
+    CK(cudaStreamSynchronize(E.stream));
+    const Tree& t = E.spot->tree;
+    // blocks the device does not hold, in arena order: they go to the host
+    // arenas (a block split over two chunks is assembled first)
+    struct Blk {
+        uint64_t off;
+        size_t cnt;
+        uint32_t node;
+    };
+    std::vector<Blk> rest[2];
+    for (uint32_t nd = 0; nd < t.size(); nd++)
+        if (t.kind[nd] == kAction && E.plan.node_sidx[nd] < 0)
+            rest[t.player[nd]].push_back({t.data_off[nd], (size_t)t.nchild[nd] * E.plan.nh[t.player[nd]], nd});
+    for (auto& r : rest) std::sort(r.begin(), r.end(), [](const Blk& a, const Blk& b) { return a.off < b.off; });
+    if (!rest[0].empty() || !rest[1].empty()) host.arenas_zero = false;
+    PinnedPair pin;
+    std::vector<float> part;
+    for (int k = 0; k < 4; k++) {
+        const int p = k % 2, which = k < 2 ? kRegrets : kStrategy;
+        Arena& ha = which == kRegrets ? host.regrets[p] : host.strat[p];
+        const uint64_t len = read_arena_len(in, t.data_size[p]);
+        const size_t nc = (len + PinnedPair::kChunk - 1) / PinnedPair::kChunk;
+        size_t b = 0;  // next block of rest[p]
+        for (size_t j = 0; j < nc; j++) {
+            const size_t off = j * PinnedPair::kChunk, cnt = std::min<size_t>(PinnedPair::kChunk, len - off);
+            float* hb = pin.h[j & 1];
+            if (j >= 2) CK(cudaEventSynchronize(pin.ev[j & 1]));  // its previous copy has left the buffer
+            if (!in.read((char*)hb, (std::streamsize)(cnt * 4))) throw Error("truncated arena");
+            CK(cudaMemcpyAsync(E.staging + off, hb, cnt * 4, cudaMemcpyHostToDevice, E.stream));
+            CK(cudaEventRecord(pin.ev[j & 1], E.stream));
+            for (; b < rest[p].size() && rest[p][b].off < off + cnt; b++) {
+                const Blk& x = rest[p][b];
+                if (x.off >= off && x.off + x.cnt <= off + cnt) {
+                    ha.write(x.node, x.off, x.cnt, hb + (x.off - off));
+                    continue;
+                }
+                // split block: its parts in this chunk and the next ones
+                const uint64_t lo = std::max<uint64_t>(x.off, off), hi = std::min<uint64_t>(x.off + x.cnt, off + cnt);
+                if (x.off >= off) part.assign(x.cnt, 0.0f);
+                std::memcpy(part.data() + (lo - x.off), hb + (lo - off), (hi - lo) * sizeof(float));
+                if (x.off + x.cnt > off + cnt) break;  // continues in the next chunk
+                ha.write(x.node, x.off, x.cnt, part.data());
+            }
+        }
+        E.encode_staging(which, p);
+        CK(cudaStreamSynchronize(E.stream));
+    }
+    for (int p = 0; p < 2; p++)  // the file holds no predictions: PCFR+ restarts them at zero
+        if (E.ar.pred[p]) {
+            CK(cudaMemsetAsync(E.ar.pred[p], 0, E.plan.arena_len[p] * (size_t)fmt_bytes(E.fmt), E.stream));
+            if (E.ar.pscale[p]) CK(cudaMemsetAsync(E.ar.pscale[p], 0, std::max<uint64_t>(E.plan.n_anodes[p], 1) * 4, E.stream));
+        }
+    E.reach_valid = false;
+    CK(cudaStreamSynchronize(E.stream));
+    E.check_err();
 }
 
 // ------------------------------------------------ allocation-free node read

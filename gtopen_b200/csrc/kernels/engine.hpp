@@ -58,8 +58,21 @@ class GpuEngine {
     // scratch of kNodeScratchElems floats: no allocation, host or device, on
     // success.  Returns the element count written to out.
     size_t read_node_static(int which, uint32_t node, float* out, size_t out_len);
+    void fill_staging(int which, int p);
     // time one kind of level launch set: used by bench for the roofline
     void discounts(float* out3);
+    // .gto written from the device arenas through a pinned double buffer (no
+    // host arena copy): the bytes sync_to_cpu into an f32 host solver,
+    // ensure_symmetric and save would write.  Header (config, locks) from
+    // `host`, iteration from this engine.
+    void save(const HostSolver& host, const std::string& path);
+    // The arena section of a .gto (`in` at its first arena) streamed into the
+    // device arenas: the state an engine built from a host solver loaded from
+    // that file starts with.  The blocks the engine does not hold (symmetric
+    // branches, children of chance nodes for dealt cards) go to `host`'s
+    // arenas, so that after sync_to_cpu it holds what a host load would.
+    // PCFR+ predictions restart at zero.
+    void load_arenas(std::istream& in, HostSolver& host);
 
   private:
     std::unique_ptr<EngineImpl> d_;

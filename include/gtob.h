@@ -183,6 +183,25 @@ int gtob_gpu_time_iterations(gtob_gpu* gpu, int n, double* ms);
 /* the last discounts the device computed (pos, neg, strat) */
 int gtob_gpu_discounts(gtob_gpu* gpu, float* out3);
 
+/* Solver::save (save.rs:92-143) of the state GpuSolver::sync_to_cpu
+ * (gpu/mod.rs:845) followed by Solver::ensure_symmetric (cfr.rs:749) leaves
+ * in an f32 host solver, written from the device arenas: the arenas are
+ * decoded on the device, symmetric branches gathered there, and the file is
+ * streamed through two 32 MiB pinned buffers -- no host arena is touched.
+ * Header (config, locks, labels) from `solver`, iteration from `gpu`; staged
+ * in path.tmp and renamed once durable, as the reference's save. */
+int gtob_gpu_save(gtob_gpu* gpu, const gtob_solver* solver, const char* path);
+/* Solver::load_with_storage (save.rs:149-227) + GpuSolver::new
+ * (gpu/mod.rs:146) with the arenas streamed from the file straight into
+ * device memory.  *solver_out gets the spot (rebuilt leniently from the
+ * saved config), locks, iteration and the blocks the device does not hold
+ * (symmetric branches, children of chance nodes for dealt cards); the blocks
+ * the device holds stay zero on the host until gtob_gpu_sync_to_cpu.
+ * *gpu_out holds the loaded state (device_format GTOB_DEVICE_*, engine
+ * GTOB_ENGINE_*).  PCFR+ predictions start at zero. */
+int gtob_gpu_load(const char* path, int storage, int device_format, int engine, gtob_solver** solver_out,
+                  gtob_gpu** gpu_out);
+
 /* No counterpart in the reference.  One action node's arena block (which:
  * GTOB_ARENA_*), decoded to f32 in the reference layout [action * nh + hand],
  * the same values gtob_gpu_export_arena gives for that node, read through a
