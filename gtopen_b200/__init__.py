@@ -48,6 +48,11 @@ class GpuInfo(C.Structure):
                 ("arena_format", C.c_int32), ("iter_bytes", C.c_double), ("upload_bytes", C.c_uint64)]
 
 
+class BatchRow(C.Structure):
+    _fields_ = [("status", C.c_int32), ("iterations", C.c_uint32), ("exploit_pct", C.c_double),
+                ("seconds", C.c_double), ("ev", C.c_double * 2)]
+
+
 class Profile(C.Structure):
     _fields_ = [("ms", C.c_double * 7), ("launches", C.c_uint32 * 7)]
 
@@ -115,6 +120,13 @@ def lib():
         "gtob_gpu_read_node_static": (I, [P, I, C.c_uint32, P, C.c_uint64, P]),
         "gtob_gpu_discounts": (I, [P, P]),
         "gtob_gpu_save": (I, [P, P, C.c_char_p]),
+        "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, C.POINTER(P)]),
+        "gtob_batch_run": (I, [P, U32, D, U32, I]),
+        "gtob_batch_size": (I, [P]),
+        "gtob_batch_row_get": (I, [P, I, C.POINTER(BatchRow)]),
+        "gtob_batch_error": (C.c_char_p, [P, I]),
+        "gtob_batch_solver": (P, [P, I]),
+        "gtob_batch_free": (None, [P]),
         "gtob_gpu_load": (I, [C.c_char_p, I, I, I, C.POINTER(P), C.POINTER(P)]),
         "gtob_set_device": (I, [I]),
         "gtob_gpu_time_iterations": (I, [P, I, C.POINTER(D)]),
@@ -248,9 +260,9 @@ class Solver:
         self._h = h
 
     def __del__(self):
-        if getattr(self, "_h", None) and _LIB is not None:
+        if getattr(self, "_h", None) and _LIB is not None and getattr(self, "_owner", None) is None:
             _LIB.gtob_solver_free(self._h)
-            self._h = None
+        self._h = None
 
     @property
     def iteration(self):
@@ -453,6 +465,49 @@ class GpuSolver:
         ms = C.c_double()
         _check(lib().gtob_gpu_time_iterations(self._h, int(n), C.byref(ms)))
         return ms.value
+
+
+class Batch:
+    """Many spots solved on one GPU at once (the reference's batch report,
+    solve_cli.rs:125-215, with the spots side by side): see gtob_batch_* in
+    include/gtob.h."""
+
+    def __init__(self, spots, storage="f32", algo="dcfr", use_iso=True, device_format=None, engine="staged"):
+        self.spots = list(spots)
+        arr = (C.c_void_p * len(self.spots))(*[sp._h for sp in self.spots])
+        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}[engine]
+        h = C.c_void_p()
+        _check(lib().gtob_batch_new(arr, len(self.spots), STORAGE[storage], ALGO[algo], int(use_iso),
+                                    DEVICE_FORMAT[device_format], eng, C.byref(h)))
+        self._h = h
+        self.storage = storage
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gtob_batch_free(self._h)
+            self._h = None
+
+    def run(self, max_iterations=300, target_pct=0.3, check_every=20, workers=8):
+        _check(lib().gtob_batch_run(self._h, int(max_iterations), float(target_pct), int(check_every), int(workers)))
+
+    def rows(self):
+        out = []
+        for i in range(len(self.spots)):
+            r = BatchRow()
+            _check(lib().gtob_batch_row_get(self._h, i, C.byref(r)))
+            out.append({"status": r.status, "iterations": r.iterations, "exploit_pct": r.exploit_pct,
+                        "seconds": r.seconds, "ev": [r.ev[0], r.ev[1]],
+                        "error": lib().gtob_batch_error(self._h, i).decode(errors="replace")})
+        return out
+
+    def solver(self, i):
+        """The i-th host solver (owned by the batch, synced after run)."""
+        h = lib().gtob_batch_solver(self._h, int(i))
+        if not h:
+            raise IndexError(i)
+        sv = Solver(self.spots[i], storage=self.storage, _handle=C.c_void_p(h))
+        sv._owner = self
+        return sv
 
 
 def set_device(device):

@@ -1,0 +1,37 @@
+// Many spots on one GPU at once: the reference's batch report
+// (solve_cli.rs:125-215, run per board with solve_quiet, solve_cli.rs:338-362)
+// with the spots solved side by side instead of one after another.  Worker
+// threads each take the next spot, build its GPU engine (own streams, own
+// CUDA graphs), solve it to the target, read its root EVs and sync it back;
+// the engines of different workers run concurrently on the device, which a
+// single spot of a few thousand nodes cannot fill.
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "solver.hpp"
+
+namespace gtob {
+
+struct BatchRow {
+    std::string error;  // empty: solved
+    uint32_t iterations = 0;
+    double exploit_pct = 0.0;  // exploitability, % of the starting pot
+    double seconds = 0.0;      // wall time of this spot: engine build, solve, EVs, sync
+    double ev[2] = {0.0, 0.0};  // reach-weighted root EV per player, pot-share (solve_cli.rs:176-188)
+};
+
+// Runs solve_quiet's loop (one iteration at a time, exploitability when the
+// iteration is a multiple of check_every or reaches max_iterations, stop at
+// target_pct or max_iterations, then sync_to_cpu) for every solver, with up to
+// `workers` spots in flight; rows[i] describes solvers[i].  Errors stay in
+// their row.  Must be called with the target device current.
+void run_batch(const std::vector<HostSolver*>& solvers, int device_format, int engine, uint32_t max_iterations,
+               double target_pct, uint32_t check_every, int workers, std::vector<BatchRow>& rows);
+
+// Per-hand compatible opponent reach mass (query.rs:463-488), f64.
+std::vector<double> valid_opp_sum(const Spot& spot, int p, const float* reach_o);
+
+}  // namespace gtob

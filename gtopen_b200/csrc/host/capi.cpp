@@ -11,6 +11,7 @@
 #include <string>
 
 #include "../kernels/engine.hpp"
+#include "batch.hpp"
 #include "core.hpp"
 #include "solver.hpp"
 
@@ -266,6 +267,58 @@ int gtob_load(const char* path, int storage, gtob_solver** out) {
     *out = new gtob_solver{HostSolver::load(path, storage)};
     API_END
 }
+
+struct gtob_batch {
+    std::vector<std::unique_ptr<gtob_solver>> solvers;
+    std::vector<BatchRow> rows;
+    int fmt = -1, engine = GTOB_ENGINE_STAGED;
+};
+int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int use_iso, int fmt, int engine,
+                   gtob_batch** out) {
+    REQUIRE(spots && out && n > 0 && (storage == 0 || storage == 1) && algo >= 0 && algo <= 2 && fmt >= -1 &&
+            fmt <= 2 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+    *out = nullptr;
+    for (int i = 0; i < n; i++) REQUIRE(spots[i]);
+    API_BEGIN
+    auto b = std::make_unique<gtob_batch>();
+    for (int i = 0; i < n; i++)
+        b->solvers.push_back(std::make_unique<gtob_solver>(
+            gtob_solver{std::make_unique<HostSolver>(spots[i]->s, storage, algo, use_iso != 0)}));
+    b->rows.resize(n);
+    b->fmt = fmt;
+    b->engine = engine;
+    *out = b.release();
+    API_END
+}
+int gtob_batch_run(gtob_batch* b, uint32_t max_iterations, double target_pct, uint32_t check_every, int workers) {
+    REQUIRE(b && check_every > 0 && workers > 0);
+    API_BEGIN
+    std::vector<HostSolver*> hs;
+    for (auto& v : b->solvers) hs.push_back(v->v.get());
+    run_batch(hs, b->fmt, b->engine, max_iterations, target_pct, check_every, workers, b->rows);
+    API_END
+}
+int gtob_batch_size(const gtob_batch* b) { return b ? (int)b->solvers.size() : 0; }
+int gtob_batch_row_get(const gtob_batch* b, int i, gtob_batch_row* out) {
+    REQUIRE(b && out && i >= 0 && i < (int)b->rows.size());
+    const BatchRow& r = b->rows[i];
+    out->status = r.error.empty() ? GTOB_OK : classify(r.error);
+    out->iterations = r.iterations;
+    out->exploit_pct = r.exploit_pct;
+    out->seconds = r.seconds;
+    out->ev[0] = r.ev[0];
+    out->ev[1] = r.ev[1];
+    return GTOB_OK;
+}
+const char* gtob_batch_error(const gtob_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->rows.size()) return "";
+    return b->rows[i].error.c_str();
+}
+gtob_solver* gtob_batch_solver(gtob_batch* b, int i) {
+    if (!b || i < 0 || i >= (int)b->solvers.size()) return nullptr;
+    return b->solvers[i].get();
+}
+void gtob_batch_free(gtob_batch* b) { delete b; }
 
 int gtob_gpu_save(gtob_gpu* g, const gtob_solver* v, const char* path) {
     REQUIRE(g && v && path);

@@ -202,6 +202,38 @@ int gtob_gpu_save(gtob_gpu* gpu, const gtob_solver* solver, const char* path);
 int gtob_gpu_load(const char* path, int storage, int device_format, int engine, gtob_solver** solver_out,
                   gtob_gpu** gpu_out);
 
+/* ---- batch of spots (solve_cli.rs:125-215 batch) ------------------------ */
+/* The reference's batch report solves one board after another
+ * (solve_quiet, solve_cli.rs:338-362).  A batch solves many spots on one GPU
+ * at once: `workers` host threads each take the next spot, build its engine
+ * (own streams and CUDA graphs), run solve_quiet's loop -- one iteration at a
+ * time, exploitability when the iteration is a multiple of check_every (the
+ * reference: 20) or reaches max_iterations, stop at target_pct or
+ * max_iterations -- read the root EVs, sync the solver back and free the
+ * engine.  Engines of different workers run concurrently on the device.
+ * gtob_batch_new creates one host solver per spot (storage, algo, use_iso as
+ * gtob_solver_new); device_format / engine as gtob_gpu_new_ex.  Call
+ * gtob_batch_run with the device current; an error in one spot stays in its
+ * row (status, gtob_batch_error) and the others go on. */
+typedef struct gtob_batch gtob_batch;
+typedef struct {
+    int32_t status;      /* GTOB_OK, or the error class of this spot */
+    uint32_t iterations; /* iterations run */
+    double exploit_pct;  /* last exploitability check, % of the starting pot */
+    double seconds;      /* wall time of this spot: engine build, solve, EVs, sync */
+    double ev[2];        /* reach-weighted root EV per player, pot-share convention (solve_cli.rs:176-188) */
+} gtob_batch_row;
+int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int use_iso, int device_format, int engine,
+                   gtob_batch** out);
+int gtob_batch_run(gtob_batch* batch, uint32_t max_iterations, double target_pct, uint32_t check_every, int workers);
+int gtob_batch_size(const gtob_batch* batch);
+int gtob_batch_row_get(const gtob_batch* batch, int i, gtob_batch_row* out);
+/* the message of a failed row ("" when the row solved) */
+const char* gtob_batch_error(const gtob_batch* batch, int i);
+/* the i-th host solver, owned by the batch (valid until gtob_batch_free) */
+gtob_solver* gtob_batch_solver(gtob_batch* batch, int i);
+void gtob_batch_free(gtob_batch* batch);
+
 /* No counterpart in the reference.  One action node's arena block (which:
  * GTOB_ARENA_*), decoded to f32 in the reference layout [action * nh + hand],
  * the same values gtob_gpu_export_arena gives for that node, read through a

@@ -324,3 +324,19 @@ def test_invalid_inputs_are_errors_not_crashes():
         hsv.lock_node([99], "freeze")
     with pytest.raises(g.GtobError):
         hsv.set_lock(0, np.zeros(3, np.float32))
+
+
+def test_batch_host_side():
+    """A batch holds one host solver per spot before it runs; without a GPU
+    the run is an error, not a crash."""
+    spots = [g.Spot(W.small_flop_spot()), g.Spot(W.iso_spot())]
+    b = g.Batch(spots, storage="compressed")
+    assert [b.solver(i).iteration for i in range(2)] == [0, 0]
+    assert b.solver(1).arena(1, 0).shape == (spots[1].data_size[0],)
+    rows = b.rows()
+    assert [r["iterations"] for r in rows] == [0, 0]
+    if g.vram_info_mb() is None:
+        with pytest.raises(g.GtobError) as e:
+            b.run(max_iterations=5)
+        assert "cuda" in str(e.value)
+
