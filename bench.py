@@ -318,6 +318,83 @@ def run_ours(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_report(args, world, rank, local):
+    """The flop report (184 suit-isomorphism classes of flops, the turn
+    config's spot on each, 1-3 bet sizes per flop): every flop solved to the
+    target through the batch API, `--report-workers` spots in flight on the
+    GPU.  Flops are dealt round-robin over the ranks (strong scaling)."""
+    import numpy as np
+
+    import gtopen_b200 as g
+    from concurrent.futures import ThreadPoolExecutor
+    from gtopen_b200 import workloads as W
+    g.set_device(local)
+    pool = ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1)))
+    t0 = time.perf_counter()
+    cfgs, spots = W.flop_report_spots(g.evaluate7, lambda cs: list(pool.map(g.Spot, cs)), n=args.report_flops)
+    build_s = time.perf_counter() - t0
+    mine = list(range(rank, len(spots), world))
+    barrier(world)
+    t1 = time.perf_counter()
+    batch = g.Batch([spots[i] for i in mine], storage=HOST_STORAGE[args.storage],
+                    device_format=DEVICE_FORMAT[args.storage], engine=args.engine)
+    batch.run(max_iterations=args.ttt_max, target_pct=args.target, check_every=20, workers=args.report_workers)
+    run_s = allmax(time.perf_counter() - t1, world)
+    rows = batch.rows()
+    bad = [r["error"] for r in rows if r["status"] != 0]
+    if bad:
+        raise RuntimeError("flop report: %d spot(s) failed: %s" % (len(bad), bad[0]))
+    its = np.array([r["iterations"] for r in rows], np.float64)
+    pct = np.array([r["exploit_pct"] for r in rows])
+    reached = int((pct <= args.target).sum())
+    stats = np.zeros(4)
+    stats[:] = [its.sum(), reached, pct.max(), len(rows)]
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor(stats[:2].tolist() + [stats[3]], dtype=torch.float64)
+        dist.all_reduce(t)
+        m = torch.tensor([stats[2]], dtype=torch.float64)
+        dist.all_reduce(m, op=dist.ReduceOp.MAX)
+        stats = np.array([t[0].item(), t[1].item(), m[0].item(), t[2].item()])
+    n = len(spots)
+    if rank != 0:
+        return
+    value = n / run_s * 3600.0
+    sizes = [sp.num_nodes for sp in spots]
+    line = {
+        "metric": "flop report: flops/hour to %.1f%% pot exploitability" % args.target, "value": value,
+        "unit": "flops/h", "n_gpus": world, "steps": n, "warmup": 0, "ms_per_step": 1000.0 * run_s / n,
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": DTYPE[args.storage],
+        "data": "synthetic (seeded spots)",
+        "config": {"workload": "flop report: %d canonical flops (seed 4), turn-config ranges (top 50%% of 1176 "
+                               "combos, weights U[0.2,1]), pot 100 stack 300, raise 2.5x, 2 raises, 1-3 bet sizes "
+                               "from {33,50,75,125,a} (trees %d-%d nodes)" % (n, min(sizes), max(sizes)),
+                   "arenas": ARENA_DESC[args.storage], "algo": "DCFR alpha 1.5 beta 0 gamma 2, alternating",
+                   "check_every": 20, "max_iterations": args.ttt_max, "workers": args.report_workers,
+                   "parallelism": "flops dealt round-robin over ranks", "engine": args.engine},
+        "report": {"reached_target": int(stats[1]), "flops": int(stats[3]), "iterations_total": int(stats[0]),
+                   "worst_exploit_pct": float(stats[2]),
+                   "median_iterations": float(np.median(its)), "median_spot_s": float(np.median(
+                       [r["seconds"] for r in rows]))},
+        "e2e": {"value": n / (run_s + build_s) * 3600.0, "unit": "flops/h",
+                "includes": "spot builds (tree, ranges, river tables; %.1f s on %d threads) + the batch run" % (
+                    build_s, pool._max_workers),
+                "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    if not args.no_cpu_baseline:
+        mid = int(np.argsort(sizes)[len(sizes) // 2])
+        r = cpu_baseline(cfgs[mid], args.storage, max(1, args.cpu_steps), args.cpu_threads)
+        per_it = float(np.mean(r["iter_s"]))
+        per_flop = r["build_s"] + per_it * float(np.median(its))
+        line["cpu_baseline"] = {"value": 3600.0 / per_flop, "unit": "flops/h", "cores": r["cores"], "kind": "port",
+                                "sample": "%d DCFR iteration(s) of the median-size flop (%d nodes) on the CPU "
+                                          "oracle, times the GPU run's median iteration count (%d) plus its spot "
+                                          "build: flops/hour extrapolated" % (len(r["iter_s"]), sizes[mid],
+                                                                             int(np.median(its)))}
+    print(json.dumps(line), flush=True)
+
+
 def time_to_target(g, cfg, args):
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage=HOST_STORAGE[args.storage], algo="dcfr", use_iso=True)
@@ -344,7 +421,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="flop", choices=["flop", "flop_narrow", "turn", "river", "bench_spot"])
+    ap.add_argument("--workload", default="flop",
+                    choices=["flop", "flop_narrow", "turn", "river", "bench_spot", "report"])
+    ap.add_argument("--report-flops", type=int, default=184)
+    ap.add_argument("--report-workers", type=int, default=8)
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32", "fp8"])
     ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged"])
     ap.add_argument("--no-e2e", action="store_true")
@@ -360,8 +440,14 @@ def main():
         args.warmup = 3
     world, rank, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference":
+        if args.impl == "reference" and args.workload == "report":
+            if rank == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the flop report has no reference-arm run; "
+                                  "its CPU baseline is extrapolated from sampled oracle iterations"}), flush=True)
+        elif args.impl == "reference":
             run_reference(args, world, rank)
+        elif args.workload == "report":
+            run_report(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

@@ -8,6 +8,11 @@ crates/solver/src/evaluator.rs:292-302), seeded per configuration:
             strength score, weights U[0.2,1], sizes {33,75,a}/{2.5x}, 2 raises
   flop   -- 3-card board, OOP top 40% / IP top 55%, weights U[0.3,1], pot 55,
             stack 975, sizes {33,75,a}, raises {2.5x,a}, 3 raises
+  flop report -- 184 suit-isomorphism classes of flops drawn without
+            replacement, each with the turn config's ranges (top 50% of the
+            flop's 1176 combos, weights U[0.2,1]), pot 100, stack 300, raise
+            2.5x, 2 raises and 1-3 bet sizes from {33,50,75,125,a}, redrawn
+            until the largest tree is at most 8x the smallest
 The strength score of a combo is its 7-card strength percentile on the board
 completed by seeded runout cards, plus 0.25 * U, so ranges are strength-shaped.
 """
@@ -167,3 +172,52 @@ def iso_spot():
             "tree": {"starting_pot": 60.0, "effective_stack": 200.0, "rake_pct": 0.0, "rake_cap": 0.0,
                      "oop": [st, st, st], "ip": [st, st, st], "allin_threshold": 0.85, "add_allin": False,
                      "max_raises": 10}}
+
+
+def canonical_flops():
+    """One flop per suit-isomorphism class (1755 classes over the 22,100
+    flops, cards.rs:183-191): the class's smallest sorted card triple under
+    the 24 suit permutations, with the class's flop count."""
+    import itertools
+    perms = list(itertools.permutations(range(4)))
+    seen = {}
+    for flop in itertools.combinations(range(52), 3):
+        key = min(tuple(sorted((c & ~3) | pm[c & 3] for c in flop)) for pm in perms)
+        seen[key] = seen.get(key, 0) + 1
+    return sorted(seen.items())
+
+
+def flop_report_spots(evaluate7, build_many, n=184, seed=4, max_ratio=8.0):
+    """Spots of the flop report: n canonical flops sampled without
+    replacement (xorshift seed), per flop the turn config's range shape and a
+    bet set of 1-3 sizes from {33,50,75,125,a}; while the largest tree
+    exceeds max_ratio x the smallest, the largest flop's bet set is redrawn.
+    build_many(list of configs) -> list of built spots (with num_nodes), so the
+    caller can build them in parallel.  Returns (configs, spots)."""
+    rng = XorShift(seed)
+    classes = [k for k, _ in canonical_flops()]
+    for i in range(len(classes) - 1, 0, -1):
+        j = rng.below(i + 1)
+        classes[i], classes[j] = classes[j], classes[i]
+    menu = ("33", "50", "75", "125", "a")
+
+    def bet_set():
+        k = 1 + rng.below(3)
+        pick = sorted({menu[rng.below(len(menu))] for _ in range(k)}, key=menu.index)
+        return tuple(pick)
+
+    cfgs = []
+    for f in classes[:n]:
+        board = list(f)
+        r = [weighted_range(rng, top_fraction(rng, board, 0.5, evaluate7), 0.2) for _ in range(2)]
+        cfgs.append({"board": "".join(card_str(c) for c in board), "range_oop": r[0], "range_ip": r[1],
+                     "tree": tree_config(100, 300, bet_set(), ("2.5x",), 2)})
+    spots = list(build_many(cfgs))
+    for _ in range(10 * n):
+        sizes_ = [sp.num_nodes for sp in spots]
+        if max(sizes_) <= max_ratio * min(sizes_):
+            break
+        i = int(np.argmax(sizes_))
+        cfgs[i]["tree"] = tree_config(100, 300, bet_set(), ("2.5x",), 2)
+        spots[i] = build_many([cfgs[i]])[0]
+    return cfgs, spots
