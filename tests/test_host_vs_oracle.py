@@ -340,3 +340,11 @@ def test_batch_host_side():
             b.run(max_iterations=5)
         assert "cuda" in str(e.value)
 
+
+def test_canonical_flops_kat():
+    """cards.rs:183-191: 1755 suit-isomorphism classes whose weights sum to
+    the 22,100 flops."""
+    classes = W.canonical_flops()
+    assert len(classes) == 1755
+    assert sum(w for _, w in classes) == 22100
+
