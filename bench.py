@@ -395,6 +395,49 @@ def run_report(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+def run_precision(args, world, rank, local):
+    """The river (c1) and turn (c2) configurations: a fixed iteration count
+    per arena format on the GPU, the GPU's own exploitability (f32 sweeps,
+    f64 reduction) and the exploitability of the same average strategy under
+    the oracle's f64 best response; iterations/s from CUDA events."""
+    import numpy as np
+
+    import gtopen_b200 as g
+    from oracle import pyoracle as po
+    g.set_device(local)
+    if rank != 0:
+        return
+    out = {}
+    for name, iters, fmts in (("river", 500, ("f32",)), ("turn", 1000, ("f32", "i16", "fp8"))):
+        cfg = make_config(name)
+        pot = cfg["tree"]["starting_pot"]
+        ospot = po.Spot(cfg)
+        for fmt in fmts:
+            spot = g.Spot(cfg)
+            host = g.Solver(spot, storage="f32", algo="dcfr", use_iso=True)
+            gpu = g.GpuSolver(host, device_format=fmt, engine=args.engine)
+            gpu.iterate(3)
+            ms = gpu.time_iterations(iters - 3)
+            e_gpu = gpu.exploitability(host) / pot * 100
+            gpu.sync_to_cpu(host)
+            host.ensure_symmetric()
+            osv = po.Solver(ospot, compressed=False, algo="dcfr", use_iso=True, prune=False)
+            for which in (0, 1):
+                for p in (0, 1):
+                    osv.set_arena(which, p, host.arena(which, p))
+            e_f64 = osv.exploitability_f64() / pot * 100
+            out["%s/%s" % (name, fmt)] = {
+                "iterations": iters, "iter_per_s": (iters - 3) / (ms / 1000.0),
+                "exploit_pct_gpu": e_gpu, "exploit_pct_f64_oracle": e_f64,
+                "gpu_minus_f64_pct": e_gpu - e_f64, "nodes": spot.num_nodes, "hands": list(spot.nh)}
+            gpu.close()
+    line = {"metric": "configs c1 (river) and c2 (turn): exploitability after a fixed iteration count per arena "
+                      "format, GPU vs f64 best-response oracle", "value": out["turn/i16"]["iter_per_s"],
+            "unit": "iter/s", "n_gpus": 1, "steps": 1000, "warmup": 3, "higher_is_better": True,
+            "data": "synthetic (seeded spots)", "configs": out}
+    print(json.dumps(line), flush=True)
+
+
 def time_to_target(g, cfg, args):
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage=HOST_STORAGE[args.storage], algo="dcfr", use_iso=True)
@@ -422,7 +465,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="flop",
-                    choices=["flop", "flop_narrow", "turn", "river", "bench_spot", "report"])
+                    choices=["flop", "flop_narrow", "turn", "river", "bench_spot", "report", "precision"])
     ap.add_argument("--report-flops", type=int, default=184)
     ap.add_argument("--report-workers", type=int, default=8)
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32", "fp8"])
@@ -440,14 +483,18 @@ def main():
         args.warmup = 3
     world, rank, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference" and args.workload == "report":
+        if args.impl == "reference" and args.workload in ("report", "precision"):
             if rank == 0:
-                print(json.dumps({"impl": "reference", "unavailable": "the flop report has no reference-arm run; "
-                                  "its CPU baseline is extrapolated from sampled oracle iterations"}), flush=True)
+                print(json.dumps({"impl": "reference", "unavailable": "the %s workload has no reference-arm run "
+                                  "(the flop report extrapolates its CPU baseline from sampled oracle iterations; "
+                                  "the precision runs compare with the oracle's f64 best response)" % args.workload}),
+                      flush=True)
         elif args.impl == "reference":
             run_reference(args, world, rank)
         elif args.workload == "report":
             run_report(args, world, rank, local)
+        elif args.workload == "precision":
+            run_precision(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:
