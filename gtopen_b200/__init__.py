@@ -48,6 +48,10 @@ class GpuInfo(C.Structure):
                 ("arena_format", C.c_int32), ("iter_bytes", C.c_double), ("upload_bytes", C.c_uint64)]
 
 
+class NodeInfo(C.Structure):
+    _fields_ = [("node", C.c_uint32), ("kind", C.c_int32), ("player", C.c_int32), ("num_actions", C.c_int32)]
+
+
 class BatchRow(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_uint32), ("exploit_pct", C.c_double),
                 ("seconds", C.c_double), ("ev", C.c_double * 2)]
@@ -120,6 +124,7 @@ def lib():
         "gtob_gpu_read_node_static": (I, [P, I, C.c_uint32, P, C.c_uint64, P]),
         "gtob_gpu_discounts": (I, [P, P]),
         "gtob_gpu_save": (I, [P, P, C.c_char_p]),
+        "gtob_gpu_node_values": (I, [P, P, P, I, C.POINTER(NodeInfo)] + [P] * 8),
         "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, C.POINTER(P)]),
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
         "gtob_batch_size": (I, [P]),
@@ -454,6 +459,39 @@ class GpuSolver:
         gpu._h = gh
         gpu.solver = solver
         return solver, gpu
+
+    def node_values(self, path, solver=None):
+        """node_view's numbers (query.rs:490-600) at the node `path` reaches
+        (ints: action indices, strings: cards), from device memory: dict with
+        node, kind, player, reach/valid/ev per player and, at an action node,
+        the actor's strategy and action_ev (num_actions x hands)."""
+        sv = solver or self.solver
+        steps = []
+        for s in path:
+            if isinstance(s, str):
+                r, su = "23456789TJQKA".index(s[0].upper()), "cdhs".index(s[1].lower())
+                steps.append(-1 - (r * 4 + su))
+            else:
+                steps.append(int(s))
+        st = np.array(steps + [0], np.int32)
+        sp = sv.spot
+        nh = sp.nh
+        reach = [np.zeros(nh[0], np.float32), np.zeros(nh[1], np.float32)]
+        valid = [np.zeros(nh[0], np.float32), np.zeros(nh[1], np.float32)]
+        ev = [np.zeros(nh[0], np.float32), np.zeros(nh[1], np.float32)]
+        mx = max(nh) * 64
+        strat, aev = np.zeros(mx, np.float32), np.zeros(mx, np.float32)
+        info = NodeInfo()
+        _check(lib().gtob_gpu_node_values(self._h, sv._h, _ptr(st), len(steps), C.byref(info), _ptr(reach[0]),
+                                          _ptr(reach[1]), _ptr(valid[0]), _ptr(valid[1]), _ptr(ev[0]), _ptr(ev[1]),
+                                          _ptr(strat), _ptr(aev)))
+        out = {"node": info.node, "kind": info.kind, "player": info.player, "reach": reach, "valid": valid,
+               "ev": ev}
+        if info.kind == 0:
+            na, h = info.num_actions, nh[info.player]
+            out["strategy"] = strat[:na * h].reshape(na, h).copy()
+            out["action_ev"] = aev[:na * h].reshape(na, h).copy()
+        return out
 
     def discounts(self):
         out = np.zeros(3, np.float32)

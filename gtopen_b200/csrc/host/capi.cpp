@@ -13,6 +13,7 @@
 #include "../kernels/engine.hpp"
 #include "batch.hpp"
 #include "core.hpp"
+#include "query.hpp"
 #include "solver.hpp"
 
 using namespace gtob;
@@ -268,6 +269,23 @@ int gtob_load(const char* path, int storage, gtob_solver** out) {
     API_END
 }
 
+int gtob_gpu_node_values(gtob_gpu* g, const gtob_solver* v, const int* steps, int nsteps, gtob_node_info* info,
+                         float* reach0, float* reach1, float* valid0, float* valid1, float* ev0, float* ev1,
+                         float* strategy, float* action_ev) {
+    REQUIRE(g && v && nsteps >= 0 && (steps || nsteps == 0));
+    API_BEGIN
+    const NodeValues nv = node_values(*g->e, *v->v, std::vector<int>(steps, steps + nsteps));
+    if (info) *info = gtob_node_info{nv.node, nv.kind, nv.player, nv.na};
+    put(reach0, nv.reach[0]);
+    put(reach1, nv.reach[1]);
+    put(valid0, nv.valid[0]);
+    put(valid1, nv.valid[1]);
+    put(ev0, nv.ev[0]);
+    put(ev1, nv.ev[1]);
+    put(strategy, nv.strategy);
+    put(action_ev, nv.action_ev);
+    API_END
+}
 struct gtob_batch {
     std::vector<std::unique_ptr<gtob_solver>> solvers;
     std::vector<BatchRow> rows;

@@ -80,6 +80,9 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
         return (uint32_t)(P.terms.size() - 1);
     };
     std::vector<uint8_t> visited(n, 0);
+    P.node_cslot.assign(n, kNoSlot);
+    P.node_rs[0].assign(n, kNoSlot);
+    P.node_rs[1].assign(n, kNoSlot);
     {  // capacity for the flat tables (no regrowth during the traversal)
         size_t nchild = 0, nterm = 0;
         for (size_t i = 0; i < n; i++) {
@@ -100,6 +103,9 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
         stack.pop_back();
         const uint32_t nd = v.node;
         visited[nd] = 1;
+        P.node_cslot[nd] = v.cslot;
+        P.node_rs[0][nd] = v.rs[0];
+        P.node_rs[1][nd] = v.rs[1];
         grow(v.level);
         P.num_visited++;
         switch (t.kind[nd]) {

@@ -138,6 +138,9 @@ struct Plan {
     std::vector<uint32_t> anode_id[2];
     std::vector<uint64_t> anode_off[2];
     std::vector<int32_t> node_sidx;
+    // per tree node the sweep visits: its cfv slot and each player's reach
+    // slot (kNoSlot for nodes it does not visit)
+    std::vector<uint32_t> node_cslot, node_rs[2];
     uint32_t num_slots = 0;
     std::vector<uint32_t> slot_key;
     std::vector<uint32_t> sorted_off[2];

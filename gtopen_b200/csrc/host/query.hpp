@@ -1,0 +1,32 @@
+// Node queries over the device arenas (query.rs:304-645 node_view's
+// numbers): the reach of both players at the node a path reaches, each
+// player's compatible opponent mass and EV, and at an action node the
+// actor's average strategy and per-action EVs -- without syncing the arenas
+// to the host.  The strategies along the path come from the device blocks,
+// the values from one average-strategy evaluation sweep per player.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "solver.hpp"
+
+namespace gtob {
+
+class GpuEngine;
+
+struct NodeValues {
+    uint32_t node = 0;  // tree index of the node the path reaches
+    int kind = 0, player = -1, na = 0;
+    std::vector<float> reach[2];  // walk reach (query.rs:304-340)
+    std::vector<float> valid[2];  // compatible opponent reach mass (query.rs:463-488)
+    std::vector<float> ev[2];     // pot-share EV, NaN where valid <= 1e-9
+    std::vector<float> strategy;  // the actor's average strategy, [action * nh + hand]
+    std::vector<float> action_ev;  // the actor's EV per action, same layout, NaN where valid <= 1e-9
+};
+
+// steps: action indices (>= 0) and dealt cards (-1 - card), from the root.
+// Through a suit-isomorphic branch the device holds the representative: its
+// values are read under the hand permutation that ensure_symmetric applies.
+NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps);
+
+}  // namespace gtob

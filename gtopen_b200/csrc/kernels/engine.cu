@@ -777,6 +777,89 @@ void GpuEngine::fill_staging(int which, int p) {
     }
 }
 
+// ------------------------------------------------ node queries
+// Average strategy of one action node (cfr.rs:679-726, the same rule the
+// evaluation sweeps use) in the reference layout [action * nh + hand].
+template <int FMT>
+__global__ void k_node_avg_sigma(const void* str, float* out, int na, int nh) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nh) return;
+    float sig[kSKA];
+    s_average_sigma<FMT>(str, na, i, sig);
+    for (int k = 0; k < na; k++) out[(size_t)k * nh + i] = sig[k];
+}
+
+void GpuEngine::node_average_strategy(uint32_t node, float* out) {
+    EngineImpl& E = *d_;
+    const Spot& sp = *E.spot;
+    if (node >= sp.tree.size() || sp.tree.kind[node] != kAction) throw Error("not an action node");
+    const int32_t s = E.plan.node_sidx[node];
+    if (s < 0) throw Error("node " + std::to_string(node) + " has no device block (a symmetric branch)");
+    const int p = sp.tree.player[node], na = sp.tree.nchild[node], nh = E.plan.nh[p];
+    if (na > kSKA && E.fmt != kFmtF32 && E.fmt != kFmtI16) throw Error("node has more actions than the FP8 path takes");
+    const XNode x = E.hx[p][(size_t)s];
+    const unsigned grid = (unsigned)((nh + kThreads - 1) / kThreads);
+    const size_t esz = (size_t)fmt_bytes(E.fmt);
+    const void* blk = (const unsigned char*)E.ar.str[p] + x.dev_off * esz;
+    if (na <= kSKA) {
+        if (E.fmt == kFmtF32) k_node_avg_sigma<kDevF32><<<grid, kThreads, 0, E.stream>>>(blk, E.staging, na, nh);
+        else if (E.fmt == kFmtFP8) k_node_avg_sigma<kDevFP8><<<grid, kThreads, 0, E.stream>>>(blk, E.staging, na, nh);
+        else k_node_avg_sigma<kDevI16><<<grid, kThreads, 0, E.stream>>>(blk, E.staging, na, nh);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(out, E.staging, (size_t)na * nh * sizeof(float), cudaMemcpyDeviceToHost, E.stream));
+        CK(cudaStreamSynchronize(E.stream));
+        return;
+    }
+    // wide nodes (f32 / 16-bit arenas only): the block to the host, the same rule there
+    std::vector<unsigned char> raw((size_t)na * nh * esz);
+    CK(cudaMemcpyAsync(raw.data(), blk, raw.size(), cudaMemcpyDeviceToHost, E.stream));
+    CK(cudaStreamSynchronize(E.stream));
+    for (int i = 0; i < nh; i++) {
+        if (E.fmt == kFmtF32) {
+            const float* v = (const float*)raw.data() + (size_t)i * na;
+            double sum = 0.0;
+            for (int k = 0; k < na; k++) sum += (double)std::fmax(v[k], 0.0f);
+            for (int k = 0; k < na; k++)
+                out[(size_t)k * nh + i] = sum > 1e-12 ? (float)((double)std::fmax(v[k], 0.0f) / sum) : 1.0f / (float)na;
+        } else {
+            const uint16_t* q = (const uint16_t*)raw.data() + (size_t)i * na;
+            unsigned sum = 0;
+            for (int k = 0; k < na; k++) sum += q[k];
+            const float inv = sum > 0 ? 1.0f / (float)sum : 0.0f;
+            for (int k = 0; k < na; k++) out[(size_t)k * nh + i] = sum > 0 ? (float)q[k] * inv : 1.0f / (float)na;
+        }
+    }
+}
+
+void GpuEngine::node_sweep_values(uint32_t node, int p, float* cfv, float* reach0, float* reach1, float* child_cfv,
+                                  uint8_t* child_ok) {
+    EngineImpl& E = *d_;
+    const Tree& t = E.spot->tree;
+    if (node >= t.size() || E.plan.node_cslot[node] == kNoSlot && E.plan.node_rs[0][node] == kNoSlot)
+        throw Error("node " + std::to_string(node) + " is not on the device (a symmetric branch or an in-place terminal)");
+    E.sweep(p, 1, nullptr);  // average strategies: down for both players, up for p
+    E.reach_valid = false;
+    const int nh = E.plan.nh[p];
+    const uint32_t cs = E.plan.node_cslot[node];
+    if (cfv && cs != kNoSlot)
+        CK(cudaMemcpyAsync(cfv, E.d.cfv + (size_t)cs * E.d.nh_max, nh * sizeof(float), cudaMemcpyDeviceToHost, E.stream));
+    float* rr[2] = {reach0, reach1};
+    for (int q = 0; q < 2; q++)
+        if (rr[q])
+            CK(cudaMemcpyAsync(rr[q], E.d.reach[q] + (size_t)E.plan.node_rs[q][node] * E.d.rstr[q],
+                               E.plan.nh[q] * sizeof(float), cudaMemcpyDeviceToHost, E.stream));
+    if (child_cfv && t.kind[node] == kAction && t.player[node] == p)
+        for (int a = 0; a < t.nchild[node]; a++) {
+            const uint32_t c = E.plan.node_cslot[t.child(node, a)];
+            child_ok[a] = c != kNoSlot;
+            if (c != kNoSlot)
+                CK(cudaMemcpyAsync(child_cfv + (size_t)a * nh, E.d.cfv + (size_t)c * E.d.nh_max, nh * sizeof(float),
+                                   cudaMemcpyDeviceToHost, E.stream));
+        }
+    CK(cudaStreamSynchronize(E.stream));
+    E.check_err();
+}
+
 // ------------------------------------------------ .gto straight from / to HBM
 // One block of a device save's image: dst <- src gathered through a hand
 // permutation table, action by action (cfr.rs:806-871 copy_branch, with

@@ -202,6 +202,31 @@ int gtob_gpu_save(gtob_gpu* gpu, const gtob_solver* solver, const char* path);
 int gtob_gpu_load(const char* path, int storage, int device_format, int engine, gtob_solver** solver_out,
                   gtob_gpu** gpu_out);
 
+/* ---- node queries over the device arenas (query.rs:304-645) ------------ */
+/* node_view's numbers (query.rs:490-600) at the node a path reaches, read
+ * from device memory instead of a synced host solver: steps are action
+ * indices (>= 0) and dealt cards (-1 - card) from the root, as
+ * gtob_solver_lock_node takes them.  The strategies along the path come from
+ * the device blocks (locks from `solver`), the values from one
+ * average-strategy evaluation sweep per player (best_response.rs:128-223).
+ * Through a suit-isomorphic branch the device holds the representative; its
+ * values are returned under the hand permutation ensure_symmetric applies.
+ * Outputs (NULL to skip): reach_p / valid_p / ev_p per hand of player p (ev
+ * in the pot-share convention, NaN where valid <= 1e-9); at an action node,
+ * strategy and action_ev (num_actions x hands of the actor, action-major).
+ * Supported on the staged and plain engines (showdowns with slots).  The
+ * sweeps reuse the engine's buffers: do not call it while another call on
+ * the same gpu handle is running. */
+typedef struct {
+    uint32_t node;       /* tree index */
+    int32_t kind;        /* 0 action, 1 chance, 2 fold, 3 showdown */
+    int32_t player;      /* actor at an action node, else -1 */
+    int32_t num_actions; /* at an action node, else 0 */
+} gtob_node_info;
+int gtob_gpu_node_values(gtob_gpu* gpu, const gtob_solver* solver, const int* steps, int nsteps, gtob_node_info* info,
+                         float* reach0, float* reach1, float* valid0, float* valid1, float* ev0, float* ev1,
+                         float* strategy, float* action_ev);
+
 /* ---- batch of spots (solve_cli.rs:125-215 batch) ------------------------ */
 /* The reference's batch report solves one board after another
  * (solve_quiet, solve_cli.rs:338-362).  A batch solves many spots on one GPU

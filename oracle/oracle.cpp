@@ -2126,6 +2126,55 @@ int orc_solver_walk_path(orc_solver* vc, const int* steps, int ns, uint32_t* nod
     return 0;
     GUARD_END(-1)
 }
+int orc_solver_node_values(orc_solver* vc, const int* steps, int ns, int p, float* cfv, float* child_cfv, float* r0,
+                           float* r1) {
+    // query.rs:490-600 (node_view's traversals): walk_path (query.rs:304-340),
+    // then traverse_avg (best_response.rs:128-223) of the node for player p
+    // with the opponent's walk reach, and of each child when p acts there
+    GUARD_BEGIN
+    Solver* s = vc->v;
+    const Spot& sp = *s->spot;
+    uint32_t ni = 0;
+    std::vector<float> reach[2] = {sp.weights[0], sp.weights[1]};
+    Dealt dealt;
+    for (int k = 0; k < ns; k++) {
+        const Node& n = s->node(ni);
+        if (n.kind == K_ACTION && steps[k] >= 0) {
+            int idx = steps[k], na = n.num_children;
+            if (idx >= na) fail("action index out of range");
+            int q = n.player, h = s->nh(q);
+            std::vector<float> sig(na * h);
+            s->average_strategy_into(ni, n, sig.data());
+            for (int i = 0; i < h; i++) reach[q][i] *= sig[idx * h + i];
+            ni = sp.tree.children[n.children_start + idx];
+        } else if (n.kind == K_CHANCE && steps[k] < 0) {
+            Card c = (Card)(-1 - steps[k]);
+            uint32_t ch = sp.tree.children[n.children_start + c];
+            if (ch == SENTINEL || dealt.contains(c)) fail("card not available here");
+            for (int q = 0; q < 2; q++)
+                for (size_t i = 0; i < sp.hands[q].size(); i++)
+                    if (sp.hands[q][i].mask & cmask(c)) reach[q][i] = 0.0f;
+            dealt = dealt.push(c);
+            ni = ch;
+        } else {
+            fail("path step does not match node kind");
+        }
+    }
+    const int h = s->nh(p);
+    const float* ro = reach[1 - p].data();
+    std::fill(cfv, cfv + h, 0.0f);
+    s->br_into(ni, p, ro, dealt, cfv, true);
+    const Node& n = s->node(ni);
+    if (child_cfv && n.kind == K_ACTION && n.player == p)
+        for (int a = 0; a < n.num_children; a++) {
+            std::fill(child_cfv + (size_t)a * h, child_cfv + (size_t)(a + 1) * h, 0.0f);
+            s->br_into(sp.tree.children[n.children_start + a], p, ro, dealt, child_cfv + (size_t)a * h, true);
+        }
+    if (r0) std::memcpy(r0, reach[0].data(), sizeof(float) * reach[0].size());
+    if (r1) std::memcpy(r1, reach[1].data(), sizeof(float) * reach[1].size());
+    return (int)ni;
+    GUARD_END(-1)
+}
 void orc_rake_to_target(float* sigma, int na, int nh, const float* reach, const float* target) {
     rake_to_target(sigma, na, nh, reach, target);
 }
