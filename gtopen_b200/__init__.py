@@ -125,6 +125,7 @@ def lib():
         "gtob_gpu_discounts": (I, [P, P]),
         "gtob_gpu_save": (I, [P, P, C.c_char_p]),
         "gtob_gpu_node_values": (I, [P, P, P, I, C.POINTER(NodeInfo)] + [P] * 8),
+        "gtob_gpu_exploit_values": (I, [P, P, P, I, I, C.POINTER(NodeInfo)] + [P] * 8),
         "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, C.POINTER(P)]),
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
         "gtob_batch_size": (I, [P]),
@@ -356,6 +357,17 @@ class Solver:
         return Solver(spot, storage=storage, _handle=h)
 
 
+def _path_steps(path):
+    """Path steps as the C ABI takes them: action indices, cards as -1 - card."""
+    out = []
+    for s in path:
+        if isinstance(s, str):
+            out.append(-1 - ("23456789TJQKA".index(s[0].upper()) * 4 + "cdhs".index(s[1].lower())))
+        else:
+            out.append(int(s))
+    return out
+
+
 class GpuSolver:
     """gpu/mod.rs GpuSolver: device buffers, CUDA-graph iterations, BR checks, syncs."""
 
@@ -491,6 +503,26 @@ class GpuSolver:
             na, h = info.num_actions, nh[info.player]
             out["strategy"] = strat[:na * h].reshape(na, h).copy()
             out["action_ev"] = aev[:na * h].reshape(na, h).copy()
+        return out
+
+    def exploit_values(self, path, exploiter, solver=None):
+        """exploit_view's numbers (query.rs:808-930) for `exploiter` at the
+        node `path` reaches, from device memory."""
+        sv = solver or self.solver
+        st = np.array(_path_steps(path) + [0], np.int32)
+        nh = sv.spot.nh[exploiter]
+        arrs = {k: np.zeros(nh, np.float32) for k in ("reach", "valid", "br_ev", "cur_ev", "gain")}
+        strat, aev = np.zeros(nh * 64, np.float32), np.zeros(nh * 64, np.float32)
+        avg = np.zeros(3, np.float32)
+        info = NodeInfo()
+        _check(lib().gtob_gpu_exploit_values(self._h, sv._h, _ptr(st), len(st) - 1, int(exploiter), C.byref(info),
+                                             *[_ptr(arrs[k]) for k in ("reach", "valid", "br_ev", "cur_ev", "gain")],
+                                             _ptr(strat), _ptr(aev), _ptr(avg)))
+        out = dict(arrs, node=info.node, kind=info.kind, player=info.player, averages=avg)
+        if info.kind == 0 and info.player == exploiter:
+            na = info.num_actions
+            out["br_strategy"] = strat[:na * nh].reshape(na, nh).copy()
+            out["action_ev"] = aev[:na * nh].reshape(na, nh).copy()
         return out
 
     def discounts(self):

@@ -286,6 +286,23 @@ int gtob_gpu_node_values(gtob_gpu* g, const gtob_solver* v, const int* steps, in
     put(action_ev, nv.action_ev);
     API_END
 }
+int gtob_gpu_exploit_values(gtob_gpu* g, const gtob_solver* v, const int* steps, int nsteps, int exploiter,
+                            gtob_node_info* info, float* reach, float* valid, float* br_ev, float* cur_ev, float* gain,
+                            float* br_strategy, float* action_ev, float* averages) {
+    REQUIRE(g && v && nsteps >= 0 && (steps || nsteps == 0) && (exploiter == 0 || exploiter == 1));
+    API_BEGIN
+    const ExploitValues x = exploit_values(*g->e, *v->v, std::vector<int>(steps, steps + nsteps), exploiter);
+    if (info) *info = gtob_node_info{x.node, x.kind, x.player, x.na};
+    put(reach, x.reach);
+    put(valid, x.valid);
+    put(br_ev, x.br_ev);
+    put(cur_ev, x.cur_ev);
+    put(gain, x.gain);
+    put(br_strategy, x.br_strategy);
+    put(action_ev, x.action_ev);
+    if (averages) std::memcpy(averages, x.avg, sizeof(x.avg));
+    API_END
+}
 struct gtob_batch {
     std::vector<std::unique_ptr<gtob_solver>> solvers;
     std::vector<BatchRow> rows;

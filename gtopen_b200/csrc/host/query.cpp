@@ -47,15 +47,14 @@ void fold_values(const Spot& sp, int p, const float* ro, float amount, float* ou
 }
 }  // namespace
 
-NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps) {
+// walk_path (query.rs:304-340) with each action node's strategy from the
+// device block of its representative under the prefix's suit permutation.
+static uint32_t walk_device(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps,
+                            std::vector<float> reach[2]) {
     const Spot& sp = *host.spot;
     const Tree& t = sp.tree;
-    const float nan = std::numeric_limits<float>::quiet_NaN();
-    NodeValues out;
-    // walk the path (query.rs:304-340), each action node's strategy from the
-    // device block of its representative under the prefix's suit permutation
-    out.reach[0] = sp.hands[0].w;
-    out.reach[1] = sp.hands[1].w;
+    reach[0] = sp.hands[0].w;
+    reach[1] = sp.hands[1].w;
     uint32_t n = 0;
     uint8_t dealt[2];
     int nd = 0;
@@ -75,7 +74,7 @@ NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector
             if (lk != host.locks.end()) sig = lk->second;
             else eng.node_average_strategy(cn, sig.data());
             const std::vector<int> m = hand_map(sp, p, perm);
-            for (size_t i = 0; i < nh; i++) out.reach[p][i] *= sig[s * nh + m[i]];
+            for (size_t i = 0; i < nh; i++) reach[p][i] *= sig[s * nh + m[i]];
             n = t.child(n, s);
         } else if (t.kind[n] == kChance && s < 0) {
             const uint8_t c = (uint8_t)(-1 - s);
@@ -85,13 +84,22 @@ NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector
             if (ch == kSentinel || was) throw Error("card " + card_name(c) + " not available here");
             for (int p = 0; p < 2; p++)
                 for (size_t i = 0; i < sp.hands[p].size(); i++)
-                    if (sp.hands[p].mask[i] >> c & 1) out.reach[p][i] = 0.0f;
+                    if (sp.hands[p].mask[i] >> c & 1) reach[p][i] = 0.0f;
             if (nd < 2) dealt[nd++] = c;
             n = ch;
         } else {
             throw Error("path step does not match the node kind");
         }
     }
+    return n;
+}
+
+NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps) {
+    const Spot& sp = *host.spot;
+    const Tree& t = sp.tree;
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    NodeValues out;
+    const uint32_t n = walk_device(eng, host, steps, out.reach);
     out.node = n;
     out.kind = t.kind[n];
     out.player = t.kind[n] == kAction ? t.player[n] : -1;
@@ -122,7 +130,7 @@ NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector
         if (fold_end) {
             fold_values(sp, p, ro, (float)(t.player[n] == p ? t.tlose[n] : t.twin[n]), cfv.data());
         } else {
-            eng.node_sweep_values(cn, p, cfv_c.data(), nullptr, nullptr, actor ? child_c.data() : nullptr, ok.data());
+            eng.node_sweep_values(cn, p, 1, cfv_c.data(), nullptr, nullptr, actor ? child_c.data() : nullptr, ok.data());
             for (int i = 0; i < nh; i++) cfv[i] = cfv_c[m[i]];
         }
         out.ev[p].assign(nh, nan);
@@ -161,6 +169,114 @@ NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector
         }
         for (int i = 0; i < nh; i++)
             if (valid[i] > 1e-9) out.ev[p][i] = (float)total[i];
+    }
+    return out;
+}
+
+ExploitValues exploit_values(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps, int p) {
+    if (p != 0 && p != 1) throw Error("exploiter must be 0 (OOP) or 1 (IP)");
+    const Spot& sp = *host.spot;
+    const Tree& t = sp.tree;
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    ExploitValues out;
+    std::array<uint8_t, 4> perm;
+    const std::vector<int> canon = host.canonical_steps(steps, &perm);
+    std::vector<float> reach[2];
+    const uint32_t n = walk_device(eng, host, canon, reach);  // query.rs:815: the canonical walk
+    out.node = n;
+    out.kind = t.kind[n];
+    out.player = t.kind[n] == kAction ? t.player[n] : -1;
+    const int nh = (int)sp.hands[p].size();
+    const float* ro = reach[1 - p].data();
+    const std::vector<double> valid = valid_opp_sum(sp, p, ro);
+    const std::vector<int> tbl = hand_map(sp, p, perm);
+    const bool actor = t.kind[n] == kAction && t.player[n] == p;
+    const int na = t.kind[n] == kAction ? t.nchild[n] : 0;
+    out.na = na;
+    auto lk = host.locks.find(n);
+    const std::vector<float>* lock = lk != host.locks.end() ? &lk->second : nullptr;
+    const double put = p == 0 ? t.put0[n] : t.put1[n];
+    const bool fold_end = t.kind[n] == kFold;
+    const float famount = fold_end ? (float)(t.player[n] == p ? t.tlose[n] : t.twin[n]) : 0.0f;
+    // best-response values: per action where p acts, else the node's
+    std::vector<float> acfv((size_t)na * nh, 0.0f), br(nh, 0.0f), cur(nh, 0.0f);
+    std::vector<uint8_t> ok(na, 0);
+    if (fold_end) {
+        fold_values(sp, p, ro, famount, br.data());
+        cur = br;
+    } else {
+        eng.node_sweep_values(n, p, 0, actor ? nullptr : br.data(), nullptr, nullptr, actor ? acfv.data() : nullptr,
+                              ok.data());
+        eng.node_sweep_values(n, p, 1, cur.data(), nullptr, nullptr, nullptr, nullptr);
+    }
+    if (actor) {
+        for (int a = 0; a < na; a++)
+            if (!ok[a]) {
+                const uint32_t c = t.child(n, a);
+                if (t.kind[c] != kFold) throw Error("exploit values need the staged or plain engine (showdowns with slots)");
+                fold_values(sp, p, ro, (float)(t.player[c] == p ? t.tlose[c] : t.twin[c]), acfv.data() + (size_t)a * nh);
+            }
+        for (int i = 0; i < nh; i++) {
+            if (lock) {
+                float v = 0.0f;
+                for (int a = 0; a < na; a++) v += (*lock)[(size_t)a * nh + i] * acfv[(size_t)a * nh + i];
+                br[i] = v;
+            } else {
+                float v = -std::numeric_limits<float>::infinity();
+                for (int a = 0; a < na; a++) v = std::fmax(v, acfv[(size_t)a * nh + i]);
+                br[i] = v;
+            }
+        }
+    }
+    auto ev_of = [&](float cfv, int j) { return valid[j] > 1e-9 ? (float)((double)cfv / valid[j] + put) : nan; };
+    out.reach.resize(nh);
+    out.valid.resize(nh);
+    out.br_ev.resize(nh);
+    out.cur_ev.resize(nh);
+    out.gain.resize(nh);
+    if (actor) {
+        out.br_strategy.assign((size_t)na * nh, 0.0f);
+        out.action_ev.assign((size_t)na * nh, nan);
+    }
+    double wsum = 0.0, bs = 0.0, cs = 0.0;
+    for (int i = 0; i < nh; i++) {
+        const int j = tbl[i];
+        out.reach[i] = reach[p][j];
+        out.valid[i] = (float)valid[j];
+        const float b = ev_of(br[j], j), c = ev_of(cur[j], j);
+        out.br_ev[i] = b;
+        out.cur_ev[i] = c;
+        out.gain[i] = (!std::isnan(b) && !std::isnan(c)) ? b - c : nan;
+        if (actor) {
+            if (lock) {
+                for (int a = 0; a < na; a++) out.br_strategy[(size_t)a * nh + i] = (*lock)[(size_t)a * nh + j];
+            } else {
+                float m = -std::numeric_limits<float>::infinity();
+                for (int a = 0; a < na; a++) m = std::fmax(m, acfv[(size_t)a * nh + j]);
+                const float eps = std::fmax(std::fabs(m) * 1e-5f, 1e-5f);
+                int w = 0;
+                for (int a = 0; a < na; a++) w += (m - acfv[(size_t)a * nh + j] <= eps) ? 1 : 0;
+                const float wf = (float)std::max(w, 1);
+                for (int a = 0; a < na; a++)
+                    out.br_strategy[(size_t)a * nh + i] = (m - acfv[(size_t)a * nh + j] <= eps) ? 1.0f / wf : 0.0f;
+            }
+            for (int a = 0; a < na; a++) out.action_ev[(size_t)a * nh + i] = ev_of(acfv[(size_t)a * nh + j], j);
+        }
+        if (!std::isnan(b) && !std::isnan(c)) {  // query.rs:901-913
+            const double w = (double)out.reach[i] * (double)out.valid[i];
+            if (w > 0.0) {
+                wsum += w;
+                bs += w * (double)b;
+                cs += w * (double)c;
+            }
+        }
+    }
+    if (wsum > 1e-12) {
+        out.avg[0] = (float)(bs / wsum);
+        out.avg[1] = (float)(cs / wsum);
+        out.avg[2] = (float)((bs - cs) / wsum);
+    } else {
+        out.avg[0] = out.avg[1] = out.avg[2] = nan;
     }
     return out;
 }

@@ -24,6 +24,21 @@ struct NodeValues {
     std::vector<float> action_ev;  // the actor's EV per action, same layout, NaN where valid <= 1e-9
 };
 
+// exploit_view's numbers (query.rs:808-930) for exploiter p, per hand of the
+// browsed branch: reach and compatible mass on the representative branch,
+// best-response and current EVs and their difference (NaN where valid <=
+// 1e-9); where p acts, the best response (one-hot, ties within 1e-5 split;
+// the lock at a locked node) and the EV of each action under it; the
+// reach x valid weighted averages of br_ev, cur_ev and gain.
+struct ExploitValues {
+    uint32_t node = 0;  // the representative node the values are read at
+    int kind = 0, player = -1, na = 0;
+    std::vector<float> reach, valid, br_ev, cur_ev, gain;
+    std::vector<float> br_strategy, action_ev;  // [action * nh + hand]
+    float avg[3];
+};
+ExploitValues exploit_values(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps, int p);
+
 // steps: action indices (>= 0) and dealt cards (-1 - card), from the root.
 // Through a suit-isomorphic branch the device holds the representative: its
 // values are read under the hand permutation that ensure_symmetric applies.

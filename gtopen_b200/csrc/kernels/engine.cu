@@ -831,13 +831,14 @@ void GpuEngine::node_average_strategy(uint32_t node, float* out) {
     }
 }
 
-void GpuEngine::node_sweep_values(uint32_t node, int p, float* cfv, float* reach0, float* reach1, float* child_cfv,
-                                  uint8_t* child_ok) {
+void GpuEngine::node_sweep_values(uint32_t node, int p, int mode, float* cfv, float* reach0, float* reach1,
+                                  float* child_cfv, uint8_t* child_ok) {
     EngineImpl& E = *d_;
     const Tree& t = E.spot->tree;
     if (node >= t.size() || E.plan.node_cslot[node] == kNoSlot && E.plan.node_rs[0][node] == kNoSlot)
         throw Error("node " + std::to_string(node) + " is not on the device (a symmetric branch or an in-place terminal)");
-    E.sweep(p, 1, nullptr);  // average strategies: down for both players, up for p
+    if (mode != 0 && mode != 1) throw Error("invalid argument: sweep mode");
+    E.sweep(p, mode, nullptr);  // down with the average strategies, up: best response (0) or average (1) for p
     E.reach_valid = false;
     const int nh = E.plan.nh[p];
     const uint32_t cs = E.plan.node_cslot[node];

@@ -62,11 +62,12 @@ class GpuEngine {
     // Average strategy of one action node the device holds (reference layout
     // [action * nh + hand]), by the rule the evaluation sweeps use.
     void node_average_strategy(uint32_t node, float* out);
-    // One average-strategy evaluation sweep for player p (best_response.rs
-    // avg_into over the whole tree), then the node's value for p, both
-    // players' reach at the node and, when p acts there, each child's value
-    // (child_ok[a] = 0 for children evaluated in place, which have no slot).
-    void node_sweep_values(uint32_t node, int p, float* cfv, float* reach0, float* reach1, float* child_cfv,
+    // One evaluation sweep for player p over the whole tree -- mode 0 best
+    // response (best_response.rs br_into), 1 average strategies (avg_into) --
+    // then the node's value for p, both players' reach at the node and, when
+    // p acts there, each child's value (child_ok[a] = 0 for children
+    // evaluated in place, which have no slot).
+    void node_sweep_values(uint32_t node, int p, int mode, float* cfv, float* reach0, float* reach1, float* child_cfv,
                            uint8_t* child_ok);
     // time one kind of level launch set: used by bench for the roofline
     void discounts(float* out3);

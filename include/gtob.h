@@ -227,6 +227,19 @@ int gtob_gpu_node_values(gtob_gpu* gpu, const gtob_solver* solver, const int* st
                          float* reach0, float* reach1, float* valid0, float* valid1, float* ev0, float* ev1,
                          float* strategy, float* action_ev);
 
+/* exploit_view's numbers (query.rs:808-930) for `exploiter` at the node a
+ * path reaches, from device memory (one best-response and one
+ * average-strategy evaluation sweep, strategies along the canonical path
+ * from the device blocks): per hand of the exploiter in the browsed branch
+ * reach, valid, br_ev, cur_ev and gain (NaN where valid <= 1e-9); where the
+ * exploiter acts, br_strategy (one-hot, ties within 1e-5 split, the lock at a
+ * locked node) and action_ev (num_actions x hands, action-major); averages =
+ * {avg_br_ev, avg_cur_ev, avg_gain} weighted by reach x valid (NaN when
+ * there is no mass).  info->node is the representative node read. */
+int gtob_gpu_exploit_values(gtob_gpu* gpu, const gtob_solver* solver, const int* steps, int nsteps, int exploiter,
+                            gtob_node_info* info, float* reach, float* valid, float* br_ev, float* cur_ev, float* gain,
+                            float* br_strategy, float* action_ev, float* averages);
+
 /* ---- batch of spots (solve_cli.rs:125-215 batch) ------------------------ */
 /* The reference's batch report solves one board after another
  * (solve_quiet, solve_cli.rs:338-362).  A batch solves many spots on one GPU

@@ -2126,11 +2126,12 @@ int orc_solver_walk_path(orc_solver* vc, const int* steps, int ns, uint32_t* nod
     return 0;
     GUARD_END(-1)
 }
-int orc_solver_node_values(orc_solver* vc, const int* steps, int ns, int p, float* cfv, float* child_cfv, float* r0,
-                           float* r1) {
+int orc_solver_node_values(orc_solver* vc, const int* steps, int ns, int p, int avg, float* cfv, float* child_cfv,
+                           float* r0, float* r1) {
     // query.rs:490-600 (node_view's traversals): walk_path (query.rs:304-340),
-    // then traverse_avg (best_response.rs:128-223) of the node for player p
-    // with the opponent's walk reach, and of each child when p acts there
+    // then traverse_avg (avg = 1, best_response.rs:128-223) or traverse_br
+    // (avg = 0, best_response.rs:19-124) of the node for player p with the
+    // opponent's walk reach, and of each child when p acts there
     GUARD_BEGIN
     Solver* s = vc->v;
     const Spot& sp = *s->spot;
@@ -2163,12 +2164,12 @@ int orc_solver_node_values(orc_solver* vc, const int* steps, int ns, int p, floa
     const int h = s->nh(p);
     const float* ro = reach[1 - p].data();
     std::fill(cfv, cfv + h, 0.0f);
-    s->br_into(ni, p, ro, dealt, cfv, true);
+    s->br_into(ni, p, ro, dealt, cfv, avg != 0);
     const Node& n = s->node(ni);
     if (child_cfv && n.kind == K_ACTION && n.player == p)
         for (int a = 0; a < n.num_children; a++) {
             std::fill(child_cfv + (size_t)a * h, child_cfv + (size_t)(a + 1) * h, 0.0f);
-            s->br_into(sp.tree.children[n.children_start + a], p, ro, dealt, child_cfv + (size_t)a * h, true);
+            s->br_into(sp.tree.children[n.children_start + a], p, ro, dealt, child_cfv + (size_t)a * h, avg != 0);
         }
     if (r0) std::memcpy(r0, reach[0].data(), sizeof(float) * reach[0].size());
     if (r1) std::memcpy(r1, reach[1].data(), sizeof(float) * reach[1].size());

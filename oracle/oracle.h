@@ -114,9 +114,10 @@ void orc_solver_root_br_cfv(orc_solver* v, int p, float* out);
 void orc_solver_discounts(int algo, uint32_t t, float* pos, float* neg, float* strat);
 /* lock creation (query.rs): path steps >= 0 are action indices, < 0 encode card (-1 - card) */
 /* node_view's traversals at the node a path reaches (query.rs:490-600):
- * cfv[nh_p] = traverse_avg(node, p), child_cfv[na*nh_p] (p acting) per child,
+ * cfv[nh_p] = traverse_avg (avg = 1) or traverse_br (avg = 0) of the node
+ * for p, child_cfv[na*nh_p] (p acting) per child,
  * walk reach of both players; returns the node index or -1 */
-int orc_solver_node_values(orc_solver* v, const int* steps, int nsteps, int p, float* cfv, float* child_cfv,
+int orc_solver_node_values(orc_solver* v, const int* steps, int nsteps, int p, int avg, float* cfv, float* child_cfv,
                            float* r0, float* r1);
 int orc_solver_walk_path(orc_solver* v, const int* steps, int nsteps, uint32_t* node,
                          float* reach0, float* reach1);

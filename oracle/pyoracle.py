@@ -86,7 +86,7 @@ def lib():
         L.orc_solver_root_br_cfv.argtypes = [P, C.c_int, P]
         L.orc_solver_discounts.argtypes = [C.c_int, C.c_uint32, P, P, P]
         L.orc_solver_walk_path.argtypes = [P, P, C.c_int, P, P, P]
-        L.orc_solver_node_values.argtypes = [P, P, C.c_int, C.c_int, P, P, P, P]
+        L.orc_solver_node_values.argtypes = [P, P, C.c_int, C.c_int, C.c_int, P, P, P, P]
         L.orc_solver_node_values.restype = C.c_int
         L.orc_rake_to_target.argtypes = [P, C.c_int, C.c_int, P, P]
         L.orc_normalize_freqs.argtypes = [P, C.c_int, P]
@@ -301,17 +301,19 @@ class Solver:
         lib().orc_solver_root_br_cfv(self.h, p, ptr(out))
         return out
 
-    def node_values(self, steps, p, na_max=8):
-        """query.rs node_view's traversals for player p at the node `steps`
-        reaches (actions >= 0, cards as -1 - card): (node, cfv, child cfvs
-        (na_max x nh, rows of p's actions when p acts), reach0, reach1)."""
+    def node_values(self, steps, p, na_max=8, avg=True):
+        """query.rs node_view's (avg) or exploit_view's (best response)
+        traversals for player p at the node `steps` reaches (actions >= 0,
+        cards as -1 - card): (node, cfv, child cfvs (na_max x nh, rows of p's
+        actions when p acts), reach0, reach1)."""
         st = np.array(list(steps) + [0], np.int32)
         h = self.spot.nh[p]
         cfv = np.zeros(h, np.float32)
         child = np.zeros((na_max, h), np.float32)
         r0 = np.zeros(self.spot.nh[0], np.float32)
         r1 = np.zeros(self.spot.nh[1], np.float32)
-        n = lib().orc_solver_node_values(self.h, ptr(st), len(steps), p, ptr(cfv), ptr(child), ptr(r0), ptr(r1))
+        n = lib().orc_solver_node_values(self.h, ptr(st), len(steps), p, int(avg), ptr(cfv), ptr(child), ptr(r0),
+                                         ptr(r1))
         if n < 0:
             raise RuntimeError("oracle node_values failed")
         return n, cfv, child, r0, r1
