@@ -28,6 +28,7 @@
 #include <map>
 #include <mutex>
 #include <stdexcept>
+#include <thread>
 #include <unordered_map>
 #include <string>
 #include <vector>
@@ -114,8 +115,56 @@ struct EngineImpl {
     cudaGraphExec_t g_eval[2] = {nullptr, nullptr};
     double* h_dot = nullptr;  // pinned
 
+    // Two pinned chunks for large device -> pageable host copies (allocated
+    // on first use): the DMA of one chunk overlaps the spread copy of the
+    // other into place, so a copy runs near the pinned rate instead of the
+    // pageable one.
+    static constexpr size_t kD2HChunk = size_t(64) << 20;  // bytes
+    unsigned char* d2h_pin[2] = {nullptr, nullptr};
+    cudaEvent_t d2h_ev[2] = {nullptr, nullptr};
+    void d2h_large(void* dst, const void* src, size_t bytes) {
+        if (bytes < 2 * kD2HChunk) {
+            CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            return;
+        }
+        for (int b = 0; b < 2; b++)
+            if (!d2h_pin[b]) {
+                CK(cudaMallocHost(&d2h_pin[b], kD2HChunk));
+                CK(cudaEventCreateWithFlags(&d2h_ev[b], cudaEventDisableTiming));
+            }
+        const size_t nc = (bytes + kD2HChunk - 1) / kD2HChunk;
+        auto issue = [&](size_t j) {
+            const size_t off = j * kD2HChunk, cnt = std::min(kD2HChunk, bytes - off);
+            CK(cudaMemcpyAsync(d2h_pin[j & 1], (const unsigned char*)src + off, cnt, cudaMemcpyDeviceToHost, stream));
+            CK(cudaEventRecord(d2h_ev[j & 1], stream));
+        };
+        const unsigned hw = std::thread::hardware_concurrency();
+        const int nt = (int)std::max(1u, std::min(8u, hw ? hw : 1u));
+        issue(0);
+        for (size_t j = 0; j < nc; j++) {
+            if (j + 1 < nc) issue(j + 1);  // its buffer's previous chunk was copied out last round
+            CK(cudaEventSynchronize(d2h_ev[j & 1]));
+            const size_t off = j * kD2HChunk, cnt = std::min(kD2HChunk, bytes - off);
+            const unsigned char* from = d2h_pin[j & 1];
+            unsigned char* to = (unsigned char*)dst + off;
+            const size_t part = (cnt + nt - 1) / nt;
+            std::vector<std::thread> ts;
+            for (int w = 1; w < nt; w++) {
+                const size_t a = std::min(cnt, w * part), e = std::min(cnt, a + part);
+                if (a < e) ts.emplace_back([=] { std::memcpy(to + a, from + a, e - a); });
+            }
+            std::memcpy(to, from, std::min(cnt, part));
+            for (auto& t : ts) t.join();
+        }
+        CK(cudaStreamSynchronize(stream));
+    }
     ~EngineImpl() {
         if (stream) cudaStreamSynchronize(stream);
+        for (int b = 0; b < 2; b++) {
+            if (d2h_ev[b]) cudaEventDestroy(d2h_ev[b]);
+            if (d2h_pin[b]) cudaFreeHost(d2h_pin[b]);
+        }
         if (g_iter) cudaGraphExecDestroy(g_iter);
         for (auto& g : g_eval)
             if (g) cudaGraphExecDestroy(g);
@@ -748,8 +797,7 @@ void GpuEngine::root_cfv(int p, int mode, float* out) {
 void GpuEngine::export_arena(int which, int p, float* out) {
     EngineImpl& E = *d_;
     fill_staging(which, p);
-    CK(cudaMemcpyAsync(out, E.staging, E.spot->tree.data_size[p] * 4, cudaMemcpyDeviceToHost, E.stream));
-    CK(cudaStreamSynchronize(E.stream));
+    E.d2h_large(out, E.staging, E.spot->tree.data_size[p] * 4);
 }
 // Device arena `which` of player p decoded into `staging` in the reference
 // layout; nodes the engine does not hold (symmetric branches) are zero.
@@ -1220,9 +1268,8 @@ void GpuEngine::sync_to_cpu(HostSolver& host, bool strategy_only) {  // gpu/mod.
                 CK(cudaMemcpyAsync(sc.data(), dsc, sc.size() * 4, cudaMemcpyDeviceToHost, E.stream));
                 uint16_t* harena = ha.kind == 1 ? (uint16_t*)ha.qi.data() : ha.qu.data();
                 std::vector<uint16_t> tmp(whole ? 0 : t.data_size[p]);
-                CK(cudaMemcpyAsync(whole ? harena : tmp.data(), E.staging, t.data_size[p] * 2, cudaMemcpyDeviceToHost,
-                                   E.stream));
                 CK(cudaStreamSynchronize(E.stream));
+                E.d2h_large(whole ? harena : tmp.data(), E.staging, t.data_size[p] * 2);
                 for (uint64_t s = 0; s < E.plan.n_anodes[p]; s++) {
                     const uint32_t nd = E.plan.anode_id[p][s];
                     if (!whole) {
