@@ -52,6 +52,10 @@ class NodeInfo(C.Structure):
     _fields_ = [("node", C.c_uint32), ("kind", C.c_int32), ("player", C.c_int32), ("num_actions", C.c_int32)]
 
 
+class RunoutRow(C.Structure):
+    _fields_ = [("card", C.c_int32), ("eq", C.c_float * 2), ("ev", C.c_float * 2)]
+
+
 class BatchRow(C.Structure):
     _fields_ = [("status", C.c_int32), ("iterations", C.c_uint32), ("exploit_pct", C.c_double),
                 ("seconds", C.c_double), ("ev", C.c_double * 2)]
@@ -124,7 +128,9 @@ def lib():
         "gtob_gpu_read_node_static": (I, [P, I, C.c_uint32, P, C.c_uint64, P]),
         "gtob_gpu_discounts": (I, [P, P]),
         "gtob_gpu_save": (I, [P, P, C.c_char_p]),
-        "gtob_gpu_node_values": (I, [P, P, P, I, C.POINTER(NodeInfo)] + [P] * 8),
+        "gtob_gpu_node_values": (I, [P, P, P, I, C.POINTER(NodeInfo)] + [P] * 10),
+        "gtob_gpu_runouts": (I, [P, P, P, I, C.POINTER(RunoutRow), P, I, I, C.POINTER(I), C.POINTER(I), C.POINTER(I),
+                                 C.POINTER(D)]),
         "gtob_gpu_exploit_values": (I, [P, P, P, I, I, C.POINTER(NodeInfo)] + [P] * 8),
         "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, C.POINTER(P)]),
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
@@ -490,20 +496,38 @@ class GpuSolver:
         nh = sp.nh
         reach = [np.zeros(nh[0], np.float32), np.zeros(nh[1], np.float32)]
         valid = [np.zeros(nh[0], np.float32), np.zeros(nh[1], np.float32)]
+        eq = [np.zeros(nh[0], np.float32), np.zeros(nh[1], np.float32)]
         ev = [np.zeros(nh[0], np.float32), np.zeros(nh[1], np.float32)]
         mx = max(nh) * 64
         strat, aev = np.zeros(mx, np.float32), np.zeros(mx, np.float32)
         info = NodeInfo()
         _check(lib().gtob_gpu_node_values(self._h, sv._h, _ptr(st), len(steps), C.byref(info), _ptr(reach[0]),
-                                          _ptr(reach[1]), _ptr(valid[0]), _ptr(valid[1]), _ptr(ev[0]), _ptr(ev[1]),
-                                          _ptr(strat), _ptr(aev)))
+                                          _ptr(reach[1]), _ptr(valid[0]), _ptr(valid[1]), _ptr(eq[0]), _ptr(eq[1]),
+                                          _ptr(ev[0]), _ptr(ev[1]), _ptr(strat), _ptr(aev)))
         out = {"node": info.node, "kind": info.kind, "player": info.player, "reach": reach, "valid": valid,
-               "ev": ev}
+               "eq": eq, "ev": ev}
         if info.kind == 0:
             na, h = info.num_actions, nh[info.player]
             out["strategy"] = strat[:na * h].reshape(na, h).copy()
             out["action_ev"] = aev[:na * h].reshape(na, h).copy()
         return out
+
+    def runouts(self, path, solver=None):
+        """query.rs runouts at the chance node `path` reaches, from device
+        memory: dict with player, pot and rows (card, freqs, eq, ev)."""
+        sv = solver or self.solver
+        st = np.array(_path_steps(path) + [0], np.int32)
+        rows = (RunoutRow * 52)()
+        freqs = np.zeros(52 * 64, np.float32)
+        n, pl, na, pot = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        _check(lib().gtob_gpu_runouts(self._h, sv._h, _ptr(st), len(st) - 1, rows, _ptr(freqs), 52, 64, C.byref(n),
+                                      C.byref(pl), C.byref(na), C.byref(pot)))
+        out = []
+        for k in range(n.value):
+            r = rows[k]
+            out.append({"card": r.card, "freqs": freqs[k * 64:k * 64 + na.value].copy(),
+                        "eq": [r.eq[0], r.eq[1]], "ev": [r.ev[0], r.ev[1]]})
+        return {"player": pl.value, "num_actions": na.value, "pot": pot.value, "rows": out}
 
     def exploit_values(self, path, exploiter, solver=None):
         """exploit_view's numbers (query.rs:808-930) for `exploiter` at the

@@ -270,8 +270,8 @@ int gtob_load(const char* path, int storage, gtob_solver** out) {
 }
 
 int gtob_gpu_node_values(gtob_gpu* g, const gtob_solver* v, const int* steps, int nsteps, gtob_node_info* info,
-                         float* reach0, float* reach1, float* valid0, float* valid1, float* ev0, float* ev1,
-                         float* strategy, float* action_ev) {
+                         float* reach0, float* reach1, float* valid0, float* valid1, float* eq0, float* eq1,
+                         float* ev0, float* ev1, float* strategy, float* action_ev) {
     REQUIRE(g && v && nsteps >= 0 && (steps || nsteps == 0));
     API_BEGIN
     const NodeValues nv = node_values(*g->e, *v->v, std::vector<int>(steps, steps + nsteps));
@@ -280,10 +280,38 @@ int gtob_gpu_node_values(gtob_gpu* g, const gtob_solver* v, const int* steps, in
     put(reach1, nv.reach[1]);
     put(valid0, nv.valid[0]);
     put(valid1, nv.valid[1]);
+    put(eq0, nv.eq[0]);
+    put(eq1, nv.eq[1]);
     put(ev0, nv.ev[0]);
     put(ev1, nv.ev[1]);
     put(strategy, nv.strategy);
     put(action_ev, nv.action_ev);
+    API_END
+}
+int gtob_gpu_runouts(gtob_gpu* g, const gtob_solver* v, const int* steps, int nsteps, gtob_runout_row* rows,
+                     float* freqs, int max_rows, int max_actions, int* n_rows, int* player, int* num_actions,
+                     double* pot) {
+    REQUIRE(g && v && nsteps >= 0 && (steps || nsteps == 0) && rows && max_rows >= 0 && max_actions >= 0 && n_rows);
+    API_BEGIN
+    const Runouts r = runouts(*g->e, *v->v, std::vector<int>(steps, steps + nsteps));
+    if ((int)r.rows.size() > max_rows)
+        throw Error("invalid argument: " + std::to_string(r.rows.size()) + " runout rows, room for " +
+                    std::to_string(max_rows));
+    if (freqs && r.na > max_actions)
+        throw Error("invalid argument: " + std::to_string(r.na) + " actions, room for " + std::to_string(max_actions));
+    for (size_t k = 0; k < r.rows.size(); k++) {
+        rows[k].card = r.rows[k].card;
+        rows[k].eq[0] = r.rows[k].eq[0];
+        rows[k].eq[1] = r.rows[k].eq[1];
+        rows[k].ev[0] = r.rows[k].ev[0];
+        rows[k].ev[1] = r.rows[k].ev[1];
+        if (freqs)
+            for (size_t a = 0; a < r.rows[k].freqs.size(); a++) freqs[k * max_actions + a] = r.rows[k].freqs[a];
+    }
+    *n_rows = (int)r.rows.size();
+    if (player) *player = r.player;
+    if (num_actions) *num_actions = r.na;
+    if (pot) *pot = r.pot;
     API_END
 }
 int gtob_gpu_exploit_values(gtob_gpu* g, const gtob_solver* v, const int* steps, int nsteps, int exploiter,

@@ -1,5 +1,6 @@
 #include "query.hpp"
 
+#include <algorithm>
 #include <cmath>
 #include <limits>
 
@@ -45,7 +46,100 @@ void fold_values(const Spot& sp, int p, const float* ro, float amount, float* ou
         out[i] = amount * ((float)(t - s[hp.c1[i]] - s[hp.c2[i]]) + same_r);
     }
 }
+// sweep_buckets (game.rs:580-653): win / tie / valid opponent mass of each
+// of p's hands on one complete board.
+void sweep_buckets(const RiverBoard& rb, const Spot& sp, int p, const float* ro, double* win, double* tie,
+                   double* valid) {
+    const std::vector<uint32_t>& ms = rb.str[p];
+    const std::vector<uint16_t>& mi = rb.idx[p];
+    const std::vector<uint32_t>& os = rb.str[1 - p];
+    const std::vector<uint16_t>& oi = rb.idx[1 - p];
+    const Hands& hm = sp.hands[p];
+    const Hands& ho = sp.hands[1 - p];
+    double t_all = 0.0, s_all[52] = {0.0};
+    for (size_t j = 0; j < oi.size(); j++) {
+        const double r = (double)ro[oi[j]];
+        t_all += r;
+        s_all[ho.c1[oi[j]]] += r;
+        s_all[ho.c2[oi[j]]] += r;
+    }
+    std::vector<double> lower(mi.size());
+    {
+        double t = 0.0, s[52] = {0.0};
+        size_t j = 0;
+        for (size_t k = 0; k < mi.size(); k++) {
+            while (j < oi.size() && os[j] < ms[k]) {
+                const double r = (double)ro[oi[j]];
+                t += r;
+                s[ho.c1[oi[j]]] += r;
+                s[ho.c2[oi[j]]] += r;
+                j++;
+            }
+            lower[k] = t - s[hm.c1[mi[k]]] - s[hm.c2[mi[k]]];
+        }
+    }
+    double t = 0.0, s[52] = {0.0};
+    size_t j = oi.size();
+    for (size_t k = mi.size(); k-- > 0;) {
+        while (j > 0 && os[j - 1] > ms[k]) {
+            j--;
+            const double r = (double)ro[oi[j]];
+            t += r;
+            s[ho.c1[oi[j]]] += r;
+            s[ho.c2[oi[j]]] += r;
+        }
+        const int i = mi[k];
+        const double higher = t - s[hm.c1[i]] - s[hm.c2[i]];
+        const uint32_t same = sp.same[p][i];
+        const double same_r = same != kSentinel ? (double)ro[same] : 0.0;
+        const double v = t_all - s_all[hm.c1[i]] - s_all[hm.c2[i]] + same_r;
+        win[i] += lower[k];
+        tie[i] += v - lower[k] - higher;
+        valid[i] += v;
+    }
+}
 }  // namespace
+
+std::vector<float> equity(const Spot& sp, int p, const float* reach_o, const uint8_t* dealt, int nd) {
+    const size_t nh = sp.hands[p].size(), no = sp.hands[1 - p].size();
+    std::vector<double> win(nh, 0.0), tie(nh, 0.0), valid(nh, 0.0);
+    const Hands& ho = sp.hands[1 - p];
+    auto blocked = [&](int c) {
+        if (sp.board_mask >> c & 1) return true;
+        for (int i = 0; i < nd; i++)
+            if (dealt[i] == c) return true;
+        return false;
+    };
+    const int board_len = (int)sp.board.size() + nd;
+    if (board_len == 5) {
+        sweep_buckets(sp.river_at(dealt, nd), sp, p, reach_o, win.data(), tie.data(), valid.data());
+    } else if (board_len == 4) {
+        std::vector<float> ro(no);
+        uint8_t d2[2] = {nd > 0 ? dealt[0] : (uint8_t)0, 0};
+        for (int c = 0; c < 52; c++) {
+            if (blocked(c)) continue;
+            for (size_t j = 0; j < no; j++) ro[j] = (ho.mask[j] >> c & 1) ? 0.0f : reach_o[j];
+            d2[nd] = (uint8_t)c;
+            sweep_buckets(sp.river_at(d2, nd + 1), sp, p, ro.data(), win.data(), tie.data(), valid.data());
+        }
+    } else {
+        std::vector<float> rt(no), ro(no);
+        for (int tc = 0; tc < 52; tc++) {
+            if (sp.board_mask >> tc & 1) continue;
+            for (size_t j = 0; j < no; j++) rt[j] = (ho.mask[j] >> tc & 1) ? 0.0f : reach_o[j];
+            for (int rc = tc + 1; rc < 52; rc++) {
+                if (sp.board_mask >> rc & 1) continue;
+                for (size_t j = 0; j < no; j++) ro[j] = (ho.mask[j] >> rc & 1) ? 0.0f : rt[j];
+                const uint8_t d2[2] = {(uint8_t)tc, (uint8_t)rc};
+                sweep_buckets(sp.river_at(d2, 2), sp, p, ro.data(), win.data(), tie.data(), valid.data());
+            }
+        }
+    }
+    std::vector<float> out(nh);
+    for (size_t i = 0; i < nh; i++)
+        out[i] = valid[i] > 1e-12 ? (float)((win[i] + 0.5 * tie[i]) / valid[i]) : std::numeric_limits<float>::quiet_NaN();
+    return out;
+}
 
 // walk_path (query.rs:304-340) with each action node's strategy from the
 // device block of its representative under the prefix's suit permutation.
@@ -94,12 +188,23 @@ static uint32_t walk_device(GpuEngine& eng, const HostSolver& host, const std::v
     return n;
 }
 
+// The cards a path deals, in order.
+static int path_dealt(const std::vector<int>& steps, uint8_t* dealt) {
+    int nd = 0;
+    for (int s : steps)
+        if (s < 0 && nd < 2) dealt[nd++] = (uint8_t)(-1 - s);
+    return nd;
+}
+
 NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps) {
     const Spot& sp = *host.spot;
     const Tree& t = sp.tree;
     const float nan = std::numeric_limits<float>::quiet_NaN();
     NodeValues out;
     const uint32_t n = walk_device(eng, host, steps, out.reach);
+    uint8_t dealt[2];
+    const int nd = path_dealt(steps, dealt);
+    for (int p = 0; p < 2; p++) out.eq[p] = equity(sp, p, out.reach[1 - p].data(), dealt, nd);
     out.node = n;
     out.kind = t.kind[n];
     out.player = t.kind[n] == kAction ? t.player[n] : -1;
@@ -169,6 +274,113 @@ NodeValues node_values(GpuEngine& eng, const HostSolver& host, const std::vector
         }
         for (int i = 0; i < nh; i++)
             if (valid[i] > 1e-9) out.ev[p][i] = (float)total[i];
+    }
+    return out;
+}
+
+Runouts runouts(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps) {
+    const Spot& sp = *host.spot;
+    const Tree& t = sp.tree;
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    std::vector<float> reach[2];
+    const uint32_t n = walk_device(eng, host, steps, reach);
+    if (t.kind[n] != kChance) throw Error("runouts report requires a chance (card) node");
+    uint8_t dealt[2];
+    const int nd = path_dealt(steps, dealt);
+    Runouts out;
+    struct Card {
+        int c;
+        uint32_t child, canon;
+        std::array<uint8_t, 4> perm;
+    };
+    std::vector<Card> cards;
+    for (int c = 51; c >= 0; c--) {
+        const uint32_t ch = t.children[t.child_start[n] + c];
+        bool was = false;
+        for (int i = 0; i < nd; i++) was = was || dealt[i] == c;
+        if (ch == kSentinel || was) continue;
+        std::vector<int> st = steps;
+        st.push_back(-1 - c);
+        Card e{c, ch, 0, {0, 1, 2, 3}};
+        std::vector<float> unused[2];
+        host.walk(host.canonical_steps(st, &e.perm), &e.canon, unused);
+        cards.push_back(e);
+    }
+    // the children's average-strategy values, one sweep per player
+    std::vector<uint32_t> uniq;
+    for (auto& e : cards)
+        if (std::find(uniq.begin(), uniq.end(), e.canon) == uniq.end()) uniq.push_back(e.canon);
+    std::vector<float> vals[2];
+    std::vector<uint8_t> ok[2];
+    for (int p = 0; p < 2; p++) {
+        vals[p].assign(uniq.size() * sp.hands[p].size(), 0.0f);
+        ok[p].assign(uniq.size(), 0);
+        eng.sweep_values(p, 1, uniq.data(), (int)uniq.size(), vals[p].data(), ok[p].data());
+    }
+    for (auto& e : cards) {
+        const uint32_t ch = e.child;
+        RunoutRow row;
+        row.card = e.c;
+        std::vector<float> rc[2] = {reach[0], reach[1]};
+        for (int p = 0; p < 2; p++)
+            for (size_t i = 0; i < rc[p].size(); i++)
+                if (sp.hands[p].mask[i] >> e.c & 1) rc[p][i] = 0.0f;
+        if (t.kind[ch] == kAction) {
+            const int p = t.player[ch], na = t.nchild[ch];
+            const size_t nh = sp.hands[p].size();
+            out.player = p;
+            out.na = na;
+            std::vector<float> sig((size_t)na * nh);
+            auto lk = host.locks.find(e.canon);
+            if (lk != host.locks.end()) sig = lk->second;
+            else eng.node_average_strategy(e.canon, sig.data());
+            const std::vector<int> m = hand_map(sp, p, e.perm);
+            double total = 0.0;
+            std::vector<double> sums(na, 0.0);
+            for (size_t i = 0; i < nh; i++) {
+                const double r = (double)rc[p][i];
+                total += r;
+                for (int a = 0; a < na; a++) sums[a] += r * (double)sig[(size_t)a * nh + m[i]];
+            }
+            for (int a = 0; a < na; a++) row.freqs.push_back(total > 1e-12 ? (float)(sums[a] / total) : 0.0f);
+        }
+        uint8_t d2[2] = {nd > 0 ? dealt[0] : (uint8_t)0, 0};
+        d2[nd] = (uint8_t)e.c;
+        const size_t u = (size_t)(std::find(uniq.begin(), uniq.end(), e.canon) - uniq.begin());
+        for (int p = 0; p < 2; p++) {
+            const size_t nh = sp.hands[p].size();
+            const float* ro = rc[1 - p].data();
+            const std::vector<double> valid = valid_opp_sum(sp, p, ro);
+            const std::vector<float> eq = equity(sp, p, ro, d2, nd + 1);
+            double num = 0.0, den = 0.0;
+            for (size_t i = 0; i < nh; i++)
+                if (!std::isnan(eq[i])) {
+                    const double w = (double)rc[p][i] * valid[i];
+                    num += w * (double)eq[i];
+                    den += w;
+                }
+            row.eq[p] = den > 1e-12 ? (float)(num / den) : nan;
+            std::vector<float> cfv(nh, 0.0f);
+            if (ok[p][u]) {
+                const std::vector<int> m = hand_map(sp, p, e.perm);
+                for (size_t i = 0; i < nh; i++) cfv[i] = vals[p][u * nh + m[i]];
+            } else if (t.kind[ch] == kFold) {
+                fold_values(sp, p, ro, (float)(t.player[ch] == p ? t.tlose[ch] : t.twin[ch]), cfv.data());
+            } else {
+                throw Error("runouts need the staged or plain engine (showdowns with slots)");
+            }
+            const double put = p == 0 ? t.put0[ch] : t.put1[ch];
+            num = den = 0.0;
+            for (size_t i = 0; i < nh; i++)
+                if (valid[i] > 1e-9 && rc[p][i] > 0.0f) {
+                    const double w = (double)rc[p][i] * valid[i];
+                    num += w * ((double)cfv[i] / valid[i] + put);
+                    den += w;
+                }
+            row.ev[p] = den > 1e-12 ? (float)(num / den) : nan;
+        }
+        if (out.pot == 0.0) out.pot = t.put0[ch] + t.put1[ch];
+        out.rows.push_back(std::move(row));
     }
     return out;
 }

@@ -19,6 +19,7 @@ struct NodeValues {
     int kind = 0, player = -1, na = 0;
     std::vector<float> reach[2];  // walk reach (query.rs:304-340)
     std::vector<float> valid[2];  // compatible opponent reach mass (query.rs:463-488)
+    std::vector<float> eq[2];     // equity over the remaining runouts (best_response.rs:292-386), NaN if none
     std::vector<float> ev[2];     // pot-share EV, NaN where valid <= 1e-9
     std::vector<float> strategy;  // the actor's average strategy, [action * nh + hand]
     std::vector<float> action_ev;  // the actor's EV per action, same layout, NaN where valid <= 1e-9
@@ -38,6 +39,26 @@ struct ExploitValues {
     float avg[3];
 };
 ExploitValues exploit_values(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps, int p);
+
+// runouts (query.rs:964-1106) at a chance node: per available card,
+// descending, the action frequencies at the following action node, and per
+// player the reach x valid weighted equity and average-strategy EV.
+struct RunoutRow {
+    int card = 0;
+    std::vector<float> freqs;
+    float eq[2], ev[2];  // NaN when no mass
+};
+struct Runouts {
+    int player = -1, na = 0;  // actor and action count at the runout nodes (-1, 0: none)
+    double pot = 0.0;
+    std::vector<RunoutRow> rows;
+};
+Runouts runouts(GpuEngine& eng, const HostSolver& host, const std::vector<int>& steps);
+
+// Equity of each of p's hands against the opponent reach, enumerating the
+// remaining runouts of the board plus `dealt` (best_response.rs:292-386,
+// game.rs:580-653 sweep_buckets); NaN where no compatible mass.
+std::vector<float> equity(const Spot& sp, int p, const float* reach_o, const uint8_t* dealt, int nd);
 
 // steps: action indices (>= 0) and dealt cards (-1 - card), from the root.
 // Through a suit-isomorphic branch the device holds the representative: its

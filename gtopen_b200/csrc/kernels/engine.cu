@@ -909,6 +909,23 @@ void GpuEngine::node_sweep_values(uint32_t node, int p, int mode, float* cfv, fl
     E.check_err();
 }
 
+void GpuEngine::sweep_values(int p, int mode, const uint32_t* nodes, int n, float* out, uint8_t* ok) {
+    EngineImpl& E = *d_;
+    if (mode != 0 && mode != 1) throw Error("invalid argument: sweep mode");
+    E.sweep(p, mode, nullptr);
+    E.reach_valid = false;
+    const int nh = E.plan.nh[p];
+    for (int k = 0; k < n; k++) {
+        const uint32_t c = nodes[k] < E.plan.node_cslot.size() ? E.plan.node_cslot[nodes[k]] : kNoSlot;
+        ok[k] = c != kNoSlot;
+        if (c != kNoSlot)
+            CK(cudaMemcpyAsync(out + (size_t)k * nh, E.d.cfv + (size_t)c * E.d.nh_max, nh * sizeof(float),
+                               cudaMemcpyDeviceToHost, E.stream));
+    }
+    CK(cudaStreamSynchronize(E.stream));
+    E.check_err();
+}
+
 // ------------------------------------------------ .gto straight from / to HBM
 // One block of a device save's image: dst <- src gathered through a hand
 // permutation table, action by action (cfr.rs:806-871 copy_branch, with

@@ -69,6 +69,9 @@ class GpuEngine {
     // evaluated in place, which have no slot).
     void node_sweep_values(uint32_t node, int p, int mode, float* cfv, float* reach0, float* reach1, float* child_cfv,
                            uint8_t* child_ok);
+    // One evaluation sweep as node_sweep_values, then the values for p of
+    // n nodes (out[k * nh_p ...]; ok[k] = 0 for a node without a slot).
+    void sweep_values(int p, int mode, const uint32_t* nodes, int n, float* out, uint8_t* ok);
     // time one kind of level launch set: used by bench for the roofline
     void discounts(float* out3);
     // .gto written from the device arenas through a pinned double buffer (no

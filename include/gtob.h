@@ -211,8 +211,10 @@ int gtob_gpu_load(const char* path, int storage, int device_format, int engine, 
  * average-strategy evaluation sweep per player (best_response.rs:128-223).
  * Through a suit-isomorphic branch the device holds the representative; its
  * values are returned under the hand permutation ensure_symmetric applies.
- * Outputs (NULL to skip): reach_p / valid_p / ev_p per hand of player p (ev
- * in the pot-share convention, NaN where valid <= 1e-9); at an action node,
+ * Outputs (NULL to skip): reach_p / valid_p / eq_p / ev_p per hand of player
+ * p (eq: equity against the opponent's reach over the remaining runouts,
+ * best_response.rs:292-386, NaN without compatible mass; ev in the pot-share
+ * convention, NaN where valid <= 1e-9); at an action node,
  * strategy and action_ev (num_actions x hands of the actor, action-major).
  * Supported on the staged and plain engines (showdowns with slots).  The
  * sweeps reuse the engine's buffers: do not call it while another call on
@@ -224,8 +226,24 @@ typedef struct {
     int32_t num_actions; /* at an action node, else 0 */
 } gtob_node_info;
 int gtob_gpu_node_values(gtob_gpu* gpu, const gtob_solver* solver, const int* steps, int nsteps, gtob_node_info* info,
-                         float* reach0, float* reach1, float* valid0, float* valid1, float* ev0, float* ev1,
-                         float* strategy, float* action_ev);
+                         float* reach0, float* reach1, float* valid0, float* valid1, float* eq0, float* eq1,
+                         float* ev0, float* ev1, float* strategy, float* action_ev);
+/* runouts (query.rs:964-1106) at the chance node a path reaches: one row per
+ * available card, descending -- the action frequencies at the following
+ * action node (freqs[row * max_actions + a], reach-weighted), and per player
+ * the reach x valid weighted equity (eq_p of node values; equity enumerates
+ * the remaining runouts, best_response.rs:292-386) and average-strategy EV
+ * (NaN when there is no mass).  *n_rows receives the row count (at most
+ * max_rows), *player / *num_actions the actor at the runout nodes (-1 / 0 for
+ * none), *pot the pot there. */
+typedef struct {
+    int32_t card;
+    float eq[2];
+    float ev[2];
+} gtob_runout_row;
+int gtob_gpu_runouts(gtob_gpu* gpu, const gtob_solver* solver, const int* steps, int nsteps, gtob_runout_row* rows,
+                     float* freqs, int max_rows, int max_actions, int* n_rows, int* player, int* num_actions,
+                     double* pot);
 
 /* exploit_view's numbers (query.rs:808-930) for `exploiter` at the node a
  * path reaches, from device memory (one best-response and one

@@ -218,3 +218,130 @@ def test_exploit_values_mirror_branch():
         for k in ("br_ev", "cur_ev", "reach", "valid"):
             va, vb = a[k][i], b[k][j]
             assert (np.isnan(va) and np.isnan(vb)) or va == vb, (k, i, j, va, vb)
+
+
+def _equity(ospot, p, ro, dealt, board):
+    """best_response.rs:292-386 / game.rs:580-653 restated over the oracle's
+    river tables (the test's own reference for the equity numbers)."""
+    oc1, oc2, _ = ospot.hands(1 - p)
+    c1, c2, _ = ospot.hands(p)
+    same = ospot.same_combo(p)
+    nh = len(c1)
+    win, tie, valid = np.zeros(nh), np.zeros(nh), np.zeros(nh)
+
+    def sweep(d, r):
+        ms, mi = ospot.river(p, d)
+        os_, oi = ospot.river(1 - p, d)
+        r = r.astype(np.float64)
+        t_all = r[oi].sum()
+        s_all = np.zeros(52)
+        np.add.at(s_all, oc1[oi], r[oi])
+        np.add.at(s_all, oc2[oi], r[oi])
+        j, t, s = 0, 0.0, np.zeros(52)
+        lower = np.zeros(len(mi))
+        for k in range(len(mi)):
+            while j < len(oi) and os_[j] < ms[k]:
+                x = oi[j]
+                t += r[x]
+                s[oc1[x]] += r[x]
+                s[oc2[x]] += r[x]
+                j += 1
+            lower[k] = t - s[c1[mi[k]]] - s[c2[mi[k]]]
+        j, t, s = len(oi), 0.0, np.zeros(52)
+        for k in range(len(mi) - 1, -1, -1):
+            while j > 0 and os_[j - 1] > ms[k]:
+                j -= 1
+                x = oi[j]
+                t += r[x]
+                s[oc1[x]] += r[x]
+                s[oc2[x]] += r[x]
+            i = mi[k]
+            higher = t - s[c1[i]] - s[c2[i]]
+            sr = r[same[i]] if same[i] != 0xFFFFFFFF else 0.0
+            v = t_all - s_all[c1[i]] - s_all[c2[i]] + sr
+            win[i] += lower[k]
+            tie[i] += v - lower[k] - higher
+            valid[i] += v
+
+    omask = lambda c: (oc1 == c) | (oc2 == c)
+    nb = len(dealt) + 3
+    if nb == 5:
+        sweep(list(dealt), ro)
+    else:
+        bd = set(board)
+        free = [c for c in range(52) if c not in bd and c not in dealt]
+        if nb == 4:
+            for c in free:
+                sweep(list(dealt) + [c], np.where(omask(c), 0.0, ro))
+        else:
+            for a in range(len(free)):
+                for b in range(a + 1, len(free)):
+                    ta, tb = free[a], free[b]
+                    sweep([ta, tb], np.where(omask(ta) | omask(tb), 0.0, ro))
+    out = np.full(nh, np.nan)
+    ok = valid > 1e-12
+    out[ok] = (win[ok] + 0.5 * tie[ok]) / valid[ok]
+    return out
+
+
+def test_equity_and_runouts_match_oracle():
+    cfg = W.small_flop_spot()
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, storage="f32", use_iso=False)
+    gpu = g.GpuSolver(host)
+    gpu.iterate(20)
+    nv = gpu.node_values([1, 1, "Ah"], host)
+    ro_turn = gpu.runouts([0, 0], host)
+    ro_river = gpu.runouts([0, 0, "Ah", 0, 0], host)
+    gpu.sync_to_cpu(host)
+    ospot = po.Spot(cfg)
+    osv = po.Solver(ospot, compressed=False, use_iso=False, prune=False)
+    for which in (0, 1):
+        for q in (0, 1):
+            osv.set_arena(which, q, host.arena(which, q))
+    card = lambda s: "23456789TJQKA".index(s[0]) * 4 + "cdhs".index(s[1])
+    board = [card(cfg["board"][i:i + 2]) for i in range(0, len(cfg["board"]), 2)]
+    # equity at a turn node (river runouts enumerated)
+    for p in (0, 1):
+        _, _, _, r0, r1 = osv.node_values(_steps([1, 1, "Ah"]), p)
+        ro = (r0, r1)[1 - p]
+        _close(nv["eq"][p], _equity(ospot, p, ro, [card("Ah")], board), ("eq", p))
+    tree = spot.tree()
+    for path, rep in (([0, 0], ro_turn), ([0, 0, "Ah", 0, 0], ro_river)):
+        dealt = [card(s) for s in path if isinstance(s, str)]
+        assert len(rep["rows"]) > 0
+        assert [r["card"] for r in rep["rows"]] == sorted([r["card"] for r in rep["rows"]], reverse=True)
+        for row in rep["rows"]:
+            c = row["card"]
+            cp = path + ["23456789TJQKA"[c >> 2] + "cdhs"[c & 3]]
+            for p in (0, 1):
+                node, cfv, _, r0, r1 = osv.node_values(_steps(cp), p)
+                reach = (r0, r1)
+                ro = reach[1 - p].astype(np.float64)
+                oc1, oc2, _ = ospot.hands(1 - p)
+                c1, c2, _ = ospot.hands(p)
+                same = ospot.same_combo(p)
+                s = np.zeros(52)
+                np.add.at(s, oc1, ro)
+                np.add.at(s, oc2, ro)
+                valid = ro.sum() - s[c1] - s[c2] + np.where(same != 0xFFFFFFFF, ro[np.minimum(same, len(ro) - 1)], 0.0)
+                rp = reach[p].astype(np.float64)
+                eq = _equity(ospot, p, reach[1 - p], dealt + [c], board)
+                m = ~np.isnan(eq)
+                w = rp[m] * valid[m]
+                exp_eq = (w * eq[m]).sum() / w.sum() if w.sum() > 1e-12 else np.nan
+                put = tree["put0" if p == 0 else "put1"][node]
+                ok = (valid > 1e-9) & (rp > 0)
+                w = rp[ok] * valid[ok]
+                exp_ev = (w * (cfv[ok] / valid[ok] + put)).sum() / w.sum() if w.sum() > 1e-12 else np.nan
+                _close([row["eq"][p]], [exp_eq], ("runout eq", path, c, p))
+                _close([row["ev"][p]], [exp_ev], ("runout ev", path, c, p))
+            if tree["kind"][node] == 0:
+                pl = int(tree["player"][node])
+                na = int(tree["nchild"][node])
+                _, _, _, r0, r1 = osv.node_values(_steps(cp), pl)
+                rp = (r0, r1)[pl].astype(np.float64)
+                sig = osv.avg_strategy(node, na, len(rp)).reshape(na, -1).astype(np.float64)
+                exp_f = (sig * rp[None, :]).sum(1) / rp.sum()
+                assert rep["player"] == pl and rep["num_actions"] == na
+                assert np.allclose(row["freqs"], exp_f, rtol=1e-5, atol=1e-6), (path, c)
