@@ -4,6 +4,11 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <atomic>
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <unordered_map>
 
 namespace gtob {
@@ -17,21 +22,253 @@ struct Visit {
     uint32_t rs[2];
     uint32_t slot;  // river slot once the board is complete, else kNoSlot
 };
+bool is_terminal(uint8_t k) { return k == kFold || k == kShowdown; }
+
+// Ids a subtree builder hands out before the merge knows its bases: kLocal + k.
+constexpr uint32_t kLocal = 0x40000000u;
+inline bool is_local(uint32_t x) { return x != kNoSlot && (x & 0xC0000000u) == kLocal; }
+
 template <class T>
-void flatten(std::vector<std::vector<std::pair<uint32_t, T>>>& by_level, std::vector<T>& flat, std::vector<Span>& span) {
+using Levels = std::vector<std::vector<std::pair<uint32_t, T>>>;
+
+// One depth-first traversal over representative branches (plan.rs:100-198).
+// The root builder covers the tree above the chance nodes and hands each
+// representative chance child to a subtree builder (a task); subtree
+// builders run on worker threads with ids of their own, which the merge
+// offsets.
+struct Builder {
+    const Spot& sp;
+    const Tree& t;
+    Plan& P;
+    std::vector<uint8_t>& visited;
+    bool fused, fuse_folds, spawn;
+    Levels<ActItem> act_l[2];  // by actor
+    Levels<EdgeItem> edge_l;
+    Levels<FoldItem> fold_l;
+    Levels<ShowItem> show_l;
+    Levels<ChanceItem> chance_l;
+    std::vector<ChildRef> crefs;
+    std::vector<TermInfo> terms;
+    std::vector<CardEntry> cards;
+    std::unordered_map<size_t, uint32_t> slot_of_key;
+    std::vector<uint32_t> slot_key;
+    uint32_t id0;  // first id: 1 for the root builder, kLocal for a subtree
+    uint64_t next_c, next_r[2];
+    uint64_t num_visited = 0, visited_terminals = 0;
+    uint32_t max_children = 0;
+    std::vector<uint32_t> nodes;  // subtree builders: the nodes visited (their slot entries are remapped)
+    std::vector<Visit> tasks;     // root builder: the subtrees handed out
+    std::vector<uint32_t> cbase_of, rbase_of[2];
+
+    Builder(const Spot& s, Plan& p, std::vector<uint8_t>& vis, bool fu, bool ff, bool root)
+        : sp(s), t(s.tree), P(p), visited(vis), fused(fu), fuse_folds(ff), spawn(root), id0(root ? 0u : kLocal) {
+        next_c = root ? 1 : kLocal;
+        next_r[0] = next_r[1] = root ? 1 : kLocal;
+    }
+    bool in_place(uint8_t kind) const { return kind == kFold ? fuse_folds : kind == kShowdown ? fused : false; }
+    void grow(uint32_t lv) {
+        if (edge_l.size() <= lv) {
+            act_l[0].resize(lv + 1);
+            act_l[1].resize(lv + 1);
+            edge_l.resize(lv + 1);
+            fold_l.resize(lv + 1);
+            show_l.resize(lv + 1);
+            chance_l.resize(lv + 1);
+        }
+    }
+    uint32_t river_slot(const uint8_t* dealt, int nd) {
+        const size_t key = sp.river_key(dealt, nd);
+        auto it = slot_of_key.find(key);
+        if (it != slot_of_key.end()) return it->second;
+        const uint32_t sl = id0 + (uint32_t)slot_key.size();
+        slot_of_key[key] = sl;
+        slot_key.push_back((uint32_t)key);
+        return sl;
+    }
+    uint32_t term_of(uint32_t c, const uint8_t* dealt, int nd) {
+        TermInfo ti{(float)t.twin[c], (float)t.tlose[c], (float)t.ttie[c], 0};
+        ti.aux = t.kind[c] == kFold ? t.player[c] : river_slot(dealt, nd);
+        terms.push_back(ti);
+        visited_terminals++;
+        num_visited++;
+        return (uint32_t)(terms.size() - 1);
+    }
+    void run(const Visit& start) {
+        std::vector<Visit> stack;
+        stack.push_back(start);
+        Visit kids[256];  // children of the node being visited (nchild is a u8)
+        while (!stack.empty()) {
+            Visit v = stack.back();
+            stack.pop_back();
+            const uint32_t nd = v.node;
+            visited[nd] = 1;
+            P.node_cslot[nd] = v.cslot;
+            P.node_rs[0][nd] = v.rs[0];
+            P.node_rs[1][nd] = v.rs[1];
+            if (!spawn) nodes.push_back(nd);
+            grow(v.level);
+            num_visited++;
+            switch (t.kind[nd]) {
+                case kAction: {
+                    const int a = t.player[nd], na = t.nchild[nd];
+                    ActItem it{};
+                    it.node = nd;
+                    it.cslot = v.cslot;
+                    it.rslot = v.rs[a];
+                    it.oslot = v.rs[1 - a];
+                    it.actor = (uint32_t)a;
+                    it.na = (uint32_t)na;
+                    it.cref = (uint32_t)crefs.size();
+                    max_children = std::max<uint32_t>(max_children, (uint32_t)na);
+                    int nkids = 0;
+                    for (int k = 0; k < na; k++) {
+                        const uint32_t c = t.child(nd, k);
+                        if (is_terminal(t.kind[c]) && in_place(t.kind[c])) {
+                            uint32_t ti = term_of(c, v.dealt, v.ndealt);
+                            // With folds in place but showdowns not (the staged and warp
+                            // engines), a fold child still gets the actor's reach slot: the
+                            // down sweep, which has the actor's strategy at hand, writes the
+                            // folding player's reach there, and the parent's up kernel reads
+                            // it instead of recomputing that strategy.
+                            const uint32_t frs = (t.kind[c] == kFold && !fused) ? (uint32_t)next_r[a]++ : kNoSlot;
+                            crefs.push_back({t.kind[c] == kFold ? kChildFold : kChildShow, kNoSlot, frs, ti});
+                            it.nterm++;
+                            continue;
+                        }
+                        Visit cv = v;
+                        cv.node = c;
+                        cv.level = v.level + 1;
+                        cv.cslot = (uint32_t)next_c++;
+                        cv.rs[a] = (uint32_t)next_r[a]++;
+                        crefs.push_back({kChildNode, cv.cslot, cv.rs[a], kNoSlot});
+                        kids[nkids++] = cv;
+                    }
+                    act_l[a][v.level].push_back({nd, it});
+                    for (int k = nkids - 1; k >= 0; k--) stack.push_back(kids[k]);
+                    break;
+                }
+                case kChance: {
+                    std::vector<int> valid = P.iso_active ? sp.perms_fixing(v.dealt, v.ndealt) : std::vector<int>{0};
+                    struct CardRep { uint8_t card, rep; uint32_t perm; };
+                    std::vector<CardRep> cr;
+                    for (int c = 0; c < 52; c++) {
+                        uint32_t ch = t.children[t.child_start[nd] + c];
+                        bool dealt = false;
+                        for (int i = 0; i < v.ndealt; i++) dealt = dealt || v.dealt[i] == c;
+                        if (ch == kSentinel || dealt) continue;
+                        uint8_t rep = (uint8_t)c;
+                        uint32_t krep = 0;
+                        for (int k : valid) {
+                            uint8_t pc = card_permute((uint8_t)c, sp.perms[k]);
+                            if (pc < rep) { rep = pc; krep = (uint32_t)k; }
+                        }
+                        cr.push_back({(uint8_t)c, rep, krep});
+                    }
+                    uint32_t rep_cslot[52], rep_term[52];
+                    ChanceItem ci{};
+                    ci.cslot = v.cslot;
+                    ci.inv = 1.0f / (float)(46 - (int)t.street[nd]);
+                    ci.rs[0] = v.rs[0];
+                    ci.rs[1] = v.rs[1];
+                    int nkids = 0;
+                    for (auto& x : cr) {
+                        if (x.card != x.rep) continue;
+                        const uint32_t c = t.children[t.child_start[nd] + x.card];
+                        uint8_t d2[2] = {v.ndealt > 0 ? v.dealt[0] : (uint8_t)0, 0};
+                        d2[v.ndealt] = x.card;
+                        if (fused && t.kind[c] == kShowdown) {
+                            rep_term[x.card] = term_of(c, d2, v.ndealt + 1);
+                            rep_cslot[x.card] = kNoSlot;
+                            continue;
+                        }
+                        Visit cv = v;
+                        cv.node = c;
+                        cv.level = v.level + 1;
+                        cv.dealt[0] = d2[0];
+                        cv.dealt[1] = d2[1];
+                        cv.ndealt = v.ndealt + 1;
+                        cv.slot = sp.board.size() + (size_t)cv.ndealt == 5 ? river_slot(cv.dealt, cv.ndealt) : kNoSlot;
+                        cv.cslot = (uint32_t)next_c++;
+                        cv.rs[0] = (uint32_t)next_r[0]++;
+                        cv.rs[1] = (uint32_t)next_r[1]++;
+                        rep_cslot[x.card] = cv.cslot;
+                        rep_term[x.card] = kNoSlot;
+                        EdgeItem e{{v.rs[0], v.rs[1]}, {cv.rs[0], cv.rs[1]}, x.card, 0};
+                        edge_l[v.level].push_back({c, e});
+                        kids[nkids++] = cv;
+                    }
+                    ci.cc_start = (uint32_t)cards.size();
+                    ci.cc_count = (uint32_t)cr.size();
+                    for (auto& x : cr) {
+                        // low byte: the dealt card; second byte: its orbit representative
+                        cards.push_back({(uint32_t)x.card | ((uint32_t)x.rep << 8), rep_cslot[x.rep], x.perm, rep_term[x.rep]});
+                        if (rep_term[x.rep] != kNoSlot) ci.nterm++;
+                    }
+                    chance_l[v.level].push_back({nd, ci});
+                    if (spawn) {  // each representative subtree becomes a task
+                        for (int k = 0; k < nkids; k++) tasks.push_back(kids[k]);
+                    } else {
+                        for (int k = nkids - 1; k >= 0; k--) stack.push_back(kids[k]);
+                    }
+                    break;
+                }
+                case kFold: {
+                    FoldItem f{v.cslot, {v.rs[0], v.rs[1]}, t.player[nd], (float)t.twin[nd], (float)t.tlose[nd]};
+                    fold_l[v.level].push_back({nd, f});
+                    visited_terminals++;
+                    break;
+                }
+                default: {
+                    ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, v.slot != kNoSlot ? v.slot : river_slot(v.dealt, v.ndealt),
+                                (float)t.twin[nd], (float)t.tlose[nd], (float)t.ttie[nd], 0};
+                    show_l[v.level].push_back({nd, si});
+                    visited_terminals++;
+                    break;
+                }
+            }
+        }
+    }
+};
+
+// Where each builder's level lists go in a flat array: level by level, the
+// builders in order (the groups, e.g. actors, one after another within a
+// level).  off[g][lv][b] = start of builder b's group-g list of level lv.
+struct FlatLayout {
+    std::vector<std::vector<std::vector<size_t>>> off;
+    std::vector<Span> span;                // per level
+    std::vector<std::vector<Span>> gspan;  // per group, per level
     size_t total = 0;
-    for (auto& lst : by_level) total += lst.size();
-    flat.reserve(total);
-    auto by_node = [](const auto& a, const auto& b) { return a.first < b.first; };
-    for (auto& lst : by_level) {
-        // the traversal visits a level's nodes in node order already; sort only if not
-        if (!std::is_sorted(lst.begin(), lst.end(), by_node)) std::sort(lst.begin(), lst.end(), by_node);
-        span.push_back({(uint32_t)flat.size(), (uint32_t)lst.size()});
-        for (auto& x : lst) flat.push_back(x.second);
-        std::vector<std::pair<uint32_t, T>>().swap(lst);
+};
+template <class T>
+FlatLayout flat_layout(size_t levels, const std::vector<std::vector<const Levels<T>*>>& lists) {
+    // lists[b][g]: builder b's group-g levels
+    const size_t nb = lists.size(), ng = nb ? lists[0].size() : 0;
+    FlatLayout L;
+    L.off.assign(ng, std::vector<std::vector<size_t>>(levels, std::vector<size_t>(nb, 0)));
+    L.gspan.assign(ng, {});
+    for (size_t lv = 0; lv < levels; lv++) {
+        const size_t l0 = L.total;
+        for (size_t g = 0; g < ng; g++) {
+            const size_t g0 = L.total;
+            for (size_t b = 0; b < nb; b++) {
+                L.off[g][lv][b] = L.total;
+                const Levels<T>& ls = *lists[b][g];
+                if (lv < ls.size()) L.total += ls[lv].size();
+            }
+            L.gspan[g].push_back({(uint32_t)g0, (uint32_t)(L.total - g0)});
+        }
+        L.span.push_back({(uint32_t)l0, (uint32_t)(L.total - l0)});
+    }
+    return L;
+}
+template <class T, class V>
+void flat_copy(const FlatLayout& L, size_t b, size_t g, Levels<T>& ls, V& flat) {
+    for (size_t lv = 0; lv < ls.size(); lv++) {
+        size_t o = L.off[g][lv][b];
+        for (auto& x : ls[lv]) flat[o++] = x.second;
+        std::vector<std::pair<uint32_t, T>>().swap(ls[lv]);
     }
 }
-bool is_terminal(uint8_t k) { return k == kFold || k == kShowdown; }
 }  // namespace
 
 Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
@@ -40,193 +277,188 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
     const bool fused = fuse_mode == kFuseAll;
     P.fused = fused;
     P.fuse_folds = fuse_mode != kFuseNone;
-    auto in_place = [&](uint8_t kind) { return kind == kFold ? P.fuse_folds : kind == kShowdown ? fused : false; };
     P.nh[0] = (int)sp.hands[0].size();
     P.nh[1] = (int)sp.hands[1].size();
     P.nh_max = std::max(P.nh[0], P.nh[1]);
     P.iso_active = use_iso && sp.perms.size() > 1;
     const size_t n = t.size();
-
-    std::vector<std::vector<std::pair<uint32_t, ActItem>>> act_l;
-    std::vector<std::vector<std::pair<uint32_t, EdgeItem>>> edge_l;
-    std::vector<std::vector<std::pair<uint32_t, FoldItem>>> fold_l;
-    std::vector<std::vector<std::pair<uint32_t, ShowItem>>> show_l;
-    std::vector<std::vector<std::pair<uint32_t, ChanceItem>>> chance_l;
-    auto grow = [&](uint32_t lv) {
-        if (act_l.size() <= lv) {
-            act_l.resize(lv + 1);
-            edge_l.resize(lv + 1);
-            fold_l.resize(lv + 1);
-            show_l.resize(lv + 1);
-            chance_l.resize(lv + 1);
-        }
-    };
-    std::unordered_map<size_t, uint32_t> slot_of_key;
-    auto river_slot = [&](const uint8_t* dealt, int nd) {
-        size_t key = sp.river_key(dealt, nd);
-        auto it = slot_of_key.find(key);
-        if (it != slot_of_key.end()) return it->second;
-        uint32_t s = (uint32_t)P.slot_key.size();
-        slot_of_key[key] = s;
-        P.slot_key.push_back((uint32_t)key);
-        return s;
-    };
-    auto term_of = [&](uint32_t c, const uint8_t* dealt, int nd) {
-        TermInfo ti{(float)t.twin[c], (float)t.tlose[c], (float)t.ttie[c], 0};
-        ti.aux = t.kind[c] == kFold ? t.player[c] : river_slot(dealt, nd);
-        P.terms.push_back(ti);
-        P.visited_terminals++;
-        P.num_visited++;
-        return (uint32_t)(P.terms.size() - 1);
-    };
     std::vector<uint8_t> visited(n, 0);
     P.node_cslot.assign(n, kNoSlot);
     P.node_rs[0].assign(n, kNoSlot);
     P.node_rs[1].assign(n, kNoSlot);
-    {  // capacity for the flat tables (no regrowth during the traversal)
-        size_t nchild = 0, nterm = 0;
-        for (size_t i = 0; i < n; i++) {
-            if (t.kind[i] == kAction) nchild += t.nchild[i];
-            else if (is_terminal(t.kind[i])) nterm++;
-        }
-        P.crefs.reserve(nchild);
-        P.terms.reserve(nterm);
-    }
 
-    uint64_t next_c = 1, next_r[2] = {1, 1};
-    std::vector<Visit> stack;
+    // the tree above the chance nodes, then every representative chance
+    // subtree on the worker threads
+    Builder root(sp, P, visited, fused, P.fuse_folds, true);
     const bool full_board = sp.board.size() == 5;
-    stack.push_back({0, 0, {0, 0}, 0, 0, {0, 0}, full_board ? river_slot(nullptr, 0) : kNoSlot});
-    Visit kids[256];  // children of the node being visited (nchild is a u8)
-    while (!stack.empty()) {
-        Visit v = stack.back();
-        stack.pop_back();
-        const uint32_t nd = v.node;
-        visited[nd] = 1;
-        P.node_cslot[nd] = v.cslot;
-        P.node_rs[0][nd] = v.rs[0];
-        P.node_rs[1][nd] = v.rs[1];
-        grow(v.level);
-        P.num_visited++;
-        switch (t.kind[nd]) {
-            case kAction: {
-                const int a = t.player[nd], na = t.nchild[nd];
-                ActItem it{};
-                it.node = nd;
-                it.cslot = v.cslot;
-                it.rslot = v.rs[a];
-                it.oslot = v.rs[1 - a];
-                it.actor = (uint32_t)a;
-                it.na = (uint32_t)na;
-                it.cref = (uint32_t)P.crefs.size();
-                P.max_children = std::max<uint32_t>(P.max_children, (uint32_t)na);
-                int nkids = 0;
-                for (int k = 0; k < na; k++) {
-                    const uint32_t c = t.child(nd, k);
-                    if (is_terminal(t.kind[c]) && in_place(t.kind[c])) {
-                        uint32_t ti = term_of(c, v.dealt, v.ndealt);
-                        // With folds in place but showdowns not (the staged and warp
-                        // engines), a fold child still gets the actor's reach slot: the
-                        // down sweep, which has the actor's strategy at hand, writes the
-                        // folding player's reach there, and the parent's up kernel reads
-                        // it instead of recomputing that strategy.
-                        const uint32_t frs = (t.kind[c] == kFold && !fused) ? (uint32_t)next_r[a]++ : kNoSlot;
-                        P.crefs.push_back({t.kind[c] == kFold ? kChildFold : kChildShow, kNoSlot, frs, ti});
-                        it.nterm++;
-                        continue;
-                    }
-                    Visit cv = v;
-                    cv.node = c;
-                    cv.level = v.level + 1;
-                    cv.cslot = (uint32_t)next_c++;
-                    cv.rs[a] = (uint32_t)next_r[a]++;
-                    P.crefs.push_back({kChildNode, cv.cslot, cv.rs[a], kNoSlot});
-                    kids[nkids++] = cv;
+    root.run({0, 0, {0, 0}, 0, 0, {0, 0}, full_board ? root.river_slot(nullptr, 0) : kNoSlot});
+    std::vector<std::unique_ptr<Builder>> subs;
+    for (size_t i = 0; i < root.tasks.size(); i++)
+        subs.push_back(std::make_unique<Builder>(sp, P, visited, fused, P.fuse_folds, false));
+    {
+        std::atomic<size_t> next{0};
+        std::exception_ptr err;
+        std::mutex mu;
+        auto work = [&] {
+            for (size_t i; (i = next.fetch_add(1)) < subs.size();) {
+                try {
+                    subs[i]->run(root.tasks[i]);
+                } catch (...) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    if (!err) err = std::current_exception();
                 }
-                act_l[v.level].push_back({nd, it});
-                for (int k = nkids - 1; k >= 0; k--) stack.push_back(kids[k]);
-                break;
             }
-            case kChance: {
-                std::vector<int> valid = P.iso_active ? sp.perms_fixing(v.dealt, v.ndealt) : std::vector<int>{0};
-                struct CardRep { uint8_t card, rep; uint32_t perm; };
-                std::vector<CardRep> cr;
-                for (int c = 0; c < 52; c++) {
-                    uint32_t ch = t.children[t.child_start[nd] + c];
-                    bool dealt = false;
-                    for (int i = 0; i < v.ndealt; i++) dealt = dealt || v.dealt[i] == c;
-                    if (ch == kSentinel || dealt) continue;
-                    uint8_t rep = (uint8_t)c;
-                    uint32_t krep = 0;
-                    for (int k : valid) {
-                        uint8_t pc = card_permute((uint8_t)c, sp.perms[k]);
-                        if (pc < rep) { rep = pc; krep = (uint32_t)k; }
-                    }
-                    cr.push_back({(uint8_t)c, rep, krep});
-                }
-                uint32_t rep_cslot[52], rep_term[52];
-                ChanceItem ci{};
-                ci.cslot = v.cslot;
-                ci.inv = 1.0f / (float)(46 - (int)t.street[nd]);
-                ci.rs[0] = v.rs[0];
-                ci.rs[1] = v.rs[1];
-                int nkids = 0;
-                for (auto& x : cr) {
-                    if (x.card != x.rep) continue;
-                    const uint32_t c = t.children[t.child_start[nd] + x.card];
-                    uint8_t d2[2] = {v.ndealt > 0 ? v.dealt[0] : (uint8_t)0, 0};
-                    d2[v.ndealt] = x.card;
-                    if (fused && t.kind[c] == kShowdown) {
-                        rep_term[x.card] = term_of(c, d2, v.ndealt + 1);
-                        rep_cslot[x.card] = kNoSlot;
-                        continue;
-                    }
-                    Visit cv = v;
-                    cv.node = c;
-                    cv.level = v.level + 1;
-                    cv.dealt[0] = d2[0];
-                    cv.dealt[1] = d2[1];
-                    cv.ndealt = v.ndealt + 1;
-                    cv.slot = sp.board.size() + (size_t)cv.ndealt == 5 ? river_slot(cv.dealt, cv.ndealt) : kNoSlot;
-                    cv.cslot = (uint32_t)next_c++;
-                    cv.rs[0] = (uint32_t)next_r[0]++;
-                    cv.rs[1] = (uint32_t)next_r[1]++;
-                    rep_cslot[x.card] = cv.cslot;
-                    rep_term[x.card] = kNoSlot;
-                    EdgeItem e{{v.rs[0], v.rs[1]}, {cv.rs[0], cv.rs[1]}, x.card, 0};
-                    edge_l[v.level].push_back({c, e});
-                    kids[nkids++] = cv;
-                }
-                ci.cc_start = (uint32_t)P.cards.size();
-                ci.cc_count = (uint32_t)cr.size();
-                for (auto& x : cr) {
-                    // low byte: the dealt card; second byte: its orbit representative
-                    P.cards.push_back({(uint32_t)x.card | ((uint32_t)x.rep << 8), rep_cslot[x.rep], x.perm, rep_term[x.rep]});
-                    if (rep_term[x.rep] != kNoSlot) ci.nterm++;
-                }
-                chance_l[v.level].push_back({nd, ci});
-                for (int k = nkids - 1; k >= 0; k--) stack.push_back(kids[k]);
-                break;
+        };
+        const unsigned hw = std::thread::hardware_concurrency();
+        const size_t nw = std::min<size_t>(subs.size(), std::max(1u, std::min(16u, hw ? hw : 1u)));
+        std::vector<std::thread> ts;
+        for (size_t w = 1; w < nw; w++) ts.emplace_back(work);
+        work();
+        for (auto& th : ts) th.join();
+        if (err) std::rethrow_exception(err);
+    }
+    // merge: river slots in first-visit order, then each subtree's ids offset
+    // by what the builders before it handed out
+    P.slot_key = root.slot_key;
+    std::unordered_map<size_t, uint32_t> slot_of_key;
+    for (size_t k = 0; k < root.slot_key.size(); k++) slot_of_key[root.slot_key[k]] = (uint32_t)k;
+    struct Bases { uint32_t c, r[2], cref, term, card; std::vector<uint32_t> slot; };
+    std::vector<Bases> bases(subs.size());
+    uint64_t nc = root.next_c, nr[2] = {root.next_r[0], root.next_r[1]};
+    size_t ncref = root.crefs.size(), nterm = root.terms.size(), ncard = root.cards.size();
+    for (size_t i = 0; i < subs.size(); i++) {
+        Builder& b = *subs[i];
+        Bases& B = bases[i];
+        B.c = (uint32_t)nc;
+        B.r[0] = (uint32_t)nr[0];
+        B.r[1] = (uint32_t)nr[1];
+        B.cref = (uint32_t)ncref;
+        B.term = (uint32_t)nterm;
+        B.card = (uint32_t)ncard;
+        nc += b.next_c - kLocal;
+        nr[0] += b.next_r[0] - kLocal;
+        nr[1] += b.next_r[1] - kLocal;
+        ncref += b.crefs.size();
+        nterm += b.terms.size();
+        ncard += b.cards.size();
+        for (uint32_t key : b.slot_key) {
+            auto it = slot_of_key.find(key);
+            if (it == slot_of_key.end()) {
+                it = slot_of_key.emplace(key, (uint32_t)P.slot_key.size()).first;
+                P.slot_key.push_back(key);
             }
-            case kFold: {
-                FoldItem f{v.cslot, {v.rs[0], v.rs[1]}, t.player[nd], (float)t.twin[nd], (float)t.tlose[nd]};
-                fold_l[v.level].push_back({nd, f});
-                P.visited_terminals++;
-                break;
-            }
-            default: {
-                ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, v.slot != kNoSlot ? v.slot : river_slot(v.dealt, v.ndealt),
-                            (float)t.twin[nd], (float)t.tlose[nd], (float)t.ttie[nd], 0};
-                show_l[v.level].push_back({nd, si});
-                P.visited_terminals++;
-                break;
-            }
+            B.slot.push_back(it->second);
         }
     }
-    P.n_cslots = next_c;
-    P.n_rslots[0] = next_r[0];
-    P.n_rslots[1] = next_r[1];
-    P.num_levels = (int)act_l.size();
+    if (nc >= kLocal || nr[0] >= kLocal || nr[1] >= kLocal) throw Error("tree too large for the plan's slot ids");
+    std::vector<Builder*> bs{&root};
+    for (auto& b : subs) bs.push_back(b.get());
+    bases.insert(bases.begin(), Bases{0, {0, 0}, 0, 0, 0, {}});  // the root's ids are final
+    size_t levels = 0;
+    for (Builder* b : bs) levels = std::max(levels, b->edge_l.size());
+    P.num_levels = (int)levels;
+    auto layout_of = [&](auto member, int groups) {
+        using L = std::remove_reference_t<decltype(member(*bs[0], 0))>;
+        std::vector<std::vector<const L*>> lists(bs.size());
+        for (size_t b = 0; b < bs.size(); b++)
+            for (int g = 0; g < groups; g++) lists[b].push_back(&member(*bs[b], g));
+        return flat_layout<typename L::value_type::value_type::second_type>(levels, lists);
+    };
+    const FlatLayout La = layout_of([](Builder& b, int g) -> Levels<ActItem>& { return b.act_l[g]; }, 2);
+    const FlatLayout Le = layout_of([](Builder& b, int) -> Levels<EdgeItem>& { return b.edge_l; }, 1);
+    const FlatLayout Lf = layout_of([](Builder& b, int) -> Levels<FoldItem>& { return b.fold_l; }, 1);
+    const FlatLayout Ls = layout_of([](Builder& b, int) -> Levels<ShowItem>& { return b.show_l; }, 1);
+    const FlatLayout Lc = layout_of([](Builder& b, int) -> Levels<ChanceItem>& { return b.chance_l; }, 1);
+    P.act.resize(La.total);
+    P.edge.resize(Le.total);
+    P.fold.resize(Lf.total);
+    P.show.resize(Ls.total);
+    P.chance.resize(Lc.total);
+    P.act_span = La.span;
+    P.act_span_actor[0] = La.gspan[0];
+    P.act_span_actor[1] = La.gspan[1];
+    P.edge_span = Le.span;
+    P.fold_span = Lf.span;
+    P.show_span = Ls.span;
+    P.chance_span = Lc.span;
+    P.crefs.resize(ncref);
+    P.terms.resize(nterm);
+    P.cards.resize(ncard);
+    // each builder: its ids offset, then its lists copied into place
+    parallel_for(bs.size(), [&](size_t i) {
+        Builder& b = *bs[i];
+        const Bases& B = bases[i];
+        auto rc = [&](uint32_t& x) { if (is_local(x)) x = B.c + (x - kLocal); };
+        auto rr = [&](uint32_t& x, int q) { if (is_local(x)) x = B.r[q] + (x - kLocal); };
+        auto rs = [&](uint32_t& x) { if (is_local(x)) x = B.slot[x - kLocal]; };
+        for (int q = 0; q < 2; q++)
+            for (auto& lv : b.act_l[q])
+                for (auto& x : lv) {
+                    ActItem& a = x.second;
+                    for (uint32_t j = a.cref; j < a.cref + a.na; j++) {
+                        ChildRef& cr = b.crefs[j];
+                        rc(cr.cslot);
+                        rr(cr.rslot, q);
+                        if (cr.term != kNoSlot) cr.term += B.term;
+                    }
+                    rc(a.cslot);
+                    rr(a.rslot, q);
+                    rr(a.oslot, 1 - q);
+                    a.cref += B.cref;
+                }
+        for (auto& lv : b.edge_l)
+            for (auto& x : lv)
+                for (int q = 0; q < 2; q++) {
+                    rr(x.second.prs[q], q);
+                    rr(x.second.crs[q], q);
+                }
+        for (auto& lv : b.fold_l)
+            for (auto& x : lv) {
+                rc(x.second.cslot);
+                for (int q = 0; q < 2; q++) rr(x.second.rs[q], q);
+            }
+        for (auto& lv : b.show_l)
+            for (auto& x : lv) {
+                rc(x.second.cslot);
+                for (int q = 0; q < 2; q++) rr(x.second.rs[q], q);
+                rs(x.second.slot);
+            }
+        for (auto& lv : b.chance_l)
+            for (auto& x : lv) {
+                rc(x.second.cslot);
+                for (int q = 0; q < 2; q++) rr(x.second.rs[q], q);
+                x.second.cc_start += B.card;
+            }
+        for (auto& ce : b.cards) {
+            rc(ce.child_cslot);
+            if (ce.term != kNoSlot) ce.term += B.term;
+        }
+        for (auto& ti : b.terms) rs(ti.aux);  // a showdown's slot; a fold's folding player stays
+        for (uint32_t nd : b.nodes) {
+            rc(P.node_cslot[nd]);
+            rr(P.node_rs[0][nd], 0);
+            rr(P.node_rs[1][nd], 1);
+        }
+        std::copy(b.crefs.begin(), b.crefs.end(), P.crefs.begin() + B.cref);
+        std::copy(b.terms.begin(), b.terms.end(), P.terms.begin() + B.term);
+        std::copy(b.cards.begin(), b.cards.end(), P.cards.begin() + B.card);
+        std::vector<ChildRef>().swap(b.crefs);
+        std::vector<TermInfo>().swap(b.terms);
+        std::vector<CardEntry>().swap(b.cards);
+        for (int q = 0; q < 2; q++) flat_copy(La, i, q, b.act_l[q], P.act);
+        flat_copy(Le, i, 0, b.edge_l, P.edge);
+        flat_copy(Lf, i, 0, b.fold_l, P.fold);
+        flat_copy(Ls, i, 0, b.show_l, P.show);
+        flat_copy(Lc, i, 0, b.chance_l, P.chance);
+    });
+    for (Builder* b : bs) {
+        P.num_visited += b->num_visited;
+        P.visited_terminals += b->visited_terminals;
+        P.max_children = std::max(P.max_children, b->max_children);
+    }
+    P.n_cslots = nc;
+    P.n_rslots[0] = nr[0];
+    P.n_rslots[1] = nr[1];
 
     // device arena layout: visited action nodes of each player in node order
     P.node_sidx.assign(n, -1);
@@ -241,26 +473,13 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
         P.arena_len[a] += (len + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
         P.visited_action_elems[a] += len;
     }
-    for (auto& lst : act_l)
-        for (auto& x : lst) {
-            int a = (int)x.second.actor;
-            x.second.sidx = (uint32_t)P.node_sidx[x.first];
-            x.second.aoff = P.anode_off[a][x.second.sidx];
+    parallel_for((P.act.size() + 65535) / 65536, [&](size_t c) {
+        for (size_t k = c * 65536; k < std::min(P.act.size(), (c + 1) * 65536); k++) {
+            ActItem& x = P.act[k];
+            x.sidx = (uint32_t)P.node_sidx[x.node];
+            x.aoff = P.anode_off[x.actor][x.sidx];
         }
-    flatten(act_l, P.act, P.act_span);
-    // within a level, player 0's nodes first: a down sweep that only has to
-    // refresh one player's reach launches over that player's sub-span
-    for (size_t l = 0; l < P.act_span.size(); l++) {
-        const Span s = P.act_span[l];
-        auto first = P.act.begin() + s.start;
-        auto mid = std::stable_partition(first, first + s.count, [](const ActItem& x) { return x.actor == 0; });
-        const uint32_t n0 = (uint32_t)(mid - first);
-        P.act_span_actor[0].push_back({s.start, n0});
-        P.act_span_actor[1].push_back({s.start + n0, s.count - n0});
-    }
-    flatten(edge_l, P.edge, P.edge_span);
-    flatten(fold_l, P.fold, P.fold_span);
-    flatten(show_l, P.show, P.show_span);
+    });
     // showdowns of a level sorted by river slot and cut into batches of at
     // most kShowBatch with one slot each: a batch's CTA loads the slot's
     // tables once for all of them
@@ -285,7 +504,6 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
         }
         P.show_batch_span.push_back({b0, (uint32_t)P.show_batch.size() - b0});
     }
-    flatten(chance_l, P.chance, P.chance_span);
 
     // per-hand card lists (fold evaluator: hands of player q holding card c)
     for (int q = 0; q < 2; q++) {

@@ -14,6 +14,13 @@
 //   * each action node's arena block is hand-major ([hand * na + action]) and
 //     starts on a 16-element boundary (32 B for 16-bit arenas, 64 B for f32).
 #pragma once
+#include <algorithm>
+#include <atomic>
+#include <exception>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
 #include <cstdint>
 #include <vector>
 
@@ -96,6 +103,52 @@ struct alignas(16) RankEntry {  // 16-byte aligned: one vector load on the devic
 };
 
 struct Span { uint32_t start, count; };
+
+// Vectors of plain records whose resize does not zero them: the plan's flat
+// tables are written in parallel right after they are sized, so the first
+// touch of their pages happens on the worker threads.
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInitAlloc<U>;
+    };
+    NoInitAlloc() = default;
+    template <class U>
+    NoInitAlloc(const NoInitAlloc<U>&) noexcept {}
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        if constexpr (sizeof...(A) == 0) ::new ((void*)p) U;
+        else ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using PodVec = std::vector<T, NoInitAlloc<T>>;
+
+// f(i) for i < n on up to 16 host threads (the first exception is rethrown).
+template <class F>
+void parallel_for(size_t n, F f) {
+    std::atomic<size_t> next{0};
+    std::exception_ptr err;
+    std::mutex mu;
+    auto work = [&] {
+        for (size_t i; (i = next.fetch_add(1)) < n;) {
+            try {
+                f(i);
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!err) err = std::current_exception();
+            }
+        }
+    };
+    const unsigned hw = std::thread::hardware_concurrency();
+    const size_t nw = std::min<size_t>(n, std::max(1u, std::min(16u, hw ? hw : 1u)));
+    std::vector<std::thread> ts;
+    for (size_t w = 1; w < nw; w++) ts.emplace_back(work);
+    work();
+    for (auto& th : ts) th.join();
+    if (err) std::rethrow_exception(err);
+}
 constexpr int kShowBatch = 16;  // showdowns of one river slot evaluated by one CTA
 struct ShowBatch {
     uint32_t start, count;  // a run of Plan::show (one level, one slot)
@@ -114,22 +167,22 @@ struct Plan {
     int nh_max = 0;
     bool iso_active = false;
     uint64_t num_visited = 0;
-    std::vector<ActItem> act;
+    PodVec<ActItem> act;
     std::vector<Span> act_span;
     std::vector<Span> act_span_actor[2];  // per level: the sub-span of each actor's nodes
-    std::vector<EdgeItem> edge;
+    PodVec<EdgeItem> edge;
     std::vector<Span> edge_span;
-    std::vector<FoldItem> fold;
+    PodVec<FoldItem> fold;
     std::vector<Span> fold_span;
-    std::vector<ShowItem> show;
+    PodVec<ShowItem> show;
     std::vector<Span> show_span;
     std::vector<ShowBatch> show_batch;      // per level, runs of same-slot showdowns
     std::vector<Span> show_batch_span;
-    std::vector<ChanceItem> chance;
+    PodVec<ChanceItem> chance;
     std::vector<Span> chance_span;
-    std::vector<CardEntry> cards;
-    std::vector<ChildRef> crefs;
-    std::vector<TermInfo> terms;
+    PodVec<CardEntry> cards;
+    PodVec<ChildRef> crefs;
+    PodVec<TermInfo> terms;
     uint32_t max_children = 0;  // over action nodes
     uint64_t n_cslots = 0;
     uint64_t n_rslots[2] = {0, 0};

@@ -49,8 +49,9 @@ const char* const kKernelNames[7] = {"copy_root", "down_action", "down_chance", 
     } while (0)
 
 static thread_local uint64_t g_uploaded = 0;  // host-to-device bytes of the engine being built
-template <class T>
-static T* dupload(const std::vector<T>& v, std::vector<void*>& owned, size_t* bytes) {
+template <class V>
+static typename V::value_type* dupload(const V& v, std::vector<void*>& owned, size_t* bytes) {
+    using T = typename V::value_type;
     T* p = nullptr;
     const size_t n = std::max<size_t>(v.size(), 1);
     CK(cudaMalloc(&p, n * sizeof(T)));
@@ -578,8 +579,9 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     if (E.warp) E.warp_smem = (size_t)kWarps * d.nh_pad * sizeof(float);
     if (E.staged) {
         // node records, packed hand words, fixed-stride card lists
-        std::vector<SNode> sn(P.act.size());
-        for (size_t k = 0; k < P.act.size(); k++) {
+        PodVec<SNode> sn(P.act.size());
+        parallel_for((P.act.size() + 65535) / 65536, [&](size_t chunk) {
+          for (size_t k = chunk * 65536; k < std::min(P.act.size(), (chunk + 1) * 65536); k++) {
             const ActItem& a = P.act[k];
             SNode& x = sn[k];
             std::memset(&x, 0, sizeof(x));
@@ -606,7 +608,8 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
                     x.tlose = t.tlose;
                 }
             }
-        }
+          }
+        });
         E.snodes = dupload(sn, O, &B);
         for (int q = 0; q < 2; q++) {
             const Hands& h = sp.hands[q];
