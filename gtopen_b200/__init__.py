@@ -132,7 +132,7 @@ def lib():
         "gtob_gpu_runouts": (I, [P, P, P, I, C.POINTER(RunoutRow), P, I, I, C.POINTER(I), C.POINTER(I), C.POINTER(I),
                                  C.POINTER(D)]),
         "gtob_gpu_exploit_values": (I, [P, P, P, I, I, C.POINTER(NodeInfo)] + [P] * 8),
-        "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, C.POINTER(P)]),
+        "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, I, C.POINTER(P)]),
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
         "gtob_batch_size": (I, [P]),
         "gtob_batch_row_get": (I, [P, I, C.POINTER(BatchRow)]),
@@ -566,13 +566,14 @@ class Batch:
     solve_cli.rs:125-215, with the spots side by side): see gtob_batch_* in
     include/gtob.h."""
 
-    def __init__(self, spots, storage="f32", algo="dcfr", use_iso=True, device_format=None, engine="staged"):
+    def __init__(self, spots, storage="f32", algo="dcfr", use_iso=True, device_format=None, engine="staged",
+                 keep_solvers=True):
         self.spots = list(spots)
         arr = (C.c_void_p * len(self.spots))(*[sp._h for sp in self.spots])
         eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}[engine]
         h = C.c_void_p()
         _check(lib().gtob_batch_new(arr, len(self.spots), STORAGE[storage], ALGO[algo], int(use_iso),
-                                    DEVICE_FORMAT[device_format], eng, C.byref(h)))
+                                    DEVICE_FORMAT[device_format], eng, int(bool(keep_solvers)), C.byref(h)))
         self._h = h
         self.storage = storage
 
@@ -598,7 +599,7 @@ class Batch:
         """The i-th host solver (owned by the batch, synced after run)."""
         h = lib().gtob_batch_solver(self._h, int(i))
         if not h:
-            raise IndexError(i)
+            raise IndexError("no solver %d (out of range, or the batch keeps none)" % i)
         sv = Solver(self.spots[i], storage=self.storage, _handle=C.c_void_p(h))
         sv._owner = self
         return sv

@@ -30,8 +30,8 @@ std::vector<double> valid_opp_sum(const Spot& spot, int p, const float* reach_o)
     return out;
 }
 
-static void solve_one(HostSolver& host, int device_format, int engine, uint32_t max_iterations, double target_pct,
-                      uint32_t check_every, BatchRow& row) {
+static void solve_one(HostSolver& host, bool sync, int device_format, int engine, uint32_t max_iterations,
+                      double target_pct, uint32_t check_every, BatchRow& row) {
     const auto t0 = std::chrono::steady_clock::now();
     const Spot& sp = *host.spot;
     const double pot = sp.config.tree.starting_pot;
@@ -63,15 +63,17 @@ static void solve_one(HostSolver& host, int device_format, int engine, uint32_t 
         }
         row.ev[p] = n / d;
     }
-    eng.sync_to_cpu(host, false);
+    if (sync) eng.sync_to_cpu(host, false);
     row.iterations = eng.iteration();
     row.exploit_pct = pct;
     row.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }
 
-void run_batch(const std::vector<HostSolver*>& solvers, int device_format, int engine, uint32_t max_iterations,
-               double target_pct, uint32_t check_every, int workers, std::vector<BatchRow>& rows) {
+void run_batch(const std::vector<std::shared_ptr<Spot>>& spots, const std::vector<HostSolver*>& solvers, int storage,
+               int algo, bool use_iso, int device_format, int engine, uint32_t max_iterations, double target_pct,
+               uint32_t check_every, int workers, std::vector<BatchRow>& rows) {
     if (check_every == 0) throw Error("invalid argument: check_every must be positive");
+    if (solvers.size() != spots.size()) throw Error("invalid argument: one solver slot per spot");
     rows.assign(solvers.size(), BatchRow{});
     int device = 0;
     const cudaError_t rc = cudaGetDevice(&device);
@@ -82,7 +84,12 @@ void run_batch(const std::vector<HostSolver*>& solvers, int device_format, int e
         for (size_t i; (i = next.fetch_add(1)) < solvers.size();) {
             try {
                 if (r != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(r));
-                solve_one(*solvers[i], device_format, engine, max_iterations, target_pct, check_every, rows[i]);
+                if (solvers[i]) {
+                    solve_one(*solvers[i], true, device_format, engine, max_iterations, target_pct, check_every, rows[i]);
+                } else {
+                    HostSolver shell(spots[i], storage, algo, use_iso, false);
+                    solve_one(shell, false, device_format, engine, max_iterations, target_pct, check_every, rows[i]);
+                }
             } catch (const std::exception& e) {
                 rows[i].error = e.what();
                 rows[i].error = rows[i].error.empty() ? "unknown error" : rows[i].error;

@@ -25,11 +25,15 @@ struct BatchRow {
 
 // Runs solve_quiet's loop (one iteration at a time, exploitability when the
 // iteration is a multiple of check_every or reaches max_iterations, stop at
-// target_pct or max_iterations, then sync_to_cpu) for every solver, with up to
-// `workers` spots in flight; rows[i] describes solvers[i].  Errors stay in
+// target_pct or max_iterations) for every spot, with up to `workers` spots in
+// flight; rows[i] describes spots[i].  A spot with a host solver in
+// solvers[i] is synced back into it; one without (nullptr) is solved against a
+// host solver that holds no arenas, built and dropped by its worker, so the
+// batch's host memory stays bounded by the spots in flight.  Errors stay in
 // their row.  Must be called with the target device current.
-void run_batch(const std::vector<HostSolver*>& solvers, int device_format, int engine, uint32_t max_iterations,
-               double target_pct, uint32_t check_every, int workers, std::vector<BatchRow>& rows);
+void run_batch(const std::vector<std::shared_ptr<Spot>>& spots, const std::vector<HostSolver*>& solvers, int storage,
+               int algo, bool use_iso, int device_format, int engine, uint32_t max_iterations, double target_pct,
+               uint32_t check_every, int workers, std::vector<BatchRow>& rows);
 
 // Per-hand compatible opponent reach mass (query.rs:463-488), f64.
 std::vector<double> valid_opp_sum(const Spot& spot, int p, const float* reach_o);

@@ -332,11 +332,13 @@ int gtob_gpu_exploit_values(gtob_gpu* g, const gtob_solver* v, const int* steps,
     API_END
 }
 struct gtob_batch {
-    std::vector<std::unique_ptr<gtob_solver>> solvers;
+    std::vector<std::shared_ptr<Spot>> spots;
+    std::vector<std::unique_ptr<gtob_solver>> solvers;  // empty entries when the batch keeps none
     std::vector<BatchRow> rows;
-    int fmt = -1, engine = GTOB_ENGINE_STAGED;
+    int storage = 0, algo = 0, fmt = -1, engine = GTOB_ENGINE_STAGED;
+    bool use_iso = true;
 };
-int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int use_iso, int fmt, int engine,
+int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int use_iso, int fmt, int engine, int keep,
                    gtob_batch** out) {
     REQUIRE(spots && out && n > 0 && (storage == 0 || storage == 1) && algo >= 0 && algo <= 2 && fmt >= -1 &&
             fmt <= 2 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
@@ -344,10 +346,16 @@ int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int us
     for (int i = 0; i < n; i++) REQUIRE(spots[i]);
     API_BEGIN
     auto b = std::make_unique<gtob_batch>();
-    for (int i = 0; i < n; i++)
-        b->solvers.push_back(std::make_unique<gtob_solver>(
-            gtob_solver{std::make_unique<HostSolver>(spots[i]->s, storage, algo, use_iso != 0)}));
+    for (int i = 0; i < n; i++) {
+        b->spots.push_back(spots[i]->s);
+        b->solvers.push_back(keep ? std::make_unique<gtob_solver>(gtob_solver{
+                                        std::make_unique<HostSolver>(spots[i]->s, storage, algo, use_iso != 0)})
+                                  : nullptr);
+    }
     b->rows.resize(n);
+    b->storage = storage;
+    b->algo = algo;
+    b->use_iso = use_iso != 0;
     b->fmt = fmt;
     b->engine = engine;
     *out = b.release();
@@ -357,8 +365,9 @@ int gtob_batch_run(gtob_batch* b, uint32_t max_iterations, double target_pct, ui
     REQUIRE(b && check_every > 0 && workers > 0);
     API_BEGIN
     std::vector<HostSolver*> hs;
-    for (auto& v : b->solvers) hs.push_back(v->v.get());
-    run_batch(hs, b->fmt, b->engine, max_iterations, target_pct, check_every, workers, b->rows);
+    for (auto& v : b->solvers) hs.push_back(v ? v->v.get() : nullptr);
+    run_batch(b->spots, hs, b->storage, b->algo, b->use_iso, b->fmt, b->engine, max_iterations, target_pct,
+              check_every, workers, b->rows);
     API_END
 }
 int gtob_batch_size(const gtob_batch* b) { return b ? (int)b->solvers.size() : 0; }
@@ -378,7 +387,7 @@ const char* gtob_batch_error(const gtob_batch* b, int i) {
     return b->rows[i].error.c_str();
 }
 gtob_solver* gtob_batch_solver(gtob_batch* b, int i) {
-    if (!b || i < 0 || i >= (int)b->solvers.size()) return nullptr;
+    if (!b || i < 0 || i >= (int)b->solvers.size() || !b->solvers[i]) return nullptr;
     return b->solvers[i].get();
 }
 void gtob_batch_free(gtob_batch* b) { delete b; }

@@ -295,28 +295,10 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
     std::vector<std::unique_ptr<Builder>> subs;
     for (size_t i = 0; i < root.tasks.size(); i++)
         subs.push_back(std::make_unique<Builder>(sp, P, visited, fused, P.fuse_folds, false));
-    {
-        std::atomic<size_t> next{0};
-        std::exception_ptr err;
-        std::mutex mu;
-        auto work = [&] {
-            for (size_t i; (i = next.fetch_add(1)) < subs.size();) {
-                try {
-                    subs[i]->run(root.tasks[i]);
-                } catch (...) {
-                    std::lock_guard<std::mutex> lk(mu);
-                    if (!err) err = std::current_exception();
-                }
-            }
-        };
-        const unsigned hw = std::thread::hardware_concurrency();
-        const size_t nw = std::min<size_t>(subs.size(), std::max(1u, std::min(16u, hw ? hw : 1u)));
-        std::vector<std::thread> ts;
-        for (size_t w = 1; w < nw; w++) ts.emplace_back(work);
-        work();
-        for (auto& th : ts) th.join();
-        if (err) std::rethrow_exception(err);
-    }
+    // small trees (a few hundred thousand nodes) build faster on one thread,
+    // and a batch builds several at once
+    const unsigned threads = n >= (size_t(1) << 20) ? 16u : 1u;
+    parallel_for(subs.size(), [&](size_t i) { subs[i]->run(root.tasks[i]); }, threads);
     // merge: river slots in first-visit order, then each subtree's ids offset
     // by what the builders before it handed out
     P.slot_key = root.slot_key;
@@ -450,7 +432,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
         flat_copy(Lf, i, 0, b.fold_l, P.fold);
         flat_copy(Ls, i, 0, b.show_l, P.show);
         flat_copy(Lc, i, 0, b.chance_l, P.chance);
-    });
+    }, threads);
     for (Builder* b : bs) {
         P.num_visited += b->num_visited;
         P.visited_terminals += b->visited_terminals;
@@ -479,7 +461,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
             x.sidx = (uint32_t)P.node_sidx[x.node];
             x.aoff = P.anode_off[x.actor][x.sidx];
         }
-    });
+    }, threads);
     // showdowns of a level sorted by river slot and cut into batches of at
     // most kShowBatch with one slot each: a batch's CTA loads the slot's
     // tables once for all of them

@@ -125,9 +125,10 @@ struct NoInitAlloc : std::allocator<T> {
 template <class T>
 using PodVec = std::vector<T, NoInitAlloc<T>>;
 
-// f(i) for i < n on up to 16 host threads (the first exception is rethrown).
+// f(i) for i < n on up to max_threads (at most 16) host threads; the first
+// exception is rethrown.
 template <class F>
-void parallel_for(size_t n, F f) {
+void parallel_for(size_t n, F f, unsigned max_threads = 16) {
     std::atomic<size_t> next{0};
     std::exception_ptr err;
     std::mutex mu;
@@ -142,7 +143,7 @@ void parallel_for(size_t n, F f) {
         }
     };
     const unsigned hw = std::thread::hardware_concurrency();
-    const size_t nw = std::min<size_t>(n, std::max(1u, std::min(16u, hw ? hw : 1u)));
+    const size_t nw = std::min<size_t>(n, std::max(1u, std::min({16u, max_threads, hw ? hw : 1u})));
     std::vector<std::thread> ts;
     for (size_t w = 1; w < nw; w++) ts.emplace_back(work);
     work();

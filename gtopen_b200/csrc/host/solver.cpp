@@ -71,9 +71,10 @@ void Arena::write(uint32_t node, uint64_t off, size_t n, const float* src) {
 }
 
 // --------------------------------------------------------------- HostSolver
-HostSolver::HostSolver(std::shared_ptr<Spot> s, int storage_mode, int algorithm, bool iso)
+HostSolver::HostSolver(std::shared_ptr<Spot> s, int storage_mode, int algorithm, bool iso, bool with_arenas)
     : spot(std::move(s)), storage(storage_mode), algo(algorithm), use_iso(iso) {
     const size_t nn = spot->tree.size();
+    if (!with_arenas) return;
     for (int p = 0; p < 2; p++) {
         regrets[p].init(storage == kStoreF32 ? 0 : 1, spot->tree.data_size[p], nn);
         strat[p].init(storage == kStoreF32 ? 0 : 2, spot->tree.data_size[p], nn);

@@ -57,7 +57,10 @@ struct HostSolver {
     // zeroed as well.
     bool arenas_zero = true;
 
-    HostSolver(std::shared_ptr<Spot> s, int storage_mode, int algorithm, bool iso);
+    // with_arenas = false: a solver that only describes the spot (algorithm,
+    // locks, iteration) for a GPU engine whose arenas never come back to the
+    // host -- nothing may read or sync its arenas.
+    HostSolver(std::shared_ptr<Spot> s, int storage_mode, int algorithm, bool iso, bool with_arenas = true);
     void ensure_preds();
     uint64_t arena_bytes() const;
     // whole-arena f32 image in the reference layout (action-major per node at data_offset)

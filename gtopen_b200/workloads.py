@@ -191,7 +191,8 @@ def flop_report_spots(evaluate7, build_many, n=184, seed=4, max_ratio=8.0):
     """Spots of the flop report: n canonical flops sampled without
     replacement (xorshift seed), per flop the turn config's range shape and a
     bet set of 1-3 sizes from {33,50,75,125,a}; while the largest tree
-    exceeds max_ratio x the smallest, the largest flop's bet set is redrawn.
+    exceeds max_ratio x the smallest, the bet set of whichever extreme lies
+    farther from the median is redrawn.
     build_many(list of configs) -> list of built spots (with num_nodes), so the
     caller can build them in parallel.  Returns (configs, spots)."""
     rng = XorShift(seed)
@@ -214,10 +215,12 @@ def flop_report_spots(evaluate7, build_many, n=184, seed=4, max_ratio=8.0):
                      "tree": tree_config(100, 300, bet_set(), ("2.5x",), 2)})
     spots = list(build_many(cfgs))
     for _ in range(10 * n):
-        sizes_ = [sp.num_nodes for sp in spots]
-        if max(sizes_) <= max_ratio * min(sizes_):
+        sizes_ = np.array([sp.num_nodes for sp in spots], np.float64)
+        if sizes_.max() <= max_ratio * sizes_.min():
             break
-        i = int(np.argmax(sizes_))
+        med = float(np.median(sizes_))
+        # redraw the extreme farther from the median (in ratio)
+        i = int(np.argmax(sizes_)) if sizes_.max() / med >= med / sizes_.min() else int(np.argmin(sizes_))
         cfgs[i]["tree"] = tree_config(100, 300, bet_set(), ("2.5x",), 2)
         spots[i] = build_many([cfgs[i]])[0]
     return cfgs, spots

@@ -267,8 +267,8 @@ int gtob_gpu_exploit_values(gtob_gpu* gpu, const gtob_solver* solver, const int*
  * reference: 20) or reaches max_iterations, stop at target_pct or
  * max_iterations -- read the root EVs, sync the solver back and free the
  * engine.  Engines of different workers run concurrently on the device.
- * gtob_batch_new creates one host solver per spot (storage, algo, use_iso as
- * gtob_solver_new); device_format / engine as gtob_gpu_new_ex.  Call
+ * storage, algo, use_iso as gtob_solver_new; device_format / engine as
+ * gtob_gpu_new_ex.  Call
  * gtob_batch_run with the device current; an error in one spot stays in its
  * row (status, gtob_batch_error) and the others go on. */
 typedef struct gtob_batch gtob_batch;
@@ -279,14 +279,19 @@ typedef struct {
     double seconds;      /* wall time of this spot: engine build, solve, EVs, sync */
     double ev[2];        /* reach-weighted root EV per player, pot-share convention (solve_cli.rs:176-188) */
 } gtob_batch_row;
+/* keep = 1: one host solver per spot, synced after its solve and returned
+ * by gtob_batch_solver; keep = 0: no solver is kept (each worker solves
+ * against a host solver without arenas and drops it), so host memory stays
+ * bounded by the spots in flight -- the report case. */
 int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int use_iso, int device_format, int engine,
-                   gtob_batch** out);
+                   int keep, gtob_batch** out);
 int gtob_batch_run(gtob_batch* batch, uint32_t max_iterations, double target_pct, uint32_t check_every, int workers);
 int gtob_batch_size(const gtob_batch* batch);
 int gtob_batch_row_get(const gtob_batch* batch, int i, gtob_batch_row* out);
 /* the message of a failed row ("" when the row solved) */
 const char* gtob_batch_error(const gtob_batch* batch, int i);
-/* the i-th host solver, owned by the batch (valid until gtob_batch_free) */
+/* the i-th host solver, owned by the batch (valid until gtob_batch_free);
+ * NULL when the batch keeps none */
 gtob_solver* gtob_batch_solver(gtob_batch* batch, int i);
 void gtob_batch_free(gtob_batch* batch);
 

@@ -94,3 +94,19 @@ def test_batch_keeps_failures_in_their_row():
     for i in (0, 2):
         assert rows[i]["status"] == 0 and rows[i]["iterations"] == 20, rows[i]
         assert np.isfinite(rows[i]["exploit_pct"])
+
+
+def test_batch_without_solvers_gives_the_same_rows():
+    """A batch that keeps no host solvers (the report mode: each worker solves
+    against a solver without arenas) reports the same rows."""
+    cfgs = _configs()
+    spots = [g.Spot(c) for c in cfgs]
+    kept = g.Batch(spots, storage="f32", use_iso=True)
+    kept.run(max_iterations=MAX_IT, target_pct=TARGET, check_every=CHECK, workers=2)
+    lean = g.Batch(spots, storage="f32", use_iso=True, keep_solvers=False)
+    lean.run(max_iterations=MAX_IT, target_pct=TARGET, check_every=CHECK, workers=3)
+    for a, b in zip(kept.rows(), lean.rows()):
+        assert (a["status"], a["iterations"], a["exploit_pct"], a["ev"]) == \
+               (b["status"], b["iterations"], b["exploit_pct"], b["ev"])
+    with pytest.raises(IndexError):
+        lean.solver(0)
