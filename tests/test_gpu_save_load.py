@@ -99,3 +99,30 @@ def test_device_save_refuses_another_spot(tmp_path):
         gpu.save(tmp_path / "x.gto", other)
     assert "not the one" in str(e.value)
     assert not os.path.exists(tmp_path / "x.gto")
+
+
+@pytest.mark.parametrize("device_format,algo", [("fp8", "dcfr"), ("f32", "pcfr+"), ("i16", "pcfr+")])
+def test_device_save_load_other_formats(tmp_path, device_format, algo):
+    """FP8 arenas and PCFR+ (whose predictions the format does not hold):
+    the device save equals the host path's file, and a device load equals a
+    host load + GpuSolver (predictions restart at zero in both)."""
+    cfg = W.small_flop_spot()
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, storage="f32", algo=algo, use_iso=False)
+    gpu = g.GpuSolver(host, device_format=device_format)
+    gpu.iterate(6)
+    pa, pb = tmp_path / "dev.gto", tmp_path / "host.gto"
+    gpu.save(pa, host)
+    gpu.sync_to_cpu(host)
+    host.ensure_symmetric()
+    host.save(pb)
+    assert pa.read_bytes() == pb.read_bytes()
+    h_host = g.Solver.load(pb, storage="f32")
+    ga = g.GpuSolver(h_host, device_format=device_format)
+    h_dev, gb = g.GpuSolver.load(pa, storage="f32", device_format=device_format)
+    for which in (0, 1):
+        for p in (0, 1):
+            assert np.array_equal(ga.export_arena(which, p), gb.export_arena(which, p)), (which, p)
+    ga.iterate(3)
+    gb.iterate(3)
+    assert ga.exploitability(h_host) == gb.exploitability(h_dev)
