@@ -152,6 +152,13 @@ def barrier(world):
 
 # --storage: compressed = i16/u16 host and device arenas (the reference CLI
 # default); f32; fp8 = f32 host arenas, FP8 E4M3 device arenas (precision study)
+# DRAM bytes (read + write) of one CFR iteration, summed over every launch of
+# one iteration in a one-pass ncu capture (dram__bytes_read.sum +
+# dram__bytes_write.sum); profiles/staged_engine_flop_iteration_traffic.md
+# has the command and the per-kernel split.  Only for the configuration
+# captured.
+MEASURED_TRAFFIC = {("flop", "compressed", "staged"): 233.65e9}
+
 HOST_STORAGE = {"compressed": "compressed", "f32": "f32", "fp8": "f32"}
 DEVICE_FORMAT = {"compressed": None, "f32": None, "fp8": "fp8"}
 DTYPE = {"compressed": "i16", "f32": "f32", "fp8": "fp8_e4m3"}
@@ -300,7 +307,7 @@ def run_ours(args, world, rank, local):
         "config": workload_config(args, cfg),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_kind": peak_kind + " (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-                     "traffic": None,
+                     "traffic": MEASURED_TRAFFIC.get((args.workload, args.storage, args.engine)),
                      "kernel": "one CFR iteration (CUDA graph of all sweep kernels); dominant kind %s (%.0f%%)"
                                % (g.KERNEL_NAMES[dominant], 100.0 * prof.ms[dominant] / tot),
                      "algorithmic_bytes_per_iter": info["iter_bytes"]},
