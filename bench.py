@@ -245,7 +245,7 @@ def run_ours(args, world, rank, local):
     peak, peak_kind = load_peak()
     achieved = info["iter_bytes"] / per_iter_s / 1e9
     prof = gpu.iterate_profiled()
-    launches_per_iter = 1 + sum(prof.launches)
+    launches_per_iter = gpu.info()["iteration_kernels"]  # kernel nodes of the iteration's CUDA graph
     kinds = {g.KERNEL_NAMES[k]: round(prof.ms[k], 3) for k in range(7)}
     tot = sum(prof.ms) or 1.0
     dominant = max(range(7), key=lambda k: prof.ms[k])

@@ -45,7 +45,8 @@ class GpuInfo(C.Structure):
     _fields_ = [("device_bytes", C.c_uint64), ("visited_nodes", C.c_uint64), ("cfv_slots", C.c_uint64),
                 ("reach_slots", C.c_uint64 * 2), ("device_action_nodes", C.c_uint64 * 2),
                 ("visited_terminals", C.c_uint64), ("num_levels", C.c_uint32), ("num_river_slots", C.c_uint32),
-                ("arena_format", C.c_int32), ("iter_bytes", C.c_double), ("upload_bytes", C.c_uint64)]
+                ("arena_format", C.c_int32), ("iter_bytes", C.c_double), ("upload_bytes", C.c_uint64),
+                ("iteration_kernels", C.c_uint32)]
 
 
 class NodeInfo(C.Structure):

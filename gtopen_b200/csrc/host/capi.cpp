@@ -483,7 +483,9 @@ int gtob_gpu_info_get(gtob_gpu* g, gtob_gpu_info* o) {
     o->arena_format = g->e->format();
     o->iter_bytes = g->e->iter_bytes();
     o->upload_bytes = g->e->upload_bytes();
-    return GTOB_OK;
+    API_BEGIN
+    o->iteration_kernels = g->e->iteration_kernels();  // captures the iteration graph if it is not yet
+    API_END
 }
 int gtob_gpu_root_cfv(gtob_gpu* g, int p, int mode, float* out) {
     REQUIRE(g && out && (p == 0 || p == 1) && (mode == 0 || mode == 1));

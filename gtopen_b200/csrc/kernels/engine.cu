@@ -479,11 +479,25 @@ struct EngineImpl {
             throw;
         }
         CK(cudaStreamEndCapture(stream, &g));
+        if (which < 0) {  // the kernels one iteration launches: the graph's kernel nodes
+            size_t nn = 0;
+            CK(cudaGraphGetNodes(g, nullptr, &nn));
+            std::vector<cudaGraphNode_t> nodes(nn);
+            if (nn) CK(cudaGraphGetNodes(g, nodes.data(), &nn));
+            uint32_t k = 0;
+            for (auto nd : nodes) {
+                cudaGraphNodeType ty;
+                CK(cudaGraphNodeGetType(nd, &ty));
+                k += ty == cudaGraphNodeTypeKernel;
+            }
+            iter_kernels = k;
+        }
         cudaGraphExec_t ex;
         CK(cudaGraphInstantiate(&ex, g, 0));
         cudaGraphDestroy(g);
         return ex;
     }
+    uint32_t iter_kernels = 0;  // kernel nodes of the captured iteration graph
 };
 
 // --------------------------------------------------------------- GpuEngine
@@ -723,6 +737,11 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
 
 GpuEngine::~GpuEngine() = default;
 uint64_t GpuEngine::upload_bytes() const { return d_->uploaded; }
+uint32_t GpuEngine::iteration_kernels() {
+    EngineImpl& E = *d_;
+    if (!E.g_iter) E.g_iter = E.capture(-1);
+    return E.iter_kernels;
+}
 
 void GpuEngine::iterate(int n) {
     EngineImpl& E = *d_;

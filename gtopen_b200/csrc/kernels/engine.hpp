@@ -52,6 +52,7 @@ class GpuEngine {
     // algorithmic bytes of one CFR iteration / one BR check (traffic model)
     double iter_bytes() const;
     uint64_t upload_bytes() const;  // host-to-device bytes the constructor copied
+    uint32_t iteration_kernels();   // kernels one iteration launches (the captured graph's kernel nodes)
     // device arena exports for tests (reference layout, decoded f32)
     void export_arena(int which, int p, float* out);
     // One action node's block (reference layout, f32) through a static device

@@ -83,6 +83,8 @@ typedef struct {
     int32_t arena_format;
     double iter_bytes; /* algorithmic bytes of one CFR iteration */
     uint64_t upload_bytes; /* host-to-device bytes copied by gtob_gpu_new (plan tables, arenas) */
+    uint32_t iteration_kernels; /* kernel launches of one iteration (kernel nodes of its CUDA graph;
+                                   reading it captures that graph if no iteration has run yet) */
 } gtob_gpu_info;
 
 /* Thread-local message of the last failed call (Result::Err text). */
