@@ -288,6 +288,13 @@ def run_ours(args, world, rank, local):
     ttt = None
     if args.ttt and rank == 0:
         ttt = time_to_target(g, cfg, args)
+    # time to 0.3% of the pot on the reference's own bench spot (bench_spot.json,
+    # 1.25M nodes; exploitability checked every 10 iterations on the GPU, as
+    # the reference CLI does), wall clock from GpuSolver::new
+    ttt_spot = None
+    if not args.no_spot_ttt and rank == 0:
+        ttt_spot = time_to_target(g, make_config("bench_spot"), args)
+        ttt_spot["spot"] = "reference bench_spot.json (Ks7h2d, 257 v 319 hands, 1,245,971 nodes)"
 
     if rank != 0:
         return
@@ -322,6 +329,8 @@ def run_ours(args, world, rank, local):
     }
     if ttt:
         line["time_to_target"] = ttt
+    if ttt_spot:
+        line["time_to_target_bench_spot"] = ttt_spot
     print(json.dumps(line), flush=True)
 
 
@@ -492,6 +501,7 @@ def main():
     ap.add_argument("--target", type=float, default=0.3)
     ap.add_argument("--check-every", type=int, default=10)
     ap.add_argument("--ttt-max", type=int, default=2000)
+    ap.add_argument("--no-spot-ttt", action="store_true", help="skip the time-to-target run on the bench spot")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
