@@ -134,6 +134,15 @@ def lib():
                                  C.POINTER(D)]),
         "gtob_gpu_exploit_values": (I, [P, P, P, I, I, C.POINTER(NodeInfo)] + [P] * 8),
         "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, I, C.POINTER(P)]),
+        "gtob_nccl_unique_id": (I, [P]),
+        "gtob_gpu_new_sharded": (I, [P, I, I, I, I, P, C.POINTER(P)]),
+        "gtob_shards_new": (I, [P, I, I, I, C.POINTER(P)]),
+        "gtob_shards_iterate": (I, [P, I]),
+        "gtob_shards_exploitability": (I, [P, P, C.POINTER(D)]),
+        "gtob_shards_export_arena": (I, [P, I, I, P]),
+        "gtob_shards_sync_to_cpu": (I, [P, P, I]),
+        "gtob_shards_free": (None, [P]),
+        "gtob_spot_shard_visited": (I, [P, I, I, I, P]),
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
         "gtob_batch_size": (I, [P]),
         "gtob_batch_row_get": (I, [P, I, C.POINTER(BatchRow)]),
@@ -560,6 +569,70 @@ class GpuSolver:
         ms = C.c_double()
         _check(lib().gtob_gpu_time_iterations(self._h, int(n), C.byref(ms)))
         return ms.value
+
+
+ENGINES = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}
+
+
+def nccl_unique_id():
+    """ncclGetUniqueId for rank 0 to share with the other ranks (bytes)."""
+    buf = (C.c_ubyte * 128)()
+    _check(lib().gtob_nccl_unique_id(buf))
+    return bytes(buf)
+
+
+def sharded_gpu_solver(solver, rank, world, nccl_id, device_format=None, engine="staged"):
+    """Shard `rank` of a spot split over `world` processes (one GPU each),
+    its top chance values summed over NCCL; every rank calls this together."""
+    buf = (C.c_ubyte * 128).from_buffer_copy(nccl_id)
+    h = C.c_void_p()
+    _check(lib().gtob_gpu_new_sharded(solver._h, DEVICE_FORMAT[device_format], ENGINES[engine], int(rank), int(world),
+                                      buf, C.byref(h)))
+    gpu = GpuSolver.__new__(GpuSolver)
+    gpu._h = h
+    gpu.solver = solver
+    return gpu
+
+
+class Shards:
+    """Every shard of one spot in this process on the current device, summing
+    the split subtrees' values on the host: the sharded computation on one GPU."""
+
+    def __init__(self, solver, nshards, device_format=None, engine="staged"):
+        h = C.c_void_p()
+        _check(lib().gtob_shards_new(solver._h, DEVICE_FORMAT[device_format], ENGINES[engine], int(nshards),
+                                     C.byref(h)))
+        self._h = h
+        self.solver = solver
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gtob_shards_free(self._h)
+            self._h = None
+
+    def iterate(self, n=1):
+        _check(lib().gtob_shards_iterate(self._h, int(n)))
+
+    def exploitability(self, solver=None):
+        v = C.c_double()
+        _check(lib().gtob_shards_exploitability(self._h, (solver or self.solver)._h, C.byref(v)))
+        return v.value
+
+    def export_arena(self, which, p):
+        out = np.zeros(self.solver.spot.data_size[p], np.float32)
+        _check(lib().gtob_shards_export_arena(self._h, int(which), int(p), _ptr(out)))
+        return out
+
+    def sync_to_cpu(self, solver=None, strategy_only=False):
+        """Every shard's nodes into one host solver (GpuSolver.sync_to_cpu per shard)."""
+        _check(lib().gtob_shards_sync_to_cpu(self._h, (solver or self.solver)._h, int(bool(strategy_only))))
+
+
+def shard_visited(spot, shard, nshards, use_iso=True):
+    """Nodes shard `shard` of `nshards` visits (the plan partition, no GPU)."""
+    out = np.zeros(spot.num_nodes, np.uint8)
+    _check(lib().gtob_spot_shard_visited(spot._h, int(use_iso), int(shard), int(nshards), _ptr(out)))
+    return out
 
 
 class Batch:

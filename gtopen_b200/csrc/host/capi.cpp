@@ -5,7 +5,9 @@
 
 #include <cuda_runtime.h>
 
+#include <cmath>
 #include <cstring>
+#include <thread>
 #include <fstream>
 #include <memory>
 #include <string>
@@ -14,6 +16,7 @@
 #include "batch.hpp"
 #include "core.hpp"
 #include "query.hpp"
+#include "shard.hpp"
 #include "solver.hpp"
 
 using namespace gtob;
@@ -21,6 +24,31 @@ using namespace gtob;
 struct gtob_spot { std::shared_ptr<Spot> s; };
 struct gtob_solver { std::unique_ptr<HostSolver> v; };
 struct gtob_gpu { std::unique_ptr<GpuEngine> e; };
+struct gtob_shards {
+    std::vector<std::unique_ptr<GpuEngine>> e;
+    int device = 0;
+    // runs f(shard) for every shard on its own thread (the host exchange
+    // needs them all at once); the first error is rethrown
+    template <class F>
+    void all(F f) {
+        std::vector<std::exception_ptr> errs(e.size());
+        std::vector<std::thread> ts;
+        for (size_t k = 0; k < e.size(); k++)
+            ts.emplace_back([&, k] {
+                try {
+                    const cudaError_t rc = cudaSetDevice(device);
+                    if (rc != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(rc));
+                    f((int)k);
+                } catch (...) {
+                    errs[k] = std::current_exception();
+                }
+            });
+        for (auto& t : ts) t.join();
+        for (auto& x : errs)
+            if (x) std::rethrow_exception(x);
+    }
+};
+
 
 static thread_local std::string g_err;
 
@@ -329,6 +357,85 @@ int gtob_gpu_exploit_values(gtob_gpu* g, const gtob_solver* v, const int* steps,
     put(br_strategy, x.br_strategy);
     put(action_ev, x.action_ev);
     if (averages) std::memcpy(averages, x.avg, sizeof(x.avg));
+    API_END
+}
+int gtob_nccl_unique_id(unsigned char out[128]) {
+    REQUIRE(out);
+    API_BEGIN
+    nccl_unique_id(out);
+    API_END
+}
+int gtob_gpu_new_sharded(const gtob_solver* v, int fmt, int engine, int rank, int world, const unsigned char id[128],
+                         gtob_gpu** out) {
+    REQUIRE(v && id && out && world >= 1 && rank >= 0 && rank < world && fmt >= -1 && fmt <= 2 &&
+            engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+    *out = nullptr;
+    API_BEGIN
+    auto red = make_nccl_reducer(rank, world, id);
+    *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt, engine, rank, world, red)};
+    API_END
+}
+int gtob_shards_new(const gtob_solver* v, int fmt, int engine, int nshards, gtob_shards** out) {
+    REQUIRE(v && out && nshards >= 1 && nshards <= 64 && fmt >= -1 && fmt <= 2 && engine >= GTOB_ENGINE_FUSED &&
+            engine <= GTOB_ENGINE_STAGED);
+    *out = nullptr;
+    API_BEGIN
+    auto g = std::make_unique<gtob_shards>();
+    const cudaError_t rc = cudaGetDevice(&g->device);
+    if (rc != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(rc));
+    auto x = std::make_shared<HostExchange>(nshards);
+    for (int k = 0; k < nshards; k++)
+        g->e.push_back(std::make_unique<GpuEngine>(*v->v, fmt, engine, k, nshards, make_host_reducer(x, k)));
+    *out = g.release();
+    API_END
+}
+int gtob_shards_iterate(gtob_shards* g, int n) {
+    REQUIRE(g && n >= 0);
+    API_BEGIN
+    g->all([&](int k) { g->e[k]->iterate(n); g->e[k]->synchronize(); });
+    API_END
+}
+int gtob_shards_exploitability(gtob_shards* g, const gtob_solver* v, double* chips) {
+    REQUIRE(g && v && chips);
+    API_BEGIN
+    std::vector<double> r(g->e.size());
+    g->all([&](int k) { r[k] = g->e[k]->exploitability(*v->v); });
+    for (double x : r)
+        if (!(x == r[0]) && !(std::isnan(x) && std::isnan(r[0]))) throw Error("shards disagree on the exploitability");
+    *chips = r[0];
+    API_END
+}
+int gtob_shards_export_arena(gtob_shards* g, int which, int p, float* out) {
+    REQUIRE(g && out && which >= 0 && which <= 2 && (p == 0 || p == 1));
+    API_BEGIN
+    const Spot& sp = *g->e[0]->plan_spot();
+    const Tree& t = sp.tree;
+    const size_t len = t.data_size[p], nh = sp.hands[p].size();
+    std::vector<std::vector<float>> img(g->e.size(), std::vector<float>(len));
+    for (size_t k = 0; k < g->e.size(); k++) g->e[k]->export_arena(which, p, img[k].data());
+    std::memset(out, 0, len * sizeof(float));
+    for (uint32_t nd = 0; nd < t.size(); nd++) {
+        if (t.kind[nd] != kAction || t.player[nd] != p) continue;
+        for (size_t k = 0; k < g->e.size(); k++)
+            if (g->e[k]->plan().node_sidx[nd] >= 0) {
+                std::memcpy(out + t.data_off[nd], img[k].data() + t.data_off[nd], t.nchild[nd] * nh * sizeof(float));
+                break;
+            }
+    }
+    API_END
+}
+int gtob_shards_sync_to_cpu(gtob_shards* g, gtob_solver* v, int strategy_only) {
+    REQUIRE(g && v);
+    API_BEGIN
+    for (auto& e : g->e) e->sync_to_cpu(*v->v, strategy_only != 0);  // each shard writes its own nodes
+    API_END
+}
+void gtob_shards_free(gtob_shards* g) { delete g; }
+int gtob_spot_shard_visited(const gtob_spot* sp, int use_iso, int shard, int nshards, uint8_t* visited) {
+    REQUIRE(sp && visited && nshards >= 1 && shard >= 0 && shard < nshards);
+    API_BEGIN
+    const Plan P = build_plan(*sp->s, use_iso != 0, kFuseFolds, shard, nshards);
+    for (size_t i = 0; i < P.node_cslot.size(); i++) visited[i] = P.node_cslot[i] != kNoSlot ? 1 : 0;
     API_END
 }
 struct gtob_batch {

@@ -10,6 +10,7 @@
 #include <mutex>
 #include <thread>
 #include <unordered_map>
+#include <unordered_set>
 
 namespace gtob {
 
@@ -271,7 +272,10 @@ void flat_copy(const FlatLayout& L, size_t b, size_t g, Levels<T>& ls, V& flat) 
 }
 }  // namespace
 
-Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
+Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nshards) {
+    if (nshards < 1 || shard < 0 || shard >= nshards) throw Error("invalid argument: shard");
+    if (nshards > 1 && fuse_mode == kFuseAll)
+        throw Error("sharding needs showdowns with slots of their own (not the fused engine)");
     const Tree& t = sp.tree;
     Plan P;
     const bool fused = fuse_mode == kFuseAll;
@@ -292,6 +296,58 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
     Builder root(sp, P, visited, fused, P.fuse_folds, true);
     const bool full_board = sp.board.size() == 5;
     root.run({0, 0, {0, 0}, 0, 0, {0, 0}, full_board ? root.river_slot(nullptr, 0) : kNoSlot});
+    P.shard = shard;
+    P.nshards = nshards;
+    // Sharded: this shard's representative subtrees, and the root builder's
+    // cfv slots renumbered so that the children of each level's top chance
+    // nodes take one contiguous run, ordered by the shard that computes them:
+    // one sum over the shards per level, after zeroing the runs of the others.
+    std::vector<uint32_t> root_perm;  // root builder's cfv slot -> final (sharded plans)
+    if (nshards > 1) {
+        struct Kid { uint32_t lv, owner, task, cslot; };
+        std::unordered_map<uint32_t, uint32_t> task_of;  // child cfv slot -> task index
+        for (size_t i = 0; i < root.tasks.size(); i++) task_of[root.tasks[i].cslot] = (uint32_t)i;
+        std::vector<Kid> kids;
+        std::unordered_set<uint32_t> seen;
+        for (size_t lv = 0; lv < root.chance_l.size(); lv++)
+            for (auto& x : root.chance_l[lv])
+                for (uint32_t k = x.second.cc_start; k < x.second.cc_start + x.second.cc_count; k++) {
+                    const uint32_t cs = root.cards[k].child_cslot;
+                    if (cs == kNoSlot || !seen.insert(cs).second) continue;
+                    const uint32_t ti = task_of.at(cs);
+                    kids.push_back({(uint32_t)lv, ti % (uint32_t)nshards, ti, cs});
+                }
+        std::sort(kids.begin(), kids.end(), [](const Kid& a, const Kid& b) {
+            return a.lv != b.lv ? a.lv < b.lv : a.owner != b.owner ? a.owner < b.owner : a.task < b.task;
+        });
+        const uint32_t nroot = (uint32_t)root.next_c;
+        root_perm.assign(nroot, kNoSlot);
+        for (const Kid& k : kids) root_perm[k.cslot] = 0;  // marked: placed below
+        uint32_t next = 0;
+        for (uint32_t c = 0; c < nroot; c++)
+            if (root_perm[c] == kNoSlot) root_perm[c] = next++;
+        P.reduce_span.assign(root.chance_l.size(), Span{0, 0});
+        P.own_span.assign(root.chance_l.size(), Span{0, 0});
+        for (size_t j = 0; j < kids.size(); j++) {
+            const Kid& k = kids[j];
+            const uint32_t at = next + (uint32_t)j;
+            root_perm[k.cslot] = at;
+            Span& r = P.reduce_span[k.lv];
+            if (!r.count) r.start = at;
+            r.count++;
+            if ((int)k.owner == shard) {
+                Span& o = P.own_span[k.lv];
+                if (!o.count) o.start = at;
+                o.count++;
+            }
+        }
+        for (size_t lv = 0; lv < P.own_span.size(); lv++)  // an empty run sits at the level's start
+            if (!P.own_span[lv].count) P.own_span[lv].start = P.reduce_span[lv].start;
+        std::vector<Visit> mine;
+        for (size_t i = 0; i < root.tasks.size(); i++)
+            if ((int)(i % (size_t)nshards) == shard) mine.push_back(root.tasks[i]);
+        root.tasks.swap(mine);
+    }
     std::vector<std::unique_ptr<Builder>> subs;
     for (size_t i = 0; i < root.tasks.size(); i++)
         subs.push_back(std::make_unique<Builder>(sp, P, visited, fused, P.fuse_folds, false));
@@ -370,7 +426,10 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode) {
     parallel_for(bs.size(), [&](size_t i) {
         Builder& b = *bs[i];
         const Bases& B = bases[i];
-        auto rc = [&](uint32_t& x) { if (is_local(x)) x = B.c + (x - kLocal); };
+        auto rc = [&](uint32_t& x) {
+            if (is_local(x)) x = B.c + (x - kLocal);
+            else if (x != kNoSlot && !root_perm.empty()) x = root_perm[x];  // a root builder's slot
+        };
         auto rr = [&](uint32_t& x, int q) { if (is_local(x)) x = B.r[q] + (x - kLocal); };
         auto rs = [&](uint32_t& x) { if (is_local(x)) x = B.slot[x - kLocal]; };
         for (int q = 0; q < 2; q++)

@@ -195,6 +195,12 @@ struct Plan {
     // per tree node the sweep visits: its cfv slot and each player's reach
     // slot (kNoSlot for nodes it does not visit)
     std::vector<uint32_t> node_cslot, node_rs[2];
+    int shard = 0, nshards = 1;
+    // per level, the contiguous cfv slots of the representative children of
+    // that level's top chance nodes, which the shards split among them, and
+    // the run of them this shard computes (the others it zeroes before each
+    // sum); empty without sharding
+    std::vector<Span> reduce_span, own_span;
     uint32_t num_slots = 0;
     std::vector<uint32_t> slot_key;
     std::vector<uint32_t> sorted_off[2];
@@ -220,6 +226,11 @@ struct Plan {
     uint64_t visited_terminals = 0;
 };
 
-Plan build_plan(const Spot& spot, bool use_iso, int fuse_mode);
+// shard / nshards: the representative subtrees below the first chance nodes
+// are dealt round-robin over nshards plans, each keeping the whole tree above
+// them; the values of those subtrees' roots are summed over the shards
+// (reduce_span: each is nonzero on one shard only) before the chance nodes
+// above them add them up (a flop sharded by turn card).
+Plan build_plan(const Spot& spot, bool use_iso, int fuse_mode, int shard = 0, int nshards = 1);
 
 }  // namespace gtob

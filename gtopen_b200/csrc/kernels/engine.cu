@@ -412,6 +412,7 @@ struct EngineImpl {
         for (int l = L - 1; l >= 0; l--) {
             if (!fork) launch_terminals(l, p, stream, pr);
             else if (l + 1 < L) CK(cudaStreamWaitEvent(stream, ev_term[l + 1], 0));
+            reduce_level(l, p);  // a shard: the children of this level's top chance nodes from every shard
             const Span sc = plan.chance_span[l];
             if (sc.count) timed(pr, 5, [&] { launch_chance(sc, p); });
             const Span sa = plan.act_span[l];
@@ -498,11 +499,34 @@ struct EngineImpl {
         return ex;
     }
     uint32_t iter_kernels = 0;  // kernel nodes of the captured iteration graph
+    std::shared_ptr<ShardReducer> reducer;  // sharded spot: sums the top chance nodes over the shards
+    bool uncaptured = false;                // the reducer syncs on the host: plain launches, no graphs
+    // the values of the level's top chance nodes' children, summed over the
+    // shards (one shard holds each, the others hold zeros)
+    void reduce_level(int l, int p) {
+        (void)p;
+        if (!reducer || l >= (int)plan.reduce_span.size() || !plan.reduce_span[l].count) return;
+        // another shard's children hold the previous sum here: zero them so
+        // that the sum adds each child's value to zeros only
+        const Span r = plan.reduce_span[l], o = plan.own_span[l];
+        const size_t w = d.nh_max;
+        if (o.start > r.start) CK(cudaMemsetAsync(d.cfv + (size_t)r.start * w, 0, (size_t)(o.start - r.start) * w * 4, stream));
+        const uint32_t oe = o.start + o.count, re = r.start + r.count;
+        if (re > oe) CK(cudaMemsetAsync(d.cfv + (size_t)oe * w, 0, (size_t)(re - oe) * w * 4, stream));
+        reducer->reduce(d.cfv + (size_t)r.start * w, (size_t)r.count * w, stream);
+    }
 };
 
 // --------------------------------------------------------------- GpuEngine
-GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new EngineImpl()) {
+GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : GpuEngine(host, fmt, engine, 0, 1, nullptr) {}
+
+GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int nshards,
+                     std::shared_ptr<ShardReducer> reducer)
+    : d_(new EngineImpl()) {
     EngineImpl& E = *d_;
+    if (nshards > 1 && !reducer) throw Error("invalid argument: a sharded engine needs a reducer");
+    E.reducer = nshards > 1 ? reducer : nullptr;
+    E.uncaptured = E.reducer && !E.reducer->capturable();
     const Spot& sp = *host.spot;
     g_uploaded = 0;
     if (engine < kEngineFused || engine > kEngineStaged) throw Error("unknown engine kind");
@@ -518,7 +542,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : d_(new Engin
     if (E.fmt != kFmtF32 && E.fmt != kFmtI16 && E.fmt != kFmtFP8) throw Error("unknown device arena format");
     if (E.fmt == kFmtFP8 && engine != kEngineStaged) throw Error("FP8 arenas run on the staged engine only");
     E.iteration = host.iteration;
-    E.plan = build_plan(sp, host.use_iso, fuse);
+    E.plan = build_plan(sp, host.use_iso, fuse, shard, nshards);
     const Plan& P = E.plan;
     if (P.max_children > 32u) throw Error("an action node with more than 32 actions is not supported on the GPU");
     E.wide = P.max_children > 8u;
@@ -739,12 +763,22 @@ GpuEngine::~GpuEngine() = default;
 uint64_t GpuEngine::upload_bytes() const { return d_->uploaded; }
 uint32_t GpuEngine::iteration_kernels() {
     EngineImpl& E = *d_;
+    if (E.uncaptured) return 0;  // no graph
     if (!E.g_iter) E.g_iter = E.capture(-1);
     return E.iter_kernels;
 }
 
 void GpuEngine::iterate(int n) {
     EngineImpl& E = *d_;
+    if (E.uncaptured) {
+        for (int k = 0; k < n; k++) {
+            E.prime();
+            E.record_iteration();
+            E.iteration++;
+        }
+        CK(cudaGetLastError());
+        return;
+    }
     for (int k = 0; k < n; k++) {
         if (!E.g_iter) E.g_iter = E.capture(-1);
         E.prime();
@@ -756,6 +790,7 @@ void GpuEngine::iterate(int n) {
 
 double GpuEngine::time_iterations(int n) {
     EngineImpl& E = *d_;
+    if (E.uncaptured) throw Error("time_iterations needs the captured iteration (not an engine of a shard group)");
     if (!E.g_iter) E.g_iter = E.capture(-1);
     E.prime();
     cudaEvent_t a, b;
@@ -797,8 +832,12 @@ double GpuEngine::exploitability(const HostSolver& host) {  // best_response.rs:
     const bool raked = host.spot->config.tree.rake_pct > 0.0;
     double br[2], v[2] = {0, 0};
     for (int mode = 0; mode < (raked ? 2 : 1); mode++) {
-        if (!E.g_eval[mode]) E.g_eval[mode] = E.capture(mode);
-        CK(cudaGraphLaunch(E.g_eval[mode], E.stream));
+        if (E.uncaptured) {
+            E.record_eval(mode);
+        } else {
+            if (!E.g_eval[mode]) E.g_eval[mode] = E.capture(mode);
+            CK(cudaGraphLaunch(E.g_eval[mode], E.stream));
+        }
         E.reach_valid = false;
         CK(cudaStreamSynchronize(E.stream));
         E.check_err();
@@ -1007,6 +1046,8 @@ struct PinnedPair {
 
 void GpuEngine::save(const HostSolver& host, const std::string& path) {
     EngineImpl& E = *d_;
+    if (E.plan.nshards > 1)
+        throw Error("invalid argument: a shard holds part of the spot (sync each shard to the host solver, then save it)");
     CK(cudaStreamSynchronize(E.stream));
     E.check_err();
     const Spot& sp = *E.spot;
@@ -1137,6 +1178,7 @@ void GpuEngine::save(const HostSolver& host, const std::string& path) {
 
 void GpuEngine::load_arenas(std::istream& in, HostSolver& host) {
     EngineImpl& E = *d_;
+    if (E.plan.nshards > 1) throw Error("invalid argument: a shard holds part of the spot (load on the host)");
     CK(cudaStreamSynchronize(E.stream));
     const Tree& t = E.spot->tree;
     // blocks the device does not hold, in arena order: they go to the host
@@ -1294,11 +1336,12 @@ void GpuEngine::sync_to_cpu(HostSolver& host, bool strategy_only) {  // gpu/mod.
             const unsigned nb = (unsigned)E.plan.n_anodes[p];
             if (!nb) continue;
             void* src = which == kRegrets ? E.ar.reg[p] : which == kStrategy ? E.ar.str[p] : E.ar.pred[p];
-            // Without suit isomorphism every action node is on the device, so the
-            // reference-layout image is the whole host arena and lands there
-            // directly; otherwise it goes through a temporary and only the
-            // device's nodes are copied (the symmetric branches keep theirs).
-            const bool whole = !E.plan.iso_active;
+            // Without suit isomorphism or shards every action node is on the
+            // device, so the reference-layout image is the whole host arena and
+            // lands there directly; otherwise it goes through a temporary and
+            // only the device's nodes are copied (the symmetric branches and
+            // the other shards' nodes keep theirs).
+            const bool whole = !E.plan.iso_active && E.plan.nshards == 1;
             if (E.fmt == kFmtI16 && ha.kind != 0) {
                 // 16-bit on both sides: quants and scales move exactly
                 k_to_host<uint16_t><<<nb, kThreads, 0, E.stream>>>((const uint16_t*)src, (uint16_t*)E.staging, E.xnodes[p], nh);
@@ -1345,6 +1388,7 @@ uint32_t GpuEngine::iteration() const { return d_->iteration; }
 int GpuEngine::format() const { return d_->fmt; }
 bool GpuEngine::fused() const { return d_->plan.fused; }
 const Plan& GpuEngine::plan() const { return d_->plan; }
+const Spot* GpuEngine::plan_spot() const { return d_->spot; }
 uint64_t GpuEngine::device_bytes() const { return d_->bytes; }
 void GpuEngine::discounts(float* out3) {
     CK(cudaMemcpyAsync(out3, d_->d.disc, 3 * sizeof(float), cudaMemcpyDeviceToHost, d_->stream));

@@ -2,6 +2,8 @@
 // (crates/solver/src/gpu/mod.rs).  Owns every device buffer; copies arenas and
 // locks out of a HostSolver and syncs results back into it.
 #pragma once
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -23,6 +25,17 @@ extern const char* const kKernelNames[7];
 
 struct EngineImpl;
 
+// Sums one device buffer over the shards of one sharded spot (see
+// build_plan): each shard calls reduce with its copy of the same count floats
+// and returns (in stream order) with it holding the sum over the shards.
+struct ShardReducer {
+    virtual ~ShardReducer() = default;
+    virtual void reduce(float* buf, size_t count, cudaStream_t stream) = 0;
+    // false: the reduction synchronises on the host, so the engine runs its
+    // sweeps as plain launches instead of captured graphs
+    virtual bool capturable() const = 0;
+};
+
 class GpuEngine {
   public:
     // fmt < 0: follow the host storage (f32 -> f32 arenas, compressed -> i16/u16).
@@ -34,6 +47,10 @@ class GpuEngine {
     // kEngineStaged (one CTA per node staging its blocks and vectors in shared
     // memory with bulk copies; fold children in place; f64).
     GpuEngine(const HostSolver& host, int fmt, int engine = 0);
+    // One shard of a sharded spot: the top of the tree and every nshards-th
+    // representative subtree below its chance nodes; `reducer` adds the
+    // shards' partial chance values after each such level of the up sweep.
+    GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int nshards, std::shared_ptr<ShardReducer> reducer);
     bool fused() const;
     ~GpuEngine();
     void iterate(int n);
@@ -48,6 +65,7 @@ class GpuEngine {
     uint32_t iteration() const;
     int format() const;
     const Plan& plan() const;
+    const Spot* plan_spot() const;  // the spot the engine was built for
     uint64_t device_bytes() const;
     // algorithmic bytes of one CFR iteration / one BR check (traffic model)
     double iter_bytes() const;

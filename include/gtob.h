@@ -260,6 +260,38 @@ int gtob_gpu_exploit_values(gtob_gpu* gpu, const gtob_solver* solver, const int*
                             gtob_node_info* info, float* reach, float* valid, float* br_ev, float* cur_ev, float* gain,
                             float* br_strategy, float* action_ev, float* averages);
 
+/* ---- one spot over several shards (a flop split by turn card) ---------- */
+/* A spot split by its first chance card: every shard holds the tree above
+ * the first chance nodes and every nshards-th representative subtree below
+ * them; before the top chance nodes add up their children, the children's
+ * values are summed over the shards (each is nonzero on the one shard that
+ * holds it, so the sum is exact and every shard computes what one engine
+ * would).  Each shard's arenas hold its own nodes and the top part. */
+/* ncclGetUniqueId (libnccl.so.2 is loaded on first use) for rank 0 to share. */
+int gtob_nccl_unique_id(unsigned char out[128]);
+/* Shard `rank` of `world` processes, one GPU each (the current device),
+ * reducing over NCCL inside the iteration's CUDA graph; every rank must call
+ * it with the same id (ncclCommInitRank: it returns once all have joined). */
+int gtob_gpu_new_sharded(const gtob_solver* solver, int device_format, int engine, int rank, int world,
+                         const unsigned char id[128], gtob_gpu** out);
+/* All nshards shards in this process on the current device, reducing on the
+ * host (no graphs; each call below runs the shards on their own threads):
+ * the whole sharded computation on one GPU, to check it against one engine. */
+typedef struct gtob_shards gtob_shards;
+int gtob_shards_new(const gtob_solver* solver, int device_format, int engine, int nshards, gtob_shards** out);
+int gtob_shards_iterate(gtob_shards* shards, int n);
+int gtob_shards_exploitability(gtob_shards* shards, const gtob_solver* solver, double* chips);
+/* an arena of all shards merged in the reference layout (each node from a
+ * shard that holds it) */
+int gtob_shards_export_arena(gtob_shards* shards, int which, int player, float* out);
+/* every shard's nodes (and the shared top part) into one host solver, as
+ * gtob_gpu_sync_to_cpu of each shard in turn */
+int gtob_shards_sync_to_cpu(gtob_shards* shards, gtob_solver* solver, int strategy_only);
+void gtob_shards_free(gtob_shards* shards);
+/* The plan partition without a GPU: visited[node] = 1 for every node shard
+ * `shard` of `nshards` visits (staged engine's plan). */
+int gtob_spot_shard_visited(const gtob_spot* spot, int use_iso, int shard, int nshards, uint8_t* visited);
+
 /* ---- batch of spots (solve_cli.rs:125-215 batch) ------------------------ */
 /* The reference's batch report solves one board after another
  * (solve_quiet, solve_cli.rs:338-362).  A batch solves many spots on one GPU

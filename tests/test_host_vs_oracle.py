@@ -348,3 +348,21 @@ def test_canonical_flops_kat():
     assert len(classes) == 1755
     assert sum(w for _, w in classes) == 22100
 
+
+@pytest.mark.parametrize("cfg_fn,use_iso", [(W.small_flop_spot, False), (W.iso_spot, True)])
+@pytest.mark.parametrize("nshards", [2, 3])
+def test_shard_partition(cfg_fn, use_iso, nshards):
+    """A flop split by turn card: every shard keeps the tree above the first
+    chance nodes, and every other visited node lies in exactly one shard."""
+    spot = g.Spot(cfg_fn())
+    full = g.shard_visited(spot, 0, 1, use_iso).astype(bool)
+    parts = [g.shard_visited(spot, k, nshards, use_iso).astype(bool) for k in range(nshards)]
+    union = np.logical_or.reduce(parts)
+    common = np.logical_and.reduce(parts)
+    assert np.array_equal(union, full)
+    count = np.sum(parts, axis=0)
+    assert np.array_equal(count[full & ~common], np.ones((full & ~common).sum()))
+    assert common.sum() < full.sum() / 2  # the shared top part is small
+    for k in range(nshards):
+        assert (parts[k] & ~common).any()
+
