@@ -152,6 +152,15 @@ def lib():
         "gtob_gpu_load": (I, [C.c_char_p, I, I, I, C.POINTER(P), C.POINTER(P)]),
         "gtob_set_device": (I, [I]),
         "gtob_gpu_time_iterations": (I, [P, I, C.POINTER(D)]),
+        "gtob_net_new": (I, [I, I, I, I, U64, C.POINTER(P)]),
+        "gtob_net_free": (None, [P]),
+        "gtob_net_get_params": (I, [P, I, P, P]),
+        "gtob_net_set_params": (I, [P, I, P, P]),
+        "gtob_net_get_grads": (I, [P, I, P, P]),
+        "gtob_net_forward": (I, [P, P, I, P]),
+        "gtob_net_gradients": (I, [P, P, P, P, I, C.POINTER(D)]),
+        "gtob_net_train": (I, [P, P, P, P, I, I, I, C.c_float, U64, P]),
+        "gtob_gemm_bf16": (I, [P, P, I, I, I, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -681,3 +690,79 @@ class Batch:
 
 def set_device(device):
     _check(lib().gtob_set_device(int(device)))
+
+
+def gemm_bf16(a_bits, b_bits):
+    """C = A B^T on the tcgen05 kernel: A (m x k) and B (n x k) as uint16 bf16
+    bit patterns, C float32 (m, n multiples of 128, k of 64)."""
+    a = np.ascontiguousarray(a_bits, np.uint16)
+    b = np.ascontiguousarray(b_bits, np.uint16)
+    m, k = a.shape
+    n = b.shape[0]
+    c = np.zeros((m, n), np.float32)
+    _check(lib().gtob_gemm_bf16(_ptr(a), _ptr(b), m, n, k, _ptr(c)))
+    return c
+
+
+class LeafNet:
+    """The turn-leaf value network: din -> nhidden x dh (GELU) -> dout, BF16
+    weights and activations, FP32 accumulation, trained on the device."""
+
+    def __init__(self, din, dh, nhidden, dout, seed=1):
+        h = C.c_void_p()
+        _check(lib().gtob_net_new(int(din), int(dh), int(nhidden), int(dout), int(seed), C.byref(h)))
+        self._h = h
+        self.din, self.dh, self.nhidden, self.dout = din, dh, nhidden, dout
+
+    def __del__(self):
+        if getattr(self, "_h", None) and _LIB is not None:
+            _LIB.gtob_net_free(self._h)
+            self._h = None
+
+    def _shape(self, layer):
+        fin = self.din if layer == 0 else self.dh
+        fout = self.dout if layer == self.nhidden else self.dh
+        return fout, fin
+
+    def params(self, layer):
+        o, i = self._shape(layer)
+        w = np.zeros((o, i), np.float32)
+        b = np.zeros(o, np.float32)
+        _check(lib().gtob_net_get_params(self._h, int(layer), _ptr(w), _ptr(b)))
+        return w, b
+
+    def set_params(self, layer, w, b):
+        o, i = self._shape(layer)
+        w = np.ascontiguousarray(w, np.float32).reshape(o, i)
+        b = np.ascontiguousarray(b, np.float32).reshape(o)
+        _check(lib().gtob_net_set_params(self._h, int(layer), _ptr(w), _ptr(b)))
+
+    def grads(self, layer):
+        o, i = self._shape(layer)
+        w = np.zeros((o, i), np.float32)
+        b = np.zeros(o, np.float32)
+        _check(lib().gtob_net_get_grads(self._h, int(layer), _ptr(w), _ptr(b)))
+        return w, b
+
+    def forward(self, x):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.din)
+        y = np.zeros((x.shape[0], self.dout), np.float32)
+        _check(lib().gtob_net_forward(self._h, _ptr(x), x.shape[0], _ptr(y)))
+        return y
+
+    def gradients(self, x, t, mask):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.din)
+        t = np.ascontiguousarray(t, np.float32).reshape(-1, self.dout)
+        m = np.ascontiguousarray(mask, np.float32).reshape(-1, self.dout)
+        loss = C.c_double()
+        _check(lib().gtob_net_gradients(self._h, _ptr(x), _ptr(t), _ptr(m), x.shape[0], C.byref(loss)))
+        return loss.value
+
+    def train(self, x, t, mask, epochs, batch=1024, lr=1e-3, seed=1):
+        x = np.ascontiguousarray(x, np.float32).reshape(-1, self.din)
+        t = np.ascontiguousarray(t, np.float32).reshape(-1, self.dout)
+        m = np.ascontiguousarray(mask, np.float32).reshape(-1, self.dout)
+        losses = np.zeros(epochs, np.float32)
+        _check(lib().gtob_net_train(self._h, _ptr(x), _ptr(t), _ptr(m), x.shape[0], int(epochs), int(batch),
+                                    C.c_float(lr), int(seed), _ptr(losses)))
+        return losses

@@ -13,6 +13,7 @@
 #include <string>
 
 #include "../kernels/engine.hpp"
+#include "../kernels/leafnet.hpp"
 #include "batch.hpp"
 #include "core.hpp"
 #include "query.hpp"
@@ -24,6 +25,9 @@ using namespace gtob;
 struct gtob_spot { std::shared_ptr<Spot> s; };
 struct gtob_solver { std::unique_ptr<HostSolver> v; };
 struct gtob_gpu { std::unique_ptr<GpuEngine> e; };
+struct gtob_net {
+    std::unique_ptr<LeafNet> n;
+};
 struct gtob_shards {
     std::vector<std::unique_ptr<GpuEngine>> e;
     int device = 0;
@@ -632,6 +636,85 @@ int gtob_gpu_discounts(gtob_gpu* g, float* out3) {
     REQUIRE(g && out3);
     API_BEGIN
     g->e->discounts(out3);
+    API_END
+}
+
+int gtob_net_new(int din, int dh, int nhidden, int dout, uint64_t seed, gtob_net** out) {
+    REQUIRE(out && din > 0 && dh > 0 && nhidden > 0 && nhidden <= 8 && dout > 0);
+    *out = nullptr;
+    API_BEGIN
+    LeafNetDims d;
+    d.din = din;
+    d.dh = dh;
+    d.nhidden = nhidden;
+    d.dout = dout;
+    *out = new gtob_net{std::make_unique<LeafNet>(d, seed)};
+    API_END
+}
+void gtob_net_free(gtob_net* n) { delete n; }
+int gtob_net_get_params(gtob_net* n, int l, float* w, float* b) {
+    REQUIRE(n && (w || b));
+    API_BEGIN
+    n->n->get_params(l, w, b);
+    API_END
+}
+int gtob_net_set_params(gtob_net* n, int l, const float* w, const float* b) {
+    REQUIRE(n && (w || b));
+    API_BEGIN
+    n->n->set_params(l, w, b);
+    API_END
+}
+int gtob_net_get_grads(gtob_net* n, int l, float* w, float* b) {
+    REQUIRE(n && (w || b));
+    API_BEGIN
+    n->n->get_grads(l, w, b);
+    API_END
+}
+int gtob_net_forward(gtob_net* n, const float* x, int rows, float* y) {
+    REQUIRE(n && x && y && rows >= 0);
+    API_BEGIN
+    n->n->forward_host(x, rows, y);
+    API_END
+}
+int gtob_net_gradients(gtob_net* n, const float* x, const float* t, const float* mask, int rows, double* loss) {
+    REQUIRE(n && x && t && mask && loss && rows > 0);
+    API_BEGIN
+    *loss = n->n->gradients_host(x, t, mask, rows);
+    API_END
+}
+int gtob_net_train(gtob_net* n, const float* x, const float* t, const float* mask, int count, int epochs, int batch,
+                   float lr, uint64_t seed, float* losses) {
+    REQUIRE(n && x && t && mask && count > 0 && epochs > 0 && batch > 0 && batch % 128 == 0 && lr > 0.0f);
+    API_BEGIN
+    n->n->train_host(x, t, mask, count, epochs, batch, lr, seed, losses);
+    API_END
+}
+int gtob_gemm_bf16(const uint16_t* a, const uint16_t* b, int m, int n, int k, float* c) {
+    REQUIRE(a && b && c && m > 0 && n > 0 && k > 0 && m % 128 == 0 && n % 128 == 0 && k % 64 == 0);
+    API_BEGIN
+    struct Buf {
+        void* p = nullptr;
+        explicit Buf(size_t bytes) {
+            const cudaError_t e = cudaMalloc(&p, bytes);
+            if (e != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(e));
+        }
+        ~Buf() { cudaFree(p); }
+    } da((size_t)m * k * 2), db((size_t)n * k * 2), dc((size_t)m * n * 4), derr(4);
+    auto ok = [](cudaError_t e) {
+        if (e != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(e));
+    };
+    ok(cudaMemcpy(da.p, a, (size_t)m * k * 2, cudaMemcpyHostToDevice));
+    ok(cudaMemcpy(db.p, b, (size_t)n * k * 2, cudaMemcpyHostToDevice));
+    ok(cudaMemset(derr.p, 0, 4));
+    GemmEpilogue e;
+    e.out_f32 = (float*)dc.p;
+    e.ld_f32 = n;
+    gemm_bf16_tn((const __nv_bfloat16*)da.p, (const __nv_bfloat16*)db.p, m, n, k, e, (unsigned*)derr.p, nullptr);
+    ok(cudaDeviceSynchronize());
+    unsigned err = 0;
+    ok(cudaMemcpy(&err, derr.p, 4, cudaMemcpyDeviceToHost));
+    if (err) throw Error("timeout: a tensor-core matrix product's wait gave up");
+    ok(cudaMemcpy(c, dc.p, (size_t)m * n * 4, cudaMemcpyDeviceToHost));
     API_END
 }
 

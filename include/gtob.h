@@ -354,6 +354,33 @@ void gtob_batch_free(gtob_batch* batch);
 int gtob_gpu_read_node_static(gtob_gpu* gpu, int which, uint32_t node, float* out, uint64_t out_len,
                               uint64_t* written);
 
+/* ---- the turn-leaf value network (depth-limited solves) ----------------- */
+/* No counterpart in the reference (its north star's learned leaf).  A fully
+ * connected net: din inputs, nhidden GELU layers of dh units, dout linear
+ * outputs; BF16 weights and activations, FP32 accumulation and master
+ * weights, every matrix product on a hand-written tcgen05 kernel.  Training
+ * minimises the masked squared error mean(mask * (y - t)^2) over rows x dout
+ * with Adam (0.9, 0.999, 1e-8). */
+typedef struct gtob_net gtob_net;
+int gtob_net_new(int din, int dh, int nhidden, int dout, uint64_t seed, gtob_net** out);
+void gtob_net_free(gtob_net* net);
+/* layer l in [0, nhidden]: weights [out x in] row-major and bias [out] (f32) */
+int gtob_net_get_params(gtob_net* net, int layer, float* w, float* b);
+int gtob_net_set_params(gtob_net* net, int layer, const float* w, const float* b);
+/* the gradients of the last gtob_net_gradients call */
+int gtob_net_get_grads(gtob_net* net, int layer, float* w, float* b);
+/* rows x din inputs -> rows x dout outputs (host buffers) */
+int gtob_net_forward(gtob_net* net, const float* x, int rows, float* y);
+/* one forward + backward; *loss = the masked mean squared error */
+int gtob_net_gradients(gtob_net* net, const float* x, const float* t, const float* mask, int rows, double* loss);
+/* epochs of shuffled batches (batch a multiple of 128); losses[epoch] = the
+ * epoch's mean batch loss (NULL: not reported) */
+int gtob_net_train(gtob_net* net, const float* x, const float* t, const float* mask, int n, int epochs, int batch,
+                   float lr, uint64_t seed, float* losses);
+/* The tensor-core matrix product alone: C[M x N] = A[M x K] * B[N x K]^T,
+ * A and B bf16 bit patterns (host), C f32; M, N multiples of 128, K of 64. */
+int gtob_gemm_bf16(const uint16_t* a, const uint16_t* b, int m, int n, int k, float* c);
+
 #ifdef __cplusplus
 }
 #endif
