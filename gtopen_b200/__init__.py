@@ -146,6 +146,7 @@ def lib():
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
         "gtob_batch_size": (I, [P]),
         "gtob_batch_row_get": (I, [P, I, C.POINTER(BatchRow)]),
+        "gtob_batch_root_cfv": (I, [P, I, I, P, I, C.POINTER(I)]),
         "gtob_batch_error": (C.c_char_p, [P, I]),
         "gtob_batch_solver": (P, [P, I]),
         "gtob_batch_free": (None, [P]),
@@ -161,6 +162,9 @@ def lib():
         "gtob_net_gradients": (I, [P, P, P, P, I, C.POINTER(D)]),
         "gtob_net_train": (I, [P, P, P, P, I, I, I, C.c_float, U64, P]),
         "gtob_gemm_bf16": (I, [P, P, I, I, I, P]),
+        "gtob_gpu_new_dl": (I, [P, P, I, I, C.POINTER(P)]),
+        "gtob_gpu_leaves": (I, [P, P, P, P, I, C.POINTER(I)]),
+        "gtob_gpu_node_sweep": (I, [P, U32, I, I, P, P, P]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -678,6 +682,14 @@ class Batch:
                         "error": lib().gtob_batch_error(self._h, i).decode(errors="replace")})
         return out
 
+    def root_cfv(self, i, p):
+        """Spot i's root counterfactual values (average strategies) per hand of p."""
+        n = C.c_int()
+        _check(lib().gtob_batch_root_cfv(self._h, int(i), int(p), None, 0, C.byref(n)))
+        out = np.zeros(n.value, np.float32)
+        _check(lib().gtob_batch_root_cfv(self._h, int(i), int(p), _ptr(out), n.value, C.byref(n)))
+        return out
+
     def solver(self, i):
         """The i-th host solver (owned by the batch, synced after run)."""
         h = lib().gtob_batch_solver(self._h, int(i))
@@ -766,3 +778,37 @@ class LeafNet:
         _check(lib().gtob_net_train(self._h, _ptr(x), _ptr(t), _ptr(m), x.shape[0], int(epochs), int(batch),
                                     C.c_float(lr), int(seed), _ptr(losses)))
         return losses
+
+
+def dl_gpu_solver(solver, net, device_format=None, engine="staged"):
+    """A depth-limited flop solve: the turn's betting chance nodes are leaves
+    valued by `net` (a LeafNet of 2705 inputs and 2652 outputs)."""
+    h = C.c_void_p()
+    _check(lib().gtob_gpu_new_dl(solver._h, net._h, DEVICE_FORMAT[device_format], ENGINES[engine], C.byref(h)))
+    gpu = GpuSolver.__new__(GpuSolver)
+    gpu._h = h
+    gpu.solver = solver
+    gpu.net = net  # the solver holds the net too; keep the Python handle alive beside it
+    return gpu
+
+
+def dl_leaves(gpu):
+    """(nodes, pots, stacks) of a depth-limited solver's leaves."""
+    n = C.c_int()
+    _check(lib().gtob_gpu_leaves(gpu._h, None, None, None, 0, C.byref(n)))
+    nodes = np.zeros(n.value, np.uint32)
+    pot = np.zeros(n.value, np.float32)
+    stack = np.zeros(n.value, np.float32)
+    _check(lib().gtob_gpu_leaves(gpu._h, _ptr(nodes), _ptr(pot), _ptr(stack), n.value, C.byref(n)))
+    return nodes, pot, stack
+
+
+def node_sweep(gpu, node, p, mode=1):
+    """One evaluation sweep (mode 0 best response, 1 average strategies), then
+    (node's value for p, reach of player 0, reach of player 1)."""
+    nh = gpu.solver.spot.nh
+    cfv = np.zeros(nh[p], np.float32)
+    r0 = np.zeros(nh[0], np.float32)
+    r1 = np.zeros(nh[1], np.float32)
+    _check(lib().gtob_gpu_node_sweep(gpu._h, int(node), int(p), int(mode), _ptr(cfv), _ptr(r0), _ptr(r1)))
+    return cfv, r0, r1

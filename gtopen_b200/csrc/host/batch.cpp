@@ -62,6 +62,7 @@ static void solve_one(HostSolver& host, bool sync, int device_format, int engine
             d += (double)h.w[i];
         }
         row.ev[p] = n / d;
+        row.root_cfv[p] = std::move(cfv);
     }
     if (sync) eng.sync_to_cpu(host, false);
     row.iterations = eng.iteration();

@@ -21,6 +21,7 @@ struct BatchRow {
     double exploit_pct = 0.0;  // exploitability, % of the starting pot
     double seconds = 0.0;      // wall time of this spot: engine build, solve, EVs, sync
     double ev[2] = {0.0, 0.0};  // reach-weighted root EV per player, pot-share (solve_cli.rs:176-188)
+    std::vector<float> root_cfv[2];  // per hand, the root's counterfactual values of the average strategies
 };
 
 // Runs solve_quiet's loop (one iteration at a time, exploitability when the

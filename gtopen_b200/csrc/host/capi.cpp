@@ -26,7 +26,7 @@ struct gtob_spot { std::shared_ptr<Spot> s; };
 struct gtob_solver { std::unique_ptr<HostSolver> v; };
 struct gtob_gpu { std::unique_ptr<GpuEngine> e; };
 struct gtob_net {
-    std::unique_ptr<LeafNet> n;
+    std::shared_ptr<LeafNet> n;
 };
 struct gtob_shards {
     std::vector<std::unique_ptr<GpuEngine>> e;
@@ -493,6 +493,14 @@ int gtob_batch_row_get(const gtob_batch* b, int i, gtob_batch_row* out) {
     out->ev[1] = r.ev[1];
     return GTOB_OK;
 }
+int gtob_batch_root_cfv(gtob_batch* b, int i, int p, float* out, int cap, int* n) {
+    REQUIRE(b && n && (p == 0 || p == 1) && i >= 0 && i < (int)b->rows.size() && cap >= 0);
+    API_BEGIN
+    const std::vector<float>& v = b->rows[i].root_cfv[p];
+    *n = (int)v.size();
+    if (out) std::memcpy(out, v.data(), std::min<size_t>(v.size(), (size_t)cap) * sizeof(float));
+    API_END
+}
 const char* gtob_batch_error(const gtob_batch* b, int i) {
     if (!b || i < 0 || i >= (int)b->rows.size()) return "";
     return b->rows[i].error.c_str();
@@ -648,7 +656,7 @@ int gtob_net_new(int din, int dh, int nhidden, int dout, uint64_t seed, gtob_net
     d.dh = dh;
     d.nhidden = nhidden;
     d.dout = dout;
-    *out = new gtob_net{std::make_unique<LeafNet>(d, seed)};
+    *out = new gtob_net{std::make_shared<LeafNet>(d, seed)};
     API_END
 }
 void gtob_net_free(gtob_net* n) { delete n; }
@@ -687,6 +695,31 @@ int gtob_net_train(gtob_net* n, const float* x, const float* t, const float* mas
     REQUIRE(n && x && t && mask && count > 0 && epochs > 0 && batch > 0 && batch % 128 == 0 && lr > 0.0f);
     API_BEGIN
     n->n->train_host(x, t, mask, count, epochs, batch, lr, seed, losses);
+    API_END
+}
+int gtob_gpu_new_dl(const gtob_solver* v, gtob_net* net, int fmt, int engine, gtob_gpu** out) {
+    REQUIRE(v && net && out && fmt >= -1 && fmt <= 2 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+    *out = nullptr;
+    API_BEGIN
+    *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt, engine, net->n)};
+    API_END
+}
+int gtob_gpu_leaves(gtob_gpu* g, uint32_t* nodes, float* pot, float* stack, int cap, int* n) {
+    REQUIRE(g && n && cap >= 0);
+    API_BEGIN
+    const auto& L = g->e->plan().leaves;
+    *n = (int)L.size();
+    for (int i = 0; i < std::min(cap, (int)L.size()); i++) {
+        if (nodes) nodes[i] = L[i].node;
+        if (pot) pot[i] = L[i].pot;
+        if (stack) stack[i] = L[i].stack;
+    }
+    API_END
+}
+int gtob_gpu_node_sweep(gtob_gpu* g, uint32_t node, int p, int mode, float* cfv, float* reach0, float* reach1) {
+    REQUIRE(g && (p == 0 || p == 1) && (mode == 0 || mode == 1));
+    API_BEGIN
+    g->e->node_sweep_values(node, p, mode, cfv, reach0, reach1, nullptr, nullptr);
     API_END
 }
 int gtob_gemm_bf16(const uint16_t* a, const uint16_t* b, int m, int n, int k, float* c) {

@@ -59,6 +59,8 @@ struct Builder {
     uint32_t max_children = 0;
     std::vector<uint32_t> nodes;  // subtree builders: the nodes visited (their slot entries are remapped)
     std::vector<Visit> tasks;     // root builder: the subtrees handed out
+    bool cut = false;             // root builder of a depth-limited plan
+    std::vector<LeafItem> leaves;
     std::vector<uint32_t> cbase_of, rbase_of[2];
 
     Builder(const Spot& s, Plan& p, std::vector<uint8_t>& vis, bool fu, bool ff, bool root)
@@ -149,6 +151,17 @@ struct Builder {
                     break;
                 }
                 case kChance: {
+                    if (cut && t.street[nd] == 1) {  // deals the turn: a leaf when betting follows
+                        uint32_t first = kSentinel;
+                        for (int c = 0; c < 52 && first == kSentinel; c++) first = t.children[t.child_start[nd] + c];
+                        if (first != kSentinel && t.kind[first] == kAction) {
+                            const double half = sp.config.tree.starting_pot / 2.0;
+                            LeafItem lf{nd, v.cslot, {v.rs[0], v.rs[1]}, (float)(t.put0[nd] + t.put1[nd]),
+                                        (float)(sp.config.tree.effective_stack - (t.put0[nd] - half)), v.level, 0};
+                            leaves.push_back(lf);
+                            break;
+                        }
+                    }
                     std::vector<int> valid = P.iso_active ? sp.perms_fixing(v.dealt, v.ndealt) : std::vector<int>{0};
                     struct CardRep { uint8_t card, rep; uint32_t perm; };
                     std::vector<CardRep> cr;
@@ -272,8 +285,10 @@ void flat_copy(const FlatLayout& L, size_t b, size_t g, Levels<T>& ls, V& flat) 
 }
 }  // namespace
 
-Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nshards) {
+Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nshards, bool cut_turn) {
     if (nshards < 1 || shard < 0 || shard >= nshards) throw Error("invalid argument: shard");
+    if (cut_turn && (nshards > 1 || sp.tree.root_street != 0))
+        throw Error("invalid argument: a depth-limited plan needs a flop spot and one shard");
     if (nshards > 1 && fuse_mode == kFuseAll)
         throw Error("sharding needs showdowns with slots of their own (not the fused engine)");
     const Tree& t = sp.tree;
@@ -294,6 +309,8 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
     // the tree above the chance nodes, then every representative chance
     // subtree on the worker threads
     Builder root(sp, P, visited, fused, P.fuse_folds, true);
+    root.cut = cut_turn;
+    P.cut_turn = cut_turn;
     const bool full_board = sp.board.size() == 5;
     root.run({0, 0, {0, 0}, 0, 0, {0, 0}, full_board ? root.river_slot(nullptr, 0) : kNoSlot});
     P.shard = shard;
@@ -498,6 +515,7 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
         P.max_children = std::max(P.max_children, b->max_children);
     }
     P.n_cslots = nc;
+    P.leaves = std::move(root.leaves);  // the root builder's slots are final
     P.n_rslots[0] = nr[0];
     P.n_rslots[1] = nr[1];
 

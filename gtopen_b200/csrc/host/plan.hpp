@@ -104,6 +104,17 @@ struct alignas(16) RankEntry {  // 16-byte aligned: one vector load on the devic
 
 struct Span { uint32_t start, count; };
 
+// A depth-limited plan's leaf: a chance node dealing the turn below which
+// the players still bet, cut from the tree; its values come from the turn
+// leaf network each sweep (kind of an action node's child: kChildNode).
+struct LeafItem {
+    uint32_t node;    // tree node id of the chance node
+    uint32_t cslot;   // its cfv slot
+    uint32_t rs[2];   // reach slots at the node
+    float pot, stack; // pot (both players' puts) and the remaining effective stack
+    uint32_t level, pad;
+};
+
 // Vectors of plain records whose resize does not zero them: the plan's flat
 // tables are written in parallel right after they are sized, so the first
 // touch of their pages happens on the worker threads.
@@ -196,6 +207,8 @@ struct Plan {
     // slot (kNoSlot for nodes it does not visit)
     std::vector<uint32_t> node_cslot, node_rs[2];
     int shard = 0, nshards = 1;
+    bool cut_turn = false;         // depth-limited: the turn's betting chance nodes are leaves
+    std::vector<LeafItem> leaves;  // (depth-limited plans)
     // per level, the contiguous cfv slots of the representative children of
     // that level's top chance nodes, which the shards split among them, and
     // the run of them this shard computes (the others it zeroes before each
@@ -231,6 +244,9 @@ struct Plan {
 // them; the values of those subtrees' roots are summed over the shards
 // (reduce_span: each is nonzero on one shard only) before the chance nodes
 // above them add them up (a flop sharded by turn card).
-Plan build_plan(const Spot& spot, bool use_iso, int fuse_mode, int shard = 0, int nshards = 1);
+// cut_turn: a depth-limited plan -- every chance node that deals the turn
+// and leads to more betting becomes a leaf (Plan::leaves) instead of a
+// subtree; all-in runouts stay exact.
+Plan build_plan(const Spot& spot, bool use_iso, int fuse_mode, int shard = 0, int nshards = 1, bool cut_turn = false);
 
 }  // namespace gtob

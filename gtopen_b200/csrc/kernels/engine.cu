@@ -21,6 +21,8 @@
 // reference's f32 arithmetic does).
 #include <cuda_runtime.h>
 
+#include "leafnet.hpp"
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -395,6 +397,9 @@ struct EngineImpl {
             down(3, 1, pr);
             reach_valid = false;
         }
+        // depth-limited: the turn leaves' values from the network, before
+        // any level of the up sweep reads them
+        if (leaf) leaf->run(p, d.reach[0], (size_t)d.rstr[0], d.reach[1], (size_t)d.rstr[1], d.cfv, (size_t)d.nh_max, stream);
         // Terminal kernels (folds and showdowns with slots of their own) read
         // only reach vectors, so in a captured sweep they run on a second
         // stream, every level of them, beside the chain of chance and action
@@ -460,6 +465,16 @@ struct EngineImpl {
     void check_err() {
         unsigned e = 0;
         CK(cudaMemcpyAsync(&e, d.err, sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+        if (leaf) {
+            unsigned ne = 0;
+            CK(cudaMemcpyAsync(&ne, leaf->net().err_word(), sizeof(unsigned), cudaMemcpyDeviceToHost, stream));
+            CK(cudaStreamSynchronize(stream));
+            if (ne) {
+                CK(cudaMemsetAsync(leaf->net().err_word(), 0, sizeof(unsigned), stream));
+                CK(cudaStreamSynchronize(stream));
+                throw Error("timeout: a tensor-core matrix product's wait gave up");
+            }
+        }
         CK(cudaStreamSynchronize(stream));
         if (e) {
             CK(cudaMemsetAsync(d.err, 0, sizeof(unsigned), stream));
@@ -499,6 +514,7 @@ struct EngineImpl {
         return ex;
     }
     uint32_t iter_kernels = 0;  // kernel nodes of the captured iteration graph
+    std::unique_ptr<LeafEvaluator> leaf;  // depth-limited solves: the turn leaves' network
     std::shared_ptr<ShardReducer> reducer;  // sharded spot: sums the top chance nodes over the shards
     bool uncaptured = false;                // the reducer syncs on the host: plain launches, no graphs
     // the values of the level's top chance nodes' children, summed over the
@@ -521,9 +537,10 @@ struct EngineImpl {
 GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : GpuEngine(host, fmt, engine, 0, 1, nullptr) {}
 
 GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int nshards,
-                     std::shared_ptr<ShardReducer> reducer)
+                     std::shared_ptr<ShardReducer> reducer, std::shared_ptr<LeafNet> leaf_net)
     : d_(new EngineImpl()) {
     EngineImpl& E = *d_;
+    if (leaf_net && nshards > 1) throw Error("invalid argument: a depth-limited solve runs on one shard");
     if (nshards > 1 && !reducer) throw Error("invalid argument: a sharded engine needs a reducer");
     E.reducer = nshards > 1 ? reducer : nullptr;
     E.uncaptured = E.reducer && !E.reducer->capturable();
@@ -542,7 +559,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
     if (E.fmt != kFmtF32 && E.fmt != kFmtI16 && E.fmt != kFmtFP8) throw Error("unknown device arena format");
     if (E.fmt == kFmtFP8 && engine != kEngineStaged) throw Error("FP8 arenas run on the staged engine only");
     E.iteration = host.iteration;
-    E.plan = build_plan(sp, host.use_iso, fuse, shard, nshards);
+    E.plan = build_plan(sp, host.use_iso, fuse, shard, nshards, leaf_net != nullptr);
     const Plan& P = E.plan;
     if (P.max_children > 32u) throw Error("an action node with more than 32 actions is not supported on the GPU");
     E.wide = P.max_children > 8u;
@@ -755,6 +772,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
         }
     }
     E.upload_locks(host);
+    if (leaf_net) E.leaf = std::make_unique<LeafEvaluator>(leaf_net, sp, P.leaves);
     CK(cudaStreamSynchronize(E.stream));
     E.uploaded = g_uploaded;
 }
@@ -1048,6 +1066,7 @@ void GpuEngine::save(const HostSolver& host, const std::string& path) {
     EngineImpl& E = *d_;
     if (E.plan.nshards > 1)
         throw Error("invalid argument: a shard holds part of the spot (sync each shard to the host solver, then save it)");
+    if (E.leaf) throw Error("invalid argument: a depth-limited solve holds no subtrees below its turn leaves");
     CK(cudaStreamSynchronize(E.stream));
     E.check_err();
     const Spot& sp = *E.spot;
@@ -1179,6 +1198,7 @@ void GpuEngine::save(const HostSolver& host, const std::string& path) {
 void GpuEngine::load_arenas(std::istream& in, HostSolver& host) {
     EngineImpl& E = *d_;
     if (E.plan.nshards > 1) throw Error("invalid argument: a shard holds part of the spot (load on the host)");
+    if (E.leaf) throw Error("invalid argument: a depth-limited solve holds no subtrees below its turn leaves");
     CK(cudaStreamSynchronize(E.stream));
     const Tree& t = E.spot->tree;
     // blocks the device does not hold, in arena order: they go to the host

@@ -24,6 +24,7 @@ struct Profile {
 extern const char* const kKernelNames[7];
 
 struct EngineImpl;
+class LeafNet;
 
 // Sums one device buffer over the shards of one sharded spot (see
 // build_plan): each shard calls reduce with its copy of the same count floats
@@ -50,7 +51,14 @@ class GpuEngine {
     // One shard of a sharded spot: the top of the tree and every nshards-th
     // representative subtree below its chance nodes; `reducer` adds the
     // shards' partial chance values after each such level of the up sweep.
-    GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int nshards, std::shared_ptr<ShardReducer> reducer);
+    GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int nshards, std::shared_ptr<ShardReducer> reducer,
+              std::shared_ptr<LeafNet> leaf_net = nullptr);
+    // A depth-limited solve of a flop spot: the tree is cut at the chance
+    // nodes dealing the turn (where betting follows) and their values come
+    // from leaf_net after every down sweep.  The net serves one engine at a
+    // time (its activation buffers are its own).
+    GpuEngine(const HostSolver& host, int fmt, int engine, std::shared_ptr<LeafNet> leaf_net)
+        : GpuEngine(host, fmt, engine, 0, 1, nullptr, std::move(leaf_net)) {}
     bool fused() const;
     ~GpuEngine();
     void iterate(int n);

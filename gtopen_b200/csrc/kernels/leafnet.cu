@@ -21,6 +21,7 @@
 #include <cudaTypedefs.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <numeric>
@@ -380,7 +381,14 @@ void gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, 
     if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % kBN || K % kBK)
         throw Error("invalid argument: matrix product shape (M, N multiples of 128, K of 64)");
     const CUtensorMap ta = tile_map(A, (uint64_t)K, (uint64_t)M), tb = tile_map(B, (uint64_t)K, (uint64_t)N);
-    LCK(cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+    // once per device, so that a captured stream makes no attribute calls
+    static std::atomic<uint64_t> prepared{0};
+    int dev = 0;
+    LCK(cudaGetDevice(&dev));
+    if (dev >= 64 || !((prepared.load() >> dev) & 1u)) {
+        LCK(cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+        if (dev < 64) prepared.fetch_or(uint64_t(1) << dev);
+    }
     k_gemm_tn<<<dim3(N / kBN, M / kBM), kGemmThreads, kGemmSmem, s>>>(ta, tb, K, e, err);
     LCK(cudaGetLastError());
 }
@@ -689,6 +697,184 @@ void LeafNet::train_host(const float* x, const float* t, const float* mask, int 
         if (losses) losses[ep] = (float)(sum / std::max(nb, 1));
     }
     cudaFree(didx);
+}
+
+// ---------------------------------------------------------------- leaves
+namespace {
+__device__ __forceinline__ float block_sum(float v, float* red) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    __syncthreads();  // red may still be read from a previous call
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    float s = 0.0f;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) s += red[w];  // same order in every thread
+    return s;
+}
+struct LeafDev {
+    const LeafItem* leaves;
+    const uint8_t* cards;
+    int ncards;
+    uint64_t board_mask;
+    const float* reach[2];
+    size_t rstr[2];
+    const uint64_t* hmask[2];
+    const uint16_t* combo[2];
+    const int16_t* hand_of[2];
+    int nh[2];
+    __nv_bfloat16* x;
+    int din_p;
+    float* y;
+    int dout_p;
+    float* mass;
+    float* err;
+};
+// one row per (leaf, turn card): the reach sums, then the input row
+__global__ void k_leaf_gather(LeafDev L) {
+    __shared__ float red[32];
+    __shared__ float inv[2];
+    const int row = blockIdx.x, li = row / L.ncards, c = L.cards[row % L.ncards];
+    const LeafItem lf = L.leaves[li];
+    for (int q = 0; q < 2; q++) {
+        const float* r = L.reach[q] + (size_t)lf.rs[q] * L.rstr[q];
+        float acc = 0.0f;
+        for (int h = threadIdx.x; h < L.nh[q]; h += blockDim.x)
+            if (!((L.hmask[q][h] >> c) & 1ull)) acc += r[h];
+        const float m = block_sum(acc, red);
+        if (threadIdx.x == 0) {
+            L.mass[row * 2 + q] = m;
+            inv[q] = m > 0.0f ? 1.0f / m : 0.0f;
+        }
+    }
+    __syncthreads();
+    const uint64_t onehot = L.board_mask | (1ull << c);
+    __nv_bfloat16* xr = L.x + (size_t)row * L.din_p;
+    for (int col = threadIdx.x; col < L.din_p; col += blockDim.x) {
+        float v = 0.0f;
+        if (col < 52) {
+            v = ((onehot >> col) & 1ull) ? 1.0f : 0.0f;
+        } else if (col == 52) {
+            v = lf.pot / lf.stack;
+        } else if (col < kLeafIn) {
+            const int q = col < 53 + 1326 ? 0 : 1, cb = col - 53 - q * 1326;
+            const int h = L.hand_of[q][cb];
+            if (h >= 0 && !((L.hmask[q][h] >> c) & 1ull))
+                v = L.reach[q][(size_t)lf.rs[q] * L.rstr[q] + h] * inv[q];
+        }
+        xr[col] = __float2bfloat16_rn(v);
+    }
+}
+// per row: sum r0 y0 + sum r1 y1 over the combos (the zero-sum error)
+__global__ void k_leaf_err(LeafDev L) {
+    __shared__ float red[32];
+    const int row = blockIdx.x;
+    const __nv_bfloat16* xr = L.x + (size_t)row * L.din_p + 53;
+    const float* yr = L.y + (size_t)row * L.dout_p;
+    float acc = 0.0f;
+    for (int k = threadIdx.x; k < kLeafOut; k += blockDim.x) acc += __bfloat162float(xr[k]) * yr[k];
+    const float e = block_sum(acc, red);
+    if (threadIdx.x == 0) L.err[row] = e;
+}
+// one block per leaf: player p's values, summed over the turn cards
+__global__ void k_leaf_scatter(LeafDev L, int p, float* cfv, size_t stride) {
+    const int li = blockIdx.x;
+    const LeafItem lf = L.leaves[li];
+    const float inv = 1.0f / 45.0f;
+    for (int h = threadIdx.x; h < L.nh[p]; h += blockDim.x) {
+        const uint64_t hm = L.hmask[p][h];
+        const int cb = L.combo[p][h];
+        float acc = 0.0f;
+        for (int j = 0; j < L.ncards; j++) {
+            const int c = L.cards[j];
+            if ((hm >> c) & 1ull) continue;
+            const int row = li * L.ncards + j;
+            const float yv = L.y[(size_t)row * L.dout_p + p * 1326 + cb] - 0.5f * L.err[row];
+            acc += yv * lf.pot * L.mass[row * 2 + (1 - p)];
+        }
+        cfv[(size_t)lf.cslot * stride + h] = acc * inv;
+    }
+}
+template <class T>
+T* dcopy(const T* h, size_t n) {
+    T* p = dnew<T>(n);
+    if (n) LCK(cudaMemcpy(p, h, n * sizeof(T), cudaMemcpyHostToDevice));
+    return p;
+}
+}  // namespace
+
+LeafEvaluator::LeafEvaluator(std::shared_ptr<LeafNet> net, const Spot& sp, const std::vector<LeafItem>& leaves)
+    : net_(std::move(net)) {
+    if (!net_) throw Error("invalid argument: no leaf network");
+    if (net_->dims().din != kLeafIn || net_->dims().dout != kLeafOut)
+        throw Error("invalid argument: the leaf network must map " + std::to_string(kLeafIn) + " inputs to " +
+                    std::to_string(kLeafOut) + " outputs");
+    if (sp.board.size() != 3) throw Error("invalid argument: a depth-limited solve needs a flop spot");
+    if (leaves.empty()) throw Error("invalid argument: the spot has no turn leaves");
+    nleaves_ = (int)leaves.size();
+    std::vector<uint8_t> cards;
+    for (uint8_t b : sp.board) board_mask_ |= 1ull << b;
+    for (int c = 0; c < 52; c++)
+        if (!((board_mask_ >> c) & 1ull)) cards.push_back((uint8_t)c);
+    ncards_ = (int)cards.size();
+    rows_ = nleaves_ * ncards_;
+    rows_p_ = pad128(rows_);
+    for (int q = 0; q < 2; q++) {
+        const Hands& H = sp.hands[q];
+        nh_[q] = (int)H.size();
+        std::vector<uint16_t> combo(H.size());
+        std::vector<int16_t> hand_of(1326, -1);
+        for (size_t h = 0; h < H.size(); h++) {
+            const int hi = H.c1[h], lo = H.c2[h];
+            combo[h] = (uint16_t)(hi * (hi - 1) / 2 + lo);
+            hand_of[combo[h]] = (int16_t)h;
+        }
+        hmask_[q] = dcopy(H.mask.data(), H.mask.size());
+        combo_[q] = dcopy(combo.data(), combo.size());
+        hand_of_[q] = dcopy(hand_of.data(), hand_of.size());
+    }
+    leaves_ = dcopy(leaves.data(), leaves.size());
+    cards_ = dcopy(cards.data(), cards.size());
+    x_ = dnew<__nv_bfloat16>((size_t)rows_p_ * net_->din_pad());  // padding rows stay zero
+    y_ = dnew<float>((size_t)rows_p_ * net_->dout_pad());
+    mass_ = dnew<float>((size_t)rows_ * 2);
+    err_ = dnew<float>((size_t)rows_);
+    net_->reserve_rows(rows_p_);
+}
+
+LeafEvaluator::~LeafEvaluator() {
+    for (void* p : {(void*)leaves_, (void*)cards_, (void*)hmask_[0], (void*)hmask_[1], (void*)combo_[0],
+                    (void*)combo_[1], (void*)hand_of_[0], (void*)hand_of_[1], (void*)x_, (void*)y_, (void*)mass_,
+                    (void*)err_})
+        cudaFree(p);
+}
+
+void LeafEvaluator::run(int p, const float* reach0, size_t rstr0, const float* reach1, size_t rstr1, float* cfv,
+                        size_t cfv_stride, cudaStream_t s) {
+    LeafDev L;
+    L.leaves = leaves_;
+    L.cards = cards_;
+    L.ncards = ncards_;
+    L.board_mask = board_mask_;
+    L.reach[0] = reach0;
+    L.reach[1] = reach1;
+    L.rstr[0] = rstr0;
+    L.rstr[1] = rstr1;
+    for (int q = 0; q < 2; q++) {
+        L.hmask[q] = hmask_[q];
+        L.combo[q] = combo_[q];
+        L.hand_of[q] = hand_of_[q];
+        L.nh[q] = nh_[q];
+    }
+    L.x = x_;
+    L.din_p = net_->din_pad();
+    L.y = y_;
+    L.dout_p = net_->dout_pad();
+    L.mass = mass_;
+    L.err = err_;
+    k_leaf_gather<<<rows_, 256, 0, s>>>(L);
+    net_->forward_device(x_, rows_p_, y_, s);
+    k_leaf_err<<<rows_, 256, 0, s>>>(L);
+    k_leaf_scatter<<<nleaves_, 256, 0, s>>>(L, p, cfv, cfv_stride);
+    LCK(cudaGetLastError());
 }
 
 }  // namespace gtob

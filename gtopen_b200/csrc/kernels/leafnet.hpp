@@ -13,6 +13,8 @@
 #include <memory>
 #include <vector>
 
+#include "../host/plan.hpp"
+
 namespace gtob {
 
 // C[M x N] = A[M x K] * B[N x K]^T, both operands row-major bf16 with K
@@ -57,6 +59,8 @@ class LeafNet {
     // epochs of Adam over n samples in shuffled batches; per-epoch mean loss
     void train_host(const float* x, const float* t, const float* mask, int n, int epochs, int batch, float lr,
                     uint64_t seed, float* losses);
+    // device buffers for rows_pad rows: call before capturing forward_device
+    void reserve_rows(int rows_pad) { ensure_rows(rows_pad); }
     // device-side forward over rows padded inputs (bf16, rows_pad x din_pad,
     // rows_pad a multiple of 128) into f32 outputs (rows_pad x dout_pad)
     void forward_device(const __nv_bfloat16* x, int rows_pad, float* y, cudaStream_t s);
@@ -83,6 +87,45 @@ class LeafNet {
     int adam_t_ = 0;
     uint32_t launches_ = 0;
     cudaStream_t stream_ = nullptr;
+};
+
+// The turn-leaf inputs and outputs of a depth-limited flop plan.  Inputs per
+// (leaf, turn card c) row, kLeafIn = 2705 values: the board and c one-hot
+// (52), pot / remaining stack, and each player's reach at the leaf over the
+// 1326 combos (hands holding c or absent are 0) divided by its sum.  Outputs
+// per row, kLeafOut = 2652: each player's counterfactual values over the
+// combos, divided by pot x the opponent's reach sum.  A leaf's values for p
+// are those of every turn card, zero-sum corrected (the outputs shifted by
+// half of sum r0 y0 + sum r1 y1), scaled back and added over the cards a hand
+// does not hold, times 1/45 (the chance node's 1 / (46 - street)).
+constexpr int kLeafIn = 52 + 1 + 2 * 1326;
+constexpr int kLeafOut = 2 * 1326;
+
+class LeafEvaluator {
+  public:
+    LeafEvaluator(std::shared_ptr<LeafNet> net, const Spot& spot, const std::vector<LeafItem>& leaves);
+    ~LeafEvaluator();
+    // the leaves' values for player p into cfv (slot stride cfv_stride)
+    void run(int p, const float* reach0, size_t rstr0, const float* reach1, size_t rstr1, float* cfv,
+             size_t cfv_stride, cudaStream_t s);
+    int rows() const { return rows_; }
+    uint32_t launches_per_run() const { return 3 + (uint32_t)net_->layers(); }
+    LeafNet& net() { return *net_; }
+
+  private:
+    std::shared_ptr<LeafNet> net_;
+    int nleaves_ = 0, ncards_ = 0, rows_ = 0, rows_p_ = 0;
+    int nh_[2] = {0, 0};
+    uint64_t board_mask_ = 0;
+    LeafItem* leaves_ = nullptr;
+    uint8_t* cards_ = nullptr;            // the turn cards, ascending
+    uint64_t* hmask_[2] = {nullptr, nullptr};
+    uint16_t* combo_[2] = {nullptr, nullptr};  // hand -> combo
+    int16_t* hand_of_[2] = {nullptr, nullptr}; // combo -> hand (-1: none)
+    __nv_bfloat16* x_ = nullptr;
+    float* y_ = nullptr;
+    float* mass_ = nullptr;  // [row][2]
+    float* err_ = nullptr;   // [row]
 };
 
 }  // namespace gtob

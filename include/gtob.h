@@ -322,6 +322,9 @@ int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int us
 int gtob_batch_run(gtob_batch* batch, uint32_t max_iterations, double target_pct, uint32_t check_every, int workers);
 int gtob_batch_size(const gtob_batch* batch);
 int gtob_batch_row_get(const gtob_batch* batch, int i, gtob_batch_row* out);
+/* spot i's root counterfactual values of the average strategies, per hand of
+ * player p (*n = hand count; empty until the spot is solved) */
+int gtob_batch_root_cfv(gtob_batch* batch, int i, int player, float* out, int cap, int* n);
 /* the message of a failed row ("" when the row solved) */
 const char* gtob_batch_error(const gtob_batch* batch, int i);
 /* the i-th host solver, owned by the batch (valid until gtob_batch_free);
@@ -377,6 +380,23 @@ int gtob_net_gradients(gtob_net* net, const float* x, const float* t, const floa
  * epoch's mean batch loss (NULL: not reported) */
 int gtob_net_train(gtob_net* net, const float* x, const float* t, const float* mask, int n, int epochs, int batch,
                    float lr, uint64_t seed, float* losses);
+/* A depth-limited flop solve: the plan cuts the tree at the chance nodes
+ * dealing the turn where betting follows (all-in runouts stay exact), and
+ * after every down sweep the net evaluates each such leaf for every turn
+ * card -- inputs: board + turn one-hot (52), pot / remaining stack, both
+ * players' reach over the 1326 combos divided by its sum (hands holding the
+ * card zeroed); outputs: both players' counterfactual values over the combos
+ * divided by pot x the opponent's reach sum -- zero-sum corrected, scaled
+ * back and averaged over the cards as the chance node would (x 1/45).  The
+ * net must map 2705 inputs to 2652 outputs; it serves one solver at a time.
+ * The other gtob_gpu_* calls work as on any solver (save and load refuse). */
+int gtob_gpu_new_dl(const gtob_solver* solver, gtob_net* net, int device_format, int engine, gtob_gpu** out);
+/* the depth-limited solver's leaves: tree node, pot, remaining stack; *n = count */
+int gtob_gpu_leaves(gtob_gpu* gpu, uint32_t* nodes, float* pot, float* stack, int cap, int* n);
+/* one evaluation sweep for player p (mode 0 best response, 1 average
+ * strategies), then node's value for p and both players' reach there (any
+ * output may be NULL) */
+int gtob_gpu_node_sweep(gtob_gpu* gpu, uint32_t node, int p, int mode, float* cfv, float* reach0, float* reach1);
 /* The tensor-core matrix product alone: C[M x N] = A[M x K] * B[N x K]^T,
  * A and B bf16 bit patterns (host), C f32; M, N multiples of 128, K of 64. */
 int gtob_gemm_bf16(const uint16_t* a, const uint16_t* b, int m, int n, int k, float* c);
