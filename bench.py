@@ -461,6 +461,101 @@ def run_precision(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
+BF16_FALLBACK = 1590.0  # TFLOP/s, burst
+
+
+def load_bf16_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return BF16_FALLBACK, "fallback"
+
+
+def run_leaf(args, world, rank, local):
+    """The depth-limited configuration: turn spots of the flop solved by the
+    plain engine (the training set), the leaf network trained on the device,
+    depth-limited solves with the trained and an untrained network, and each
+    resulting flop strategy judged on the full tree (player p's flop locked,
+    the rest re-solved: p's loss of game value, % pot).  Also the tcgen05
+    product's throughput against the bf16 peak."""
+    import numpy as np
+    from concurrent.futures import ThreadPoolExecutor
+
+    import gtopen_b200 as g
+    from gtopen_b200 import leafdata as LD
+    g.set_device(local)
+    if rank != 0:
+        return
+    t_all = time.perf_counter()
+    cfg = LD.dl_flop_spot(g.evaluate7)
+    spot = g.Spot(cfg)
+    probe = g.dl_gpu_solver(g.Solver(spot, storage="compressed", use_iso=False),
+                            g.LeafNet(LD.LEAF_IN, 128, 1, LD.LEAF_OUT, seed=1), device_format="f32")
+    _, pots, stacks = g.dl_leaves(probe)
+    probe.close()
+    leaf_pots = sorted(set((float(a), float(b)) for a, b in zip(pots, stacks)))
+    pool = ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1)))
+    t = time.perf_counter()
+    X, T, M, info = LD.training_set(g, cfg, leaf_pots, args.leaf_spots, seed=1, workers=16, build_pool=pool)
+    gen_s = time.perf_counter() - t
+    nval = max(128, args.leaf_spots // 10)
+    Xt, Tt, Mt = X[nval:], T[nval:], M[nval:]
+    Xv, Tv, Mv = X[:nval], T[:nval], M[:nval]
+    net = g.LeafNet(LD.LEAF_IN, 1024, 3, LD.LEAF_OUT, seed=7)
+    untrained = g.LeafNet(LD.LEAF_IN, 1024, 3, LD.LEAF_OUT, seed=7)
+    val0 = net.gradients(Xv, Tv, Mv)
+    t = time.perf_counter()
+    losses = net.train(Xt, Tt, Mt, epochs=args.leaf_epochs, batch=256, lr=args.leaf_lr, seed=3)
+    train_s = time.perf_counter() - t
+    val1 = net.gradients(Xv, Tv, Mv)
+    rows_seen = args.leaf_epochs * (len(Xt) // 256) * 256
+    dims = [(2816, 1024), (1024, 1024), (1024, 1024), (1024, 2688)]
+    fwd = sum(2.0 * i * o for i, o in dims)
+    flops = rows_seen * (3.0 * fwd - 2.0 * 2816 * 1024)  # forward, dW, dX (no dX into the inputs)
+    # the product alone, operands resident: the forward pass's widest shape at the training batch
+    peak, peak_kind = load_bf16_peak()
+    gm, gn, gk = 4096, 1024, 2816
+    gms = g.gemm_time_ms(gm, gn, gk, reps=50)
+    g_tflops = 2.0 * gm * gn * gk / (gms / 1000.0) / 1e12
+    judge = LD.FlopJudge(g, cfg, iterations=args.leaf_judge_iters)
+    res = {}
+    for name, n in (("trained", net), ("untrained", untrained)):
+        host = g.Solver(spot, storage="compressed", use_iso=False)
+        dl = g.dl_gpu_solver(host, n, device_format="f32")
+        t = time.perf_counter()
+        dl.iterate(args.leaf_dl_iters)
+        dl.synchronize()
+        dl_s = time.perf_counter() - t
+        e_cut = dl.exploitability(host) / cfg["tree"]["starting_pot"] * 100
+        strat = LD.dl_flop_strategies(g, dl, spot)
+        kern = dl.info()["iteration_kernels"]
+        dl.close()
+        l0, l1, ex = judge.loss(strat)
+        res[name] = {"loss_pct_pot": [l0, l1], "loss_sum_pct_pot": l0 + l1, "locked_solve_exploit_pct": ex,
+                     "dl_iterations": args.leaf_dl_iters, "dl_s": dl_s, "dl_exploit_pct_cut_game": e_cut,
+                     "dl_iteration_kernels": kern}
+    line = {"metric": "depth-limited flop solve (config 5): flop-strategy loss vs the full-tree solve, "
+                      "trained vs untrained turn-leaf network",
+            "value": res["trained"]["loss_sum_pct_pot"], "unit": "% pot (sum over players)", "n_gpus": 1,
+            "higher_is_better": False, "dtype": "bf16 (network), f32 (solve)", "data": "synthetic (seeded spots)",
+            "config": {"workload": "dl_flop c5: flop %s, 1.94M-node full tree cut at 11 turn leaves, "
+                                   "network 2705-1024x3-2652" % cfg["board"],
+                       "training_spots": len(Xt), "validation_spots": nval},
+            "trained": res["trained"], "untrained": res["untrained"],
+            "full_solve": {"iterations": judge.iterations, "exploit_pct": judge.full_exploit},
+            "training": {"spots_generated": args.leaf_spots, "generate_s": gen_s,
+                         "turn_solve_exploit_pct_mean": float(info["exploit_pct"].mean()),
+                         "epochs": args.leaf_epochs, "train_s": train_s, "loss_first": float(losses[0]),
+                         "loss_last": float(losses[-1]), "val_loss_before": val0, "val_loss_after": val1,
+                         "tflops": flops / train_s / 1e12},
+            "roofline": {"bound": "tensor", "kernel": "k_gemm_tn %dx%dx%d" % (gm, gn, gk), "achieved": g_tflops,
+                         "peak": peak, "unit": "TFLOP/s", "frac": g_tflops / peak,
+                         "peak_kind": peak_kind + " bf16 dense", "ms": gms},
+            "wall_s": time.perf_counter() - t_all}
+    print(json.dumps(line), flush=True)
+
+
 def time_to_target(g, cfg, args):
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage=HOST_STORAGE[args.storage], algo="dcfr", use_iso=True)
@@ -488,7 +583,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="flop",
-                    choices=["flop", "flop_narrow", "turn", "river", "bench_spot", "report", "precision"])
+                    choices=["flop", "flop_narrow", "turn", "river", "bench_spot", "report", "precision", "leaf"])
+    ap.add_argument("--leaf-spots", type=int, default=2048, help="turn spots solved for the leaf network")
+    ap.add_argument("--leaf-epochs", type=int, default=60)
+    ap.add_argument("--leaf-lr", type=float, default=3e-4)
+    ap.add_argument("--leaf-dl-iters", type=int, default=400)
+    ap.add_argument("--leaf-judge-iters", type=int, default=400)
     ap.add_argument("--report-flops", type=int, default=184)
     ap.add_argument("--report-workers", type=int, default=8)
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32", "fp8"])
@@ -507,7 +607,7 @@ def main():
         args.warmup = 3
     world, rank, local = dist_setup(args.gpus)
     try:
-        if args.impl == "reference" and args.workload in ("report", "precision"):
+        if args.impl == "reference" and args.workload in ("report", "precision", "leaf"):
             if rank == 0:
                 print(json.dumps({"impl": "reference", "unavailable": "the %s workload has no reference-arm run "
                                   "(the flop report extrapolates its CPU baseline from sampled oracle iterations; "
@@ -519,6 +619,8 @@ def main():
             run_report(args, world, rank, local)
         elif args.workload == "precision":
             run_precision(args, world, rank, local)
+        elif args.workload == "leaf":
+            run_leaf(args, world, rank, local)
         else:
             run_ours(args, world, rank, local)
     finally:

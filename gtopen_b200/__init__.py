@@ -165,6 +165,8 @@ def lib():
         "gtob_gpu_new_dl": (I, [P, P, I, I, C.POINTER(P)]),
         "gtob_gpu_leaves": (I, [P, P, P, P, I, C.POINTER(I)]),
         "gtob_gpu_node_sweep": (I, [P, U32, I, I, P, P, P]),
+        "gtob_gpu_node_strategy": (I, [P, U32, P]),
+        "gtob_gemm_time": (I, [I, I, I, I, C.POINTER(D)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -812,3 +814,17 @@ def node_sweep(gpu, node, p, mode=1):
     r1 = np.zeros(nh[1], np.float32)
     _check(lib().gtob_gpu_node_sweep(gpu._h, int(node), int(p), int(mode), _ptr(cfv), _ptr(r0), _ptr(r1)))
     return cfv, r0, r1
+
+
+def node_strategy(gpu, node, num_actions, player):
+    """The average strategy (num_actions x hands) of an action node on the device."""
+    out = np.zeros(num_actions * gpu.solver.spot.nh[player], np.float32)
+    _check(lib().gtob_gpu_node_strategy(gpu._h, int(node), _ptr(out)))
+    return out.reshape(num_actions, -1)
+
+
+def gemm_time_ms(m, n, k, reps=20):
+    """Mean device ms of the tcgen05 product on m x k and n x k bf16 operands."""
+    ms = C.c_double()
+    _check(lib().gtob_gemm_time(int(m), int(n), int(k), int(reps), C.byref(ms)))
+    return ms.value

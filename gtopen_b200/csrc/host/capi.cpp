@@ -722,6 +722,18 @@ int gtob_gpu_node_sweep(gtob_gpu* g, uint32_t node, int p, int mode, float* cfv,
     g->e->node_sweep_values(node, p, mode, cfv, reach0, reach1, nullptr, nullptr);
     API_END
 }
+int gtob_gpu_node_strategy(gtob_gpu* g, uint32_t node, float* out) {
+    REQUIRE(g && out);
+    API_BEGIN
+    g->e->node_average_strategy(node, out);
+    API_END
+}
+int gtob_gemm_time(int m, int n, int k, int reps, double* ms) {
+    REQUIRE(ms && m > 0 && n > 0 && k > 0 && m % 128 == 0 && n % 128 == 0 && k % 64 == 0 && reps > 0);
+    API_BEGIN
+    *ms = gemm_time_ms(m, n, k, reps);
+    API_END
+}
 int gtob_gemm_bf16(const uint16_t* a, const uint16_t* b, int m, int n, int k, float* c) {
     REQUIRE(a && b && c && m > 0 && n > 0 && k > 0 && m % 128 == 0 && n % 128 == 0 && k % 64 == 0);
     API_BEGIN

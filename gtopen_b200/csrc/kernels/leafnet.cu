@@ -393,6 +393,36 @@ void gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, 
     LCK(cudaGetLastError());
 }
 
+double gemm_time_ms(int m, int n, int k, int reps) {
+    __nv_bfloat16* a = dnew<__nv_bfloat16>((size_t)m * k);
+    __nv_bfloat16* b = dnew<__nv_bfloat16>((size_t)n * k);
+    float* c = dnew<float>((size_t)m * n);
+    unsigned* err = dnew<unsigned>(1);
+    cudaStream_t s;
+    cudaEvent_t e0, e1;
+    LCK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    LCK(cudaEventCreate(&e0));
+    LCK(cudaEventCreate(&e1));
+    GemmEpilogue ep;
+    ep.out_f32 = c;
+    ep.ld_f32 = n;
+    gemm_bf16_tn(a, b, m, n, k, ep, err, s);  // warm-up (and the attribute call)
+    LCK(cudaEventRecord(e0, s));
+    for (int r = 0; r < reps; r++) gemm_bf16_tn(a, b, m, n, k, ep, err, s);
+    LCK(cudaEventRecord(e1, s));
+    LCK(cudaEventSynchronize(e1));
+    float ms = 0.0f;
+    LCK(cudaEventElapsedTime(&ms, e0, e1));
+    unsigned e = 0;
+    LCK(cudaMemcpy(&e, err, sizeof(e), cudaMemcpyDeviceToHost));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaStreamDestroy(s);
+    for (void* p : {(void*)a, (void*)b, (void*)c, (void*)err}) cudaFree(p);
+    if (e) throw Error("timeout: a tensor-core matrix product's wait gave up");
+    return (double)ms / reps;
+}
+
 // ---------------------------------------------------------------- LeafNet
 struct LeafNet::Layer {
     int in = 0, out = 0, in_p = 0, out_p = 0;

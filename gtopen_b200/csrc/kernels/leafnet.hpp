@@ -37,6 +37,9 @@ struct GemmEpilogue {
 void gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& e,
                   unsigned* err, cudaStream_t s);
 
+// mean ms of reps products on m x k, n x k operands (f32 output), events
+double gemm_time_ms(int m, int n, int k, int reps);
+
 struct LeafNetDims {
     int din = 0, dh = 0, nhidden = 0, dout = 0;  // as given (unpadded)
 };

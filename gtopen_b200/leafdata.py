@@ -183,3 +183,81 @@ def training_set(g, flop_cfg, leaf_pots, n, seed=1, max_iterations=300, target_p
             M[k, q * 1326 + cb] = 1.0
         pcts[k] = rows[k]["exploit_pct"]
     return X, T, M, {"exploit_pct": pcts, "board3": board3, "cards": cards}
+
+
+# ---------------------------------------------------------------- judging
+def flop_action_nodes(spot):
+    """(node, player, num_actions) of every flop action node."""
+    t = spot.tree()
+    idx = np.where((t["kind"] == 0) & (t["street"] == 0))[0]
+    return [(int(n), int(t["player"][n]), int(t["nchild"][n])) for n in idx]
+
+
+def pair_mass(spot):
+    """sum over card-disjoint hand pairs of w0 * w1 (f64)."""
+    c1a, c2a, w0, same0 = spot.hands(0)
+    c1b, c2b, w1, _ = spot.hands(1)
+    w0 = w0.astype(np.float64)
+    w1 = w1.astype(np.float64)
+    s = np.zeros(52)
+    np.add.at(s, c1b.astype(np.int64), w1)
+    np.add.at(s, c2b.astype(np.int64), w1)
+    ok = same0 != 0xFFFFFFFF
+    same_w = np.where(ok, w1[np.where(ok, same0, 0).astype(np.int64)], 0.0)
+    valid = w1.sum() - s[c1a.astype(np.int64)] - s[c2a.astype(np.int64)] + same_w
+    return float(np.dot(w0, valid))
+
+
+def root_value(gpu, spot, p, pm):
+    """Player p's value at the root under the average strategies, chips per
+    unit of pair mass."""
+    cfv = gpu.root_cfv(p, mode=1).astype(np.float64)
+    w = spot.hands(p)[2].astype(np.float64)
+    return float(np.dot(w, cfv)) / pm
+
+
+def dl_flop_strategies(g, gpu, spot):
+    """{node: average strategy (num_actions x hands)} of a solver's flop nodes."""
+    return {n: g.node_strategy(gpu, n, na, pl) for n, pl, na in flop_action_nodes(spot)}
+
+
+class FlopJudge:
+    """Exact judge of a flop strategy on the full tree: player p's flop
+    nodes locked to it, the rest of the tree solved (both players free
+    everywhere else), p's game value compared with the unlocked solve's.
+    The loss (% pot) is what committing to that flop strategy costs p against
+    the best continuation; each solve's exploitability bounds its noise."""
+
+    def __init__(self, g, cfg, iterations=400, device_format="i16"):
+        self.g = g
+        self.cfg = cfg
+        self.spot = g.Spot(cfg)
+        self.host = g.Solver(self.spot, storage="compressed", use_iso=False)
+        self.pot = cfg["tree"]["starting_pot"]
+        self.pm = pair_mass(self.spot)
+        self.iterations = iterations
+        self.device_format = device_format
+        self.full, self.full_exploit = self._solve({})
+
+    def _solve(self, locks):
+        self.host.clear_locks()
+        for n, sigma in locks.items():
+            self.host.set_lock(n, sigma)
+        gpu = self.g.GpuSolver(self.host, device_format=self.device_format)
+        gpu.iterate(self.iterations)
+        v = [root_value(gpu, self.spot, p, self.pm) for p in (0, 1)]
+        e = gpu.exploitability(self.host) / self.pot * 100
+        gpu.close()
+        return v, e
+
+    def loss(self, strategies):
+        """(loss of player 0, loss of player 1, exploitability of each locked
+        solve), % pot."""
+        out, ex = [], []
+        players = {n: pl for n, pl, _ in flop_action_nodes(self.spot)}
+        for p in (0, 1):
+            v, e = self._solve({n: s for n, s in strategies.items() if players[n] == p})
+            out.append((self.full[p] - v[p]) / self.pot * 100)
+            ex.append(e)
+        self.host.clear_locks()
+        return out[0], out[1], ex

@@ -397,6 +397,12 @@ int gtob_gpu_leaves(gtob_gpu* gpu, uint32_t* nodes, float* pot, float* stack, in
  * strategies), then node's value for p and both players' reach there (any
  * output may be NULL) */
 int gtob_gpu_node_sweep(gtob_gpu* gpu, uint32_t node, int p, int mode, float* cfv, float* reach0, float* reach1);
+/* the average strategy [action * hands + hand] of an action node the GPU
+ * solver holds */
+int gtob_gpu_node_strategy(gtob_gpu* gpu, uint32_t node, float* out);
+/* mean device time (CUDA events, after one untimed launch) of the
+ * tensor-core product on m x k and n x k bf16 operands resident in HBM */
+int gtob_gemm_time(int m, int n, int k, int reps, double* ms);
 /* The tensor-core matrix product alone: C[M x N] = A[M x K] * B[N x K]^T,
  * A and B bf16 bit patterns (host), C f32; M, N multiples of 128, K of 64. */
 int gtob_gemm_bf16(const uint16_t* a, const uint16_t* b, int m, int n, int k, float* c);
