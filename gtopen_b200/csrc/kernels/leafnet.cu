@@ -39,18 +39,22 @@ namespace gtob {
 
 namespace {
 
-constexpr int kBM = 128, kBN = 128, kBK = 64, kStages = 4;
+constexpr int kBM = 128, kBK = 64, kStages = 4;
 constexpr int kGemmThreads = 128;
 constexpr uint32_t kTileABytes = kBM * kBK * 2;
-constexpr uint32_t kTileBBytes = kBN * kBK * 2;
-constexpr uint32_t kStageBytes = kTileABytes + kTileBBytes;
-constexpr size_t kGemmSmem = (size_t)kStages * kStageBytes + 1024;  // + room to align the ring to 1 KiB
 constexpr unsigned long long kNetWaitNs = 2000000000ull;
 constexpr unsigned kErrGemmWait = 16u;
-// instruction descriptor: kind::f16, D f32 (bits 4-5 = 1), A and B bf16
-// (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
-constexpr uint32_t kIdesc =
-    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kBN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+// A 128 x BN output tile (BN = 128 or 256: TMEM columns, B rows per stage).
+template <int BN>
+struct TileCfg {
+    static constexpr uint32_t kTileB = BN * kBK * 2;
+    static constexpr uint32_t kStage = kTileABytes + kTileB;
+    static constexpr size_t kSmem = (size_t)kStages * kStage + 1024;  // + room to align the ring to 1 KiB
+    // instruction descriptor: kind::f16, D f32 (bits 4-5 = 1), A and B bf16
+    // (bits 7-9, 10-12 = 1), both K-major, N >> 3 at bit 17, M >> 4 at bit 24
+    static constexpr uint32_t kIdesc =
+        (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(kBM >> 4) << 24);
+};
 
 __device__ __forceinline__ uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ unsigned long long gtimer() {
@@ -97,11 +101,11 @@ __device__ __forceinline__ uint64_t sw128_desc(const void* p) {
     return (uint64_t)((a >> 4) & 0x3FFFu) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) | ((uint64_t)1 << 46) |
            ((uint64_t)2 << 61);
 }
-__device__ __forceinline__ void tm_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t accumulate) {
+__device__ __forceinline__ void tm_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-        "l"(a), "l"(b), "r"(kIdesc), "r"(accumulate)
+        "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 __device__ __forceinline__ void tm_commit(uint64_t* bar) {
@@ -174,6 +178,7 @@ __device__ __forceinline__ void epilogue16(const GemmEpilogue& e, int row, int c
     }
 }
 
+template <int BN>
 __global__ void __launch_bounds__(kGemmThreads, 1)
     k_gemm_tn(const __grid_constant__ CUtensorMap ta, const __grid_constant__ CUtensorMap tb, int K, GemmEpilogue e,
               unsigned* err) {
@@ -183,7 +188,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     __shared__ uint32_t tbase;
     __shared__ int aborted;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * kBN, nk = K / kBK;
+    using T = TileCfg<BN>;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN, nk = K / kBK;
     if (threadIdx.x == 0) {
         for (int s = 0; s < kStages; s++) {
             bar_init(&full[s], 1);
@@ -195,7 +201,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&tbase)),
-                     "r"((uint32_t)kBN)
+                     "r"((uint32_t)BN)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -211,8 +217,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 aborted = 1;
                 break;
             }
-            uint8_t* sa = ring + (size_t)s * kStageBytes;
-            bar_expect_tx(&full[s], kStageBytes);
+            uint8_t* sa = ring + (size_t)s * T::kStage;
+            bar_expect_tx(&full[s], T::kStage);
             tma_2d(sa, &ta, kb * kBK, m0, &full[s]);
             tma_2d(sa + kTileABytes, &tb, kb * kBK, n0, &full[s]);
         }
@@ -225,10 +231,10 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
                 break;
             }
             tm_fence_after();
-            const uint8_t* sa = ring + (size_t)s * kStageBytes;
+            const uint8_t* sa = ring + (size_t)s * T::kStage;
             const uint64_t da = sw128_desc(sa), db = sw128_desc(sa + kTileABytes);
 #pragma unroll
-            for (int k = 0; k < kBK / 16; k++) tm_mma(tmem, da + 2 * k, db + 2 * k, (kb | k) ? 1u : 0u);
+            for (int k = 0; k < kBK / 16; k++) tm_mma(tmem, da + 2 * k, db + 2 * k, T::kIdesc, (kb | k) ? 1u : 0u);
             tm_commit(&empty[s]);  // the stage is free once these products have read it
         }
         tm_commit(&done);  // arrives when every product issued above has finished
@@ -241,7 +247,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     if (good) {
         const int row = m0 + warp * 32 + lane;
         const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int c = 0; c < kBN; c += 16) {
+        for (int c = 0; c < BN; c += 16) {
             float v[16];
             tm_ld16(lane_base + (uint32_t)c, v);
             epilogue16(e, row, n0 + c, v);
@@ -251,7 +257,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     __syncthreads();
     if (warp == 0) {
         tm_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kBN)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN)
                      : "memory");
     }
 }
@@ -345,12 +351,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     }
     return fn;
 }
-// a row-major bf16 matrix (rows x inner) read in 64 x 128 boxes, 128-byte swizzle
-CUtensorMap tile_map(const void* base, uint64_t inner, uint64_t rows) {
+// a row-major bf16 matrix (rows x inner) read in 64 x box_rows boxes, 128-byte swizzle
+CUtensorMap tile_map(const void* base, uint64_t inner, uint64_t rows, uint32_t box_rows) {
     CUtensorMap m;
     cuuint64_t dims[2] = {inner, rows};
     cuuint64_t strides[1] = {inner * 2};
-    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)kBM};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
     const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides,
                                    box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -376,21 +382,31 @@ uint64_t xs_next(uint64_t& s) {
 
 }  // namespace
 
-void gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& e,
-                  unsigned* err, cudaStream_t s) {
-    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % kBN || K % kBK)
-        throw Error("invalid argument: matrix product shape (M, N multiples of 128, K of 64)");
-    const CUtensorMap ta = tile_map(A, (uint64_t)K, (uint64_t)M), tb = tile_map(B, (uint64_t)K, (uint64_t)N);
+template <int BN>
+static void launch_gemm(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& e,
+                        unsigned* err, cudaStream_t s) {
+    const CUtensorMap ta = tile_map(A, (uint64_t)K, (uint64_t)M, kBM);
+    const CUtensorMap tb = tile_map(B, (uint64_t)K, (uint64_t)N, (uint32_t)BN);
     // once per device, so that a captured stream makes no attribute calls
     static std::atomic<uint64_t> prepared{0};
     int dev = 0;
     LCK(cudaGetDevice(&dev));
     if (dev >= 64 || !((prepared.load() >> dev) & 1u)) {
-        LCK(cudaFuncSetAttribute(k_gemm_tn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGemmSmem));
+        LCK(cudaFuncSetAttribute(k_gemm_tn<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TileCfg<BN>::kSmem));
         if (dev < 64) prepared.fetch_or(uint64_t(1) << dev);
     }
-    k_gemm_tn<<<dim3(N / kBN, M / kBM), kGemmThreads, kGemmSmem, s>>>(ta, tb, K, e, err);
+    k_gemm_tn<BN><<<dim3(N / BN, M / kBM), kGemmThreads, TileCfg<BN>::kSmem, s>>>(ta, tb, K, e, err);
     LCK(cudaGetLastError());
+}
+
+void gemm_bf16_tn(const __nv_bfloat16* A, const __nv_bfloat16* B, int M, int N, int K, const GemmEpilogue& e,
+                  unsigned* err, cudaStream_t s) {
+    if (M <= 0 || N <= 0 || K <= 0 || M % kBM || N % 128 || K % kBK)
+        throw Error("invalid argument: matrix product shape (M, N multiples of 128, K of 64)");
+    // 128 x 256 tiles where N allows (twice the work per instruction and per
+    // tile, half the tiles), else 128 x 128
+    if (N % 256 == 0) launch_gemm<256>(A, B, M, N, K, e, err, s);
+    else launch_gemm<128>(A, B, M, N, K, e, err, s);
 }
 
 double gemm_time_ms(int m, int n, int k, int reps) {
