@@ -57,7 +57,7 @@ struct Builder {
     uint64_t next_c, next_r[2];
     uint64_t num_visited = 0, visited_terminals = 0;
     uint32_t max_children = 0;
-    std::vector<uint32_t> nodes;  // subtree builders: the nodes visited (their slot entries are remapped)
+    std::vector<uint32_t> nodes;  // the nodes visited (their slot entries are remapped at the merge)
     std::vector<Visit> tasks;     // root builder: the subtrees handed out
     bool cut = false;             // root builder of a depth-limited plan
     std::vector<LeafItem> leaves;
@@ -108,7 +108,7 @@ struct Builder {
             P.node_cslot[nd] = v.cslot;
             P.node_rs[0][nd] = v.rs[0];
             P.node_rs[1][nd] = v.rs[1];
-            if (!spawn) nodes.push_back(nd);
+            nodes.push_back(nd);
             grow(v.level);
             num_visited++;
             switch (t.kind[nd]) {
@@ -515,7 +515,11 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
         P.max_children = std::max(P.max_children, b->max_children);
     }
     P.n_cslots = nc;
-    P.leaves = std::move(root.leaves);  // the root builder's slots are final
+    P.leaves = std::move(root.leaves);  // the root builder's slots are final (depth-limited plans have one shard)
+    if (nshards > 1) {  // the renumbered top part: the per-node slot table must follow it
+        for (const ActItem& a : P.act)
+            if (P.node_cslot[a.node] != a.cslot) throw Error("internal: a sharded plan's node slot table is stale");
+    }
     P.n_rslots[0] = nr[0];
     P.n_rslots[1] = nr[1];
 
