@@ -2,13 +2,15 @@
 // with fused epilogues, and the elementwise pieces of training around it
 // (packing, transposes, masked squared error, bias gradients, Adam).
 //
-// k_gemm_tn, one 128 x 128 output tile per CTA, 4 warps:
-//   * warp 0 lane 0 streams 128 x 64 tiles of A and B into a 4-stage ring of
-//     shared memory with TMA (cp.async.bulk.tensor, 128-byte swizzle), one
-//     mbarrier per stage counting the bytes;
-//   * warp 1 lane 0 issues tcgen05.mma (kind::f16, BF16 in, FP32 accumulate)
-//     into a 128-column tensor-memory accumulator, four K=16 steps per stage,
-//     and frees each stage with tcgen05.commit on its "empty" mbarrier;
+// k_gemm_tn<BN>, one 128 x BN output tile per CTA (BN = 256 where N is a
+// multiple of 256, else 128), 4 warps:
+//   * warp 0 lane 0 streams 128 x 64 tiles of A and BN x 64 tiles of B into a
+//     4-stage ring of shared memory with TMA (cp.async.bulk.tensor, 128-byte
+//     swizzle), one mbarrier per stage counting the bytes;
+//   * warp 1 lane 0 issues tcgen05.mma (kind::f16, BF16 in, FP32 accumulate,
+//     M = 128, N = BN) into a BN-column tensor-memory accumulator, four K=16
+//     steps per stage, and frees each stage with tcgen05.commit on its
+//     "empty" mbarrier;
 //   * then all four warps read their 32 accumulator lanes with tcgen05.ld and
 //     apply the epilogue (bias, pre-activation store, GELU' product, GELU,
 //     f32 / bf16 stores) straight to global memory.
