@@ -164,6 +164,7 @@ def lib():
         "gtob_gemm_bf16": (I, [P, P, I, I, I, P]),
         "gtob_gpu_new_dl": (I, [P, P, I, I, C.POINTER(P)]),
         "gtob_gpu_leaves": (I, [P, P, P, P, I, C.POINTER(I)]),
+        "gtob_spot_dl_plan": (I, [P, P, P, P, I, C.POINTER(I), P]),
         "gtob_gpu_node_sweep": (I, [P, U32, I, I, P, P, P]),
         "gtob_gpu_node_strategy": (I, [P, U32, P]),
         "gtob_gemm_time": (I, [I, I, I, I, C.POINTER(D)]),
@@ -792,6 +793,19 @@ def dl_gpu_solver(solver, net, device_format=None, engine="staged"):
     gpu.solver = solver
     gpu.net = net  # the solver holds the net too; keep the Python handle alive beside it
     return gpu
+
+
+def dl_plan(spot):
+    """The depth-limited plan of a flop spot, built on the host: (leaf nodes,
+    pots, stacks, visited mask over the tree's nodes)."""
+    n = C.c_int()
+    _check(lib().gtob_spot_dl_plan(spot._h, None, None, None, 0, C.byref(n), None))
+    nodes = np.zeros(n.value, np.uint32)
+    pot = np.zeros(n.value, np.float32)
+    stack = np.zeros(n.value, np.float32)
+    vis = np.zeros(spot.num_nodes, np.uint8)
+    _check(lib().gtob_spot_dl_plan(spot._h, _ptr(nodes), _ptr(pot), _ptr(stack), n.value, C.byref(n), _ptr(vis)))
+    return nodes, pot, stack, vis
 
 
 def dl_leaves(gpu):

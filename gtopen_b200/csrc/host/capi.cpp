@@ -442,6 +442,21 @@ int gtob_spot_shard_visited(const gtob_spot* sp, int use_iso, int shard, int nsh
     for (size_t i = 0; i < P.node_cslot.size(); i++) visited[i] = P.node_cslot[i] != kNoSlot ? 1 : 0;
     API_END
 }
+int gtob_spot_dl_plan(const gtob_spot* sp, uint32_t* nodes, float* pot, float* stack, int cap, int* n,
+                      uint8_t* visited) {
+    REQUIRE(sp && n && cap >= 0);
+    API_BEGIN
+    const Plan P = build_plan(*sp->s, false, kFuseFolds, 0, 1, true);
+    *n = (int)P.leaves.size();
+    for (int i = 0; i < std::min(cap, (int)P.leaves.size()); i++) {
+        if (nodes) nodes[i] = P.leaves[i].node;
+        if (pot) pot[i] = P.leaves[i].pot;
+        if (stack) stack[i] = P.leaves[i].stack;
+    }
+    if (visited)
+        for (size_t i = 0; i < P.node_cslot.size(); i++) visited[i] = P.node_cslot[i] != kNoSlot ? 1 : 0;
+    API_END
+}
 struct gtob_batch {
     std::vector<std::shared_ptr<Spot>> spots;
     std::vector<std::unique_ptr<gtob_solver>> solvers;  // empty entries when the batch keeps none

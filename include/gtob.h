@@ -391,6 +391,11 @@ int gtob_net_train(gtob_net* net, const float* x, const float* t, const float* m
  * net must map 2705 inputs to 2652 outputs; it serves one solver at a time.
  * The other gtob_gpu_* calls work as on any solver (save and load refuse). */
 int gtob_gpu_new_dl(const gtob_solver* solver, gtob_net* net, int device_format, int engine, gtob_gpu** out);
+/* The depth-limited plan of a flop spot without a GPU: its leaves (tree
+ * node, pot, remaining stack; *n = count) and, if visited is not NULL, one
+ * byte per tree node, 1 for the nodes its sweeps visit. */
+int gtob_spot_dl_plan(const gtob_spot* spot, uint32_t* nodes, float* pot, float* stack, int cap, int* n,
+                      uint8_t* visited);
 /* the depth-limited solver's leaves: tree node, pot, remaining stack; *n = count */
 int gtob_gpu_leaves(gtob_gpu* gpu, uint32_t* nodes, float* pot, float* stack, int cap, int* n);
 /* one evaluation sweep for player p (mode 0 best response, 1 average

@@ -3,6 +3,7 @@ rows, the zero-sum correction of the scatter's host mirror, and the claim
 the training data rests on -- below every betting turn leaf of the flop tree
 lies exactly the tree of the turn spot with that leaf's pot and stack."""
 import numpy as np
+import pytest
 
 import gtopen_b200 as g
 from gtopen_b200 import leafdata as LD
@@ -93,3 +94,28 @@ def test_leaf_values_zero_sum():
             total += float(np.dot(r, v[p]))
             scale += float(np.dot(r, np.abs(v[p])))
     assert abs(total) <= 1e-5 * scale
+
+
+def test_dl_plan_cut():
+    """The depth-limited plan visits the flop's betting, its 11 betting turn
+    leaves (not below them) and the 4 all-in runouts in full."""
+    cfg = LD.dl_flop_spot(g.evaluate7)
+    spot = g.Spot(cfg)
+    t, ch = spot.tree(), spot.children()
+    nodes, pots, stacks, vis = g.dl_plan(spot)
+    assert len(nodes) == 11
+    assert sorted(set(np.round(pots, 1))) == [100.0, 166.0, 250.0, 265.0, 475.0, 512.5]
+    half = cfg["tree"]["starting_pot"] / 2
+    for n, p_, s_ in zip(nodes, pots, stacks):
+        assert t["nchild"][n] == 52 and t["street"][n] == 1
+        assert abs(p_ - (t["put0"][n] + t["put1"][n])) < 1e-3
+        assert abs(s_ - (cfg["tree"]["effective_stack"] - (t["put0"][n] - half))) < 1e-3
+        kids = ch[t["child_start"][n]:t["child_start"][n] + 52]
+        assert not any(vis[int(c)] for c in kids if c != 0xFFFFFFFF)  # nothing below a leaf
+    v = vis.astype(bool)
+    # every visited action node bets on the flop; later-street nodes are runout
+    # chance nodes and showdowns below all-ins
+    assert np.all(t["street"][v & (t["kind"] == 0)] == 0)
+    assert np.any(v & (t["kind"] == 1) & (t["street"] == 2))  # runouts deal the river too
+    with pytest.raises(g.GtobError):
+        g.dl_plan(g.Spot(W.turn_spot(g.evaluate7)))  # a turn spot has no turn leaves to cut
