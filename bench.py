@@ -490,10 +490,7 @@ def run_leaf(args, world, rank, local):
     t_all = time.perf_counter()
     cfg = LD.dl_flop_spot(g.evaluate7)
     spot = g.Spot(cfg)
-    probe = g.dl_gpu_solver(g.Solver(spot, storage="compressed", use_iso=False),
-                            g.LeafNet(LD.LEAF_IN, 128, 1, LD.LEAF_OUT, seed=1), device_format="f32")
-    _, pots, stacks = g.dl_leaves(probe)
-    probe.close()
+    _, pots, stacks, _ = g.dl_plan(spot)  # the leaves of the host-built plan
     leaf_pots = sorted(set((float(a), float(b)) for a, b in zip(pots, stacks)))
     pool = ThreadPoolExecutor(max(1, min(16, os.cpu_count() or 1)))
     t = time.perf_counter()

@@ -71,10 +71,7 @@ def test_trained_network_gains_over_untrained():
 
     cfg = LD.dl_flop_spot(g.evaluate7)
     spot = g.Spot(cfg)
-    probe = g.dl_gpu_solver(g.Solver(spot, storage="compressed", use_iso=False),
-                            g.LeafNet(LD.LEAF_IN, 128, 1, LD.LEAF_OUT, seed=1), device_format="f32")
-    _, pots, stacks = g.dl_leaves(probe)
-    probe.close()
+    _, pots, stacks, _ = g.dl_plan(spot)  # the leaves of the host-built plan
     leaf_pots = sorted(set((float(a), float(b)) for a, b in zip(pots, stacks)))
     X, T, M, info = LD.training_set(g, cfg, leaf_pots, 256, seed=1, workers=16, build_pool=ThreadPoolExecutor(8))
     assert info["exploit_pct"].max() <= 0.3 + 1e-9
