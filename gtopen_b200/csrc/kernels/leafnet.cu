@@ -672,14 +672,20 @@ void LeafNet::forward_device(const __nv_bfloat16* x, int rows_pad, float* y, cud
 }
 
 namespace {
+// a device buffer freed when its scope ends, on error paths too
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    explicit DevBuf(size_t n) : p(dnew<T>(n)) {}
+    ~DevBuf() { cudaFree(p); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
 // host rows -> device table (n x w f32) once per call
 struct DevTable {
-    float* p = nullptr;
-    DevTable(const float* h, size_t n) {
-        p = dnew<float>(n);
-        LCK(cudaMemcpy(p, h, n * 4, cudaMemcpyHostToDevice));
-    }
-    ~DevTable() { cudaFree(p); }
+    DevBuf<float> buf;
+    float* p;
+    DevTable(const float* h, size_t n) : buf(n), p(buf.p) { LCK(cudaMemcpy(p, h, n * 4, cudaMemcpyHostToDevice)); }
 };
 }  // namespace
 
@@ -690,12 +696,12 @@ void LeafNet::forward_host(const float* x, int rows, float* y) {
     DevTable X(x, (size_t)rows * d_.din);
     std::vector<int> idx(rows);
     std::iota(idx.begin(), idx.end(), 0);
-    int* didx = dnew<int>(rows);
+    DevBuf<int> idx_buf(rows);
+    int* didx = idx_buf.p;
     LCK(cudaMemcpy(didx, idx.data(), rows * 4, cudaMemcpyHostToDevice));
     k_gather_rows_bf16<<<rp, 256, 0, stream_>>>(X.p, didx, rows, d_.din, din_p_, x_);
     forward(x_, rp, y_, false, stream_);
     check(stream_);
-    cudaFree(didx);
     LCK(cudaMemcpy2D(y, d_.dout * 4, y_, dout_p_ * 4, d_.dout * 4, rows, cudaMemcpyDeviceToHost));
 }
 
@@ -706,14 +712,14 @@ double LeafNet::gradients_host(const float* x, const float* t, const float* mask
     DevTable X(x, (size_t)rows * d_.din), T(t, (size_t)rows * d_.dout), M(mask, (size_t)rows * d_.dout);
     std::vector<int> idx(rows);
     std::iota(idx.begin(), idx.end(), 0);
-    int* didx = dnew<int>(rows);
+    DevBuf<int> idx_buf(rows);
+    int* didx = idx_buf.p;
     LCK(cudaMemcpy(didx, idx.data(), rows * 4, cudaMemcpyHostToDevice));
     k_gather_rows_bf16<<<rp, 256, 0, stream_>>>(X.p, didx, rows, d_.din, din_p_, x_);
     k_gather_rows_f32<<<rp, 256, 0, stream_>>>(T.p, didx, rows, d_.dout, dout_p_, t_);
     k_gather_rows_f32<<<rp, 256, 0, stream_>>>(M.p, didx, rows, d_.dout, dout_p_, m_);
     forward(x_, rp, y_, true, stream_);
     const double loss = backward(t_, m_, rp, rows, stream_);
-    cudaFree(didx);
     return loss;
 }
 
@@ -722,7 +728,8 @@ void LeafNet::train_host(const float* x, const float* t, const float* mask, int 
     if (n <= 0 || epochs <= 0 || batch <= 0 || batch % 128) throw Error("invalid argument: training sizes");
     ensure_rows(batch);
     DevTable X(x, (size_t)n * d_.din), T(t, (size_t)n * d_.dout), M(mask, (size_t)n * d_.dout);
-    int* didx = dnew<int>(batch);
+    DevBuf<int> idx_buf(batch);
+    int* didx = idx_buf.p;
     std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
     uint64_t s = seed * 0x9E3779B97F4A7C15ull + 1;
@@ -744,7 +751,6 @@ void LeafNet::train_host(const float* x, const float* t, const float* mask, int 
         check(stream_);
         if (losses) losses[ep] = (float)(sum / std::max(nb, 1));
     }
-    cudaFree(didx);
 }
 
 // ---------------------------------------------------------------- leaves
