@@ -343,14 +343,14 @@ __global__ void k_to_bf16(const float* __restrict__ in, size_t n, __nv_bfloat16*
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    if (!fn) {
+    // resolved once (a function-local static: thread-safe; a failed lookup is retried)
+    static const PFN_cuTensorMapEncodeTiled_v12000 fn = [] {
         void* p = nullptr;
         cudaDriverEntryPointQueryResult q;
         LCK(cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q));
         if (q != cudaDriverEntryPointSuccess || !p) throw Error("cuda: cuTensorMapEncodeTiled is not available");
-        fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
-    }
+        return (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }();
     return fn;
 }
 // a row-major bf16 matrix (rows x inner) read in 64 x box_rows boxes, 128-byte swizzle
