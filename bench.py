@@ -476,7 +476,7 @@ def run_leaf(args, world, rank, local):
     """The depth-limited configuration: turn spots of the flop solved by the
     plain engine (the training set), the leaf network trained on the device,
     depth-limited solves with the trained and an untrained network, and each
-    resulting flop strategy judged on the full tree (player p's flop locked,
+    resulting flop strategy checked on the full tree (player p's flop locked,
     the rest re-solved: p's loss of game value, % pot).  Also the tcgen05
     product's throughput against the bf16 peak."""
     import numpy as np
@@ -515,7 +515,7 @@ def run_leaf(args, world, rank, local):
     gm, gn, gk = 4096, 1024, 2816
     gms = g.gemm_time_ms(gm, gn, gk, reps=50)
     g_tflops = 2.0 * gm * gn * gk / (gms / 1000.0) / 1e12
-    judge = LD.FlopJudge(g, cfg, iterations=args.leaf_judge_iters)
+    check = LD.FullTreeCheck(g, cfg, iterations=args.leaf_check_iters)
     res = {}
     for name, n in (("trained", net), ("untrained", untrained)):
         host = g.Solver(spot, storage="compressed", use_iso=False)
@@ -528,7 +528,7 @@ def run_leaf(args, world, rank, local):
         strat = LD.dl_flop_strategies(g, dl, spot)
         kern = dl.info()["iteration_kernels"]
         dl.close()
-        l0, l1, ex = judge.loss(strat)
+        l0, l1, ex = check.loss(strat)
         res[name] = {"loss_pct_pot": [l0, l1], "loss_sum_pct_pot": l0 + l1, "locked_solve_exploit_pct": ex,
                      "dl_iterations": args.leaf_dl_iters, "dl_s": dl_s, "dl_exploit_pct_cut_game": e_cut,
                      "dl_iteration_kernels": kern}
@@ -540,7 +540,7 @@ def run_leaf(args, world, rank, local):
                                    "network 2705-1024x3-2652" % cfg["board"],
                        "training_spots": len(Xt), "validation_spots": nval},
             "trained": res["trained"], "untrained": res["untrained"],
-            "full_solve": {"iterations": judge.iterations, "exploit_pct": judge.full_exploit},
+            "full_solve": {"iterations": check.iterations, "exploit_pct": check.full_exploit},
             "training": {"spots_generated": args.leaf_spots, "generate_s": gen_s,
                          "turn_solve_exploit_pct_mean": float(info["exploit_pct"].mean()),
                          "epochs": args.leaf_epochs, "train_s": train_s, "loss_first": float(losses[0]),
@@ -585,7 +585,7 @@ def main():
     ap.add_argument("--leaf-epochs", type=int, default=60)
     ap.add_argument("--leaf-lr", type=float, default=3e-4)
     ap.add_argument("--leaf-dl-iters", type=int, default=400)
-    ap.add_argument("--leaf-judge-iters", type=int, default=400)
+    ap.add_argument("--leaf-check-iters", type=int, default=400)
     ap.add_argument("--report-flops", type=int, default=184)
     ap.add_argument("--report-workers", type=int, default=8)
     ap.add_argument("--storage", default="compressed", choices=["compressed", "f32", "fp8"])

@@ -221,8 +221,8 @@ def dl_flop_strategies(g, gpu, spot):
     return {n: g.node_strategy(gpu, n, na, pl) for n, pl, na in flop_action_nodes(spot)}
 
 
-class FlopJudge:
-    """Exact judge of a flop strategy on the full tree: player p's flop
+class FullTreeCheck:
+    """An exact check of a flop strategy on the full tree: player p's flop
     nodes locked to it, the rest of the tree solved (both players free
     everywhere else), p's game value compared with the unlocked solve's.
     The loss (% pot) is what committing to that flop strategy costs p against

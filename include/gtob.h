@@ -358,7 +358,8 @@ int gtob_gpu_read_node_static(gtob_gpu* gpu, int which, uint32_t node, float* ou
                               uint64_t* written);
 
 /* ---- the turn-leaf value network (depth-limited solves) ----------------- */
-/* No counterpart in the reference (its north star's learned leaf).  A fully
+/* No counterpart in the reference: a learned stand-in for the turn subtree
+ * at the leaves of depth-limited solves.  A fully
  * connected net: din inputs, nhidden GELU layers of dh units, dout linear
  * outputs; BF16 weights and activations, FP32 accumulation and master
  * weights, every matrix product on a hand-written tcgen05 kernel.  Training

@@ -81,14 +81,14 @@ def test_trained_network_gains_over_untrained():
     net.train(X[64:], T[64:], M[64:], epochs=20, batch=128, lr=3e-4, seed=3)
     v1 = net.gradients(X[:64], T[:64], M[:64])
     assert v1 < 0.8 * v0, (v0, v1)
-    judge = LD.FlopJudge(g, cfg, iterations=200)
+    check = LD.FullTreeCheck(g, cfg, iterations=200)
     losses = {}
     for name, n in (("trained", net), ("untrained", untrained)):
         dl = g.dl_gpu_solver(g.Solver(spot, storage="compressed", use_iso=False), n, device_format="f32")
         dl.iterate(200)
         strat = LD.dl_flop_strategies(g, dl, spot)
         dl.close()
-        l0, l1, ex = judge.loss(strat)
+        l0, l1, ex = check.loss(strat)
         assert max(ex) < 0.5, ex
         losses[name] = l0 + l1
     assert losses["trained"] < 0.5 * losses["untrained"], losses
