@@ -22,7 +22,7 @@ _LIB = None
 
 STORAGE = {"f32": 0, "compressed": 1, "i16": 1}
 ALGO = {"dcfr": 0, "cfr+": 1, "cfrplus": 1, "pcfr+": 2, "pcfrplus": 2}
-DEVICE_FORMAT = {None: -1, "follow": -1, "f32": 0, "i16": 1, "fp8": 2}
+DEVICE_FORMAT = {None: -1, "follow": -1, "f32": 0, "i16": 1, "fp8": 2, "i16sr": 3}
 NODE_SCRATCH_ELEMS = 16384  # GTOB_NODE_SCRATCH_ELEMS
 KERNEL_NAMES = ["copy_root", "down_action", "down_chance", "up_fold", "up_show", "up_chance", "up_action"]
 

@@ -67,6 +67,7 @@ struct Dev {
     // staged engine extras
     const uint32_t* hinfo[2];   // per hand: c1 | c2 << 6 | same << 16 (0xFFFF: no same combo)
     const uint16_t* hcard52[2]; // per card: the hands holding it, 52 slots, 0xFFFF after the last
+    const uint32_t* node_id[2];  // tree node id of each device action node (per player, by sidx)
 };
 struct Arenas {
     void* reg[2];
@@ -75,6 +76,7 @@ struct Arenas {
     float* rscale[2];
     float* sscale[2];
     float* pscale[2];
+    int sr;  // 16-bit requantisation: 0 round to nearest even (store.rs), 1 stochastic rounding
 };
 
 // ----------------------------------------------------------- small helpers
@@ -99,6 +101,106 @@ __device__ __forceinline__ uint16_t sat_u16(float x) {
     asm("cvt.rni.sat.u16.f32 %0, %1;" : "=h"(r) : "f"(x));
     return x != x ? (uint16_t)0 : (uint16_t)r;
 }
+// ------------------------------------------------ exact terminal sums
+// Fold and showdown values need sums of opponent reach over hand subsets
+// (game.rs:478-485, 512-575; the reference sums in f64 in one fixed order).
+// Here the sums are exact, so any summation order gives the same bits: each
+// reach value r (f32, >= 0) of one opponent vector goes on one fixed-point
+// grid, q = round-half-even(r * 2^S) in an int64, with S = 51 - E for the
+// vector's largest value < 2^E -- q < 2^51, and a sum of at most 1326 of
+// them stays below 2^62.  Sums and differences are exact integer
+// arithmetic; each difference becomes f32 once (correctly rounded, then
+// scaled by 2^-S).  The grid step is 2^-51 of the vector's top power of two,
+// about the rounding step of a running f64 sum.  Everything after the casts
+// is the reference's f32 arithmetic.
+__device__ __forceinline__ int fix_scale(float maxv) {
+    const uint32_t u = __float_as_uint(maxv);
+    const int e = (int)((u >> 23) & 0xFFu);
+    const uint32_t m = u & 0x7FFFFFu;
+    if (e == 0 && m == 0) return 0;
+    const int E = e != 0 ? e - 126 : (32 - __clz((int)m)) - 149;  // maxv < 2^E
+    return 51 - E;
+}
+__device__ __forceinline__ float pow2f(int k) { return __uint_as_float((uint32_t)(127 + k) << 23); }  // k in [-126,127]
+__device__ __forceinline__ long long fix_q(float r, int S) {  // the scalings are exact
+    float x = r;
+    if (S > 100) {
+        x = __fmul_rn(x, pow2f(100));
+        S -= 100;
+    }
+    return __float2ll_rn(__fmul_rn(x, pow2f(S)));
+}
+__device__ __forceinline__ float fix_f(long long v, int S) {
+    float y = __ll2float_rn(v);
+    if (S > 100) {
+        y = __fmul_rn(y, pow2f(-100));
+        S -= 100;
+    }
+    return __fmul_rn(y, pow2f(-S));
+}
+// Accumulator types of the terminal sums: long long = the exact sums above
+// (every engine), float = f32 sums like the reference GPU kernels (the
+// fused32 engine).  q: one reach value onto the accumulator; f: a sum back
+// to f32.  The scale argument is only used by the exact type.
+template <class T>
+struct Acc;
+template <>
+struct Acc<long long> {
+    static constexpr bool kExact = true;
+    __device__ static long long q(float r, int S) { return fix_q(r, S); }
+    __device__ static float f(long long v, int S) { return fix_f(v, S); }
+};
+template <>
+struct Acc<float> {
+    static constexpr bool kExact = false;
+    __device__ static float q(float r, int) { return r; }
+    __device__ static float f(float v, int) { return v; }
+};
+__device__ __forceinline__ long long shfl_up_ll(long long v, int x) { return __shfl_up_sync(0xffffffffu, v, x); }
+
+// Stochastic rounding of the 16-bit arenas' requantisation: x -> floor(x + u)
+// with u in [0, 1) drawn from a hash of (tree node, hand, action, iteration)
+// -- the SplitMix64 output function (Steele, Lea and Flood, "Fast splittable
+// pseudorandom number generators", 2014) over a 64-bit key -- so the stored
+// value is unbiased and increments below half a quantisation step still
+// accumulate in expectation.  The low 24 bits feed the regret, bits 40..63
+// the strategy sum.  Deterministic: the oracle draws the same numbers.
+__device__ __forceinline__ uint64_t sr_hash(uint32_t node, uint32_t hand, uint32_t action, uint32_t t) {
+    uint64_t z = (((uint64_t)node << 32) | (uint64_t)(hand << 4 | action)) + (uint64_t)t * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ float sr_u_lo(uint64_t h) { return __fmul_rn((float)(uint32_t)(h & 0xFFFFFFu), 0x1p-24f); }
+__device__ __forceinline__ float sr_u_hi(uint64_t h) { return __fmul_rn((float)(uint32_t)(h >> 40), 0x1p-24f); }
+__device__ __forceinline__ int16_t sr_i16(float x, float u) {  // floor(x + u), saturated, NaN -> 0
+    const float y = __fadd_rn(x, u);
+    short r;
+    asm("cvt.rmi.sat.s16.f32 %0, %1;" : "=h"(r) : "f"(y));
+    return y != y ? (int16_t)0 : (int16_t)r;
+}
+__device__ __forceinline__ uint16_t sr_u16(float x, float u) {
+    const float y = __fadd_rn(x, u);
+    unsigned short r;
+    asm("cvt.rmi.sat.u16.f32 %0, %1;" : "=h"(r) : "f"(y));
+    return y != y ? (uint16_t)0 : (uint16_t)r;
+}
+
+// One entry's 16-bit requantisation after an update: store.rs's round to
+// nearest even (sr = 0) or stochastic rounding keyed by (tree node, hand,
+// action, iteration).
+__device__ __forceinline__ void requant16(float nr, float ns, float rk, float sk, int sr, uint32_t node, int i, int k,
+                                          uint32_t t, int16_t* rq, uint16_t* sq) {
+    if (sr) {
+        const uint64_t h = sr_hash(node, (uint32_t)i, (uint32_t)k, t);
+        *rq = rk > 0.0f ? sr_i16(nr * rk, sr_u_lo(h)) : (int16_t)0;
+        *sq = sk > 0.0f ? sr_u16(fmaxf(ns, 0.0f) * sk, sr_u_hi(h)) : (uint16_t)0;
+    } else {
+        *rq = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
+        *sq = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
+    }
+}
+
 __device__ __forceinline__ float block_max(float v, float* sh) {  // order-independent
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     __syncthreads();
@@ -265,19 +367,29 @@ __device__ __forceinline__ void node_sigma(const Dev& d, const Arenas& ar, const
 // per dependent load level instead of one per card.
 constexpr int kCardsPerWarp = (52 + kWarps - 1) / kWarps;
 
+// Scale of the exact sums over one opponent reach vector (all threads of a
+// kThreads CTA; 0 for the f32 accumulator).  sh: kWarps floats.
 template <class T>
-__device__ T fold_sums(const Dev& d, int o, const float* ro, T* S, T* s_red) {
+__device__ __forceinline__ int vec_scale(const float* ro, int n, float* sh) {
+    if (!Acc<T>::kExact) return 0;
+    float m = 0.0f;
+    for (int j = threadIdx.x; j < n; j += blockDim.x) m = fmaxf(m, ro[j]);
+    return fix_scale(block_max(m, sh));
+}
+template <class T>
+__device__ T fold_sums(const Dev& d, int o, const float* ro, T* S, T* s_red, int& sc) {
     const int nho = d.nh[o];
+    sc = vec_scale<T>(ro, nho, (float*)s_red);
     T t = 0;
 #pragma unroll
     for (int u = 0; u < kMaxHpt; u++) {
         const int j = threadIdx.x + u * kThreads;
-        if (j < nho) t += (T)ro[j];
+        if (j < nho) t += Acc<T>::q(ro[j], sc);
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t* off = d.hcard_off[o];
     const uint16_t* idx = d.hcard_idx[o];
-    float v[kCardsPerWarp][2];
+    T v[kCardsPerWarp][2];
 #pragma unroll
     for (int ci = 0; ci < kCardsPerWarp; ci++) {
         const int c = warp + ci * kWarps;
@@ -285,13 +397,13 @@ __device__ T fold_sums(const Dev& d, int o, const float* ro, T* S, T* s_red) {
 #pragma unroll
         for (int h = 0; h < 2; h++) {
             const uint32_t k = b + lane + 32 * h;
-            v[ci][h] = k < e ? ro[idx[k]] : 0.0f;
+            v[ci][h] = k < e ? Acc<T>::q(ro[idx[k]], sc) : (T)0;
         }
     }
     const T total = block_sum<T>(t, s_red);
 #pragma unroll
     for (int ci = 0; ci < kCardsPerWarp; ci++) {
-        T s = (T)v[ci][0] + (T)v[ci][1];
+        T s = v[ci][0] + v[ci][1];
 #pragma unroll
         for (int x = 16; x > 0; x >>= 1) s += __shfl_xor_sync(0xffffffffu, s, x);
         const int c = warp + ci * kWarps;
@@ -301,12 +413,13 @@ __device__ T fold_sums(const Dev& d, int o, const float* ro, T* S, T* s_red) {
     return total;
 }
 template <class T>
-__device__ void fold_write(const Dev& d, int p, const float* ro, T total, const T* S, float amount, float* out) {
+__device__ void fold_write(const Dev& d, int p, const float* ro, T total, const T* S, int sc, float amount,
+                           float* out) {
     const int nhp = d.nh[p];
     for (int i = threadIdx.x; i < nhp; i += blockDim.x) {
         const uint32_t sm = d.same[p][i];
         const float same_r = sm != kSentinel ? ro[sm] : 0.0f;
-        const float valid = (float)(total - S[d.c1[p][i]] - S[d.c2[p][i]]) + same_r;
+        const float valid = Acc<T>::f(total - S[d.c1[p][i]] - S[d.c2[p][i]], sc) + same_r;
         out[i] = amount * valid;
     }
 }
@@ -362,11 +475,12 @@ __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* r
     T* S = Q + 2 * m + 52;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t c0 = coff[0];
+    const int sc = vec_scale<T>(ro, d.nh[o], (float*)s_w);
     if (threadIdx.x < 52) Q[(coff[threadIdx.x] - c0) + threadIdx.x] = 0;  // each card's exclusive prefix starts at 0
 #pragma unroll
     for (int u = 0; u < kMaxHpt; u++) {
         const int k = threadIdx.x + u * kThreads;
-        if (k < m) R[k] = (T)ro[sidx[k]];
+        if (k < m) R[k] = Acc<T>::q(ro[sidx[k]], sc);
     }
     __syncthreads();
     block_exclusive_scan<T>(R, P, m, s_w);
@@ -411,11 +525,11 @@ __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* r
     for (int k = threadIdx.x; k < mp; k += blockDim.x) {
         const RankEntry e = re[k];
         const int a1 = e.cards & 0xFF, a2 = e.cards >> 8;
-        const float lower = (float)(P[e.lb] - Q[e.q1lo] - Q[e.q2lo]);
-        const float higher = (float)((total - P[e.ub]) - (S[a1] - Q[e.q1hi]) - (S[a2] - Q[e.q2hi]));
+        const float lower = Acc<T>::f(P[e.lb] - Q[e.q1lo] - Q[e.q2lo], sc);
+        const float higher = Acc<T>::f((total - P[e.ub]) - (S[a1] - Q[e.q1hi]) - (S[a2] - Q[e.q2hi]), sc);
         const uint32_t sm = d.same[p][e.idx];
         const float same_r = sm != kSentinel ? ro[sm] : 0.0f;
-        const float valid = (float)(total - S[a1] - S[a2]) + same_r;
+        const float valid = Acc<T>::f(total - S[a1] - S[a2], sc) + same_r;
         const float tied = valid - lower - higher;
         out[e.idx] = win * lower + lose * higher + tie * tied;
     }
@@ -481,23 +595,26 @@ __global__ void __launch_bounds__(kThreads) k_down_chance(Dev d, const EdgeItem*
     }
 }
 
-// Plain engine terminal kernels (f64 sums): one CTA per terminal, result to its cfv slot.
+// Plain engine terminal kernels (exact sums): one CTA per terminal, result to its cfv slot.
 __global__ void __launch_bounds__(kThreads) k_fold(Dev d, const FoldItem* items, int p) {
-    __shared__ double S[52];
-    __shared__ double s_red[kWarps];
+    __shared__ long long S[52];
+    __shared__ long long s_red[kWarps];
     const FoldItem f = items[blockIdx.x];
     const int o = 1 - p;
     const float* ro = d.reach[o] + (size_t)f.rs[o] * d.rstr[o];
-    const double total = fold_sums<double>(d, o, ro, S, s_red);
-    fold_write<double>(d, p, ro, total, S, (int)f.folder == p ? f.tlose : f.twin, d.cfv + (size_t)f.cslot * d.nh_max);
+    int sc;
+    const long long total = fold_sums<long long>(d, o, ro, S, s_red, sc);
+    fold_write<long long>(d, p, ro, total, S, sc, (int)f.folder == p ? f.tlose : f.twin,
+                          d.cfv + (size_t)f.cslot * d.nh_max);
 }
 __global__ void __launch_bounds__(kThreads) k_showdown(Dev d, const ShowItem* items, int p) {
-    extern __shared__ double sh[];
-    __shared__ double s_w[kWarps];
+    extern __shared__ long long sh[];
+    __shared__ long long s_w[kWarps];
     const ShowItem s = items[blockIdx.x];
     const int o = 1 - p;
     const float* ro = d.reach[o] + (size_t)s.rs[o] * d.rstr[o];
-    eval_showdown<double>(d, p, s.slot, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, sh, s_w);
+    eval_showdown<long long>(d, p, s.slot, ro, s.twin, s.tlose, s.ttie, d.cfv + (size_t)s.cslot * d.nh_max, sh,
+                             s_w);
 }
 
 // Chance node (cfr.rs:637-663): sum of representative children through the
@@ -612,6 +729,7 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
             __syncthreads();
         }
         TT total = 0;
+        int fsc = 0;
         bool have_sums = false;
         int t = 0;
         for (int k = 0; k < na; k++) {
@@ -621,9 +739,9 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
             const TermInfo tm = d.terms[c.term];
             float* dst = tv + (size_t)t * d.nh_pad;
             if (c.kind == kChildFold) {
-                if (!have_sums) total = fold_sums<TT>(d, o, rk, s_S, s_redt);
+                if (!have_sums) total = fold_sums<TT>(d, o, rk, s_S, s_redt, fsc);
                 have_sums = a == p;  // every terminal below my own node shares one opponent reach
-                fold_write<TT>(d, p, rk, total, s_S, (int)tm.aux == p ? tm.tlose : tm.twin, dst);
+                fold_write<TT>(d, p, rk, total, s_S, fsc, (int)tm.aux == p ? tm.tlose : tm.twin, dst);
                 __syncthreads();
             } else {
                 eval_showdown<TT>(d, p, tm.aux, rk, tm.twin, tm.tlose, tm.ttie, dst, scr, s_redt);
@@ -712,6 +830,7 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
     int16_t* PQ = (int16_t*)ar.pred[p];
     const float kr = ar.rscale[p][it.sidx] / 32767.0f;
     const float kss = ar.sscale[p][it.sidx] / 65535.0f * ds;
+    const uint32_t t_sr = ar.sr ? *d.iter : 0u;
     float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
     for (int pass = 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
@@ -745,8 +864,7 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
                         smax = fmaxf(smax, ns);
                         if (PQ) pmax = fmaxf(pmax, fabsf(v[k] - o_));
                     } else {
-                        RQ[b + k] = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
-                        SQ[b + k] = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
+                        requant16(nr, ns, rk, sk, ar.sr, it.node, i, k, t_sr, &RQ[b + k], &SQ[b + k]);
                         if (PQ) PQ[b + k] = pk > 0.0f ? sat_i16((v[k] - o_) * pk) : (int16_t)0;
                     }
                 }
@@ -779,35 +897,40 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
-// Fold summary of one opponent reach vector by one warp (game.rs:478-485):
-// the total (lane-strided f64 partials, fixed tree) and the 52 per-card sums
-// (lane c and lane c + 32 each sum card c's hand list sequentially in hand
-// order -- the reference CPU engine's order).  S: 52 doubles private to the warp.
-__device__ double warp_fold_sums(const Dev& d, int o, const float* ro, double* S) {
+// Fold summary of one opponent reach vector by one warp (game.rs:478-485),
+// exact sums: the vector's grid scale (warp max), the total and the 52
+// per-card sums (lane c and lane c + 32 each sum card c's hand list).  S: 52
+// entries private to the warp.
+__device__ long long warp_fold_sums(const Dev& d, int o, const float* ro, long long* S, int& sc) {
     const int lane = threadIdx.x & 31, nho = d.nh[o];
-    double t = 0.0;
+    float mx = 0.0f;
+    for (int j = lane; j < nho; j += 32) mx = fmaxf(mx, ro[j]);
+    sc = fix_scale(warp_max(mx));
+    long long t = 0;
 #pragma unroll 4
-    for (int j = lane; j < nho; j += 32) t += (double)ro[j];
+    for (int j = lane; j < nho; j += 32) t += fix_q(ro[j], sc);
 #pragma unroll
     for (int cc = 0; cc < 2; cc++) {
         const int c = lane + 32 * cc;
         if (c < 52) {
             const uint32_t b = d.hcard_off[o][c], e = d.hcard_off[o][c + 1];
-            double s = 0.0;
+            long long s = 0;
 #pragma unroll 4
-            for (uint32_t k = b; k < e; k++) s += (double)ro[d.hcard_idx[o][k]];
+            for (uint32_t k = b; k < e; k++) s += fix_q(ro[d.hcard_idx[o][k]], sc);
             S[c] = s;
         }
     }
     __syncwarp();
-    return warp_sum(t);
+#pragma unroll
+    for (int x = 16; x > 0; x >>= 1) t += __shfl_xor_sync(0xffffffffu, t, x);
+    return t;
 }
 // One hand's fold value from the warp's summary.
-__device__ __forceinline__ float fold_value(const Dev& d, int p, int i, const float* ro, double total, const double* S,
-                                            float amount) {
+__device__ __forceinline__ float fold_value(const Dev& d, int p, int i, const float* ro, long long total,
+                                            const long long* S, int sc, float amount) {
     const uint32_t sm = d.same[p][i];
     const float same_r = sm != kSentinel ? ro[sm] : 0.0f;
-    return amount * ((float)(total - S[d.c1[p][i]] - S[d.c2[p][i]]) + same_r);
+    return amount * (fix_f(total - S[d.c1[p][i]] - S[d.c2[p][i]], sc) + same_r);
 }
 
 #define WARP_ITEM(count)                                              \
@@ -839,16 +962,17 @@ __global__ void __launch_bounds__(kThreads) kw_down_action(Dev d, Arenas ar, con
 
 // Plain-layout fold terminal, one warp per fold: result to its cfv slot.
 __global__ void __launch_bounds__(kThreads) kw_fold(Dev d, const FoldItem* items, int count, int p) {
-    __shared__ double s_S[kWarps][52];
+    __shared__ long long s_S[kWarps][52];
     WARP_ITEM(count)
     const FoldItem f = items[wid];
     const int o = 1 - p;
     const float* ro = d.reach[o] + (size_t)f.rs[o] * d.rstr[o];
-    double* S = s_S[threadIdx.x >> 5];
-    const double total = warp_fold_sums(d, o, ro, S);
+    long long* S = s_S[threadIdx.x >> 5];
+    int sc;
+    const long long total = warp_fold_sums(d, o, ro, S, sc);
     const float amount = (int)f.folder == p ? f.tlose : f.twin;
     float* out = d.cfv + (size_t)f.cslot * d.nh_max;
-    for (int i = lane; i < d.nh[p]; i += 32) out[i] = fold_value(d, p, i, ro, total, S, amount);
+    for (int i = lane; i < d.nh[p]; i += 32) out[i] = fold_value(d, p, i, ro, total, S, sc, amount);
 }
 
 // Up sweep, action nodes, one warp per node.  Fold children are evaluated in
@@ -861,7 +985,7 @@ template <int FMT, int EVAL, int KA>
 __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const ActItem* items, int count, int p,
                                                          int mode) {
     extern __shared__ float wsm[];
-    __shared__ double s_S[kWarps][52];
+    __shared__ long long s_S[kWarps][52];
     WARP_ITEM(count)
     const int w = threadIdx.x >> 5;
     const ActItem it = items[wid];
@@ -884,8 +1008,9 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
     }
     const long long loff = d.lock_off[a][it.sidx];
     float sig[KA];
-    double ftotal = 0.0;
-    const double* S = s_S[w];
+    long long ftotal = 0;
+    int fsc = 0;
+    const long long* S = s_S[w];
     const float* fro = nullptr;
     if (fk >= 0) {
         const float* ro = d.reach[o] + (size_t)(a == o ? it.rslot : it.oslot) * d.rstr[o];
@@ -903,12 +1028,13 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
             __syncwarp();
             fro = rf;
         }
-        ftotal = warp_fold_sums(d, o, fro, s_S[w]);
+        ftotal = warp_fold_sums(d, o, fro, s_S[w], fsc);
     }
     float* out = d.cfv + (size_t)it.cslot * d.nh_max;
     const float* cfv = d.cfv;
     const size_t stride = (size_t)d.nh_max;
-#define CHILD_V(k, i) ((k) == fk ? fold_value(d, p, (i), fro, ftotal, S, famount) : cfv[(size_t)cs[k] * stride + (i)])
+#define CHILD_V(k, i) \
+    ((k) == fk ? fold_value(d, p, (i), fro, ftotal, S, fsc, famount) : cfv[(size_t)cs[k] * stride + (i)])
     if (a != p) {  // opponent node: sum of children
         for (int i = lane; i < nh; i += 32) {
             float acc = 0.0f;
@@ -988,6 +1114,7 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
     int16_t* PQ = (int16_t*)ar.pred[p];
     const float kr = ar.rscale[p][it.sidx] / 32767.0f;
     const float kss = ar.sscale[p][it.sidx] / 65535.0f * ds;
+    const uint32_t t_sr = ar.sr ? *d.iter : 0u;
     float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
     for (int pass = 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
@@ -1021,8 +1148,7 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
                         smax = fmaxf(smax, ns);
                         if (PQ) pmax = fmaxf(pmax, fabsf(v[k] - o_));
                     } else {
-                        RQ[b + k] = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
-                        SQ[b + k] = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
+                        requant16(nr, ns, rk, sk, ar.sr, it.node, i, k, t_sr, &RQ[b + k], &SQ[b + k]);
                         if (PQ) PQ[b + k] = pk > 0.0f ? sat_i16((v[k] - o_) * pk) : (int16_t)0;
                     }
                 }

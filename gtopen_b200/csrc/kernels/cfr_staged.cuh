@@ -265,38 +265,51 @@ __device__ __forceinline__ void s_block_max3(float& a, float& b, float& c, float
     }
 }
 
-// Fold summary of a staged opponent reach vector (game.rs:478-485): total
-// and per-card sums in f64, each a fixed-order sum.  Threads 2c and 2c+1 sum
-// the even and odd entries of card c's hand list (ascending hand index; the
-// list ends at the first 0xFFFF) and add the two halves; the total is a
-// fixed-tree block sum.
-__device__ double s_fold_sums(const Dev& d, int o, const float* ro, double* S, double* s_red) {
+// Fold summary of a staged opponent reach vector (game.rs:478-485), exact
+// sums (cfr_kernels.cuh): the vector's grid scale, the total and the
+// per-card sums.  Threads 2c and 2c+1 sum the even and odd entries of card
+// c's hand list (the list ends at the first 0xFFFF) and add the two halves.
+// s_red: kSWarps entries; returns the total, *sc the scale.
+__device__ long long s_fold_sums(const Dev& d, int o, const float* ro, long long* S, long long* s_red, int* sc_out) {
     const int nho = d.nh[o];
-    double t = 0.0;
-    for (int j = threadIdx.x; j < nho; j += kSThreads) t += (double)ro[j];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float mx = 0.0f;
+    for (int j = threadIdx.x; j < nho; j += kSThreads) mx = fmaxf(mx, ro[j]);
+    mx = warp_max(mx);
+    float* fred = (float*)s_red;
+    if (lane == 0) fred[warp] = mx;
+    __syncthreads();
+    mx = fred[0];
+#pragma unroll
+    for (int k = 1; k < kSWarps; k++) mx = fmaxf(mx, fred[k]);
+    const int sc = fix_scale(mx);
+    long long t = 0;
+    for (int j = threadIdx.x; j < nho; j += kSThreads) t += fix_q(ro[j], sc);
     if (threadIdx.x < 104) {  // warps 0..3, whole lane pairs
         const int c = threadIdx.x >> 1, par = threadIdx.x & 1;
         const uint16_t* idx = d.hcard52[o] + c * 52 + par;
-        double s = 0.0;
+        long long s = 0;
         for (int k = 0; k + par < 52; k += 8) {  // index loads first, then the sums
             uint16_t x[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) x[u] = k + 2 * u + par < 52 ? idx[k + 2 * u] : (uint16_t)0xFFFFu;
 #pragma unroll
             for (int u = 0; u < 4; u++)
-                if (x[u] != 0xFFFFu) s += (double)ro[x[u]];
+                if (x[u] != 0xFFFFu) s += fix_q(ro[x[u]], sc);
             if (x[3] == 0xFFFFu) break;
         }
         s += __shfl_xor_sync(0xffffffffu >> (threadIdx.x >= 96 ? 24 : 0), s, 1);
         if (par == 0) S[c] = s;
     }
-    t = warp_sum(t);
+#pragma unroll
+    for (int x = 16; x > 0; x >>= 1) t += __shfl_xor_sync(0xffffffffu, t, x);
+    __syncthreads();  // everyone has read fred before it is reused as the totals
     if (lane == 0) s_red[warp] = t;
     __syncthreads();
-    double total = 0.0;
+    long long total = 0;
 #pragma unroll
     for (int k = 0; k < kSWarps; k++) total += s_red[k];
+    *sc_out = sc;
     return total;
 }
 
@@ -433,16 +446,16 @@ __global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const SNo
 // reach; every other child's cfv is staged from its slot.
 struct UpShared {  // static shared memory of ks_up
     int flag;
-    double S[52];
-    double dred[kSWarps];
+    long long S[52];
+    long long dred[kSWarps];
     float red[3 * kSWarps];
 };
 template <int FMT, int EVAL, int NA, bool MINE>
 __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const SNode& it, int p, int mode,
                                            unsigned char* sm, UpShared& us) {
     int& s_flag = us.flag;
-    double* s_S = us.S;
-    double* s_dred = us.dred;
+    long long* s_S = us.S;
+    long long* s_dred = us.dred;
     float* s_red = us.red;
     const int a = (int)it.actor, o = 1 - p, nh = d.nh[p], nho = d.nh[o];
     constexpr int na = NA;  // the node's action count, a compile-time constant in this instance
@@ -515,9 +528,10 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     if (!wait_staged(d, bar, &s_flag)) return;
 
     float sig[kSKA];
-    double ftotal = 0.0;
+    long long ftotal = 0;
     if (fk >= 0) {
-        ftotal = s_fold_sums(d, o, ro, s_S, s_dred);
+        int fsc;
+        ftotal = s_fold_sums(d, o, ro, s_S, s_dred, &fsc);
         // the fold child's values go where a staged child's cfv would be
         // (fold_value of cfr_kernels.cuh with the hand's cards and same combo
         // packed in one word)
@@ -525,7 +539,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
             const uint32_t h = d.hinfo[p][i];
             const uint32_t sm_ = h >> 16;
             const float same_r = sm_ != 0xFFFFu ? ro[sm_] : 0.0f;
-            cv[fk * vstride + i] = famount * ((float)(ftotal - s_S[h & 63u] - s_S[(h >> 6) & 63u]) + same_r);
+            cv[fk * vstride + i] = famount * (fix_f(ftotal - s_S[h & 63u] - s_S[(h >> 6) & 63u], fsc) + same_r);
         }
         __syncthreads();
     }
@@ -651,6 +665,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
         s_block_max3(rmax, smax, pmax, s_red);
         const float rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
         const float sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
+        const uint32_t nid = ar.sr ? d.node_id[p][it.sidx] : 0u, t_sr = ar.sr ? *d.iter : 0u;
         for (int i = threadIdx.x; i < nh; i += kSThreads) {
             const int b = i * na;
 #pragma unroll
@@ -658,8 +673,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
                 if (k < na) {
                     const float nr = cv[k * vstride + i];
                     const float ns = __uint_as_float((uint32_t)SQ_lo[b + k] | ((uint32_t)SQ[b + k] << 16));
-                    RQ[b + k] = rk > 0.0f ? sat_i16(nr * rk) : (int16_t)0;
-                    SQ[b + k] = sk > 0.0f ? sat_u16(fmaxf(ns, 0.0f) * sk) : (uint16_t)0;
+                    requant16(nr, ns, rk, sk, ar.sr, nid, i, k, t_sr, &RQ[b + k], &SQ[b + k]);
                 }
         }
     }
@@ -669,6 +683,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     typename Q::R* RQ = (typename Q::R*)b_reg;
     typename Q::S* SQ = (typename Q::S*)b_str;
     typename Q::R* PQ = (typename Q::R*)b_pred;
+    const uint32_t nid2 = ar.sr && !one_pass ? d.node_id[p][it.sidx] : 0u, t_sr2 = ar.sr && !one_pass ? *d.iter : 0u;
     for (int pass = one_pass ? 2 : 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
         if (pass == 1) {
@@ -699,8 +714,13 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
                         smax = fmaxf(smax, ns);
                         if (use_pred) pmax = fmaxf(pmax, fabsf(v[k] - o_));
                     } else {
-                        RQ[b + k] = rk > 0.0f ? Q::er(nr * rk) : (typename Q::R)0;
-                        SQ[b + k] = sk > 0.0f ? Q::es(fmaxf(ns, 0.0f) * sk) : (typename Q::S)0;
+                        if (FMT == kDevI16) {
+                            requant16(nr, ns, rk, sk, ar.sr, nid2, i, k, t_sr2, (int16_t*)&RQ[b + k],
+                                      (uint16_t*)&SQ[b + k]);
+                        } else {
+                            RQ[b + k] = rk > 0.0f ? Q::er(nr * rk) : (typename Q::R)0;
+                            SQ[b + k] = sk > 0.0f ? Q::es(fmaxf(ns, 0.0f) * sk) : (typename Q::S)0;
+                        }
                         if (use_pred) PQ[b + k] = pk > 0.0f ? Q::er((v[k] - o_) * pk) : (typename Q::R)0;
                     }
                 }
@@ -735,21 +755,37 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode
 
 // ------------------------------------------------- batched showdowns
 // One CTA per batch of up to kShowBatch showdowns of one level that share a
-// river slot: the slot's opponent strength order and per-card position lists
-// are loaded into shared memory once (the rank entries are read in place and
-// stay in L1 across the batch), and the showdowns' opponent reach vectors
-// stream through two bulk-copy buffers.
+// river slot (game.rs:501-577 with the plan's rank tables).  The slot's
+// tables go to shared memory once per batch -- the opponent hands in strength
+// order, the 52 card lists (each the board's opponent hands holding the card,
+// in strength order) as the hand and card of every entry -- and the
+// showdowns' opponent reach vectors stream through two double-buffered
+// bulk-copy stages, two showdowns at a time.
+//
+// Per pair, with exact sums (cfr_kernels.cuh):
+//   1. the two vectors' grid scales (block max);
+//   2. ONE segmented scan over the concatenation [strength order (m entries)
+//      | card lists (2m entries)], every thread taking a contiguous chunk:
+//      a serial scan of its chunk, a shuffle scan of the chunks' (segment
+//      seen, sum) pairs, the warps' carries through shared memory, and a
+//      pass adding the carry to the chunk's entries before its first segment
+//      start.  Output U: U[k] = reach of the k weakest opponent hands (k in
+//      0..m), then card c's prefixes at msort + 1 + qbase(c) + j (the
+//      layout the rank entries index);
+//   3. per hand of mine, its rank entry's eight prefix values.
+// Every thread works in every phase, with four block barriers per pair.
 struct ShowTab {  // one slot's tables: shared-memory copies, or HBM for the last three
-    const uint16_t* sidx;  // m opponent hands, ascending strength (shared)
-    const uint32_t* coff;  // 53 card-list offsets relative to the slot's first entry (shared)
-    const uint16_t* bpos;  // per-card sorted positions, ne entries (shared)
+    const uint16_t* sidx;   // m opponent hands, ascending strength
+    const uint32_t* coff;   // 53 card-list offsets relative to the slot's first entry
+    const uint16_t* hidx;   // the opponent hand of each card-list entry (ne = 2m entries)
+    const uint8_t* ccard;   // the card of each card-list entry
     const RankEntry* rank;  // mp entries (global, L1-resident across the batch)
-    const uint16_t* zero;  // nz blocked traverser hands (global)
-    const uint32_t* same;  // traverser same-combo map, nh entries (global)
-    int m, mp, nz;
+    const uint16_t* zero;   // nz blocked traverser hands (global)
+    const uint32_t* same;   // traverser same-combo map, nh entries (global)
+    int m, ne, mp, nz;
 };
 struct ShowTabLayout {  // byte offsets of the tables inside the table region
-    unsigned sidx, coff, bpos, total;
+    unsigned sidx, coff, hidx, ccard, total;
 };
 __host__ __device__ inline unsigned r16u(unsigned b) { return (b + 15u) & ~15u; }
 __host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad) {
@@ -759,8 +795,10 @@ __host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad) {
     o += r16u(2u * nh_pad);
     L.coff = o;
     o += r16u(53u * 4u);
-    L.bpos = o;
+    L.hidx = o;
     o += r16u(4u * nh_pad);
+    L.ccard = o;
+    o += r16u(2u * nh_pad);
     L.total = o;
     return L;
 }
@@ -772,20 +810,27 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
     tb.m = (int)d.sorted_cnt[o][slot];
     const uint32_t* coff_g = d.ccard_off[o] + (size_t)slot * 53;
     const uint32_t c0 = coff_g[0];
-    const uint32_t ne = coff_g[52] - c0;
+    tb.ne = (int)(coff_g[52] - c0);
     tb.mp = (int)d.rank_cnt[p][slot];
     const uint32_t z0 = d.zero_off[p][slot];
     tb.nz = (int)(d.zero_off[p][slot + 1] - z0);
     uint16_t* t_sidx = (uint16_t*)(tabs + TL.sidx);
     uint32_t* t_coff = (uint32_t*)(tabs + TL.coff);
-    uint16_t* t_bpos = (uint16_t*)(tabs + TL.bpos);
+    uint16_t* t_hidx = (uint16_t*)(tabs + TL.hidx);
+    uint8_t* t_card = (uint8_t*)(tabs + TL.ccard);
     const uint16_t* g_sidx = d.sorted_idx[o] + d.sorted_off[o][slot];
     for (int k = threadIdx.x; k < tb.m; k += blockDim.x) t_sidx[k] = g_sidx[k];
     if (threadIdx.x < 53) t_coff[threadIdx.x] = coff_g[threadIdx.x] - c0;
-    for (uint32_t k = threadIdx.x; k < ne; k += blockDim.x) t_bpos[k] = d.ccard_pos[o][c0 + k];
+    const uint16_t* g_pos = d.ccard_pos[o] + c0;
+    const uint8_t* g_card = d.ccard_card[o] + c0;
+    for (int k = threadIdx.x; k < tb.ne; k += blockDim.x) {
+        t_hidx[k] = g_sidx[g_pos[k]];
+        t_card[k] = g_card[k];
+    }
     tb.sidx = t_sidx;
     tb.coff = t_coff;
-    tb.bpos = t_bpos;
+    tb.hidx = t_hidx;
+    tb.ccard = t_card;
     // read in place (L1-resident across the batch): keeps the CTA's shared
     // memory small, so more batches run per SM
     tb.rank = d.rank[p] + d.rank_off[p][slot];
@@ -793,130 +838,162 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
     tb.same = d.same[p];
 }
 
-// Showdown CTAs have NT threads: 256 for large hand lists, 128 for small ones.
+// Entry f of the concatenated scan input: its opponent hand, whether it
+// starts a segment, and its output index in U.
+__device__ __forceinline__ void show_entry(const ShowTab& tb, int msort, int f, int& h, bool& head, int& oi) {
+    if (f < tb.m) {
+        h = tb.sidx[f];
+        head = f == 0;
+        oi = f + 1;
+    } else {
+        const int t = f - tb.m, c = tb.ccard[t];
+        h = tb.hidx[t];
+        head = t == (int)tb.coff[c];
+        oi = msort + 2 + t + c;
+    }
+}
 
-// ------------------------------------------- showdowns two at a time
-// Two showdowns of one batch evaluated together by the CTA (game.rs:501-577
-// with the rank tables): they share the board's tables, so every index load,
-// rank-entry decode and address computation is done once for both, and the
-// two reach / prefix values travel as pairs (float2 / double2) in one
-// shared-memory access.  Per showdown: R = opponent reach in strength order;
-// then, at the same time, Q = per-card prefixes (threads 0..51 each run one
-// card's list in strength order, as the reference's running card sums do) and
-// P = R's exclusive prefix (threads 64..NT-1: contiguous chunks, a shuffle
-// scan, the warp totals); then the rank entries.
+// Showdown CTAs have NT threads: 256 for large hand lists, 128 for small ones.
 template <int NT>
-__device__ void cta_showdown2(const ShowTab& tb, const float* roA, const float* roB, const ShowItem& ia,
-                              const ShowItem& ib, float* outA, float* outB, float2* R, double2* P, double2* Q,
-                              double2* S, double2* s_w) {
-    constexpr int kPT = NT - 64;  // P threads
+__device__ void cta_showdown2(const ShowTab& tb, int nho, int msort, const float* roA, const float* roB,
+                              const ShowItem& ia, const ShowItem& ib, float* outA, float* outB, longlong2* U,
+                              longlong2* s_w, int* s_wf, float2* s_mx) {
+    constexpr int kW = NT / 32;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int m = tb.m;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = threadIdx.x; k < m; k += NT) {
-        const int h = tb.sidx[k];
-        R[k] = make_float2(roA[h], roB[h]);
+    // 1. grid scales of the two vectors
+    float mxA = 0.0f, mxB = 0.0f;
+    for (int j = tid; j < nho; j += NT) {
+        mxA = fmaxf(mxA, roA[j]);
+        mxB = fmaxf(mxB, roB[j]);
+    }
+    mxA = warp_max(mxA);
+    mxB = warp_max(mxB);
+    if (lane == 0) s_mx[warp] = make_float2(mxA, mxB);
+    __syncthreads();
+    mxA = s_mx[0].x;
+    mxB = s_mx[0].y;
+#pragma unroll
+    for (int k = 1; k < kW; k++) {
+        mxA = fmaxf(mxA, s_mx[k].x);
+        mxB = fmaxf(mxB, s_mx[k].y);
+    }
+    const int scA = fix_scale(mxA), scB = fix_scale(mxB);
+    // 2. segmented scan, chunk [f0, f1) per thread
+    const int F = m + tb.ne;
+    const int chunk = (F + NT - 1) / NT;
+    const int f0 = min(tid * chunk, F), f1 = min(f0 + chunk, F);
+    long long ax = 0, ay = 0;
+    bool seen = false;
+    for (int f = f0; f < f1; f++) {
+        int h, oi;
+        bool head;
+        show_entry(tb, msort, f, h, head, oi);
+        if (head) {
+            ax = 0;
+            ay = 0;
+            seen = true;
+        }
+        ax += fix_q(roA[h], scA);
+        ay += fix_q(roB[h], scB);
+        U[oi] = make_longlong2(ax, ay);
+    }
+    if (tid == 0) U[0] = make_longlong2(0, 0);
+    if (tid < 52) U[msort + 1 + tb.coff[tid] + tid] = make_longlong2(0, 0);
+    bool fl = seen;
+    long long sx = ax, sy = ay;
+#pragma unroll
+    for (int x = 1; x < 32; x <<= 1) {
+        const int fu = __shfl_up_sync(0xffffffffu, (int)fl, x);
+        const long long ux = __shfl_up_sync(0xffffffffu, sx, x);
+        const long long uy = __shfl_up_sync(0xffffffffu, sy, x);
+        if (lane >= x) {
+            if (!fl) {
+                sx += ux;
+                sy += uy;
+            }
+            fl = fl || fu;
+        }
+    }
+    int ef = __shfl_up_sync(0xffffffffu, (int)fl, 1);
+    long long ex = __shfl_up_sync(0xffffffffu, sx, 1), ey = __shfl_up_sync(0xffffffffu, sy, 1);
+    if (lane == 0) {
+        ef = 0;
+        ex = 0;
+        ey = 0;
+    }
+    if (lane == 31) {
+        s_w[warp] = make_longlong2(sx, sy);
+        s_wf[warp] = (int)fl;
     }
     __syncthreads();
-    const int pt = (int)threadIdx.x - 64, pw = warp - 2;
-    const int chunk = (m + kPT - 1) / kPT;
-    const int lo = pt >= 0 ? min(pt * chunk, m) : 0, hi = pt >= 0 ? min(lo + chunk, m) : 0;
-    double lx = 0.0, ly = 0.0, ix = 0.0, iy = 0.0;
-    if (pt >= 0) {
-        for (int k = lo; k < hi; k++) {
-            const float2 r = R[k];
-            lx += (double)r.x;
-            ly += (double)r.y;
+    long long cx = 0, cy = 0;
+    for (int k = 0; k < warp; k++) {
+        if (s_wf[k]) {
+            cx = s_w[k].x;
+            cy = s_w[k].y;
+        } else {
+            cx += s_w[k].x;
+            cy += s_w[k].y;
         }
-        ix = lx;
-        iy = ly;
-#pragma unroll
-        for (int x = 1; x < 32; x <<= 1) {
-            const double yx = __shfl_up_sync(0xffffffffu, ix, x);
-            const double yy = __shfl_up_sync(0xffffffffu, iy, x);
-            if (lane >= x) {
-                ix += yx;
-                iy += yy;
-            }
+    }
+    if (ef) {
+        cx = ex;
+        cy = ey;
+    } else {
+        cx += ex;
+        cy += ey;
+    }
+    if (cx | cy) {
+        for (int f = f0; f < f1; f++) {
+            int h, oi;
+            bool head;
+            show_entry(tb, msort, f, h, head, oi);
+            if (head) break;
+            longlong2 v = U[oi];
+            v.x += cx;
+            v.y += cy;
+            U[oi] = v;
         }
-        if (lane == 31) s_w[pw] = make_double2(ix, iy);
-    } else if (threadIdx.x < 52) {
-        const int c = threadIdx.x;
-        const uint32_t b = tb.coff[c], e = tb.coff[c + 1];
-        double qx = 0.0, qy = 0.0;
-        Q[b + c] = make_double2(0.0, 0.0);
-        uint32_t t = b;
-        for (; t + 4 <= e; t += 4) {
-            float2 r[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) r[u] = R[tb.bpos[t + u]];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                qx += (double)r[u].x;
-                qy += (double)r[u].y;
-                Q[t + u + c + 1] = make_double2(qx, qy);
-            }
-        }
-        for (; t < e; t++) {
-            const float2 r = R[tb.bpos[t]];
-            qx += (double)r.x;
-            qy += (double)r.y;
-            Q[t + c + 1] = make_double2(qx, qy);
-        }
-        S[c] = make_double2(qx, qy);
     }
     __syncthreads();
-    if (pt >= 0) {
-        double wx = 0.0, wy = 0.0;
-#pragma unroll
-        for (int k = 0; k < kPT / 32; k++)
-            if (k < pw) {
-                wx += s_w[k].x;
-                wy += s_w[k].y;
-            }
-        double rx = wx + (ix - lx), ry = wy + (iy - ly);
-        for (int k = lo; k < hi; k++) {
-            P[k] = make_double2(rx, ry);
-            const float2 r = R[k];
-            rx += (double)r.x;
-            ry += (double)r.y;
-        }
-        if (threadIdx.x == NT - 1) P[m] = make_double2(rx, ry);
-    }
-    __syncthreads();
-    const double2 total = P[m];
-    for (int k = threadIdx.x; k < tb.mp; k += NT) {
+    // 3. the rank entries of my hands
+    const longlong2 total = U[m];
+    const longlong2* Q = U + msort + 1;
+    for (int k = tid; k < tb.mp; k += NT) {
         const RankEntry e = tb.rank[k];
         const int a1 = e.cards & 0xFF, a2 = e.cards >> 8;
-        const double2 plb = P[e.lb], pub = P[e.ub], q1lo = Q[e.q1lo], q2lo = Q[e.q2lo], q1hi = Q[e.q1hi],
-                      q2hi = Q[e.q2hi], s1 = S[a1], s2 = S[a2];
+        const longlong2 plb = U[e.lb], pub = U[e.ub], q1lo = Q[e.q1lo], q2lo = Q[e.q2lo], q1hi = Q[e.q1hi],
+                        q2hi = Q[e.q2hi], s1 = Q[tb.coff[a1 + 1] + a1], s2 = Q[tb.coff[a2 + 1] + a2];
         const uint32_t sm = tb.same[e.idx];
         {
-            const float lower = (float)(plb.x - q1lo.x - q2lo.x);
-            const float higher = (float)((total.x - pub.x) - (s1.x - q1hi.x) - (s2.x - q2hi.x));
+            const float lower = fix_f(plb.x - q1lo.x - q2lo.x, scA);
+            const float higher = fix_f((total.x - pub.x) - (s1.x - q1hi.x) - (s2.x - q2hi.x), scA);
             const float same_r = sm != kSentinel ? roA[sm] : 0.0f;
-            const float valid = (float)(total.x - s1.x - s2.x) + same_r;
+            const float valid = fix_f(total.x - s1.x - s2.x, scA) + same_r;
             const float tied = valid - lower - higher;
             outA[e.idx] = ia.twin * lower + ia.tlose * higher + ia.ttie * tied;
         }
         if (outB) {
-            const float lower = (float)(plb.y - q1lo.y - q2lo.y);
-            const float higher = (float)((total.y - pub.y) - (s1.y - q1hi.y) - (s2.y - q2hi.y));
+            const float lower = fix_f(plb.y - q1lo.y - q2lo.y, scB);
+            const float higher = fix_f((total.y - pub.y) - (s1.y - q1hi.y) - (s2.y - q2hi.y), scB);
             const float same_r = sm != kSentinel ? roB[sm] : 0.0f;
-            const float valid = (float)(total.y - s1.y - s2.y) + same_r;
+            const float valid = fix_f(total.y - s1.y - s2.y, scB) + same_r;
             const float tied = valid - lower - higher;
             outB[e.idx] = ib.twin * lower + ib.tlose * higher + ib.ttie * tied;
         }
     }
-    for (int z = threadIdx.x; z < tb.nz; z += NT) {
+    for (int z = tid; z < tb.nz; z += NT) {
         outA[tb.zero[z]] = 0.0f;
         if (outB) outB[tb.zero[z]] = 0.0f;
     }
     __syncthreads();
 }
 // Shared memory of ks_show_pair: two barriers, four reach buffers (two
-// stages of a pair), R pairs, P/Q/S pairs, then the slot tables.
+// stages of a pair), the prefix array U (3 msort + 53 pairs), then the slot
+// tables.
 __host__ __device__ inline unsigned show_pair_scratch_bytes(int nh_pad, int msort) {
-    return 32u + 4u * 4u * (unsigned)nh_pad + r16u(8u * (unsigned)msort) + (3u * (unsigned)msort + 105u) * 16u;
+    return 32u + 4u * 4u * (unsigned)nh_pad + (3u * (unsigned)msort + 53u) * 16u;
 }
 inline size_t show_pair_smem_bytes(int nh_pad, int msort) {
     return (size_t)show_pair_scratch_bytes(nh_pad, msort) + show_tab_layout(nh_pad).total;
@@ -925,7 +1002,9 @@ template <int NT>
 __global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items, const ShowBatch* batches, int p,
                                                     int msort) {
     extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ double2 s_w[NT / 32];
+    __shared__ longlong2 s_w[NT / 32];
+    __shared__ int s_wf[NT / 32];
+    __shared__ float2 s_mx[NT / 32];
     __shared__ int s_flag;
     __shared__ ShowItem s_it[kShowBatch];
     const ShowBatch bt = batches[blockIdx.x];
@@ -933,10 +1012,7 @@ __global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items,
     const int n = (int)bt.count, npairs = (n + 1) / 2;
     uint64_t* bars = (uint64_t*)sm;
     float* rbuf = (float*)(sm + 32);
-    float2* R = (float2*)(rbuf + 4 * d.nh_pad);
-    double2* P = (double2*)((unsigned char*)R + r16u(8u * (unsigned)msort));
-    double2* Q = P + msort + 1;
-    double2* S = Q + 2 * msort + 52;
+    longlong2* U = (longlong2*)(rbuf + 4 * d.nh_pad);
     unsigned char* tabs = sm + show_pair_scratch_bytes(d.nh_pad, msort);
     const ShowTabLayout TL = show_tab_layout(d.nh_pad);
     if (threadIdx.x < n) s_it[threadIdx.x] = items[bt.start + threadIdx.x];
@@ -989,8 +1065,8 @@ __global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items,
         const ShowItem& ib = s_it[two ? j0 + 1 : j0];
         const float* roA = rbuf + (size_t)(2 * st) * d.nh_pad;
         const float* roB = two ? roA + d.nh_pad : roA;
-        cta_showdown2<NT>(tb, roA, roB, ia, ib, d.cfv + (size_t)ia.cslot * d.nh_max,
-                          two ? d.cfv + (size_t)ib.cslot * d.nh_max : nullptr, R, P, Q, S, s_w);
+        cta_showdown2<NT>(tb, d.nh[o], msort, roA, roB, ia, ib, d.cfv + (size_t)ia.cslot * d.nh_max,
+                          two ? d.cfv + (size_t)ib.cslot * d.nh_max : nullptr, U, s_w, s_wf, s_mx);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0 && q + 2 < npairs) issue(q + 2);

@@ -259,7 +259,7 @@ struct EngineImpl {
     }
     template <int FMT, int KA>
     void up_action(const Span& sa, int p, int eval) {
-        if (term64) up_action_t<FMT, KA, double>(sa, p, eval);
+        if (term64) up_action_t<FMT, KA, long long>(sa, p, eval);
         else up_action_t<FMT, KA, float>(sa, p, eval);
     }
     template <int FMT, int KA, class TT>
@@ -361,7 +361,7 @@ struct EngineImpl {
     void launch_chance(const Span& sc, int p) {
         // runout showdowns: f32 sums in the fused engine, f64 in the plain one
         if (plan.fused && !term64) k_chance<float><<<sc.count, kThreads, chance_smem, stream>>>(d, chance + sc.start, p);
-        else k_chance<double><<<sc.count, kThreads, chance_smem, stream>>>(d, chance + sc.start, p);
+        else k_chance<long long><<<sc.count, kThreads, chance_smem, stream>>>(d, chance + sc.start, p);
     }
 
     // Down sweep.  qmask: the players whose reach vectors are recomputed.  In a
@@ -555,6 +555,10 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
     E.spot = &sp;
     E.algo = host.algo;
     E.pcfr = host.algo == kPcfrPlus;
+    if (fmt == kFmtI16SR) {  // 16-bit arenas, stochastic rounding in the update
+        E.ar.sr = 1;
+        fmt = kFmtI16;
+    }
     E.fmt = fmt < 0 ? (host.storage == kStoreF32 ? kFmtF32 : kFmtI16) : fmt;
     if (E.fmt != kFmtF32 && E.fmt != kFmtI16 && E.fmt != kFmtFP8) throw Error("unknown device arena format");
     if (E.fmt == kFmtFP8 && engine != kEngineStaged) throw Error("FP8 arenas run on the staged engine only");
@@ -613,6 +617,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
         d.zero_off[q] = dupload(P.zero_off[q], O, &B);
         d.zero_idx[q] = dupload(P.zero_idx[q], O, &B);
         d.reach[q] = (float*)dalloc(P.n_rslots[q] * (size_t)d.rstr[q] * sizeof(float), O, &B);
+        d.node_id[q] = dupload(P.anode_id[q], O, &B);
     }
     d.cards = dupload(P.cards, O, &B);
     d.crefs = dupload(P.crefs, O, &B);
@@ -695,15 +700,15 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
     set_smem((const void*)k_showdown, E.show_smem);
     set_smem((const void*)k_chance<float>, E.chance_smem);
-    set_smem((const void*)k_chance<double>, E.chance_smem);
+    set_smem((const void*)k_chance<long long>, E.chance_smem);
     EngineImpl::set_up_smem<kDevF32, 8, float>(E.act_smem);
     EngineImpl::set_up_smem<kDevI16, 8, float>(E.act_smem);
     EngineImpl::set_up_smem<kDevF32, 32, float>(E.act_smem);
     EngineImpl::set_up_smem<kDevI16, 32, float>(E.act_smem);
-    EngineImpl::set_up_smem<kDevF32, 8, double>(E.act_smem);
-    EngineImpl::set_up_smem<kDevI16, 8, double>(E.act_smem);
-    EngineImpl::set_up_smem<kDevF32, 32, double>(E.act_smem);
-    EngineImpl::set_up_smem<kDevI16, 32, double>(E.act_smem);
+    EngineImpl::set_up_smem<kDevF32, 8, long long>(E.act_smem);
+    EngineImpl::set_up_smem<kDevI16, 8, long long>(E.act_smem);
+    EngineImpl::set_up_smem<kDevF32, 32, long long>(E.act_smem);
+    EngineImpl::set_up_smem<kDevI16, 32, long long>(E.act_smem);
     EngineImpl::set_warp_smem<kDevF32, 8>(E.warp_smem);
     EngineImpl::set_warp_smem<kDevI16, 8>(E.warp_smem);
     EngineImpl::set_warp_smem<kDevF32, 32>(E.warp_smem);
@@ -1405,7 +1410,7 @@ void GpuEngine::synchronize() {
 }
 void GpuEngine::update_locks(const HostSolver& host) { d_->upload_locks(host); }
 uint32_t GpuEngine::iteration() const { return d_->iteration; }
-int GpuEngine::format() const { return d_->fmt; }
+int GpuEngine::format() const { return d_->fmt == kFmtI16 && d_->ar.sr ? kFmtI16SR : d_->fmt; }
 bool GpuEngine::fused() const { return d_->plan.fused; }
 const Plan& GpuEngine::plan() const { return d_->plan; }
 const Spot* GpuEngine::plan_spot() const { return d_->spot; }

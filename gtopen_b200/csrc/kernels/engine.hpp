@@ -13,7 +13,10 @@
 
 namespace gtob {
 
-enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1, kFmtFP8 = 2 };  // FP8: E4M3 with a per-node scale
+// FP8: E4M3 with a per-node scale.  I16SR: the i16/u16 arenas, requantised
+// after each update with stochastic rounding instead of store.rs's round to
+// nearest (an engine option: the layout and every other rule are I16's).
+enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1, kFmtFP8 = 2, kFmtI16SR = 3 };
 constexpr size_t kNodeScratchElems = 16384;  // 64 KiB of f32: the read_node_static limit
 enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2, kEngineWarp = 3, kEngineStaged = 4 };
 

@@ -35,6 +35,7 @@ extern "C" {
 #define GTOB_DEVICE_F32 0
 #define GTOB_DEVICE_I16 1
 #define GTOB_DEVICE_FP8 2         /* FP8 E4M3 arenas with a per-node scale (precision study; staged engine) */
+#define GTOB_DEVICE_I16_SR 3      /* i16/u16 arenas requantised with stochastic rounding after each update */
 #define GTOB_ENGINE_FUSED 0     /* terminals in their parents' kernels, f64 terminal sums */
 #define GTOB_ENGINE_PLAIN 1     /* one launch per node kind and level, f64 terminal sums */
 #define GTOB_ENGINE_FUSED_F32 2 /* fused with f32 terminal sums (the reference GPU kernels'

@@ -881,9 +881,137 @@ static Spot* new_spot(const TreeConfig& cfg, const std::string& board_s, const s
     return sp.release();
 }
 
+// Exact terminal sums: the GPU engine's order-independent form of the
+// terminal sweeps below.  The reference sums opponent reach in f64 in one
+// fixed order (game.rs:478-485, 512-575) and casts each difference to f32.
+// Here every reach value r (f32, >= 0) of one opponent vector is put on one
+// fixed-point grid -- q = round-half-even(r * 2^S) as an int64, with S = 51 - E
+// where the vector's largest value is < 2^E, so q < 2^51 and a sum of at most
+// 1326 of them stays below 2^62 -- the sums and differences are exact integer
+// arithmetic in any order, and each difference becomes f32 once:
+// f32(x) correctly rounded, then scaled by 2^-S.  The grid's step is 2^-51 of
+// the vector's top power of two, about the rounding step of the reference's
+// f64 running sums; what stays the reference's is everything after the
+// casts (same-combo add, tie term, payoff products in f32).
+static int fix_scale(float maxv) {
+    uint32_t u;
+    std::memcpy(&u, &maxv, 4);
+    const int e = (int)((u >> 23) & 0xFFu);
+    const uint32_t m = u & 0x7FFFFFu;
+    if (e == 0 && m == 0) return 0;                                        // all zero
+    const int E = e != 0 ? e - 126 : (32 - __builtin_clz(m)) - 149;        // maxv < 2^E
+    return 51 - E;
+}
+static inline float pow2f(int k) {  // 2^k, k in [-126, 127]
+    uint32_t u = (uint32_t)(127 + k) << 23;
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+static inline int64_t fix_q(float r, int S) {  // round-half-even(r * 2^S); the scalings are exact
+    float x = r;
+    if (S > 100) { x *= pow2f(100); S -= 100; }
+    x *= pow2f(S);
+    return (int64_t)std::nearbyint((double)x);  // |x| < 2^52: exact in f64, rounded half-even
+}
+static inline float fix_f(int64_t v, int S) {  // f32(v * 2^-S): one rounding, then exact scaling
+    float y = (float)v;
+    if (S > 100) { y *= pow2f(-100); S -= 100; }
+    return y * pow2f(-S);
+}
+static int vec_scale(const float* r, int n) {
+    float m = 0.0f;
+    for (int j = 0; j < n; j++) m = std::max(m, r[j]);
+    return fix_scale(m);
+}
+static void fold_cfv_exact(const std::vector<Hand>& me, const std::vector<Hand>& opp, const float* reach_o,
+                           const std::vector<uint32_t>& same, float amount, float* out) {
+    const int S = vec_scale(reach_o, (int)opp.size());
+    int64_t t = 0, s[52] = {0};
+    for (size_t j = 0; j < opp.size(); j++) {
+        const int64_t q = fix_q(reach_o[j], S);
+        t += q;
+        s[opp[j].c1] += q;
+        s[opp[j].c2] += q;
+    }
+    for (size_t i = 0; i < me.size(); i++) {
+        float same_r = same[i] != SENTINEL ? reach_o[same[i]] : 0.0f;
+        float valid = fix_f(t - s[me[i].c1] - s[me[i].c2], S) + same_r;
+        out[i] = amount * valid;
+    }
+}
+static void showdown_cfv_exact(const RiverEval& ev, int p, const std::vector<Hand>& me, const std::vector<Hand>& opp,
+                               const float* reach_o, const std::vector<uint32_t>& same, float win, float lose,
+                               float tie, float* out) {
+    const auto& mine = ev.sorted[p];
+    const auto& opps = ev.sorted[1 - p];
+    const int S = vec_scale(reach_o, (int)opp.size());  // the whole opponent vector's scale
+    int64_t t_all = 0, s_all[52] = {0};
+    for (auto& x : opps) {
+        const int64_t q = fix_q(reach_o[x.second], S);
+        t_all += q;
+        s_all[opp[x.second].c1] += q;
+        s_all[opp[x.second].c2] += q;
+    }
+    std::vector<float> lower(mine.size());
+    {
+        int64_t t = 0, s[52] = {0};
+        size_t j = 0;
+        for (size_t k = 0; k < mine.size(); k++) {
+            while (j < opps.size() && opps[j].first < mine[k].first) {
+                const int64_t q = fix_q(reach_o[opps[j].second], S);
+                const Hand& h = opp[opps[j].second];
+                t += q;
+                s[h.c1] += q;
+                s[h.c2] += q;
+                j++;
+            }
+            const Hand& h = me[mine[k].second];
+            lower[k] = fix_f(t - s[h.c1] - s[h.c2], S);
+        }
+    }
+    int64_t t = 0, s[52] = {0};
+    size_t j = opps.size();
+    for (size_t k = mine.size(); k-- > 0;) {
+        uint16_t i = mine[k].second;
+        while (j > 0 && opps[j - 1].first > mine[k].first) {
+            j--;
+            const int64_t q = fix_q(reach_o[opps[j].second], S);
+            const Hand& h = opp[opps[j].second];
+            t += q;
+            s[h.c1] += q;
+            s[h.c2] += q;
+        }
+        const Hand& h = me[i];
+        float higher = fix_f(t - s[h.c1] - s[h.c2], S);
+        float same_r = same[i] != SENTINEL ? reach_o[same[i]] : 0.0f;
+        float valid = fix_f(t_all - s_all[h.c1] - s_all[h.c2], S) + same_r;
+        float lo = lower[k];
+        float ti = valid - lo - higher;
+        out[i] = win * lo + lose * higher + tie * ti;
+    }
+}
+
 // terminal evaluation (game.rs:470-577)
+static void showdown_cfv_f64(const RiverEval& ev, int p, const std::vector<Hand>& me, const std::vector<Hand>& opp,
+                             const float* reach_o, const std::vector<uint32_t>& same, float win, float lose, float tie,
+                             float* out);
+static void fold_cfv_f64(const std::vector<Hand>& me, const std::vector<Hand>& opp, const float* reach_o,
+                         const std::vector<uint32_t>& same, float amount, float* out);
+// sums: 0 = the reference's f64 running sums, 1 = exact fixed-point sums
 static void fold_cfv(const std::vector<Hand>& me, const std::vector<Hand>& opp, const float* reach_o,
-                     const std::vector<uint32_t>& same, float amount, float* out) {
+                     const std::vector<uint32_t>& same, float amount, float* out, int sums) {
+    if (sums) fold_cfv_exact(me, opp, reach_o, same, amount, out);
+    else fold_cfv_f64(me, opp, reach_o, same, amount, out);
+}
+static void showdown_cfv(const RiverEval& ev, int p, const std::vector<Hand>& me, const std::vector<Hand>& opp,
+                         const float* reach_o, const std::vector<uint32_t>& same, float win, float lose, float tie,
+                         float* out, int sums) {
+    if (sums) showdown_cfv_exact(ev, p, me, opp, reach_o, same, win, lose, tie, out);
+    else showdown_cfv_f64(ev, p, me, opp, reach_o, same, win, lose, tie, out);
+}
+static void fold_cfv_f64(const std::vector<Hand>& me, const std::vector<Hand>& opp, const float* reach_o,
+                         const std::vector<uint32_t>& same, float amount, float* out) {
     double t = 0, s[52] = {0};
     for (size_t j = 0; j < opp.size(); j++) {
         double r = reach_o[j];
@@ -897,9 +1025,9 @@ static void fold_cfv(const std::vector<Hand>& me, const std::vector<Hand>& opp, 
         out[i] = amount * valid;
     }
 }
-static void showdown_cfv(const RiverEval& ev, int p, const std::vector<Hand>& me, const std::vector<Hand>& opp,
-                         const float* reach_o, const std::vector<uint32_t>& same, float win, float lose, float tie,
-                         float* out) {
+static void showdown_cfv_f64(const RiverEval& ev, int p, const std::vector<Hand>& me, const std::vector<Hand>& opp,
+                             const float* reach_o, const std::vector<uint32_t>& same, float win, float lose, float tie,
+                             float* out) {
     const auto& mine = ev.sorted[p];
     const auto& opps = ev.sorted[1 - p];
     double t_all = 0, s_all[52] = {0};
@@ -1019,6 +1147,49 @@ static float quantize_u16(const float* src, int n, float max, uint16_t* dst) {  
     if (!(max > 0.0f && std::isfinite(max))) { std::fill(dst, dst + n, (uint16_t)0); return 0.0f; }
     float k = 65535.0f / max;
     for (int i = 0; i < n; i++) dst[i] = sat_u16(std::nearbyint(std::fmax(src[i], 0.0f) * k));
+    return max;
+}
+// Stochastic rounding of the 16-bit requantisation (the engine's optional
+// rounding mode; store.rs rounds to nearest even): x -> floor(x + u) with u in
+// [0, 1) from the SplitMix64 output function (Steele, Lea and Flood, "Fast
+// splittable pseudorandom number generators", 2014) over the key
+// (tree node << 32 | hand << 4 | action) + iteration * 0x9E3779B97F4A7C15;
+// the low 24 bits feed the regret, bits 40..63 the strategy sum.
+static inline uint64_t sr_hash(uint32_t node, uint32_t hand, uint32_t action, uint32_t t) {
+    uint64_t z = (((uint64_t)node << 32) | (uint64_t)(hand << 4 | action)) + (uint64_t)t * 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+static inline float sr_u_lo(uint64_t h) { return (float)(uint32_t)(h & 0xFFFFFFu) * 0x1p-24f; }
+static inline float sr_u_hi(uint64_t h) { return (float)(uint32_t)(h >> 40) * 0x1p-24f; }
+static inline int16_t sr_i16(float x, float u) {  // floor(x + u), saturating, NaN -> 0
+    float y = x + u;
+    if (y != y) return 0;
+    y = std::floor(y);
+    return (int16_t)std::fmin(32767.0f, std::fmax(-32768.0f, y));
+}
+static inline uint16_t sr_u16(float x, float u) {
+    float y = x + u;
+    if (y != y) return 0;
+    y = std::floor(y);
+    return (uint16_t)std::fmin(65535.0f, std::fmax(0.0f, y));
+}
+// quantize_i16 / quantize_u16 with stochastic rounding; src and dst are the
+// node's action-major block (entry a * h + i), t the iteration.
+static float quantize_i16_sr(const float* src, int na, int h, float max, uint32_t node, uint32_t t, int16_t* dst) {
+    if (!(max > 0.0f && std::isfinite(max))) { std::fill(dst, dst + na * h, (int16_t)0); return 0.0f; }
+    float k = 32767.0f / max;
+    for (int a = 0; a < na; a++)
+        for (int i = 0; i < h; i++) dst[a * h + i] = sr_i16(src[a * h + i] * k, sr_u_lo(sr_hash(node, i, a, t)));
+    return max;
+}
+static float quantize_u16_sr(const float* src, int na, int h, float max, uint32_t node, uint32_t t, uint16_t* dst) {
+    if (!(max > 0.0f && std::isfinite(max))) { std::fill(dst, dst + na * h, (uint16_t)0); return 0.0f; }
+    float k = 65535.0f / max;
+    for (int a = 0; a < na; a++)
+        for (int i = 0; i < h; i++)
+            dst[a * h + i] = sr_u16(std::fmax(src[a * h + i], 0.0f) * k, sr_u_hi(sr_hash(node, i, a, t)));
     return max;
 }
 static float encode_i16(const float* src, int n, int16_t* dst) {  // store.rs:199-205
@@ -1186,6 +1357,8 @@ struct Solver {
     int algo;
     bool use_iso;
     bool prune;
+    int sums = 0;  // terminal sums: 0 = the reference's f64 running sums, 1 = exact fixed point (the GPU's)
+    int sr = 0;    // 16-bit requantisation: 0 round to nearest even (store.rs), 1 stochastic rounding
     Store regrets[2], strat[2];
     bool have_preds = false;
     Store preds[2];
@@ -1342,8 +1515,13 @@ struct Solver {
                 smax = std::fmax(smax, s);
             }
         }
-        regrets[p].scale[idx] = quantize_i16(rb.data(), cnt, rmax, rq);
-        strat[p].scale[idx] = quantize_u16(sb.data(), cnt, smax, sq);
+        if (sr) {
+            regrets[p].scale[idx] = quantize_i16_sr(rb.data(), na, h, rmax, idx, iteration, rq);
+            strat[p].scale[idx] = quantize_u16_sr(sb.data(), na, h, smax, idx, iteration, sq);
+        } else {
+            regrets[p].scale[idx] = quantize_i16(rb.data(), cnt, rmax, rq);
+            strat[p].scale[idx] = quantize_u16(sb.data(), cnt, smax, sq);
+        }
         if (pc) {
             float pmax = 0.0f;
             for (int a = 0; a < na; a++)
@@ -1436,10 +1614,10 @@ struct Solver {
         const Spot& sp = *spot;
         if (n.kind == K_FOLD) {
             float amount = (float)(n.player == p ? n.t_lose : n.t_win);
-            fold_cfv(sp.hands[p], sp.hands[1 - p], reach_o, sp.same_combo[p], amount, out);
+            fold_cfv(sp.hands[p], sp.hands[1 - p], reach_o, sp.same_combo[p], amount, out, sums);
         } else if (n.kind == K_SHOWDOWN) {
             showdown_cfv(sp.river_get(dealt), p, sp.hands[p], sp.hands[1 - p], reach_o, sp.same_combo[p],
-                         (float)n.t_win, (float)n.t_lose, (float)n.t_tie, out);
+                         (float)n.t_win, (float)n.t_lose, (float)n.t_tie, out, sums);
         } else if (n.kind == K_CHANCE) {
             chance_node(n, p, reach_p, reach_o, dealt, out,
                         [&](uint32_t c, const float* rp, const float* ro, const Dealt& dd, float* o) {
@@ -1531,10 +1709,10 @@ struct Solver {
         const Spot& sp = *spot;
         if (n.kind == K_FOLD) {
             float amount = (float)(n.player == p ? n.t_lose : n.t_win);
-            fold_cfv(sp.hands[p], sp.hands[1 - p], reach_o, sp.same_combo[p], amount, out);
+            fold_cfv(sp.hands[p], sp.hands[1 - p], reach_o, sp.same_combo[p], amount, out, sums);
         } else if (n.kind == K_SHOWDOWN) {
             showdown_cfv(sp.river_get(dealt), p, sp.hands[p], sp.hands[1 - p], reach_o, sp.same_combo[p],
-                         (float)n.t_win, (float)n.t_lose, (float)n.t_tie, out);
+                         (float)n.t_win, (float)n.t_lose, (float)n.t_tie, out, sums);
         } else if (n.kind == K_CHANCE) {
             std::vector<float> dummy(h, 1.0f);
             chance_node(n, p, dummy.data(), reach_o, dealt, out,
@@ -2009,14 +2187,15 @@ double orc_spot_pair_weight_sum(const orc_spot* s) {
     Solver tmp(s->s, false, DCFR, false, false);
     return tmp.pair_weight_sum();
 }
-void orc_fold_cfv(const orc_spot* s, int p, const float* ro, float amount, float* out) {
-    fold_cfv(s->s->hands[p], s->s->hands[1 - p], ro, s->s->same_combo[p], amount, out);
+void orc_fold_cfv(const orc_spot* s, int p, const float* ro, float amount, int exact, float* out) {
+    fold_cfv(s->s->hands[p], s->s->hands[1 - p], ro, s->s->same_combo[p], amount, out, exact);
 }
 void orc_showdown_cfv(const orc_spot* s, int p, const uint8_t* dealt, int nd, const float* ro, float win, float lose,
-                      float tie, float* out) {
+                      float tie, int exact, float* out) {
     Dealt d;
     for (int i = 0; i < nd; i++) d = d.push(dealt[i]);
-    showdown_cfv(s->s->river_get(d), p, s->s->hands[p], s->s->hands[1 - p], ro, s->s->same_combo[p], win, lose, tie, out);
+    showdown_cfv(s->s->river_get(d), p, s->s->hands[p], s->s->hands[1 - p], ro, s->s->same_combo[p], win, lose, tie, out,
+                 exact);
 }
 void orc_fp8_encode(const float* x, int n, uint8_t* out) {
     for (int i = 0; i < n; i++) out[i] = f32_to_e4m3(x[i]);
@@ -2027,6 +2206,8 @@ void orc_fp8_decode(const uint8_t* q, int n, float* out) {
 orc_solver* orc_solver_new(orc_spot* s, int compressed, int algo, int use_iso, int prune) {
     return new orc_solver{new Solver(s->s, compressed, algo, use_iso != 0, prune != 0)};
 }
+void orc_solver_set_sums(orc_solver* v, int exact) { v->v->sums = exact ? 1 : 0; }
+void orc_solver_set_rounding(orc_solver* v, int stochastic) { v->v->sr = stochastic ? 1 : 0; }
 void orc_solver_free(orc_solver* v) {
     if (v) { delete v->v; delete v; }
 }

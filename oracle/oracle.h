@@ -85,10 +85,11 @@ void orc_spot_perms(const orc_spot* s, uint8_t* perms4, uint16_t* hand_perm0, ui
 int orc_spot_river(const orc_spot* s, int p, const uint8_t* dealt, int ndealt, uint32_t* str, uint16_t* idx);
 double orc_spot_pair_weight_sum(const orc_spot* s);
 
-/* terminal evaluators (game.rs) */
-void orc_fold_cfv(const orc_spot* s, int p, const float* reach_o, float amount, float* out);
+/* terminal evaluators (game.rs); exact = 0: the reference's f64 running sums,
+   1: exact fixed-point sums (the GPU engine's order-independent arithmetic) */
+void orc_fold_cfv(const orc_spot* s, int p, const float* reach_o, float amount, int exact, float* out);
 void orc_showdown_cfv(const orc_spot* s, int p, const uint8_t* dealt, int ndealt, const float* reach_o,
-                      float win, float lose, float tie, float* out);
+                      float win, float lose, float tie, int exact, float* out);
 
 /* solver (cfr.rs / best_response.rs) */
 /* FP8 E4M3 codec of the precision-study arenas (round to nearest even, saturating to +-448) */
@@ -97,6 +98,10 @@ void orc_fp8_decode(const uint8_t* q, int n, float* out);
 /* compressed: 0 f32 arenas, 1 i16 regrets / u16 strategy sums (store.rs), 2 FP8 E4M3 (precision study) */
 orc_solver* orc_solver_new(orc_spot* s, int compressed, int algo, int use_iso, int prune);
 void orc_solver_free(orc_solver* v);
+/* terminal sums of the solver's sweeps: 0 the reference's f64 (default), 1 exact fixed point */
+void orc_solver_set_sums(orc_solver* v, int exact);
+/* 16-bit arenas' requantisation after an update: 0 round to nearest even (store.rs, default), 1 stochastic */
+void orc_solver_set_rounding(orc_solver* v, int stochastic);
 void orc_solver_iterate(orc_solver* v, int n);
 uint32_t orc_solver_iteration(const orc_solver* v);
 double orc_solver_exploitability(orc_solver* v);

@@ -63,8 +63,10 @@ def lib():
         L.orc_spot_river.argtypes = [P, C.c_int, P, C.c_int, P, P]
         L.orc_spot_pair_weight_sum.restype = C.c_double
         L.orc_spot_pair_weight_sum.argtypes = [P]
-        L.orc_fold_cfv.argtypes = [P, C.c_int, P, C.c_float, P]
-        L.orc_showdown_cfv.argtypes = [P, C.c_int, P, C.c_int, P, C.c_float, C.c_float, C.c_float, P]
+        L.orc_fold_cfv.argtypes = [P, C.c_int, P, C.c_float, C.c_int, P]
+        L.orc_showdown_cfv.argtypes = [P, C.c_int, P, C.c_int, P, C.c_float, C.c_float, C.c_float, C.c_int, P]
+        L.orc_solver_set_sums.argtypes = [P, C.c_int]
+        L.orc_solver_set_rounding.argtypes = [P, C.c_int]
         L.orc_solver_new.restype = P
         L.orc_solver_new.argtypes = [P, C.c_int, C.c_int, C.c_int, C.c_int]
         L.orc_solver_free.argtypes = [P]
@@ -222,17 +224,18 @@ class Spot:
     def pair_weight_sum(self):
         return lib().orc_spot_pair_weight_sum(self.h)
 
-    def fold_cfv(self, p, reach_o, amount):
+    def fold_cfv(self, p, reach_o, amount, exact=False):
         out = np.zeros(self.nh[p], np.float32)
         r = np.ascontiguousarray(reach_o, np.float32)
-        lib().orc_fold_cfv(self.h, p, ptr(r), float(amount), ptr(out))
+        lib().orc_fold_cfv(self.h, p, ptr(r), float(amount), int(exact), ptr(out))
         return out
 
-    def showdown_cfv(self, p, dealt, reach_o, win, lose, tie):
+    def showdown_cfv(self, p, dealt, reach_o, win, lose, tie, exact=False):
         out = np.zeros(self.nh[p], np.float32)
         r = np.ascontiguousarray(reach_o, np.float32)
         d = np.array(dealt, np.uint8)
-        lib().orc_showdown_cfv(self.h, p, ptr(d), len(dealt), ptr(r), float(win), float(lose), float(tie), ptr(out))
+        lib().orc_showdown_cfv(self.h, p, ptr(d), len(dealt), ptr(r), float(win), float(lose), float(tie),
+                               int(exact), ptr(out))
         return out
 
 
@@ -241,12 +244,21 @@ ALGOS = {"dcfr": 0, "cfr+": 1, "pcfr+": 2}
 
 class Solver:
     """The reference CPU engine (cfr.rs); prune=True reproduces it exactly,
-    prune=False gives the no-pruning semantics of a level-synchronous sweep."""
+    prune=False gives the no-pruning semantics of a level-synchronous sweep.
+    exact=False sums terminal reach in f64 as the reference does (game.rs);
+    exact=True uses the GPU engine's exact fixed-point terminal sums.
+    stochastic=True requantises the 16-bit arenas with the engine's
+    stochastic rounding instead of store.rs's round-to-nearest."""
 
-    def __init__(self, spot, compressed=False, algo="dcfr", use_iso=True, prune=True, fp8=False):
+    def __init__(self, spot, compressed=False, algo="dcfr", use_iso=True, prune=True, fp8=False, exact=False,
+                 stochastic=False):
         self.spot = spot
         mode = 2 if fp8 else int(bool(compressed))
         self.h = lib().orc_solver_new(spot.h, mode, ALGOS[algo], int(use_iso), int(prune))
+        if exact:
+            lib().orc_solver_set_sums(self.h, 1)
+        if stochastic:
+            lib().orc_solver_set_rounding(self.h, 1)
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -79,7 +79,7 @@ def _check(cfg, use_iso, device_format, paths):
     gpu.sync_to_cpu(host)
     host.ensure_symmetric()
     ospot = po.Spot(cfg)
-    osv = po.Solver(ospot, compressed=False, use_iso=use_iso, prune=False)
+    osv = po.Solver(ospot, compressed=False, use_iso=use_iso, prune=False, exact=True)
     for which in (0, 1):
         for p in (0, 1):
             osv.set_arena(which, p, host.arena(which, p))
@@ -171,7 +171,7 @@ def test_exploit_values_match_oracle(device_format):
     got = {(tuple(pa), p): gpu.exploit_values(pa, p, host) for pa in paths for p in (0, 1)}
     gpu.sync_to_cpu(host)
     ospot = po.Spot(cfg)
-    osv = po.Solver(ospot, compressed=False, use_iso=False, prune=False)
+    osv = po.Solver(ospot, compressed=False, use_iso=False, prune=False, exact=True)
     for which in (0, 1):
         for q in (0, 1):
             osv.set_arena(which, q, host.arena(which, q))
@@ -295,7 +295,7 @@ def test_equity_and_runouts_match_oracle():
     ro_river = gpu.runouts([0, 0, "Ah", 0, 0], host)
     gpu.sync_to_cpu(host)
     ospot = po.Spot(cfg)
-    osv = po.Solver(ospot, compressed=False, use_iso=False, prune=False)
+    osv = po.Solver(ospot, compressed=False, use_iso=False, prune=False, exact=True)
     for which in (0, 1):
         for q in (0, 1):
             osv.set_arena(which, q, host.arena(which, q))

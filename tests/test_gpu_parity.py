@@ -2,9 +2,13 @@
 
 The oracle runs the reference CPU engine's arithmetic with zero-reach pruning
 off, which is the level-synchronous sweep's semantics (the reference's own GPU
-tests note the pruning difference, tests/gpu.rs:67-69).  Bars: average
-strategies within 1e-4 absolute after N iterations, regrets within 1e-4
-relative to the arena scale, exploitability within 0.01% of the pot.
+tests note the pruning difference, tests/gpu.rs:67-69), and with the engine's
+exact terminal sums (pyoracle exact=True: the fold and showdown reach sums of
+game.rs:470-577 taken exactly, so their order does not matter).  Bars:
+average strategies within 1e-4 absolute after N iterations, regrets within
+1e-4 relative to the arena scale, exploitability within 0.01% of the pot;
+with exact sums the arenas are expected to be bit-identical, and
+test_arenas_bit_identical holds every engine to that.
 """
 import numpy as np
 import pytest
@@ -37,12 +41,16 @@ def _avg_strategies(spot, arena_fn):
 
 
 def _run_pair(cfg, iters, storage="f32", algo="dcfr", use_iso=False, engine="fused"):
+    """storage: "f32", "compressed" (i16/u16, store.rs rounding) or "i16sr"
+    (i16/u16 requantised with stochastic rounding)."""
+    sr = storage == "i16sr"
     ospot = po.Spot(cfg)
-    osv = po.Solver(ospot, compressed=storage != "f32", algo=algo, use_iso=use_iso, prune=False)
+    osv = po.Solver(ospot, compressed=storage != "f32", algo=algo, use_iso=use_iso, prune=False, exact=True,
+                    stochastic=sr)
     osv.iterate(iters)
     spot = g.Spot(cfg)
-    host = g.Solver(spot, storage=storage, algo=algo, use_iso=use_iso)
-    gpu = g.GpuSolver(host, engine=engine)
+    host = g.Solver(spot, storage="compressed" if sr else storage, algo=algo, use_iso=use_iso)
+    gpu = g.GpuSolver(host, engine=engine, device_format="i16sr" if sr else None)
     gpu.iterate(iters)
     gpu.sync_to_cpu(host)
     return ospot, osv, spot, host, gpu
@@ -101,26 +109,45 @@ def test_cfrplus_pcfrplus_match_oracle(algo, storage, engine):
 ])
 def test_fused32_exploitability_matches_oracle(name, cfg_fn, iters):
     """f32 terminal sums (the reference GPU kernels' precision) round near-tied
-    regrets differently from the f64 CPU engine: on the small flop fixture
-    that drift exceeds the 0.01%-of-pot bar after 20 iterations, which is
-    why the default engines sum terminals in f64.  On the river spot the
-    exploitability still agrees."""
+    regrets differently from the CPU engine's f64 sums: on the small flop
+    fixture that drift exceeds the 0.01%-of-pot bar after 20 iterations,
+    which is why the default engines sum terminals exactly.  On the river
+    spot the exploitability still agrees with the reference's f64 sums."""
     cfg = cfg_fn()
-    ospot, osv, spot, host, gpu = _run_pair(cfg, iters, engine="fused32")
+    ospot = po.Spot(cfg)
+    osv = po.Solver(ospot, compressed=False, use_iso=False, prune=False)  # the reference's f64 sums
+    osv.iterate(iters)
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, storage="f32", use_iso=False)
+    gpu = g.GpuSolver(host, engine="fused32")
+    gpu.iterate(iters)
     pot = cfg["tree"]["starting_pot"]
     assert abs(osv.exploitability() - gpu.exploitability(host)) / pot * 100 < EXPL_TOL_PCT
 
 
-@pytest.mark.parametrize("engine", ["fused", "warp", "staged"])
-def test_i16_quants_match_oracle_bitwise_mostly(engine):
-    """16-bit arenas: the device requantises exactly like store.rs; decoded values agree."""
-    cfg = W.small_flop_spot()
-    ospot, osv, spot, host, gpu = _run_pair(cfg, 10, storage="compressed", engine=engine)
-    for p in (0, 1):
-        for which in (0, 1):
-            a, b = osv.arena(which, p), host.arena(which, p)
-            frac_equal = float(np.mean(a == b))
-            assert frac_equal > 0.999, (which, p, frac_equal)
+@pytest.mark.parametrize("engine", ["fused", "plain", "warp", "staged"])
+@pytest.mark.parametrize("storage,algo", [("f32", "dcfr"), ("compressed", "dcfr"), ("f32", "pcfr+"),
+                                          ("compressed", "cfr+"), ("i16sr", "dcfr"), ("i16sr", "pcfr+")])
+def test_arenas_bit_identical(engine, storage, algo):
+    """With exact terminal sums every engine's regrets and strategy sums equal
+    the oracle's bit for bit (16-bit arenas: every quant and scale, as store.rs
+    requantises them, or with the stochastic rounding both sides draw from
+    the same hash), on a flop spot with folds, showdowns and both chance
+    levels, and on an all-in runout spot."""
+    cfgs = [W.small_flop_spot()]
+    r = W.small_flop_spot()
+    for st in r["tree"]["oop"] + r["tree"]["ip"]:
+        st["bet"] = [{"PotPct": 75.0}, "AllIn"]
+        st["raise"] = ["AllIn"]
+    r["tree"]["effective_stack"] = 120.0
+    cfgs.append(r)
+    for k, cfg in enumerate(cfgs):
+        ospot, osv, spot, host, gpu = _run_pair(cfg, 12, storage=storage, algo=algo, engine=engine)
+        for p in (0, 1):
+            for which in (0, 1):
+                a, b = osv.arena(which, p), host.arena(which, p)
+                neq = int(np.count_nonzero(a != b))
+                assert neq == 0, (k, which, p, neq, a.size, float(np.abs(a - b).max()))
 
 
 @pytest.mark.parametrize("engine", ["fused", "plain", "warp", "staged"])
@@ -242,7 +269,7 @@ def test_locks_match_oracle(engine):
     updated; every other node matches the oracle."""
     cfg = W.small_flop_spot()
     ospot = po.Spot(cfg)
-    osv = po.Solver(ospot, prune=False, use_iso=False)
+    osv = po.Solver(ospot, prune=False, use_iso=False, exact=True)
     spot = g.Spot(cfg)
     host = g.Solver(spot, use_iso=False)
     osv.iterate(5)
@@ -276,7 +303,7 @@ def test_fp8_arenas_match_oracle(name, cfg_fn, iters, algo):
     strategies within 1e-4, exploitability within 0.01% of the pot."""
     cfg = cfg_fn()
     ospot = po.Spot(cfg)
-    osv = po.Solver(ospot, fp8=True, algo=algo, prune=False)
+    osv = po.Solver(ospot, fp8=True, algo=algo, prune=False, exact=True)
     osv.iterate(iters)
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage="f32", algo=algo)

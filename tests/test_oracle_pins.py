@@ -280,3 +280,84 @@ def test_fp8_arenas_precision_study():
     assert res["f32"][1] < 0.1 and res["i16"][1] < 0.15
     assert res["fp8"][1] < res["fp8"][0] and res["fp8"][1] < 4.0
     assert res["fp8"][1] > 10 * res["f32"][1]  # the stall, as recorded
+
+
+def _exact_terms_numpy(spot, p, dealt, ro, win, lose, tie):
+    """Independent restatement of the exact terminal sums: every opponent
+    reach value on the grid 2^-S (S = 51 - E, the vector's max < 2^E), the
+    compatible weaker / stronger / all opponent mass of each hand summed by
+    explicit masks in int64, each sum to f32 once, then the reference's f32
+    arithmetic (game.rs:470-577)."""
+    o = 1 - p
+    c1m, c2m, _ = spot.hands(p)
+    c1o, c2o, _ = spot.hands(o)
+    mx = float(ro.max())
+    S = 51 - np.frexp(mx)[1] if mx > 0 else 0
+    q = np.rint(ro.astype(np.float64) * 2.0 ** S).astype(np.int64)
+
+    def f32(x):
+        return np.float32(np.int64(x)) * np.float32(2.0 ** -S)
+
+    st_m, ix_m = spot.river(p, dealt)
+    st_o, ix_o = spot.river(o, dealt)
+    strength_o = np.full(len(c1o), -1, np.int64)
+    strength_o[ix_o] = st_o
+    fold = np.zeros(len(c1m), np.float32)
+    show = np.zeros(len(c1m), np.float32)
+    pos = {int(i): int(s) for s, i in zip(st_m, ix_m)}
+    for i in range(len(c1m)):
+        dis = (c1o != c1m[i]) & (c1o != c2m[i]) & (c2o != c1m[i]) & (c2o != c2m[i])
+        same = np.nonzero((np.minimum(c1o, c2o) == min(c1m[i], c2m[i])) & (np.maximum(c1o, c2o) == max(c1m[i], c2m[i])))[0]
+        q_same = int(q[same[0]]) if len(same) else 0
+        same_r = np.float32(ro[same[0]]) if len(same) else np.float32(0)
+        valid = np.float32(f32(int(q[dis].sum()) - q_same) + same_r)
+        fold[i] = np.float32(10.0) * valid
+        if i in pos:
+            s = pos[i]
+            ok = dis & (strength_o >= 0)
+            lo = f32(int(q[ok & (strength_o < s)].sum()))
+            hi = f32(int(q[ok & (strength_o > s)].sum()))
+            # valid over the board's hands: total minus the two card sums (the same combo counted twice)
+            on = strength_o >= 0
+            has1 = (c1o == c1m[i]) | (c2o == c1m[i])
+            has2 = (c1o == c2m[i]) | (c2o == c2m[i])
+            vq = int(q[on].sum()) - int(q[on & has1].sum()) - int(q[on & has2].sum())
+            va = np.float32(f32(vq) + same_r)
+            ti = np.float32(np.float32(va - lo) - hi)
+            show[i] = np.float32(np.float32(np.float32(np.float32(win) * lo) + np.float32(np.float32(lose) * hi))
+                                 + np.float32(np.float32(tie) * ti))
+    return fold, show
+
+
+def test_exact_terminal_sums_restated():
+    """The oracle's exact fold and showdown sums (the GPU engine's
+    arithmetic) equal an independent numpy restatement bit for bit, on reach
+    vectors of ordinary, tiny (1e-25) and mixed magnitudes; and they stay
+    within a few f32 rounding steps of the reference's f64 running sums."""
+    cfg = W.small_flop_spot()
+    spot = po.Spot(cfg)
+    rng = np.random.default_rng(11)
+    dealt = [int(c) for c in rng.choice([c for c in range(52) if c not in cards(cfg["board"])], 2, replace=False)]
+    c1o, c2o, _ = spot.hands(1)
+    blocked = np.isin(c1o, dealt) | np.isin(c2o, dealt)
+    for scale in (1.0, 1e-25, None):
+        ro = rng.random(spot.nh[1]).astype(np.float32)
+        ro[rng.random(spot.nh[1]) < 0.2] = 0.0
+        if scale is None:
+            ro *= (10.0 ** rng.integers(-30, 1, spot.nh[1])).astype(np.float32)
+        else:
+            ro *= np.float32(scale)
+        ro[blocked] = 0.0
+        win, lose, tie = 37.5, -37.5, 0.0
+        fold, show = _exact_terms_numpy(spot, 0, dealt, ro, win, lose, tie)
+        a = spot.fold_cfv(0, ro, 10.0, exact=True)
+        b = spot.showdown_cfv(0, dealt, ro, win, lose, tie, exact=True)
+        st, ix = spot.river(0, dealt)
+        assert np.array_equal(a.view(np.uint32), fold.view(np.uint32)), scale
+        assert np.array_equal(b[ix].view(np.uint32), show[ix].view(np.uint32)), scale
+        a64 = spot.fold_cfv(0, ro, 10.0)
+        b64 = spot.showdown_cfv(0, dealt, ro, win, lose, tie)
+        big = max(float(np.abs(a64).max()), 1e-45)
+        assert float(np.abs(a - a64).max()) <= 4 * np.finfo(np.float32).eps * big, scale
+        bigs = max(float(np.abs(b64).max()), 1e-45)
+        assert float(np.abs(b - b64).max()) <= 64 * np.finfo(np.float32).eps * bigs, scale
