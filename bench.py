@@ -44,15 +44,21 @@ def load_peak():
         return PEAK_FALLBACK, "fallback"
 
 
-def make_config(name):
-    import gtopen_b200 as g
+def make_config(name, evaluate7=None):
+    """The workload's spot config.  evaluate7 draws the strength-shaped ranges:
+    the product's evaluator by default; the reference arm passes the oracle's
+    (bit-identical, pinned to the reference's evaluator tests) so that its
+    process never loads the product library."""
     from gtopen_b200 import workloads as W
+    if evaluate7 is None:
+        import gtopen_b200 as g
+        evaluate7 = g.evaluate7
     if name == "flop":
-        return W.flop_spot(g.evaluate7, seed=3)
+        return W.flop_spot(evaluate7, seed=3)
     if name == "flop_narrow":  # the flop's board and ranges on a narrow tree (profiling case)
-        return W.flop_spot(g.evaluate7, seed=3, bet=("75", "a"), raise_=("a",), max_raises=2)
+        return W.flop_spot(evaluate7, seed=3, bet=("75", "a"), raise_=("a",), max_raises=2)
     if name == "turn":
-        return W.turn_spot(g.evaluate7, seed=2)
+        return W.turn_spot(evaluate7, seed=2)
     if name == "river":
         return W.river_spot(seed=1)
     if name == "bench_spot":
@@ -159,11 +165,15 @@ def barrier(world):
 # captured.
 MEASURED_TRAFFIC = {("flop", "compressed", "staged"): 233.65e9}
 
-HOST_STORAGE = {"compressed": "compressed", "f32": "f32", "fp8": "f32"}
-DEVICE_FORMAT = {"compressed": None, "f32": None, "fp8": "fp8"}
-DTYPE = {"compressed": "i16", "f32": "f32", "fp8": "fp8_e4m3"}
-ARENA_DESC = {"compressed": "i16/u16 per-node scale", "f32": "f32", "fp8": "FP8 E4M3 per-node scale"}
-HOST_BYTES = {"compressed": 2, "f32": 4, "fp8": 4}
+# i16sr = i16/u16 arenas whose update requantises with stochastic rounding
+# (the default: store.rs's round-to-nearest stalls on the flop workload)
+HOST_STORAGE = {"compressed": "compressed", "i16sr": "compressed", "f32": "f32", "fp8": "f32"}
+DEVICE_FORMAT = {"compressed": None, "i16sr": "i16sr", "f32": None, "fp8": "fp8"}
+DTYPE = {"compressed": "i16", "i16sr": "i16", "f32": "f32", "fp8": "fp8_e4m3"}
+ARENA_DESC = {"compressed": "i16/u16 per-node scale, round to nearest (store.rs)",
+              "i16sr": "i16/u16 per-node scale, stochastic rounding", "f32": "f32",
+              "fp8": "FP8 E4M3 per-node scale"}
+HOST_BYTES = {"compressed": 2, "i16sr": 2, "f32": 4, "fp8": 4}
 
 
 def cpu_baseline(cfg, storage, steps, threads=None):
@@ -174,8 +184,8 @@ def cpu_baseline(cfg, storage, steps, threads=None):
     t0 = time.perf_counter()
     spot = po.Spot(cfg)
     build_s = time.perf_counter() - t0
-    sv = po.Solver(spot, compressed=storage == "compressed", fp8=storage == "fp8", algo="dcfr", use_iso=True,
-                   prune=True)
+    sv = po.Solver(spot, compressed=storage in ("compressed", "i16sr"), fp8=storage == "fp8", algo="dcfr",
+                   use_iso=True, prune=True, stochastic=storage == "i16sr")
     times = []
     for _ in range(steps):
         t = time.perf_counter()
@@ -187,7 +197,8 @@ def cpu_baseline(cfg, storage, steps, threads=None):
 def run_reference(args, world, rank):
     if rank != 0:
         return
-    cfg = make_config(args.workload)
+    from oracle import pyoracle as po
+    cfg = make_config(args.workload, evaluate7=po.evaluate7)
     k = max(1, args.steps)
     w = max(0, args.warmup)
     r = cpu_baseline(cfg, args.storage, k + w, args.cpu_threads)
@@ -285,9 +296,26 @@ def run_ours(args, world, rank, local):
                "exploitability_pct_pot": e / cfg["tree"]["starting_pot"] * 100}
         gpu2.close()
 
-    ttt = None
-    if args.ttt and rank == 0:
+    # time to the target on this workload (wall clock from GpuSolver::new,
+    # exploitability checked on the GPU every check_every iterations), the
+    # f32 arenas' run beside it, and the plain f32 kernels' iteration time
+    ttt = ttt_f32 = plain = None
+    if not args.no_ttt and rank == 0:
         ttt = time_to_target(g, cfg, args)
+        if args.storage != "f32":
+            ttt_f32 = time_to_target(g, cfg, args, storage="f32")
+        try:
+            plain_ms = plain_f32_speed(g, cfg, 5)
+        except g.GtobError as e:  # e.g. the plain engine's terminal slots exceed device memory
+            plain_ms, plain = None, {"unavailable": str(e)}
+        if plain_ms:
+            plain = {"ms_per_iter": plain_ms, "iter_per_s": 1000.0 / plain_ms, "steps": 5,
+                     "speedup_per_iter": (value / world) / (1000.0 / plain_ms)}
+        if plain_ms and ttt_f32 and ttt_f32["reached"]:
+            # the plain kernels would need the f32 run's iterations at their own speed
+            plain["time_to_target_est_s"] = ttt_f32["iterations"] * plain_ms / 1000.0
+            if ttt and ttt["reached"]:
+                plain["speedup_time_to_target"] = plain["time_to_target_est_s"] / ttt["wall_s"]
     # time to 0.3% of the pot on the reference's own bench spot (bench_spot.json,
     # 1.25M nodes; exploitability checked every 10 iterations on the GPU, as
     # the reference CLI does), wall clock from GpuSolver::new
@@ -300,12 +328,13 @@ def run_ours(args, world, rank, local):
         return
     base = None
     if not args.no_cpu_baseline:
-        r = cpu_baseline(cfg, args.storage, args.cpu_steps, args.cpu_threads)
-        v = len(r["iter_s"]) / sum(r["iter_s"])
+        r = cpu_baseline(cfg, args.storage, args.cpu_steps + 1, args.cpu_threads)
+        timed = r["iter_s"][1:]  # the first iteration is the warm-up
+        v = len(timed) / sum(timed)
         base = {"value": v, "unit": "iter/s", "cores": r["cores"], "kind": "port",
-                "sample": "%d DCFR iteration(s) of the same spot on the CPU oracle (reference cfr.rs semantics, "
-                          "i16 arenas, pruning on, OpenMP over chance cards); spot build %.1fs excluded"
-                          % (len(r["iter_s"]), r["build_s"])}
+                "sample": "%d DCFR iterations of the same spot after 1 warm-up iteration on the CPU oracle "
+                          "(reference cfr.rs semantics, %s arenas, pruning on, OpenMP over chance cards); "
+                          "spot build %.1fs excluded" % (len(timed), ARENA_DESC[args.storage], r["build_s"])}
     line = {
         "metric": "CFR iterations/s (time-to-0.3%-pot exploitability & HBM GB/s vs peak)",
         "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -329,6 +358,10 @@ def run_ours(args, world, rank, local):
     }
     if ttt:
         line["time_to_target"] = ttt
+    if ttt_f32:
+        line["time_to_target_f32"] = ttt_f32
+    if plain:
+        line["plain_f32_kernels"] = plain
     if ttt_spot:
         line["time_to_target_bench_spot"] = ttt_spot
     print(json.dumps(line), flush=True)
@@ -553,11 +586,13 @@ def run_leaf(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def time_to_target(g, cfg, args):
+def time_to_target(g, cfg, args, storage=None, engine=None):
+    storage = storage or args.storage
+    engine = engine or args.engine
     spot = g.Spot(cfg)
-    host = g.Solver(spot, storage=HOST_STORAGE[args.storage], algo="dcfr", use_iso=True)
+    host = g.Solver(spot, storage=HOST_STORAGE[storage], algo="dcfr", use_iso=True)
     t = time.perf_counter()
-    gpu = g.GpuSolver(host, device_format=DEVICE_FORMAT[args.storage], engine=args.engine)
+    gpu = g.GpuSolver(host, device_format=DEVICE_FORMAT[storage], engine=engine)
     pot = cfg["tree"]["starting_pot"]
     pct = None
     while gpu.iteration < args.ttt_max:
@@ -570,7 +605,21 @@ def time_to_target(g, cfg, args):
     it = gpu.iteration
     gpu.close()
     return {"target_pct_pot": args.target, "reached": pct is not None and pct <= args.target, "iterations": it,
-            "wall_s": dt, "final_pct_pot": pct, "check_every": args.check_every}
+            "wall_s": dt, "final_pct_pot": pct, "check_every": args.check_every, "arenas": ARENA_DESC[storage],
+            "engine": engine}
+
+
+def plain_f32_speed(g, cfg, steps):
+    """The plain f32 kernels (one launch per node kind and level, f32 arenas)
+    on the same spot: device time per iteration."""
+    spot = g.Spot(cfg)
+    host = g.Solver(spot, storage="f32", algo="dcfr", use_iso=True)
+    gpu = g.GpuSolver(host, engine="plain")
+    gpu.iterate(2)
+    gpu.synchronize()
+    ms = gpu.time_iterations(steps) / steps
+    gpu.close()
+    return ms
 
 
 def main():
@@ -588,13 +637,14 @@ def main():
     ap.add_argument("--leaf-check-iters", type=int, default=400)
     ap.add_argument("--report-flops", type=int, default=184)
     ap.add_argument("--report-workers", type=int, default=8)
-    ap.add_argument("--storage", default="compressed", choices=["compressed", "f32", "fp8"])
+    ap.add_argument("--storage", default="i16sr", choices=["i16sr", "compressed", "f32", "fp8"])
     ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=1)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="timed CPU-oracle iterations (after one warm-up)")
     ap.add_argument("--cpu-threads", type=int, default=0)
-    ap.add_argument("--ttt", action="store_true", help="also measure wall time to the exploitability target")
+    ap.add_argument("--no-ttt", action="store_true",
+                    help="skip the time-to-target runs on the workload (i16 and f32 arenas) and the plain f32 timing")
     ap.add_argument("--target", type=float, default=0.3)
     ap.add_argument("--check-every", type=int, default=10)
     ap.add_argument("--ttt-max", type=int, default=2000)

@@ -159,20 +159,26 @@ struct Acc<float> {
 __device__ __forceinline__ long long shfl_up_ll(long long v, int x) { return __shfl_up_sync(0xffffffffu, v, x); }
 
 // Stochastic rounding of the 16-bit arenas' requantisation: x -> floor(x + u)
-// with u in [0, 1) drawn from a hash of (tree node, hand, action, iteration)
-// -- the SplitMix64 output function (Steele, Lea and Flood, "Fast splittable
-// pseudorandom number generators", 2014) over a 64-bit key -- so the stored
-// value is unbiased and increments below half a quantisation step still
-// accumulate in expectation.  The low 24 bits feed the regret, bits 40..63
+// with u in [0, 1) drawn from a hash of (tree node, iteration, hand, action),
+// so the stored value is unbiased and increments below half a quantisation
+// step still accumulate in expectation.  The hash is lowbias32 (Chris
+// Wellons, "Hash Prospector", public domain): sr_base once per node and
+// iteration, sr_bits per entry; the low 16 bits feed the regret, the high 16
 // the strategy sum.  Deterministic: the oracle draws the same numbers.
-__device__ __forceinline__ uint64_t sr_hash(uint32_t node, uint32_t hand, uint32_t action, uint32_t t) {
-    uint64_t z = (((uint64_t)node << 32) | (uint64_t)(hand << 4 | action)) + (uint64_t)t * 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
+__host__ __device__ __forceinline__ uint32_t lowbias32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
 }
-__device__ __forceinline__ float sr_u_lo(uint64_t h) { return __fmul_rn((float)(uint32_t)(h & 0xFFFFFFu), 0x1p-24f); }
-__device__ __forceinline__ float sr_u_hi(uint64_t h) { return __fmul_rn((float)(uint32_t)(h >> 40), 0x1p-24f); }
+__device__ __forceinline__ uint32_t sr_base(uint32_t node, uint32_t t) { return lowbias32(node ^ lowbias32(t)); }
+__device__ __forceinline__ uint32_t sr_bits(uint32_t base, uint32_t hand, uint32_t action) {
+    return lowbias32(base + ((hand << 4) | action) * 0x9E3779B9u);
+}
+__device__ __forceinline__ float sr_u_lo(uint32_t h) { return __fmul_rn((float)(h & 0xFFFFu), 0x1p-16f); }
+__device__ __forceinline__ float sr_u_hi(uint32_t h) { return __fmul_rn((float)(h >> 16), 0x1p-16f); }
 __device__ __forceinline__ int16_t sr_i16(float x, float u) {  // floor(x + u), saturated, NaN -> 0
     const float y = __fadd_rn(x, u);
     short r;
@@ -187,12 +193,12 @@ __device__ __forceinline__ uint16_t sr_u16(float x, float u) {
 }
 
 // One entry's 16-bit requantisation after an update: store.rs's round to
-// nearest even (sr = 0) or stochastic rounding keyed by (tree node, hand,
-// action, iteration).
-__device__ __forceinline__ void requant16(float nr, float ns, float rk, float sk, int sr, uint32_t node, int i, int k,
-                                          uint32_t t, int16_t* rq, uint16_t* sq) {
+// nearest even (sr = 0) or stochastic rounding (base = sr_base(tree node,
+// iteration)).
+__device__ __forceinline__ void requant16(float nr, float ns, float rk, float sk, int sr, uint32_t base, int i, int k,
+                                          int16_t* rq, uint16_t* sq) {
     if (sr) {
-        const uint64_t h = sr_hash(node, (uint32_t)i, (uint32_t)k, t);
+        const uint32_t h = sr_bits(base, (uint32_t)i, (uint32_t)k);
         *rq = rk > 0.0f ? sr_i16(nr * rk, sr_u_lo(h)) : (int16_t)0;
         *sq = sk > 0.0f ? sr_u16(fmaxf(ns, 0.0f) * sk, sr_u_hi(h)) : (uint16_t)0;
     } else {
@@ -830,7 +836,7 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
     int16_t* PQ = (int16_t*)ar.pred[p];
     const float kr = ar.rscale[p][it.sidx] / 32767.0f;
     const float kss = ar.sscale[p][it.sidx] / 65535.0f * ds;
-    const uint32_t t_sr = ar.sr ? *d.iter : 0u;
+    const uint32_t sr_b = ar.sr ? sr_base(it.node, *d.iter) : 0u;
     float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
     for (int pass = 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
@@ -864,7 +870,7 @@ __global__ void __launch_bounds__(kThreads) k_up_action(Dev d, Arenas ar, const 
                         smax = fmaxf(smax, ns);
                         if (PQ) pmax = fmaxf(pmax, fabsf(v[k] - o_));
                     } else {
-                        requant16(nr, ns, rk, sk, ar.sr, it.node, i, k, t_sr, &RQ[b + k], &SQ[b + k]);
+                        requant16(nr, ns, rk, sk, ar.sr, sr_b, i, k, &RQ[b + k], &SQ[b + k]);
                         if (PQ) PQ[b + k] = pk > 0.0f ? sat_i16((v[k] - o_) * pk) : (int16_t)0;
                     }
                 }
@@ -1114,7 +1120,7 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
     int16_t* PQ = (int16_t*)ar.pred[p];
     const float kr = ar.rscale[p][it.sidx] / 32767.0f;
     const float kss = ar.sscale[p][it.sidx] / 65535.0f * ds;
-    const uint32_t t_sr = ar.sr ? *d.iter : 0u;
+    const uint32_t sr_b = ar.sr ? sr_base(it.node, *d.iter) : 0u;
     float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
     for (int pass = 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
@@ -1148,7 +1154,7 @@ __global__ void __launch_bounds__(kThreads) kw_up_action(Dev d, Arenas ar, const
                         smax = fmaxf(smax, ns);
                         if (PQ) pmax = fmaxf(pmax, fabsf(v[k] - o_));
                     } else {
-                        requant16(nr, ns, rk, sk, ar.sr, it.node, i, k, t_sr, &RQ[b + k], &SQ[b + k]);
+                        requant16(nr, ns, rk, sk, ar.sr, sr_b, i, k, &RQ[b + k], &SQ[b + k]);
                         if (PQ) PQ[b + k] = pk > 0.0f ? sat_i16((v[k] - o_) * pk) : (int16_t)0;
                     }
                 }

@@ -267,9 +267,10 @@ __device__ __forceinline__ void s_block_max3(float& a, float& b, float& c, float
 
 // Fold summary of a staged opponent reach vector (game.rs:478-485), exact
 // sums (cfr_kernels.cuh): the vector's grid scale, the total and the
-// per-card sums.  Threads 2c and 2c+1 sum the even and odd entries of card
-// c's hand list (the list ends at the first 0xFFFF) and add the two halves.
-// s_red: kSWarps entries; returns the total, *sc the scale.
+// per-card sums.  Integer sums do not depend on their order, so every thread
+// takes hands j = tid, tid + 128, ... and adds each hand's grid value to its
+// two cards' sums with shared-memory atomics.  s_red: kSWarps entries;
+// returns the total, *sc_out the scale.
 __device__ long long s_fold_sums(const Dev& d, int o, const float* ro, long long* S, long long* s_red, int* sc_out) {
     const int nho = d.nh[o];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -278,32 +279,26 @@ __device__ long long s_fold_sums(const Dev& d, int o, const float* ro, long long
     mx = warp_max(mx);
     float* fred = (float*)s_red;
     if (lane == 0) fred[warp] = mx;
+    if (threadIdx.x < 52) S[threadIdx.x] = 0;
     __syncthreads();
     mx = fred[0];
 #pragma unroll
     for (int k = 1; k < kSWarps; k++) mx = fmaxf(mx, fred[k]);
     const int sc = fix_scale(mx);
     long long t = 0;
-    for (int j = threadIdx.x; j < nho; j += kSThreads) t += fix_q(ro[j], sc);
-    if (threadIdx.x < 104) {  // warps 0..3, whole lane pairs
-        const int c = threadIdx.x >> 1, par = threadIdx.x & 1;
-        const uint16_t* idx = d.hcard52[o] + c * 52 + par;
-        long long s = 0;
-        for (int k = 0; k + par < 52; k += 8) {  // index loads first, then the sums
-            uint16_t x[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) x[u] = k + 2 * u + par < 52 ? idx[k + 2 * u] : (uint16_t)0xFFFFu;
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-                if (x[u] != 0xFFFFu) s += fix_q(ro[x[u]], sc);
-            if (x[3] == 0xFFFFu) break;
+    const uint32_t* hi = d.hinfo[o];
+    for (int j = threadIdx.x; j < nho; j += kSThreads) {
+        const long long q = fix_q(ro[j], sc);
+        if (q) {
+            const uint32_t h = hi[j];
+            t += q;
+            atomicAdd((unsigned long long*)&S[h & 63u], (unsigned long long)q);
+            atomicAdd((unsigned long long*)&S[(h >> 6) & 63u], (unsigned long long)q);
         }
-        s += __shfl_xor_sync(0xffffffffu >> (threadIdx.x >= 96 ? 24 : 0), s, 1);
-        if (par == 0) S[c] = s;
     }
 #pragma unroll
     for (int x = 16; x > 0; x >>= 1) t += __shfl_xor_sync(0xffffffffu, t, x);
-    __syncthreads();  // everyone has read fred before it is reused as the totals
+    __syncthreads();  // every thread has read fred before it is reused as the totals
     if (lane == 0) s_red[warp] = t;
     __syncthreads();
     long long total = 0;
@@ -665,7 +660,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
         s_block_max3(rmax, smax, pmax, s_red);
         const float rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
         const float sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
-        const uint32_t nid = ar.sr ? d.node_id[p][it.sidx] : 0u, t_sr = ar.sr ? *d.iter : 0u;
+        const uint32_t sr_b = ar.sr ? sr_base(d.node_id[p][it.sidx], *d.iter) : 0u;
         for (int i = threadIdx.x; i < nh; i += kSThreads) {
             const int b = i * na;
 #pragma unroll
@@ -673,7 +668,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
                 if (k < na) {
                     const float nr = cv[k * vstride + i];
                     const float ns = __uint_as_float((uint32_t)SQ_lo[b + k] | ((uint32_t)SQ[b + k] << 16));
-                    requant16(nr, ns, rk, sk, ar.sr, nid, i, k, t_sr, &RQ[b + k], &SQ[b + k]);
+                    requant16(nr, ns, rk, sk, ar.sr, sr_b, i, k, &RQ[b + k], &SQ[b + k]);
                 }
         }
     }
@@ -683,7 +678,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     typename Q::R* RQ = (typename Q::R*)b_reg;
     typename Q::S* SQ = (typename Q::S*)b_str;
     typename Q::R* PQ = (typename Q::R*)b_pred;
-    const uint32_t nid2 = ar.sr && !one_pass ? d.node_id[p][it.sidx] : 0u, t_sr2 = ar.sr && !one_pass ? *d.iter : 0u;
+    const uint32_t sr_b2 = ar.sr && !one_pass ? sr_base(d.node_id[p][it.sidx], *d.iter) : 0u;
     for (int pass = one_pass ? 2 : 0; pass < 2; pass++) {
         float rk = 0.0f, sk = 0.0f, pk = 0.0f;
         if (pass == 1) {
@@ -715,7 +710,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
                         if (use_pred) pmax = fmaxf(pmax, fabsf(v[k] - o_));
                     } else {
                         if (FMT == kDevI16) {
-                            requant16(nr, ns, rk, sk, ar.sr, nid2, i, k, t_sr2, (int16_t*)&RQ[b + k],
+                            requant16(nr, ns, rk, sk, ar.sr, sr_b2, i, k, (int16_t*)&RQ[b + k],
                                       (uint16_t*)&SQ[b + k]);
                         } else {
                             RQ[b + k] = rk > 0.0f ? Q::er(nr * rk) : (typename Q::R)0;
@@ -756,11 +751,12 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode
 // ------------------------------------------------- batched showdowns
 // One CTA per batch of up to kShowBatch showdowns of one level that share a
 // river slot (game.rs:501-577 with the plan's rank tables).  The slot's
-// tables go to shared memory once per batch -- the opponent hands in strength
-// order, the 52 card lists (each the board's opponent hands holding the card,
-// in strength order) as the hand and card of every entry -- and the
-// showdowns' opponent reach vectors stream through two double-buffered
-// bulk-copy stages, two showdowns at a time.
+// tables go to shared memory once per batch -- one word per scan entry (the
+// opponent hands in strength order, then the 52 card lists, each the board's
+// opponent hands holding the card in strength order) with the entry's hand,
+// segment start and output index -- and the showdowns' opponent reach
+// vectors stream through two double-buffered bulk-copy stages, two
+// showdowns at a time.
 //
 // Per pair, with exact sums (cfr_kernels.cuh):
 //   1. the two vectors' grid scales (block max);
@@ -775,37 +771,34 @@ __global__ void __launch_bounds__(kSThreads) ks_up(Dev d, Arenas ar, const SNode
 //   3. per hand of mine, its rank entry's eight prefix values.
 // Every thread works in every phase, with four block barriers per pair.
 struct ShowTab {  // one slot's tables: shared-memory copies, or HBM for the last three
-    const uint16_t* sidx;   // m opponent hands, ascending strength
     const uint32_t* coff;   // 53 card-list offsets relative to the slot's first entry
-    const uint16_t* hidx;   // the opponent hand of each card-list entry (ne = 2m entries)
-    const uint8_t* ccard;   // the card of each card-list entry
+    const uint32_t* ent;    // per scan entry: opponent hand | segment start << 12 | output index << 16
     const RankEntry* rank;  // mp entries (global, L1-resident across the batch)
     const uint16_t* zero;   // nz blocked traverser hands (global)
     const uint32_t* same;   // traverser same-combo map, nh entries (global)
     int m, ne, mp, nz;
 };
 struct ShowTabLayout {  // byte offsets of the tables inside the table region
-    unsigned sidx, coff, hidx, ccard, total;
+    unsigned coff, ent, total;
 };
 __host__ __device__ inline unsigned r16u(unsigned b) { return (b + 15u) & ~15u; }
 __host__ __device__ inline ShowTabLayout show_tab_layout(int nh_pad) {
     ShowTabLayout L;
     unsigned o = 0;
-    L.sidx = o;
-    o += r16u(2u * nh_pad);
     L.coff = o;
     o += r16u(53u * 4u);
-    L.hidx = o;
-    o += r16u(4u * nh_pad);
-    L.ccard = o;
-    o += r16u(2u * nh_pad);
+    L.ent = o;
+    o += r16u(12u * nh_pad);  // 3m entries of 4 bytes (m <= nh_pad)
     L.total = o;
     return L;
 }
 
-// Slot tables of a batch into shared memory (all threads of the CTA).
-__device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char* tabs, const ShowTabLayout& TL,
-                              ShowTab& tb) {
+// Slot tables of a batch into shared memory (all threads of the CTA).  The
+// scan input is the concatenation [opponent hands in strength order (m) |
+// card lists (ne = 2m)]; entry f's output index in U is f + 1 in the first
+// part and msort + 2 + t + c for entry t of card c's list.
+__device__ void load_show_tab(const Dev& d, int p, uint32_t slot, int msort, unsigned char* tabs,
+                              const ShowTabLayout& TL, ShowTab& tb) {
     const int o = 1 - p;
     tb.m = (int)d.sorted_cnt[o][slot];
     const uint32_t* coff_g = d.ccard_off[o] + (size_t)slot * 53;
@@ -814,43 +807,35 @@ __device__ void load_show_tab(const Dev& d, int p, uint32_t slot, unsigned char*
     tb.mp = (int)d.rank_cnt[p][slot];
     const uint32_t z0 = d.zero_off[p][slot];
     tb.nz = (int)(d.zero_off[p][slot + 1] - z0);
-    uint16_t* t_sidx = (uint16_t*)(tabs + TL.sidx);
     uint32_t* t_coff = (uint32_t*)(tabs + TL.coff);
-    uint16_t* t_hidx = (uint16_t*)(tabs + TL.hidx);
-    uint8_t* t_card = (uint8_t*)(tabs + TL.ccard);
+    uint32_t* t_ent = (uint32_t*)(tabs + TL.ent);
     const uint16_t* g_sidx = d.sorted_idx[o] + d.sorted_off[o][slot];
-    for (int k = threadIdx.x; k < tb.m; k += blockDim.x) t_sidx[k] = g_sidx[k];
     if (threadIdx.x < 53) t_coff[threadIdx.x] = coff_g[threadIdx.x] - c0;
     const uint16_t* g_pos = d.ccard_pos[o] + c0;
     const uint8_t* g_card = d.ccard_card[o] + c0;
-    for (int k = threadIdx.x; k < tb.ne; k += blockDim.x) {
-        t_hidx[k] = g_sidx[g_pos[k]];
-        t_card[k] = g_card[k];
+    const int m = tb.m, F = m + tb.ne;
+    for (int f = threadIdx.x; f < F; f += blockDim.x) {
+        uint32_t h, head, oi;
+        if (f < m) {
+            h = g_sidx[f];
+            head = f == 0;
+            oi = (uint32_t)f + 1u;
+        } else {
+            const int t = f - m;
+            const uint32_t c = g_card[t];
+            h = g_sidx[g_pos[t]];
+            head = t == 0 || g_card[t - 1] != c;
+            oi = (uint32_t)msort + 2u + (uint32_t)t + c;
+        }
+        t_ent[f] = h | head << 12 | oi << 16;
     }
-    tb.sidx = t_sidx;
     tb.coff = t_coff;
-    tb.hidx = t_hidx;
-    tb.ccard = t_card;
+    tb.ent = t_ent;
     // read in place (L1-resident across the batch): keeps the CTA's shared
     // memory small, so more batches run per SM
     tb.rank = d.rank[p] + d.rank_off[p][slot];
     tb.zero = d.zero_idx[p] + z0;
     tb.same = d.same[p];
-}
-
-// Entry f of the concatenated scan input: its opponent hand, whether it
-// starts a segment, and its output index in U.
-__device__ __forceinline__ void show_entry(const ShowTab& tb, int msort, int f, int& h, bool& head, int& oi) {
-    if (f < tb.m) {
-        h = tb.sidx[f];
-        head = f == 0;
-        oi = f + 1;
-    } else {
-        const int t = f - tb.m, c = tb.ccard[t];
-        h = tb.hidx[t];
-        head = t == (int)tb.coff[c];
-        oi = msort + 2 + t + c;
-    }
 }
 
 // Showdown CTAs have NT threads: 256 for large hand lists, 128 for small ones.
@@ -879,16 +864,17 @@ __device__ void cta_showdown2(const ShowTab& tb, int nho, int msort, const float
         mxB = fmaxf(mxB, s_mx[k].y);
     }
     const int scA = fix_scale(mxA), scB = fix_scale(mxB);
-    // 2. segmented scan, chunk [f0, f1) per thread
+    // 2. segmented scan, chunk [f0, f1) per thread; an odd chunk length puts
+    // the lanes' runs in distinct shared-memory banks
     const int F = m + tb.ne;
-    const int chunk = (F + NT - 1) / NT;
+    const int chunk = ((F + NT - 1) / NT) | 1;
     const int f0 = min(tid * chunk, F), f1 = min(f0 + chunk, F);
     long long ax = 0, ay = 0;
     bool seen = false;
     for (int f = f0; f < f1; f++) {
-        int h, oi;
-        bool head;
-        show_entry(tb, msort, f, h, head, oi);
+        const uint32_t en = tb.ent[f];
+        const int h = (int)(en & 0xFFFu), oi = (int)(en >> 16);
+        const bool head = (en >> 12) & 1u;
         if (head) {
             ax = 0;
             ay = 0;
@@ -946,10 +932,9 @@ __device__ void cta_showdown2(const ShowTab& tb, int nho, int msort, const float
     }
     if (cx | cy) {
         for (int f = f0; f < f1; f++) {
-            int h, oi;
-            bool head;
-            show_entry(tb, msort, f, h, head, oi);
-            if (head) break;
+            const uint32_t en = tb.ent[f];
+            if ((en >> 12) & 1u) break;
+            const int oi = (int)(en >> 16);
             longlong2 v = U[oi];
             v.x += cx;
             v.y += cy;
@@ -1017,7 +1002,7 @@ __global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items,
     const ShowTabLayout TL = show_tab_layout(d.nh_pad);
     if (threadIdx.x < n) s_it[threadIdx.x] = items[bt.start + threadIdx.x];
     ShowTab tb;
-    load_show_tab(d, p, bt.slot, tabs, TL, tb);
+    load_show_tab(d, p, bt.slot, msort, tabs, TL, tb);
     const unsigned rbytes = round16((unsigned)d.nh[o] * 4u);
     if (threadIdx.x == 0) {
         s_flag = 0;

@@ -71,8 +71,20 @@ static void* dalloc(size_t bytes, std::vector<void*>& owned, size_t* total) {
     CK(cudaMemset(p, 0, std::max<size_t>(bytes, 16)));
     return p;
 }
+// A kernel's dynamic shared-memory limit is per function and process: raise it
+// to what this engine launches with, never lower it (engines of different
+// spots run side by side in a batch).  The default limit is 48 KB minus the
+// kernel's static shared memory, so the attribute is set for any size.
 static void set_smem(const void* fn, size_t bytes) {
-    if (bytes > 48 * 1024) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    static std::mutex mu;
+    static std::map<std::pair<int, const void*>, size_t> set;  // (device, kernel) -> limit set
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lk(mu);
+    size_t& cur = set[{dev, fn}];
+    if (bytes <= cur) return;
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
 }
 
 struct EngineImpl {
@@ -233,9 +245,24 @@ struct EngineImpl {
             if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     }
 
+    // A launch's configuration error (resources, shared memory) is reported
+    // at the launch, naming its kind, instead of surfacing later as an
+    // invalidated stream capture.
+    void launch_ok(int kind) const {
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess)
+            throw Error(std::string("cuda: ") + cudaGetErrorString(e) + " launching a " + kKernelNames[kind] +
+                        " kernel (dynamic shared memory: showdowns " + std::to_string(show_pair_smem) + " B, up " +
+                        std::to_string(st_mine_smem) + "/" + std::to_string(st_opp_smem) + " B, down " +
+                        std::to_string(st_down_smem) + " B)");
+    }
     template <class F>
     void timed(Profile* pr, int kind, F launch) {
-        if (!pr) { launch(); return; }
+        if (!pr) {
+            launch();
+            launch_ok(kind);
+            return;
+        }
         cudaEvent_t a, b;
         CK(cudaEventCreate(&a));
         CK(cudaEventCreate(&b));
@@ -695,6 +722,15 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
         E.show_pair_smem = show_pair_smem_bytes(d.nh_pad, (int)P.max_sorted);
         set_smem((const void*)ks_show_pair<128>, E.show_pair_smem);
         set_smem((const void*)ks_show_pair<256>, E.show_pair_smem);
+        for (const void* fn : {(const void*)ks_show_pair<128>, (const void*)ks_show_pair<256>}) {
+            cudaFuncAttributes fa;
+            CK(cudaFuncGetAttributes(&fa, fn));
+            if ((size_t)fa.maxDynamicSharedSizeBytes < E.show_pair_smem || fa.maxThreadsPerBlock < 256)
+                throw Error("showdown kernel limits: " + std::to_string(fa.maxDynamicSharedSizeBytes) +
+                            " B dynamic shared memory (needs " + std::to_string(E.show_pair_smem) + "), " +
+                            std::to_string(fa.maxThreadsPerBlock) + " threads, " + std::to_string(fa.numRegs) +
+                            " registers, " + std::to_string(fa.sharedSizeBytes) + " B static");
+        }
     }
     if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
@@ -1311,7 +1347,10 @@ size_t GpuEngine::read_node_static(int which, uint32_t node, float* out, size_t 
     if (node >= sp.tree.size() || sp.tree.kind[node] != kAction) throw Error("node " + std::to_string(node) + " is not an action node");
     const int p = sp.tree.player[node];
     const int32_t s = E.plan.node_sidx[node];
-    if (s < 0) throw Error("node " + std::to_string(node) + " has no device block (a symmetric branch the engine skips)");
+    if (s < 0)
+        throw Error("node " + std::to_string(node) +
+                    " has no block on this engine's device (a symmetric branch the engine skips, or a node of "
+                    "another shard)");
     if (which == kPreds && !E.pcfr) throw Error("the engine keeps no predictions (not PCFR+)");
     const XNode x = E.hx[p][(size_t)s];
     const int nh = E.plan.nh[p];
@@ -1344,6 +1383,7 @@ size_t GpuEngine::read_node_static(int which, uint32_t node, float* out, size_t 
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, scratch, n * sizeof(float), cudaMemcpyDeviceToHost, E.stream));
     CK(cudaStreamSynchronize(E.stream));
+    E.check_err();  // a sticky device error of an earlier iteration is reported, not returned as data
     return n;
 }
 

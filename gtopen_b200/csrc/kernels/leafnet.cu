@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     uint8_t* ring = dsm + ((1024u - (su32(dsm) & 1023u)) & 1023u);  // 1 KiB aligned: the swizzle atoms
     __shared__ __align__(8) uint64_t full[kStages], empty[kStages], done;
     __shared__ uint32_t tbase;
-    __shared__ int aborted;
+    __shared__ int aborted, issued;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     using T = TileCfg<BN>;
     const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN, nk = K / kBK;
@@ -199,6 +199,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
         }
         bar_init(&done, 1);
         aborted = 0;
+        issued = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -212,7 +213,8 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     tm_fence_after();
     const uint32_t tmem = tbase;
     if (warp == 0 && lane == 0) {  // producer
-        for (int kb = 0; kb < nk; kb++) {
+        int kb = 0;
+        for (; kb < nk; kb++) {
             const int s = kb % kStages;
             if (kb >= kStages && !bar_wait(&empty[s], ((kb / kStages) & 1) ^ 1)) {
                 atomicOr(err, kErrGemmWait);
@@ -224,6 +226,7 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
             tma_2d(sa, &ta, kb * kBK, m0, &full[s]);
             tma_2d(sa + kTileABytes, &tb, kb * kBK, n0, &full[s]);
         }
+        issued = kb;
     } else if (warp == 1 && lane == 0) {  // MMA issuer
         for (int kb = 0; kb < nk; kb++) {
             const int s = kb % kStages;
@@ -245,6 +248,19 @@ __global__ void __launch_bounds__(kGemmThreads, 1)
     const bool ok = bar_wait(&done, 0);
     const int good = __syncthreads_and(ok ? 1 : 0) && !aborted;
     if (!ok && threadIdx.x == 0) atomicOr(err, kErrGemmWait);
+    if (!good) {
+        // Abort: let the work already started finish before the CTA frees
+        // its TMEM and exits -- a second bounded wait for the products in
+        // flight (done arrives once every issued product has completed; the
+        // MMA thread commits it on its error path too), and, on the
+        // producer, for the tile loads it issued that no product waited
+        // for (at most the last kStages: a load is only issued once the
+        // product kStages before it has read its stage).
+        if (!ok) bar_wait(&done, 0);
+        if (warp == 0 && lane == 0)
+            for (int kb = issued > kStages ? issued - kStages : 0; kb < issued; kb++)
+                bar_wait(&full[kb % kStages], (kb / kStages) & 1);
+    }
     tm_fence_after();
     if (good) {
         const int row = m0 + warp * 32 + lane;

@@ -1151,18 +1151,24 @@ static float quantize_u16(const float* src, int n, float max, uint16_t* dst) {  
 }
 // Stochastic rounding of the 16-bit requantisation (the engine's optional
 // rounding mode; store.rs rounds to nearest even): x -> floor(x + u) with u in
-// [0, 1) from the SplitMix64 output function (Steele, Lea and Flood, "Fast
-// splittable pseudorandom number generators", 2014) over the key
-// (tree node << 32 | hand << 4 | action) + iteration * 0x9E3779B97F4A7C15;
-// the low 24 bits feed the regret, bits 40..63 the strategy sum.
-static inline uint64_t sr_hash(uint32_t node, uint32_t hand, uint32_t action, uint32_t t) {
-    uint64_t z = (((uint64_t)node << 32) | (uint64_t)(hand << 4 | action)) + (uint64_t)t * 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
+// [0, 1) from the lowbias32 integer hash (Chris Wellons, "Hash Prospector",
+// public domain): base = h(node ^ h(iteration)), bits = h(base + (hand << 4 |
+// action) * 0x9E3779B9); the low 16 bits feed the regret, the high 16 the
+// strategy sum.
+static inline uint32_t lowbias32(uint32_t x) {
+    x ^= x >> 16;
+    x *= 0x7feb352du;
+    x ^= x >> 15;
+    x *= 0x846ca68bu;
+    x ^= x >> 16;
+    return x;
 }
-static inline float sr_u_lo(uint64_t h) { return (float)(uint32_t)(h & 0xFFFFFFu) * 0x1p-24f; }
-static inline float sr_u_hi(uint64_t h) { return (float)(uint32_t)(h >> 40) * 0x1p-24f; }
+static inline uint32_t sr_bits(uint32_t node, uint32_t t, uint32_t hand, uint32_t action) {
+    const uint32_t base = lowbias32(node ^ lowbias32(t));
+    return lowbias32(base + ((hand << 4) | action) * 0x9E3779B9u);
+}
+static inline float sr_u_lo(uint32_t h) { return (float)(h & 0xFFFFu) * 0x1p-16f; }
+static inline float sr_u_hi(uint32_t h) { return (float)(h >> 16) * 0x1p-16f; }
 static inline int16_t sr_i16(float x, float u) {  // floor(x + u), saturating, NaN -> 0
     float y = x + u;
     if (y != y) return 0;
@@ -1181,7 +1187,7 @@ static float quantize_i16_sr(const float* src, int na, int h, float max, uint32_
     if (!(max > 0.0f && std::isfinite(max))) { std::fill(dst, dst + na * h, (int16_t)0); return 0.0f; }
     float k = 32767.0f / max;
     for (int a = 0; a < na; a++)
-        for (int i = 0; i < h; i++) dst[a * h + i] = sr_i16(src[a * h + i] * k, sr_u_lo(sr_hash(node, i, a, t)));
+        for (int i = 0; i < h; i++) dst[a * h + i] = sr_i16(src[a * h + i] * k, sr_u_lo(sr_bits(node, t, i, a)));
     return max;
 }
 static float quantize_u16_sr(const float* src, int na, int h, float max, uint32_t node, uint32_t t, uint16_t* dst) {
@@ -1189,7 +1195,7 @@ static float quantize_u16_sr(const float* src, int na, int h, float max, uint32_
     float k = 65535.0f / max;
     for (int a = 0; a < na; a++)
         for (int i = 0; i < h; i++)
-            dst[a * h + i] = sr_u16(std::fmax(src[a * h + i], 0.0f) * k, sr_u_hi(sr_hash(node, i, a, t)));
+            dst[a * h + i] = sr_u16(std::fmax(src[a * h + i], 0.0f) * k, sr_u_hi(sr_bits(node, t, i, a)));
     return max;
 }
 static float encode_i16(const float* src, int n, int16_t* dst) {  // store.rs:199-205

@@ -117,6 +117,12 @@ def ptr(a):
 _KIND = {"PotPct": 0, "PrevMult": 1}
 
 
+def evaluate7(cards):
+    """7-card strength (evaluator.rs:68-174), the oracle's restatement."""
+    c = np.ascontiguousarray(cards, np.uint8)
+    return int(lib().orc_evaluate7(ptr(c)))
+
+
 def make_config(cfg):
     """dict SpotConfig -> ctypes Config (keeps the byte strings alive on the object)."""
     c = Config()

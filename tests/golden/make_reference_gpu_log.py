@@ -13,7 +13,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: make_reference_gpu_log.py <path of the reference project>")
+    ref = sys.argv[1]
     path = os.path.join(ref, "bench", "gpu_f32_dcfr.log")
     pts = []
     with open(path) as f:

@@ -188,6 +188,31 @@ def test_bench_trajectory_golden():
             assert "%.4f" % a == "%.4f" % b, (mode, a, b)
 
 
+def test_exact_sums_reproduce_reference_logs():
+    """The exact fixed-point terminal sums (the GPU engine's arithmetic) with
+    the reference CPU engine's pruning reproduce the reference's printed CPU
+    logs (bench/new_f32_dcfr.log, new_i16_dcfr.log) to the printed digits at
+    all ten checkpoints; without pruning they stay within 0.001% of the pot
+    of the f64 sums.  Recorded by tests/golden/make_noprune_trajectory.py."""
+    g = json.load(open(os.path.join(HERE, "golden", "bench_trajectory_noprune.json")))
+    ref = json.load(open(os.path.join(HERE, "golden", "bench_trajectory.json")))
+    pot = g["pot"]
+    for mode in ("f32_dcfr", "i16_dcfr"):
+        for a, b in zip(g["pruned_exact"][mode], ref["modes"][mode]["reference"]):
+            assert "%.4f" % a == "%.4f" % b, (mode, a, b)
+        for a, b in zip(g["modes"][mode], g["modes_f64"][mode]):
+            assert abs(a - b) / pot * 100 < 1e-3, (mode, a, b)
+
+
+@pytest.mark.slow
+def test_exact_sums_first_checkpoint_rerun():
+    """Re-runs the first checkpoint of the exact-sum, pruned f32 trajectory."""
+    cfg = json.load(open(os.path.join(HERE, "golden", "bench_spot.json")))
+    sv = po.Solver(po.Spot(cfg), compressed=False, algo="dcfr", use_iso=True, prune=True, exact=True)
+    sv.iterate(10)
+    assert "%.4f" % sv.exploitability() == "33.7904"
+
+
 @pytest.mark.slow
 def test_bench_trajectory_rerun():
     """Re-runs the 100-iteration f32 trajectory (about 3 minutes on 8 cores)."""

@@ -1,7 +1,8 @@
 """The allocation-free entry point gtob_gpu_read_node_static against the
 existing gtob_gpu_export_arena: the same node block, bit for bit, on two
-calls in a row (the static scratch is reused by the second call), for f32
-and 16-bit arenas; and a block larger than the static scratch is refused.
+calls in a row (the static scratch is reused by the second call), for f32,
+16-bit and FP8 arenas and for PCFR+'s predictions; and a block larger than
+the static scratch is refused.
 Collected last on purpose: it must pass alone and after every other test.
 """
 import numpy as np
@@ -27,24 +28,28 @@ def _two_nodes(spot):
     return 0, int(ip[0])
 
 
-@pytest.mark.parametrize("storage", ["f32", "compressed"])
-def test_static_read_equals_export_two_calls_in_a_row(storage):
+@pytest.mark.parametrize("storage,device_format,algo", [("f32", None, "dcfr"), ("compressed", None, "dcfr"),
+                                                      ("f32", "fp8", "dcfr"), ("f32", None, "pcfr+"),
+                                                      ("compressed", None, "pcfr+")])
+def test_static_read_equals_export_two_calls_in_a_row(storage, device_format, algo):
     spot = g.Spot(W.small_flop_spot())
-    host = g.Solver(spot, storage=storage, use_iso=False)
-    gpu = g.GpuSolver(host)
+    host = g.Solver(spot, storage=storage, algo=algo, use_iso=False)
+    gpu = g.GpuSolver(host, device_format=device_format)
     gpu.iterate(7)
     a, b = _two_nodes(spot)
+    kinds = (0, 1, 2) if algo == "pcfr+" else (0, 1)  # regrets, strategy sums, predictions
     for rnd in range(2):
-        # two calls in a row through the static scratch ...
-        ra = gpu.read_node_static(0, a)
-        sb = gpu.read_node_static(1, b)
-        # ... against the existing allocating entry point
-        ea = _slice(gpu.export_arena(0, 0), spot, a)
-        eb = _slice(gpu.export_arena(1, 1), spot, b)
-        assert ra.shape == ea.shape and sb.shape == eb.shape
-        assert np.array_equal(ra, ea), (storage, rnd, float(np.abs(ra - ea).max()))
-        assert np.array_equal(sb, eb), (storage, rnd, float(np.abs(sb - eb).max()))
-        assert np.any(ra != 0.0) and np.any(sb != 0.0)
+        for which in kinds:
+            # two calls in a row through the static scratch ...
+            ra = gpu.read_node_static(which, a)
+            sb = gpu.read_node_static(which, b)
+            # ... against the existing allocating entry point
+            ea = _slice(gpu.export_arena(which, 0), spot, a)
+            eb = _slice(gpu.export_arena(which, 1), spot, b)
+            assert ra.shape == ea.shape and sb.shape == eb.shape
+            assert np.array_equal(ra, ea), (storage, device_format, which, rnd, float(np.abs(ra - ea).max()))
+            assert np.array_equal(sb, eb), (storage, device_format, which, rnd, float(np.abs(sb - eb).max()))
+            assert np.any(ra != 0.0) and np.any(sb != 0.0)
         gpu.iterate(3)
 
 
