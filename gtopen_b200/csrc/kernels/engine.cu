@@ -717,15 +717,19 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
         E.st_down_smem = SLayout(d.nh_pad, esz, E.pcfr, kSDown).total;
         EngineImpl::set_staged_smem<kDevF32>(E.st_mine_smem, E.st_opp_smem);
         EngineImpl::set_staged_smem<kDevI16>(E.st_mine_smem, E.st_opp_smem);
+        EngineImpl::set_staged_smem<kDevFP8>(E.st_mine_smem, E.st_opp_smem);
         set_smem((const void*)ks_down<kDevF32>, E.st_down_smem);
         set_smem((const void*)ks_down<kDevI16>, E.st_down_smem);
+        set_smem((const void*)ks_down<kDevFP8>, E.st_down_smem);
         E.show_pair_smem = show_pair_smem_bytes(d.nh_pad, (int)P.max_sorted);
         set_smem((const void*)ks_show_pair<128>, E.show_pair_smem);
         set_smem((const void*)ks_show_pair<256>, E.show_pair_smem);
-        for (const void* fn : {(const void*)ks_show_pair<128>, (const void*)ks_show_pair<256>}) {
+        const std::pair<const void*, int> show_fns[2] = {{(const void*)ks_show_pair<128>, 128},
+                                                         {(const void*)ks_show_pair<256>, 256}};
+        for (const auto& fn_nt : show_fns) {
             cudaFuncAttributes fa;
-            CK(cudaFuncGetAttributes(&fa, fn));
-            if ((size_t)fa.maxDynamicSharedSizeBytes < E.show_pair_smem || fa.maxThreadsPerBlock < 256)
+            CK(cudaFuncGetAttributes(&fa, fn_nt.first));
+            if ((size_t)fa.maxDynamicSharedSizeBytes < E.show_pair_smem || fa.maxThreadsPerBlock < fn_nt.second)
                 throw Error("showdown kernel limits: " + std::to_string(fa.maxDynamicSharedSizeBytes) +
                             " B dynamic shared memory (needs " + std::to_string(E.show_pair_smem) + "), " +
                             std::to_string(fa.maxThreadsPerBlock) + " threads, " + std::to_string(fa.numRegs) +
