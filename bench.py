@@ -638,7 +638,7 @@ def main():
     ap.add_argument("--report-flops", type=int, default=184)
     ap.add_argument("--report-workers", type=int, default=8)
     ap.add_argument("--storage", default="i16sr", choices=["i16sr", "compressed", "f32", "fp8"])
-    ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged"])
+    ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged", "staged_river"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3, help="timed CPU-oracle iterations (after one warm-up)")

@@ -46,7 +46,7 @@ class GpuInfo(C.Structure):
                 ("reach_slots", C.c_uint64 * 2), ("device_action_nodes", C.c_uint64 * 2),
                 ("visited_terminals", C.c_uint64), ("num_levels", C.c_uint32), ("num_river_slots", C.c_uint32),
                 ("arena_format", C.c_int32), ("iter_bytes", C.c_double), ("upload_bytes", C.c_uint64),
-                ("iteration_kernels", C.c_uint32)]
+                ("iteration_kernels", C.c_uint32), ("river_programs", C.c_uint32)]
 
 
 class NodeInfo(C.Structure):
@@ -411,7 +411,7 @@ class GpuSolver:
         terminal sums), "fused32" (fused, f32 terminal sums) or "warp" (one
         warp per action node, fold children evaluated by that warp)."""
         h = C.c_void_p()
-        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}[engine]
+        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4, "staged_river": 5}[engine]
         _check(lib().gtob_gpu_new_ex(solver._h, DEVICE_FORMAT[device_format], eng, C.byref(h)))
         self._h = h
         self.solver = solver
@@ -492,7 +492,7 @@ class GpuSolver:
         device memory.  Returns (solver, gpu); the host solver holds only the
         blocks the device does not, the rest after gpu.sync_to_cpu()."""
         sh, gh = C.c_void_p(), C.c_void_p()
-        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}[engine]
+        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4, "staged_river": 5}[engine]
         _check(lib().gtob_gpu_load(os.fspath(path).encode(), STORAGE[storage], DEVICE_FORMAT[device_format], eng,
                                    C.byref(sh), C.byref(gh)))
         with open(path, "rb") as f:
@@ -587,7 +587,7 @@ class GpuSolver:
         return ms.value
 
 
-ENGINES = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}
+ENGINES = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4, "staged_river": 5}
 
 
 def nccl_unique_id():
@@ -660,7 +660,7 @@ class Batch:
                  keep_solvers=True):
         self.spots = list(spots)
         arr = (C.c_void_p * len(self.spots))(*[sp._h for sp in self.spots])
-        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4}[engine]
+        eng = {"fused": 0, "plain": 1, "fused32": 2, "warp": 3, "staged": 4, "staged_river": 5}[engine]
         h = C.c_void_p()
         _check(lib().gtob_batch_new(arr, len(self.spots), STORAGE[storage], ALGO[algo], int(use_iso),
                                     DEVICE_FORMAT[device_format], eng, int(bool(keep_solvers)), C.byref(h)))

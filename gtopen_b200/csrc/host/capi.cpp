@@ -372,7 +372,7 @@ int gtob_nccl_unique_id(unsigned char out[128]) {
 int gtob_gpu_new_sharded(const gtob_solver* v, int fmt, int engine, int rank, int world, const unsigned char id[128],
                          gtob_gpu** out) {
     REQUIRE(v && id && out && world >= 1 && rank >= 0 && rank < world && fmt >= -1 && fmt <= 3 &&
-            engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+            engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED_RIVER);
     *out = nullptr;
     API_BEGIN
     auto red = make_nccl_reducer(rank, world, id);
@@ -381,7 +381,7 @@ int gtob_gpu_new_sharded(const gtob_solver* v, int fmt, int engine, int rank, in
 }
 int gtob_shards_new(const gtob_solver* v, int fmt, int engine, int nshards, gtob_shards** out) {
     REQUIRE(v && out && nshards >= 1 && nshards <= 64 && fmt >= -1 && fmt <= 3 && engine >= GTOB_ENGINE_FUSED &&
-            engine <= GTOB_ENGINE_STAGED);
+            engine <= GTOB_ENGINE_STAGED_RIVER);
     *out = nullptr;
     API_BEGIN
     auto g = std::make_unique<gtob_shards>();
@@ -467,7 +467,7 @@ struct gtob_batch {
 int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int use_iso, int fmt, int engine, int keep,
                    gtob_batch** out) {
     REQUIRE(spots && out && n > 0 && (storage == 0 || storage == 1) && algo >= 0 && algo <= 2 && fmt >= -1 &&
-            fmt <= 3 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+            fmt <= 3 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED_RIVER);
     *out = nullptr;
     for (int i = 0; i < n; i++) REQUIRE(spots[i]);
     API_BEGIN
@@ -534,7 +534,7 @@ int gtob_gpu_save(gtob_gpu* g, const gtob_solver* v, const char* path) {
 }
 int gtob_gpu_load(const char* path, int storage, int fmt, int engine, gtob_solver** solver_out, gtob_gpu** gpu_out) {
     REQUIRE(path && solver_out && gpu_out && (storage == 0 || storage == 1) && fmt >= -1 && fmt <= 3 &&
-            engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+            engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED_RIVER);
     *solver_out = nullptr;
     *gpu_out = nullptr;
     API_BEGIN
@@ -549,7 +549,7 @@ int gtob_gpu_load(const char* path, int storage, int fmt, int engine, gtob_solve
 }
 int gtob_gpu_new(const gtob_solver* v, int fmt, gtob_gpu** out) { return gtob_gpu_new_ex(v, fmt, GTOB_ENGINE_STAGED, out); }
 int gtob_gpu_new_ex(const gtob_solver* v, int fmt, int engine, gtob_gpu** out) {
-    REQUIRE(v && out && fmt >= -1 && fmt <= 3 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+    REQUIRE(v && out && fmt >= -1 && fmt <= 3 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED_RIVER);
     *out = nullptr;
     API_BEGIN
     *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt, engine)};
@@ -617,6 +617,7 @@ int gtob_gpu_info_get(gtob_gpu* g, gtob_gpu_info* o) {
     o->arena_format = g->e->format();
     o->iter_bytes = g->e->iter_bytes();
     o->upload_bytes = g->e->upload_bytes();
+    o->river_programs = g->e->river_programs();
     API_BEGIN
     o->iteration_kernels = g->e->iteration_kernels();  // captures the iteration graph if it is not yet
     API_END
@@ -713,7 +714,7 @@ int gtob_net_train(gtob_net* n, const float* x, const float* t, const float* mas
     API_END
 }
 int gtob_gpu_new_dl(const gtob_solver* v, gtob_net* net, int fmt, int engine, gtob_gpu** out) {
-    REQUIRE(v && net && out && fmt >= -1 && fmt <= 3 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED);
+    REQUIRE(v && net && out && fmt >= -1 && fmt <= 3 && engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED_RIVER);
     *out = nullptr;
     API_BEGIN
     *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt, engine, net->n)};

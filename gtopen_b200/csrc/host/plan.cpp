@@ -4,6 +4,7 @@
 #include "plan.hpp"
 
 #include <algorithm>
+#include <cstring>
 #include <atomic>
 #include <exception>
 #include <memory>
@@ -22,6 +23,7 @@ struct Visit {
     uint32_t cslot;
     uint32_t rs[2];
     uint32_t slot;  // river slot once the board is complete, else kNoSlot
+    uint8_t from_chance;  // the node's parent deals a card (or it is a river spot's root)
 };
 bool is_terminal(uint8_t k) { return k == kFold || k == kShowdown; }
 
@@ -43,10 +45,10 @@ struct Builder {
     Plan& P;
     std::vector<uint8_t>& visited;
     bool fused, fuse_folds, spawn;
-    Levels<ActItem> act_l[2];  // by actor
+    Levels<ActItem> act_l[4];  // by actor and river round: [2 * actor + in_river]
     Levels<EdgeItem> edge_l;
     Levels<FoldItem> fold_l;
-    Levels<ShowItem> show_l;
+    Levels<ShowItem> show_l[2];  // [in_river]: showdowns that end a river betting round
     Levels<ChanceItem> chance_l;
     std::vector<ChildRef> crefs;
     std::vector<TermInfo> terms;
@@ -59,6 +61,7 @@ struct Builder {
     uint32_t max_children = 0;
     std::vector<uint32_t> nodes;  // the nodes visited (their slot entries are remapped at the merge)
     std::vector<Visit> tasks;     // root builder: the subtrees handed out
+    std::vector<Visit> rroots;    // roots of river betting rounds (their visits)
     bool cut = false;             // root builder of a depth-limited plan
     std::vector<LeafItem> leaves;
     std::vector<uint32_t> cbase_of, rbase_of[2];
@@ -71,11 +74,11 @@ struct Builder {
     bool in_place(uint8_t kind) const { return kind == kFold ? fuse_folds : kind == kShowdown ? fused : false; }
     void grow(uint32_t lv) {
         if (edge_l.size() <= lv) {
-            act_l[0].resize(lv + 1);
-            act_l[1].resize(lv + 1);
+            for (auto& x : act_l) x.resize(lv + 1);
             edge_l.resize(lv + 1);
             fold_l.resize(lv + 1);
-            show_l.resize(lv + 1);
+            show_l[0].resize(lv + 1);
+            show_l[1].resize(lv + 1);
             chance_l.resize(lv + 1);
         }
     }
@@ -141,12 +144,15 @@ struct Builder {
                         Visit cv = v;
                         cv.node = c;
                         cv.level = v.level + 1;
+                        cv.from_chance = 0;
                         cv.cslot = (uint32_t)next_c++;
                         cv.rs[a] = (uint32_t)next_r[a]++;
                         crefs.push_back({kChildNode, cv.cslot, cv.rs[a], kNoSlot});
                         kids[nkids++] = cv;
                     }
-                    act_l[a][v.level].push_back({nd, it});
+                    const int in_river = t.street[nd] == 2 ? 1 : 0;
+                    if (in_river && v.from_chance) rroots.push_back(v);
+                    act_l[2 * a + in_river][v.level].push_back({nd, it});
                     for (int k = nkids - 1; k >= 0; k--) stack.push_back(kids[k]);
                     break;
                 }
@@ -198,6 +204,7 @@ struct Builder {
                         Visit cv = v;
                         cv.node = c;
                         cv.level = v.level + 1;
+                        cv.from_chance = 1;
                         cv.dealt[0] = d2[0];
                         cv.dealt[1] = d2[1];
                         cv.ndealt = v.ndealt + 1;
@@ -235,7 +242,7 @@ struct Builder {
                 default: {
                     ShowItem si{v.cslot, {v.rs[0], v.rs[1]}, v.slot != kNoSlot ? v.slot : river_slot(v.dealt, v.ndealt),
                                 (float)t.twin[nd], (float)t.tlose[nd], (float)t.ttie[nd], 0};
-                    show_l[v.level].push_back({nd, si});
+                    show_l[!v.from_chance && t.street[nd] == 2 ? 1 : 0][v.level].push_back({nd, si});
                     visited_terminals++;
                     break;
                 }
@@ -283,9 +290,96 @@ void flat_copy(const FlatLayout& L, size_t b, size_t g, Levels<T>& ls, V& flat) 
         std::vector<std::pair<uint32_t, T>>().swap(ls[lv]);
     }
 }
+// River programs (plan.hpp): one depth-first step list per river betting
+// round.  P.river stays false, and the level sweeps keep these nodes, when a
+// round does not fit the river kernel (an action node with more than kSKA
+// actions, deeper than kRiverMaxDepth, or players not alternating from OOP).
+constexpr int kRiverMaxActions = 4;
+void build_river_programs(const Spot& sp, Plan& P, std::vector<Visit>& roots, unsigned threads) {
+    const Tree& t = sp.tree;
+    const size_t n = roots.size();
+    if (!n) return;
+    std::vector<std::vector<RStep>> prog(n);
+    std::vector<uint32_t> depth(n, 0);
+    std::atomic<bool> ok{true};
+    parallel_for((n + 255) / 256, [&](size_t c) {
+        struct Fr { uint32_t node; uint32_t depth, k, next; };
+        std::vector<Fr> st;
+        for (size_t r = c * 256; r < std::min(n, (c + 1) * 256); r++) {
+            std::vector<RStep>& out = prog[r];
+            auto node_step = [&](uint8_t op, uint32_t nd, uint32_t d, uint32_t k) {
+                const int a = t.player[nd], na = t.nchild[nd];
+                if (na > kRiverMaxActions || d >= (uint32_t)kRiverMaxDepth || a != (int)(d & 1) ||
+                    t.kind[nd] != kAction || P.node_sidx[nd] < 0)
+                    ok = false;
+                RStep x{};
+                x.op = op;
+                x.depth = (uint8_t)d;
+                x.k = (uint8_t)k;
+                x.x = (uint8_t)(na | a << 7);
+                x.sidx = (uint32_t)std::max(P.node_sidx[nd], 0);
+                x.aoff = P.node_sidx[nd] >= 0 ? P.anode_off[a][P.node_sidx[nd]] : 0;
+                out.push_back(x);
+            };
+            st.clear();
+            node_step(kREnter, roots[r].node, 0, 0);
+            st.push_back({roots[r].node, 0, 0, 0});
+            while (!st.empty() && ok) {
+                Fr& f = st.back();
+                if (f.next < t.nchild[f.node]) {
+                    const uint32_t j = f.next++;
+                    const uint32_t ch = t.child(f.node, (int)j);
+                    const uint32_t d = f.depth;
+                    if (t.kind[ch] == kFold || t.kind[ch] == kShowdown) {
+                        RStep x{};
+                        x.op = t.kind[ch] == kFold ? kRFold : kRShow;
+                        x.depth = (uint8_t)d;
+                        x.k = (uint8_t)j;
+                        x.x = t.kind[ch] == kFold ? t.player[ch] : 0;
+                        const float tw = (float)t.twin[ch];
+                        std::memcpy(&x.sidx, &tw, 4);
+                        x.pay[0] = (float)t.tlose[ch];
+                        x.pay[1] = (float)t.ttie[ch];
+                        out.push_back(x);
+                    } else if (t.kind[ch] == kAction) {
+                        node_step(kREnter, ch, d + 1, j);
+                        depth[r] = std::max(depth[r], d + 1);
+                        st.push_back({ch, d + 1, j, 0});
+                    } else {
+                        ok = false;  // a chance node inside a river round
+                    }
+                } else {
+                    node_step(kRExit, f.node, f.depth, f.k);
+                    st.pop_back();
+                }
+            }
+        }
+    }, threads);
+    if (!ok) return;
+    std::vector<uint32_t> order(n);
+    for (size_t r = 0; r < n; r++) order[r] = (uint32_t)r;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return prog[a].size() > prog[b].size(); });
+    size_t total = 0;
+    P.rtrees.resize(n);
+    for (size_t i = 0; i < n; i++) {
+        const uint32_t r = order[i];
+        const Visit& v = roots[r];
+        P.rtrees[i] = RTree{(uint32_t)total, (uint32_t)prog[r].size(), {v.rs[0], v.rs[1]}, v.cslot, v.slot, v.node,
+                            depth[r]};
+        total += prog[r].size();
+        P.river_depth = std::max<int>(P.river_depth, (int)depth[r]);
+    }
+    P.rsteps.resize(total);
+    parallel_for((n + 1023) / 1024, [&](size_t c) {
+        for (size_t i = c * 1024; i < std::min(n, (c + 1) * 1024); i++)
+            std::copy(prog[order[i]].begin(), prog[order[i]].end(), P.rsteps.begin() + P.rtrees[i].step_start);
+    }, threads);
+    P.river = true;
+}
 }  // namespace
 
-Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nshards, bool cut_turn) {
+Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nshards, bool cut_turn, bool river) {
     if (nshards < 1 || shard < 0 || shard >= nshards) throw Error("invalid argument: shard");
     if (cut_turn && (nshards > 1 || sp.tree.root_street != 0))
         throw Error("invalid argument: a depth-limited plan needs a flop spot and one shard");
@@ -312,7 +406,8 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
     root.cut = cut_turn;
     P.cut_turn = cut_turn;
     const bool full_board = sp.board.size() == 5;
-    root.run({0, 0, {0, 0}, 0, 0, {0, 0}, full_board ? root.river_slot(nullptr, 0) : kNoSlot});
+    root.run({0, 0, {0, 0}, 0, 0, {0, 0}, full_board ? root.river_slot(nullptr, 0) : kNoSlot,
+              (uint8_t)(t.root_street == 2 ? 1 : 0)});
     P.shard = shard;
     P.nshards = nshards;
     // Sharded: this shard's representative subtrees, and the root builder's
@@ -419,10 +514,10 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
             for (int g = 0; g < groups; g++) lists[b].push_back(&member(*bs[b], g));
         return flat_layout<typename L::value_type::value_type::second_type>(levels, lists);
     };
-    const FlatLayout La = layout_of([](Builder& b, int g) -> Levels<ActItem>& { return b.act_l[g]; }, 2);
+    const FlatLayout La = layout_of([](Builder& b, int g) -> Levels<ActItem>& { return b.act_l[g]; }, 4);
     const FlatLayout Le = layout_of([](Builder& b, int) -> Levels<EdgeItem>& { return b.edge_l; }, 1);
     const FlatLayout Lf = layout_of([](Builder& b, int) -> Levels<FoldItem>& { return b.fold_l; }, 1);
-    const FlatLayout Ls = layout_of([](Builder& b, int) -> Levels<ShowItem>& { return b.show_l; }, 1);
+    const FlatLayout Ls = layout_of([](Builder& b, int g) -> Levels<ShowItem>& { return b.show_l[g]; }, 2);
     const FlatLayout Lc = layout_of([](Builder& b, int) -> Levels<ChanceItem>& { return b.chance_l; }, 1);
     P.act.resize(La.total);
     P.edge.resize(Le.total);
@@ -430,8 +525,12 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
     P.show.resize(Ls.total);
     P.chance.resize(Lc.total);
     P.act_span = La.span;
-    P.act_span_actor[0] = La.gspan[0];
-    P.act_span_actor[1] = La.gspan[1];
+    for (int a = 0; a < 2; a++) {  // groups [upper actor 0 | river actor 0 | upper actor 1 | river actor 1]
+        P.act_span_upper[a] = La.gspan[2 * a];
+        for (size_t lv = 0; lv < levels; lv++)
+            P.act_span_actor[a].push_back(
+                {La.gspan[2 * a][lv].start, La.gspan[2 * a][lv].count + La.gspan[2 * a + 1][lv].count});
+    }
     P.edge_span = Le.span;
     P.fold_span = Lf.span;
     P.show_span = Ls.span;
@@ -449,9 +548,10 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
         };
         auto rr = [&](uint32_t& x, int q) { if (is_local(x)) x = B.r[q] + (x - kLocal); };
         auto rs = [&](uint32_t& x) { if (is_local(x)) x = B.slot[x - kLocal]; };
-        for (int q = 0; q < 2; q++)
-            for (auto& lv : b.act_l[q])
+        for (int g = 0; g < 4; g++)
+            for (auto& lv : b.act_l[g])
                 for (auto& x : lv) {
+                    const int q = g >> 1;
                     ActItem& a = x.second;
                     for (uint32_t j = a.cref; j < a.cref + a.na; j++) {
                         ChildRef& cr = b.crefs[j];
@@ -475,7 +575,8 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
                 rc(x.second.cslot);
                 for (int q = 0; q < 2; q++) rr(x.second.rs[q], q);
             }
-        for (auto& lv : b.show_l)
+        for (auto& sl : b.show_l)
+          for (auto& lv : sl)
             for (auto& x : lv) {
                 rc(x.second.cslot);
                 for (int q = 0; q < 2; q++) rr(x.second.rs[q], q);
@@ -492,6 +593,12 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
             if (ce.term != kNoSlot) ce.term += B.term;
         }
         for (auto& ti : b.terms) rs(ti.aux);  // a showdown's slot; a fold's folding player stays
+        for (auto& v : b.rroots) {
+            rc(v.cslot);
+            rr(v.rs[0], 0);
+            rr(v.rs[1], 1);
+            rs(v.slot);
+        }
         for (uint32_t nd : b.nodes) {
             rc(P.node_cslot[nd]);
             rr(P.node_rs[0][nd], 0);
@@ -503,10 +610,11 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
         std::vector<ChildRef>().swap(b.crefs);
         std::vector<TermInfo>().swap(b.terms);
         std::vector<CardEntry>().swap(b.cards);
-        for (int q = 0; q < 2; q++) flat_copy(La, i, q, b.act_l[q], P.act);
+        for (int g = 0; g < 4; g++) flat_copy(La, i, g, b.act_l[g], P.act);
         flat_copy(Le, i, 0, b.edge_l, P.edge);
         flat_copy(Lf, i, 0, b.fold_l, P.fold);
-        flat_copy(Ls, i, 0, b.show_l, P.show);
+        flat_copy(Ls, i, 0, b.show_l[0], P.show);
+        flat_copy(Ls, i, 1, b.show_l[1], P.show);
         flat_copy(Lc, i, 0, b.chance_l, P.chance);
     }, threads);
     for (Builder* b : bs) {
@@ -546,24 +654,28 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
     // showdowns of a level sorted by river slot and cut into batches of at
     // most kShowBatch with one slot each: a batch's CTA loads the slot's
     // tables once for all of them
+    // (per level: the showdowns outside river rounds, then those inside)
     for (size_t l = 0; l < P.show_span.size(); l++) {
-        const Span s = P.show_span[l];
-        auto first = P.show.begin() + s.start;
-        {  // stable counting sort by slot
-            std::vector<uint32_t> cnt(P.slot_key.size() + 1, 0);
-            for (uint32_t k = 0; k < s.count; k++) cnt[first[k].slot + 1]++;
-            for (size_t k = 1; k < cnt.size(); k++) cnt[k] += cnt[k - 1];
-            std::vector<ShowItem> tmp(s.count);
-            for (uint32_t k = 0; k < s.count; k++) tmp[cnt[first[k].slot]++] = first[k];
-            std::copy(tmp.begin(), tmp.end(), first);
-        }
         const uint32_t b0 = (uint32_t)P.show_batch.size();
-        for (uint32_t k = 0; k < s.count;) {
-            const uint32_t slot = P.show[s.start + k].slot;
-            uint32_t e = k;
-            while (e < s.count && e - k < (uint32_t)kShowBatch && P.show[s.start + e].slot == slot) e++;
-            P.show_batch.push_back({s.start + k, e - k, slot, 0});
-            k = e;
+        for (int g = 0; g < 2; g++) {
+            const Span s = Ls.gspan[g][l];
+            auto first = P.show.begin() + s.start;
+            {  // stable counting sort by slot
+                std::vector<uint32_t> cnt(P.slot_key.size() + 1, 0);
+                for (uint32_t k = 0; k < s.count; k++) cnt[first[k].slot + 1]++;
+                for (size_t k = 1; k < cnt.size(); k++) cnt[k] += cnt[k - 1];
+                std::vector<ShowItem> tmp(s.count);
+                for (uint32_t k = 0; k < s.count; k++) tmp[cnt[first[k].slot]++] = first[k];
+                std::copy(tmp.begin(), tmp.end(), first);
+            }
+            for (uint32_t k = 0; k < s.count;) {
+                const uint32_t slot = P.show[s.start + k].slot;
+                uint32_t e = k;
+                while (e < s.count && e - k < (uint32_t)kShowBatch && P.show[s.start + e].slot == slot) e++;
+                P.show_batch.push_back({s.start + k, e - k, slot, 0});
+                k = e;
+            }
+            if (g == 0) P.show_batch_span_upper.push_back({b0, (uint32_t)P.show_batch.size() - b0});
         }
         P.show_batch_span.push_back({b0, (uint32_t)P.show_batch.size() - b0});
     }
@@ -661,6 +773,11 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
     for (int p = 0; p < 2; p++) {
         P.zero_off[p].push_back((uint32_t)P.zero_idx[p].size());
         P.bin_off[p].push_back((uint32_t)P.bin_start[p].size());
+    }
+    if (river && fuse_mode == kFuseFolds) {
+        std::vector<Visit> roots;
+        for (Builder* b : bs) roots.insert(roots.end(), b->rroots.begin(), b->rroots.end());
+        build_river_programs(sp, P, roots, threads);
     }
     return P;
 }

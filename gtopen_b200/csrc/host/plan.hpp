@@ -115,6 +115,35 @@ struct LeafItem {
     uint32_t level, pad;
 };
 
+// River subtree programs.  Every visited river betting round (an action node
+// on the river whose parent deals the river, or the root of a river spot)
+// is solved by one CTA walking the subtree depth first (cfr_river.cuh); its
+// walk is a list of steps in pre-order, children in order:
+//   kREnter  an action node: its depth, its index among its parent's children,
+//            action count, actor, per-player compact index and arena offset;
+//   kRExit   the same node once its last child is done (the same fields);
+//   kRFold / kRShow  a terminal child of the node at `depth`: its index k and
+//            payoffs (fold: the folding player in `x`).
+enum RStepOp : uint8_t { kREnter = 0, kRExit = 1, kRFold = 2, kRShow = 3 };
+struct alignas(16) RStep {
+    uint8_t op, depth, k, x;  // x: na | actor << 7 (enter / exit), folding player (fold)
+    uint32_t sidx;            // enter / exit: compact index; terminals: bits of twin
+    union {
+        uint64_t aoff;        // enter / exit: arena offset (elements) in the actor's arena
+        float pay[2];         // terminals: tlose, ttie
+    };
+};
+static_assert(sizeof(RStep) == 16, "RStep layout");
+struct alignas(16) RTree {
+    uint32_t step_start, step_count;
+    uint32_t rs[2];  // both players' reach slots at the subtree root
+    uint32_t cslot;  // the root's cfv slot (its value for the traverser goes there)
+    uint32_t slot;   // the river board (dense river slot)
+    uint32_t node;   // tree node id of the root
+    uint32_t depth;  // deepest action node below the root (root = 0)
+};
+constexpr int kRiverMaxDepth = 8;  // river subtrees deeper than this keep the level sweeps
+
 // Vectors of plain records whose resize does not zero them: the plan's flat
 // tables are written in parallel right after they are sized, so the first
 // touch of their pages happens on the worker threads.
@@ -237,6 +266,16 @@ struct Plan {
     std::vector<uint16_t> hcard_idx[2];
     uint64_t visited_action_elems[2] = {0, 0};
     uint64_t visited_terminals = 0;
+    // River programs (staged engine).  Action nodes and showdowns inside
+    // river betting rounds sit after the other nodes of their level (within
+    // each actor's run for action nodes); the *_upper spans leave them out,
+    // and the river sweep solves them with one program per subtree instead.
+    bool river = false;                        // programs built (every river subtree qualifies)
+    std::vector<Span> act_span_upper[2];       // per level and actor: nodes outside river rounds
+    std::vector<Span> show_batch_span_upper;   // per level: batches of showdowns outside river rounds
+    std::vector<RTree> rtrees;                 // largest first
+    PodVec<RStep> rsteps;
+    int river_depth = 0;                       // deepest river action node (root = 0), over all programs
 };
 
 // shard / nshards: the representative subtrees below the first chance nodes
@@ -247,6 +286,8 @@ struct Plan {
 // cut_turn: a depth-limited plan -- every chance node that deals the turn
 // and leads to more betting becomes a leaf (Plan::leaves) instead of a
 // subtree; all-in runouts stay exact.
-Plan build_plan(const Spot& spot, bool use_iso, int fuse_mode, int shard = 0, int nshards = 1, bool cut_turn = false);
+// river: also build the river programs (fuse_mode kFuseFolds only).
+Plan build_plan(const Spot& spot, bool use_iso, int fuse_mode, int shard = 0, int nshards = 1, bool cut_turn = false,
+                bool river = false);
 
 }  // namespace gtob

@@ -68,6 +68,10 @@ struct Dev {
     const uint32_t* hinfo[2];   // per hand: c1 | c2 << 6 | same << 16 (0xFFFF: no same combo)
     const uint16_t* hcard52[2]; // per card: the hands holding it, 52 slots, 0xFFFF after the last
     const uint32_t* node_id[2];  // tree node id of each device action node (per player, by sidx)
+    // river programs: per player o, the showdown table images of every river
+    // board (river_tab_words words each) and their word offsets (num_slots + 1)
+    const uint32_t* rtab[2];
+    const uint32_t* rtab_off[2];
 };
 struct Arenas {
     void* reg[2];

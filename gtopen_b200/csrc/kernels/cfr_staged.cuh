@@ -242,26 +242,28 @@ __device__ __forceinline__ void s_node_sigma(const Dev& d, long long loff, int a
     }
 }
 
-// Block maxima of three values behind one barrier (sh: 3 * kSWarps floats,
+// Block maxima of three values behind one barrier (sh: 3 * NT / 32 floats,
 // written once per CTA).
+template <int NT = kSThreads>
 __device__ __forceinline__ void s_block_max3(float& a, float& b, float& c, float* sh) {
+    constexpr int W = NT / 32;
     a = warp_max(a);
     b = warp_max(b);
     c = warp_max(c);
     if ((threadIdx.x & 31) == 0) {
         sh[threadIdx.x >> 5] = a;
-        sh[kSWarps + (threadIdx.x >> 5)] = b;
-        sh[2 * kSWarps + (threadIdx.x >> 5)] = c;
+        sh[W + (threadIdx.x >> 5)] = b;
+        sh[2 * W + (threadIdx.x >> 5)] = c;
     }
     __syncthreads();
     a = sh[0];
-    b = sh[kSWarps];
-    c = sh[2 * kSWarps];
+    b = sh[W];
+    c = sh[2 * W];
 #pragma unroll
-    for (int k = 1; k < kSWarps; k++) {
+    for (int k = 1; k < W; k++) {
         a = fmaxf(a, sh[k]);
-        b = fmaxf(b, sh[kSWarps + k]);
-        c = fmaxf(c, sh[2 * kSWarps + k]);
+        b = fmaxf(b, sh[W + k]);
+        c = fmaxf(c, sh[2 * W + k]);
     }
 }
 
@@ -445,6 +447,211 @@ struct UpShared {  // static shared memory of ks_up
     long long dred[kSWarps];
     float red[3 * kSWarps];
 };
+// The traverser's node once its children's values are staged (cv, row k at
+// cv + k * vstride) and, for the update, its regret / strategy-sum /
+// prediction blocks (b_reg, b_str, b_pred) and own reach (rp): a locked
+// node's value, an evaluation sweep's value (best response or average), or
+// the CFR update (cfr.rs:297-409) with the blocks and scales written back.
+// The node's value per hand goes to out[i] (added to it when acc_out).
+__device__ __forceinline__ void s_put(float* out, int i, float v, bool add) {
+    if (add) out[i] += v;
+    else out[i] = v;
+}
+template <int FMT, int EVAL, int NA, int NT>
+__device__ __forceinline__ void s_mine_node(const Dev& d, const Arenas& ar, int p, int mode, long long loff, float kr,
+                                            float kp, float sscale, uint32_t sidx, uint64_t aoff, bool use_pred,
+                                            unsigned char* b_reg, unsigned char* b_str, unsigned char* b_pred,
+                                            float* cv, int vstride, const float* rp, float* out, bool acc_out,
+                                            float* s_red) {
+    const int nh = d.nh[p];
+    constexpr int na = NA;
+    const int esz = fmt_bytes(FMT);
+    const unsigned blk = round16((unsigned)(na * nh * esz));
+    float sig[kSKA];
+#define CHILD_V(k, i) (cv[(k) * vstride + (i)])
+    if (loff >= 0) {  // locked: fixed sigma, no update
+        for (int i = threadIdx.x; i < nh; i += NT) {
+            float acc = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) acc += d.lock_sig[loff + (long long)k * nh + i] * CHILD_V(k, i);
+            s_put(out, i, acc, acc_out);
+        }
+        return;
+    }
+    if (EVAL) {
+        for (int i = threadIdx.x; i < nh; i += NT) {
+            float acc;
+            if (mode == 0) {
+                acc = CHILD_V(0, i);
+#pragma unroll
+                for (int k = 1; k < kSKA; k++)
+                    if (k < na) {
+                        const float v = CHILD_V(k, i);
+                        if (v > acc) acc = v;
+                    }
+            } else {
+                s_average_sigma<FMT>(b_str, na, i, sig);
+                acc = 0.0f;
+#pragma unroll
+                for (int k = 0; k < kSKA; k++)
+                    if (k < na) acc += sig[k] * CHILD_V(k, i);
+            }
+            s_put(out, i, acc, acc_out);
+        }
+        return;
+    }
+    const float pos = d.disc[0], neg = d.disc[1], ds = d.disc[2];
+    const void* predp = use_pred ? b_pred : nullptr;
+    float v[kSKA];
+    if (FMT == kDevF32) {
+        float* R = (float*)b_reg;
+        float* Sg = (float*)b_str;
+        float* PR = (float*)b_pred;
+        for (int i = threadIdx.x; i < nh; i += NT) {
+            s_regret_sigma<FMT>(b_reg, predp, 0.0f, 0.0f, na, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float r_p = rp[i];
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const float r = R[b + k];
+                    R[b + k] = r * (r > 0.0f ? pos : neg) + (v[k] - o_);
+                    Sg[b + k] = Sg[b + k] * ds + r_p * sig[k];
+                    if (use_pred) PR[b + k] = v[k] - o_;
+                }
+            s_put(out, i, o_, acc_out);
+        }
+        __syncthreads();
+        store_block((unsigned char*)ar.reg[p] + aoff * esz, b_reg, blk);
+        store_block((unsigned char*)ar.str[p] + aoff * esz, b_str, blk);
+        if (use_pred) store_block((unsigned char*)ar.pred[p] + aoff * esz, b_pred, blk);
+        return;
+    }
+    // Quantised arenas (cfr.rs:350-407): 16-bit, or FP8 with the same steps.
+    using Q = QT<FMT == kDevFP8 ? kDevFP8 : kDevI16>;
+    const float kss = sscale / Q::kS * ds;
+    float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
+    const bool one_pass = FMT == kDevI16 && !use_pred;
+    if (one_pass) {
+        int16_t* RQ = (int16_t*)b_reg;
+        uint16_t* SQ = (uint16_t*)b_str;
+        // Pass 1 computes every entry's new regret and strategy sum and the
+        // node's maxima, keeping the f32 values in place of what it consumed:
+        // the new regret where the child's value was, the new strategy sum's
+        // bits split over the entry's two old 16-bit quants (each entry is
+        // read and rewritten by the thread that owns its hand).  Pass 2 only
+        // requantises.
+        uint16_t* SQ_lo = (uint16_t*)b_reg;
+        for (int i = threadIdx.x; i < nh; i += NT) {
+            s_regret_sigma<FMT>(b_reg, nullptr, kr, kp, na, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float r_p = rp[i];
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const int16_t qv = RQ[b + k];
+                    const float nr = (float)qv * kr * (qv > 0 ? pos : neg) + (v[k] - o_);
+                    const float ns = (float)SQ[b + k] * kss + r_p * sig[k];
+                    rmax = fmaxf(rmax, fabsf(nr));
+                    smax = fmaxf(smax, ns);
+                    cv[k * vstride + i] = nr;
+                    const uint32_t bits = __float_as_uint(ns);
+                    SQ_lo[b + k] = (uint16_t)(bits & 0xFFFFu);
+                    SQ[b + k] = (uint16_t)(bits >> 16);
+                }
+            s_put(out, i, o_, acc_out);
+        }
+        s_block_max3<NT>(rmax, smax, pmax, s_red);
+        const float rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
+        const float sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
+        const uint32_t sr_b = ar.sr ? sr_base(d.node_id[p][sidx], *d.iter) : 0u;
+        for (int i = threadIdx.x; i < nh; i += NT) {
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const float nr = cv[k * vstride + i];
+                    const float ns = __uint_as_float((uint32_t)SQ_lo[b + k] | ((uint32_t)SQ[b + k] << 16));
+                    requant16(nr, ns, rk, sk, ar.sr, sr_b, i, k, &RQ[b + k], &SQ[b + k]);
+                }
+        }
+    }
+    // Otherwise (PCFR+ predictions, or FP8, whose quants leave no room for
+    // the f32 values): pass 1 finds the maxima, pass 2 recomputes from the
+    // unchanged staged quants and requantises in place.
+    typename Q::R* RQ = (typename Q::R*)b_reg;
+    typename Q::S* SQ = (typename Q::S*)b_str;
+    typename Q::R* PQ = (typename Q::R*)b_pred;
+    const uint32_t sr_b2 = ar.sr && !one_pass ? sr_base(d.node_id[p][sidx], *d.iter) : 0u;
+    for (int pass = one_pass ? 2 : 0; pass < 2; pass++) {
+        float rk = 0.0f, sk = 0.0f, pk = 0.0f;
+        if (pass == 1) {
+            s_block_max3<NT>(rmax, smax, pmax, s_red);
+            rk = (rmax > 0.0f && isfinite(rmax)) ? Q::kR / rmax : 0.0f;
+            sk = (smax > 0.0f && isfinite(smax)) ? Q::kS / smax : 0.0f;
+            pk = (pmax > 0.0f && isfinite(pmax)) ? Q::kR / pmax : 0.0f;
+        }
+        for (int i = threadIdx.x; i < nh; i += NT) {
+            s_regret_sigma<FMT>(b_reg, predp, kr, kp, na, i, sig);
+            float o_ = 0.0f;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    v[k] = CHILD_V(k, i);
+                    o_ += sig[k] * v[k];
+                }
+            const float r_p = rp[i];
+            const int b = i * na;
+#pragma unroll
+            for (int k = 0; k < kSKA; k++)
+                if (k < na) {
+                    const float dv = Q::dr(RQ[b + k]);  // the discount follows the stored sign
+                    const float nr = dv * kr * (dv > 0.0f ? pos : neg) + (v[k] - o_);
+                    const float ns = Q::ds(SQ[b + k]) * kss + r_p * sig[k];
+                    if (pass == 0) {
+                        rmax = fmaxf(rmax, fabsf(nr));
+                        smax = fmaxf(smax, ns);
+                        if (use_pred) pmax = fmaxf(pmax, fabsf(v[k] - o_));
+                    } else {
+                        if (FMT == kDevI16) {
+                            requant16(nr, ns, rk, sk, ar.sr, sr_b2, i, k, (int16_t*)&RQ[b + k],
+                                      (uint16_t*)&SQ[b + k]);
+                        } else {
+                            RQ[b + k] = rk > 0.0f ? Q::er(nr * rk) : (typename Q::R)0;
+                            SQ[b + k] = sk > 0.0f ? Q::es(fmaxf(ns, 0.0f) * sk) : (typename Q::S)0;
+                        }
+                        if (use_pred) PQ[b + k] = pk > 0.0f ? Q::er((v[k] - o_) * pk) : (typename Q::R)0;
+                    }
+                }
+            if (pass == 1) s_put(out, i, o_, acc_out);
+        }
+    }
+#undef CHILD_V
+    __syncthreads();
+    store_block((unsigned char*)ar.reg[p] + aoff * esz, b_reg, blk);
+    store_block((unsigned char*)ar.str[p] + aoff * esz, b_str, blk);
+    if (use_pred) store_block((unsigned char*)ar.pred[p] + aoff * esz, b_pred, blk);
+    if (threadIdx.x == 0) {
+        ar.rscale[p][sidx] = (rmax > 0.0f && isfinite(rmax)) ? rmax : 0.0f;
+        ar.sscale[p][sidx] = (smax > 0.0f && isfinite(smax)) ? smax : 0.0f;
+        if (use_pred) ar.pscale[p][sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
+    }
+}
 template <int FMT, int EVAL, int NA, bool MINE>
 __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const SNode& it, int p, int mode,
                                            unsigned char* sm, UpShared& us) {
@@ -522,7 +729,6 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     }
     if (!wait_staged(d, bar, &s_flag)) return;
 
-    float sig[kSKA];
     long long ftotal = 0;
     if (fk >= 0) {
         int fsc;
@@ -550,188 +756,9 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
         }
         return;
     }
-    if (loff >= 0) {  // locked: fixed sigma, no update
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
-            float acc = 0.0f;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) acc += d.lock_sig[loff + (long long)k * nh + i] * CHILD_V(k, i);
-            out[i] = acc;
-        }
-        return;
-    }
-    if (EVAL) {
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
-            float acc;
-            if (mode == 0) {
-                acc = CHILD_V(0, i);
-#pragma unroll
-                for (int k = 1; k < kSKA; k++)
-                    if (k < na) {
-                        const float v = CHILD_V(k, i);
-                        if (v > acc) acc = v;
-                    }
-            } else {
-                s_average_sigma<FMT>(b_str, na, i, sig);
-                acc = 0.0f;
-#pragma unroll
-                for (int k = 0; k < kSKA; k++)
-                    if (k < na) acc += sig[k] * CHILD_V(k, i);
-            }
-            out[i] = acc;
-        }
-        return;
-    }
-    const float pos = d.disc[0], neg = d.disc[1], ds = d.disc[2];
-    const void* predp = use_pred ? b_pred : nullptr;
-    float v[kSKA];
-    if (FMT == kDevF32) {
-        float* R = (float*)b_reg;
-        float* Sg = (float*)b_str;
-        float* PR = (float*)b_pred;
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
-            s_regret_sigma<FMT>(b_reg, predp, 0.0f, 0.0f, na, i, sig);
-            float o_ = 0.0f;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) {
-                    v[k] = CHILD_V(k, i);
-                    o_ += sig[k] * v[k];
-                }
-            const float r_p = rp[i];
-            const int b = i * na;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) {
-                    const float r = R[b + k];
-                    R[b + k] = r * (r > 0.0f ? pos : neg) + (v[k] - o_);
-                    Sg[b + k] = Sg[b + k] * ds + r_p * sig[k];
-                    if (use_pred) PR[b + k] = v[k] - o_;
-                }
-            out[i] = o_;
-        }
-        __syncthreads();
-        store_block((unsigned char*)ar.reg[p] + it.aoff * esz, b_reg, blk);
-        store_block((unsigned char*)ar.str[p] + it.aoff * esz, b_str, blk);
-        if (use_pred) store_block((unsigned char*)ar.pred[p] + it.aoff * esz, b_pred, blk);
-        return;
-    }
-    // Quantised arenas (cfr.rs:350-407): 16-bit, or FP8 with the same steps.
-    using Q = QT<FMT == kDevFP8 ? kDevFP8 : kDevI16>;
-    const float kss = sscale / Q::kS * ds;
-    float rmax = 0.0f, smax = 0.0f, pmax = 0.0f;
-    const bool one_pass = FMT == kDevI16 && !use_pred;
-    if (one_pass) {
-        int16_t* RQ = (int16_t*)b_reg;
-        uint16_t* SQ = (uint16_t*)b_str;
-        // Pass 1 computes every entry's new regret and strategy sum and the
-        // node's maxima, keeping the f32 values in place of what it consumed:
-        // the new regret where the child's value was, the new strategy sum's
-        // bits split over the entry's two old 16-bit quants (each entry is
-        // read and rewritten by the thread that owns its hand).  Pass 2 only
-        // requantises.
-        uint16_t* SQ_lo = (uint16_t*)b_reg;
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
-            s_regret_sigma<FMT>(b_reg, nullptr, kr, kp, na, i, sig);
-            float o_ = 0.0f;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) {
-                    v[k] = CHILD_V(k, i);
-                    o_ += sig[k] * v[k];
-                }
-            const float r_p = rp[i];
-            const int b = i * na;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) {
-                    const int16_t qv = RQ[b + k];
-                    const float nr = (float)qv * kr * (qv > 0 ? pos : neg) + (v[k] - o_);
-                    const float ns = (float)SQ[b + k] * kss + r_p * sig[k];
-                    rmax = fmaxf(rmax, fabsf(nr));
-                    smax = fmaxf(smax, ns);
-                    cv[k * vstride + i] = nr;
-                    const uint32_t bits = __float_as_uint(ns);
-                    SQ_lo[b + k] = (uint16_t)(bits & 0xFFFFu);
-                    SQ[b + k] = (uint16_t)(bits >> 16);
-                }
-            out[i] = o_;
-        }
-        s_block_max3(rmax, smax, pmax, s_red);
-        const float rk = (rmax > 0.0f && isfinite(rmax)) ? 32767.0f / rmax : 0.0f;
-        const float sk = (smax > 0.0f && isfinite(smax)) ? 65535.0f / smax : 0.0f;
-        const uint32_t sr_b = ar.sr ? sr_base(d.node_id[p][it.sidx], *d.iter) : 0u;
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
-            const int b = i * na;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) {
-                    const float nr = cv[k * vstride + i];
-                    const float ns = __uint_as_float((uint32_t)SQ_lo[b + k] | ((uint32_t)SQ[b + k] << 16));
-                    requant16(nr, ns, rk, sk, ar.sr, sr_b, i, k, &RQ[b + k], &SQ[b + k]);
-                }
-        }
-    }
-    // Otherwise (PCFR+ predictions, or FP8, whose quants leave no room for
-    // the f32 values): pass 1 finds the maxima, pass 2 recomputes from the
-    // unchanged staged quants and requantises in place.
-    typename Q::R* RQ = (typename Q::R*)b_reg;
-    typename Q::S* SQ = (typename Q::S*)b_str;
-    typename Q::R* PQ = (typename Q::R*)b_pred;
-    const uint32_t sr_b2 = ar.sr && !one_pass ? sr_base(d.node_id[p][it.sidx], *d.iter) : 0u;
-    for (int pass = one_pass ? 2 : 0; pass < 2; pass++) {
-        float rk = 0.0f, sk = 0.0f, pk = 0.0f;
-        if (pass == 1) {
-            s_block_max3(rmax, smax, pmax, s_red);
-            rk = (rmax > 0.0f && isfinite(rmax)) ? Q::kR / rmax : 0.0f;
-            sk = (smax > 0.0f && isfinite(smax)) ? Q::kS / smax : 0.0f;
-            pk = (pmax > 0.0f && isfinite(pmax)) ? Q::kR / pmax : 0.0f;
-        }
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
-            s_regret_sigma<FMT>(b_reg, predp, kr, kp, na, i, sig);
-            float o_ = 0.0f;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) {
-                    v[k] = CHILD_V(k, i);
-                    o_ += sig[k] * v[k];
-                }
-            const float r_p = rp[i];
-            const int b = i * na;
-#pragma unroll
-            for (int k = 0; k < kSKA; k++)
-                if (k < na) {
-                    const float dv = Q::dr(RQ[b + k]);  // the discount follows the stored sign
-                    const float nr = dv * kr * (dv > 0.0f ? pos : neg) + (v[k] - o_);
-                    const float ns = Q::ds(SQ[b + k]) * kss + r_p * sig[k];
-                    if (pass == 0) {
-                        rmax = fmaxf(rmax, fabsf(nr));
-                        smax = fmaxf(smax, ns);
-                        if (use_pred) pmax = fmaxf(pmax, fabsf(v[k] - o_));
-                    } else {
-                        if (FMT == kDevI16) {
-                            requant16(nr, ns, rk, sk, ar.sr, sr_b2, i, k, (int16_t*)&RQ[b + k],
-                                      (uint16_t*)&SQ[b + k]);
-                        } else {
-                            RQ[b + k] = rk > 0.0f ? Q::er(nr * rk) : (typename Q::R)0;
-                            SQ[b + k] = sk > 0.0f ? Q::es(fmaxf(ns, 0.0f) * sk) : (typename Q::S)0;
-                        }
-                        if (use_pred) PQ[b + k] = pk > 0.0f ? Q::er((v[k] - o_) * pk) : (typename Q::R)0;
-                    }
-                }
-            if (pass == 1) out[i] = o_;
-        }
-    }
+    s_mine_node<FMT, EVAL, NA, kSThreads>(d, ar, p, mode, loff, kr, kp, sscale, it.sidx, it.aoff, use_pred, b_reg,
+                                           b_str, b_pred, cv, vstride, rp, out, false, s_red);
 #undef CHILD_V
-    __syncthreads();
-    store_block((unsigned char*)ar.reg[p] + it.aoff * esz, b_reg, blk);
-    store_block((unsigned char*)ar.str[p] + it.aoff * esz, b_str, blk);
-    if (use_pred) store_block((unsigned char*)ar.pred[p] + it.aoff * esz, b_pred, blk);
-    if (threadIdx.x == 0) {
-        ar.rscale[p][it.sidx] = (rmax > 0.0f && isfinite(rmax)) ? rmax : 0.0f;
-        ar.sscale[p][it.sidx] = (smax > 0.0f && isfinite(smax)) ? smax : 0.0f;
-        if (use_pred) ar.pscale[p][it.sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
-    }
 }
 // MINE: the launch's nodes are the traverser's (the update), else the
 // opponent's (sum of children); a launch never mixes the two.

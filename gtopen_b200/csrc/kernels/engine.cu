@@ -37,6 +37,7 @@
 
 #include "cfr_kernels.cuh"
 #include "cfr_staged.cuh"
+#include "cfr_river.cuh"
 #include "engine.hpp"
 
 namespace gtob {
@@ -125,6 +126,16 @@ struct EngineImpl {
     size_t st_mine_smem = 0, st_opp_smem = 0, st_down_smem = 0;  // staged kernels
     SNode* snodes = nullptr;                   // staged node records (same order as act)
     size_t show_pair_smem = 0;                                    // batched showdowns
+    // river programs (cfr_river.cuh): each river betting round solved by one
+    // CTA; the level sweeps then cover only the nodes outside river rounds
+    bool river = false;
+    bool levels_only = false;  // set while a query needs every node's slots (level sweeps everywhere)
+    RTree* rtrees = nullptr;
+    RStep* rsteps = nullptr;
+    int ntrees = 0;
+    RLayout rl[2]{};     // per traverser
+    int river_grid = 0;  // persistent CTAs (one per SM)
+    bool use_river() const { return river && !levels_only; }
     size_t chance_smem = 0;  // runout chance dynamic smem
     cudaGraphExec_t g_iter = nullptr;
     cudaGraphExec_t g_eval[2] = {nullptr, nullptr};
@@ -335,9 +346,14 @@ struct EngineImpl {
     // Up sweep of one level's action nodes.  The staged engine launches the
     // traverser's nodes and the opponent's separately (each launch's kernel is
     // specialised for its side and sized for its shared memory).
+    // The action nodes of level l the level sweeps cover: all of them, or,
+    // with river programs, those outside river betting rounds.
+    Span act_level(int l, int actor) const {
+        return use_river() ? plan.act_span_upper[actor][l] : plan.act_span_actor[actor][l];
+    }
     void launch_up_level(int l, int p, int eval) {
         if (staged) {
-            const Span mine = plan.act_span_actor[p][l], opp = plan.act_span_actor[1 - p][l];
+            const Span mine = act_level(l, p), opp = act_level(l, 1 - p);
             if (fmt == kFmtF32) {
                 staged_up<kDevF32, true>(mine, p, eval);
                 staged_up<kDevF32, false>(opp, p, eval);
@@ -400,8 +416,15 @@ struct EngineImpl {
         timed(pr, 0, [&] { k_copy_root<<<4, kThreads, 0, stream>>>(d); });
         const int L = plan.num_levels;
         for (int l = 0; l < L; l++) {
-            const Span sa = qmask == 3 ? plan.act_span[l] : plan.act_span_actor[qmask == 1 ? 0 : 1][l];
-            if (sa.count) timed(pr, 1, [&] { launch_down_action(sa, mode); });
+            if (use_river()) {  // two runs when both players' reach is refreshed
+                for (int q = 0; q < 2; q++) {
+                    const Span sq = act_level(l, q);
+                    if ((qmask >> q & 1) && sq.count) timed(pr, 1, [&] { launch_down_action(sq, mode); });
+                }
+            } else {
+                const Span sa = qmask == 3 ? plan.act_span[l] : plan.act_span_actor[qmask == 1 ? 0 : 1][l];
+                if (sa.count) timed(pr, 1, [&] { launch_down_action(sa, mode); });
+            }
             const Span se = plan.edge_span[l];
             if (se.count)
                 timed(pr, 2, [&] { k_down_chance<<<se.count, kThreads, 0, stream>>>(d, edge + se.start, qmask); });
@@ -427,6 +450,9 @@ struct EngineImpl {
         // depth-limited: the turn leaves' values from the network, before
         // any level of the up sweep reads them
         if (leaf) leaf->run(p, d.reach[0], (size_t)d.rstr[0], d.reach[1], (size_t)d.rstr[1], d.cfv, (size_t)d.nh_max, stream);
+        // every river betting round at once, before any level of the up sweep
+        // reads a round's root value (counted with the up sweep's action kind)
+        if (use_river()) timed(pr, 6, [&] { launch_river(p, eval); });
         // Terminal kernels (folds and showdowns with slots of their own) read
         // only reach vectors, so in a captured sweep they run on a second
         // stream, every level of them, beside the chain of chance and action
@@ -447,8 +473,8 @@ struct EngineImpl {
             reduce_level(l, p);  // a shard: the children of this level's top chance nodes from every shard
             const Span sc = plan.chance_span[l];
             if (sc.count) timed(pr, 5, [&] { launch_chance(sc, p); });
-            const Span sa = plan.act_span[l];
-            if (sa.count) timed(pr, 6, [&] { launch_up_level(l, p, eval); });
+            const bool any = use_river() ? act_level(l, 0).count + act_level(l, 1).count > 0 : plan.act_span[l].count > 0;
+            if (any) timed(pr, 6, [&] { launch_up_level(l, p, eval); });
         }
         if (fork) {
             CK(cudaEventRecord(ev_join, side));
@@ -456,14 +482,30 @@ struct EngineImpl {
         }
         CK(cudaGetLastError());
     }
+    template <int FMT>
+    void launch_river_t(int p, int eval) {
+        const RLayout& L = rl[p];
+        const int ms = (int)plan.max_sorted;
+        if (eval < 0)
+            kr_river<FMT, 0, kRiverNT><<<river_grid, kRiverNT, L.total, stream>>>(d, ar, rtrees, rsteps, ntrees, p, 0,
+                                                                               ms, L);
+        else
+            kr_river<FMT, 1, kRiverNT><<<river_grid, kRiverNT, L.total, stream>>>(d, ar, rtrees, rsteps, ntrees, p,
+                                                                               eval, ms, L);
+    }
+    void launch_river(int p, int eval) {
+        if (fmt == kFmtF32) launch_river_t<kDevF32>(p, eval);
+        else if (fmt == kFmtFP8) launch_river_t<kDevFP8>(p, eval);
+        else launch_river_t<kDevI16>(p, eval);
+    }
     void launch_terminals(int l, int p, cudaStream_t st, Profile* pr) {
         const Span sf = plan.fold_span[l];
         if (sf.count) timed(pr, 3, [&] { k_fold<<<sf.count, kThreads, 0, st>>>(d, fold + sf.start, p); });
         const Span ss = plan.show_span[l];
-        if (ss.count)
+        const Span sb = use_river() ? plan.show_batch_span_upper[l] : plan.show_batch_span[l];
+        if (staged ? sb.count > 0 : ss.count > 0)
             timed(pr, 4, [&] {
                 if (staged) {
-                    const Span sb = plan.show_batch_span[l];
                     if (plan.max_sorted > 384)
                         ks_show_pair<256><<<sb.count, 256, show_pair_smem, st>>>(d, show, show_batch + sb.start, p,
                                                                                   (int)plan.max_sorted);
@@ -560,6 +602,85 @@ struct EngineImpl {
     }
 };
 
+
+// River programs (cfr_river.cuh): the subtree list and steps, each river
+// board's showdown table image per player, the kernel's shared-memory layout
+// per traverser and its grid.  E.river stays false when the layout does not
+// fit the device's shared memory.
+template <int FMT>
+static void river_smem_attrs(size_t bytes) {
+    set_smem((const void*)kr_river<FMT, 0, kRiverNT>, bytes);
+    set_smem((const void*)kr_river<FMT, 1, kRiverNT>, bytes);
+}
+static void setup_river(EngineImpl& E, const Spot& sp) {
+    const Plan& P = E.plan;
+    if (!P.river || P.rtrees.empty()) return;
+    int dev = 0, optin = 0, nsm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    cudaFuncAttributes fa;
+    CK(cudaFuncGetAttributes(&fa, (const void*)kr_river<kDevI16, 0, kRiverNT>));
+    const int esz = fmt_bytes(E.fmt == kFmtF32 ? kDevF32 : E.fmt == kFmtFP8 ? kDevFP8 : kDevI16);
+    const int depth = P.river_depth + 1;
+    int nslot = 6;
+    size_t need = 0;
+    for (; nslot >= 2; nslot--) {
+        need = 0;
+        for (int p = 0; p < 2; p++) {
+            E.rl[p] = river_layout(E.d.nh_pad, esz, E.pcfr, depth, p, (int)P.max_sorted, nslot);
+            need = std::max<size_t>(need, E.rl[p].total);
+        }
+        if (need + fa.sharedSizeBytes <= (size_t)optin) break;
+    }
+    if (nslot < 2) return;  // the level sweeps keep the river
+    auto& O = E.owned;
+    size_t& B = E.bytes;
+    E.rtrees = dupload(P.rtrees, O, &B);
+    E.rsteps = dupload(P.rsteps, O, &B);
+    E.ntrees = (int)P.rtrees.size();
+    const uint32_t msort = P.max_sorted;
+    for (int o = 0; o < 2; o++) {
+        std::vector<uint32_t> img, off;
+        for (uint32_t sl = 0; sl < P.num_slots; sl++) {
+            off.push_back((uint32_t)img.size());
+            const uint32_t m = P.sorted_cnt[o][sl], soff = P.sorted_off[o][sl];
+            const uint32_t* co = P.ccard_off[o].data() + (size_t)sl * 53;
+            const uint32_t c0 = co[0], ne = co[52] - c0;
+            const size_t base = img.size();
+            img.resize(base + river_tab_words((int)m, (int)ne), 0u);
+            for (int c = 0; c < 53; c++) img[base + c] = co[c] - c0;
+            uint32_t* ent = img.data() + base + 56;
+            for (uint32_t f = 0; f < m + ne; f++) {
+                uint32_t h, head, oi;
+                if (f < m) {
+                    h = P.sorted_idx[o][soff + f];
+                    head = f == 0;
+                    oi = f + 1;
+                } else {
+                    const uint32_t t = f - m, c = P.ccard_card[o][c0 + t];
+                    h = P.sorted_idx[o][soff + P.ccard_pos[o][c0 + t]];
+                    head = t == 0 || P.ccard_card[o][c0 + t - 1] != c;
+                    oi = msort + 2 + t + c;
+                }
+                if (h > 0xFFFu || oi > 0xFFFFu) return;  // beyond the packed entry's fields: keep the level sweeps
+                ent[f] = h | head << 12 | oi << 16;
+            }
+        }
+        off.push_back((uint32_t)img.size());
+        E.d.rtab[o] = dupload(img, O, &B);
+        E.d.rtab_off[o] = dupload(off, O, &B);
+    }
+    river_smem_attrs<kDevF32>(need);
+    river_smem_attrs<kDevI16>(need);
+    river_smem_attrs<kDevFP8>(need);
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kr_river<kDevI16, 0, kRiverNT>, kRiverNT, need));
+    if (per_sm < 1) return;
+    E.river_grid = std::min(per_sm * nsm, E.ntrees);
+    E.river = true;
+}
+
 // --------------------------------------------------------------- GpuEngine
 GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine) : GpuEngine(host, fmt, engine, 0, 1, nullptr) {}
 
@@ -573,11 +694,12 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
     E.uncaptured = E.reducer && !E.reducer->capturable();
     const Spot& sp = *host.spot;
     g_uploaded = 0;
-    if (engine < kEngineFused || engine > kEngineStaged) throw Error("unknown engine kind");
-    const int fuse = engine == kEnginePlain                               ? kFuseNone
-                     : (engine == kEngineWarp || engine == kEngineStaged) ? kFuseFolds
-                                                                          : kFuseAll;
-    E.warp = engine == kEngineWarp || engine == kEngineStaged;  // staged falls back to warp kernels
+    if (engine < kEngineFused || engine > kEngineStagedRiver) throw Error("unknown engine kind");
+    const bool staged_kind = engine == kEngineStaged || engine == kEngineStagedRiver;
+    const int fuse = engine == kEnginePlain                        ? kFuseNone
+                     : (engine == kEngineWarp || staged_kind)      ? kFuseFolds
+                                                                   : kFuseAll;
+    E.warp = engine == kEngineWarp || staged_kind;  // staged falls back to warp kernels
     E.term64 = engine != kEngineFused32;
     E.spot = &sp;
     E.algo = host.algo;
@@ -588,13 +710,14 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
     }
     E.fmt = fmt < 0 ? (host.storage == kStoreF32 ? kFmtF32 : kFmtI16) : fmt;
     if (E.fmt != kFmtF32 && E.fmt != kFmtI16 && E.fmt != kFmtFP8) throw Error("unknown device arena format");
-    if (E.fmt == kFmtFP8 && engine != kEngineStaged) throw Error("FP8 arenas run on the staged engine only");
+    if (E.fmt == kFmtFP8 && !staged_kind) throw Error("FP8 arenas run on the staged engine only");
     E.iteration = host.iteration;
-    E.plan = build_plan(sp, host.use_iso, fuse, shard, nshards, leaf_net != nullptr);
+    E.plan = build_plan(sp, host.use_iso, fuse, shard, nshards, leaf_net != nullptr,
+                        engine == kEngineStagedRiver && !leaf_net);
     const Plan& P = E.plan;
     if (P.max_children > 32u) throw Error("an action node with more than 32 actions is not supported on the GPU");
     E.wide = P.max_children > 8u;
-    E.staged = engine == kEngineStaged && P.max_children <= (uint32_t)kSKA;
+    E.staged = staged_kind && P.max_children <= (uint32_t)kSKA;
     if (E.fmt == kFmtFP8 && !E.staged) throw Error("FP8 arenas need nodes of at most 4 actions (the staged kernels)");
     if (P.nh_max > kThreads * kMaxHpt) throw Error("more than 1536 hands per player is not supported on the GPU");
     CK(cudaStreamCreateWithFlags(&E.stream, cudaStreamNonBlocking));
@@ -735,6 +858,7 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
                             std::to_string(fa.maxThreadsPerBlock) + " threads, " + std::to_string(fa.numRegs) +
                             " registers, " + std::to_string(fa.sharedSizeBytes) + " B static");
         }
+        setup_river(E, sp);
     }
     if (max_nterm && !E.warp) E.act_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)max_nterm * d.nh_pad * sizeof(float);
     if (runouts) E.chance_smem = (size_t)d.scr_elems * tsz + 2 * (size_t)d.nh_pad * sizeof(float);
@@ -824,6 +948,8 @@ GpuEngine::GpuEngine(const HostSolver& host, int fmt, int engine, int shard, int
 
 GpuEngine::~GpuEngine() = default;
 uint64_t GpuEngine::upload_bytes() const { return d_->uploaded; }
+uint32_t GpuEngine::river_programs() const { return d_->river ? (uint32_t)d_->ntrees : 0u; }
+
 uint32_t GpuEngine::iteration_kernels() {
     EngineImpl& E = *d_;
     if (E.uncaptured) return 0;  // no graph
@@ -1010,7 +1136,14 @@ void GpuEngine::node_sweep_values(uint32_t node, int p, int mode, float* cfv, fl
     if (node >= t.size() || E.plan.node_cslot[node] == kNoSlot && E.plan.node_rs[0][node] == kNoSlot)
         throw Error("node " + std::to_string(node) + " is not on the device (a symmetric branch or an in-place terminal)");
     if (mode != 0 && mode != 1) throw Error("invalid argument: sweep mode");
-    E.sweep(p, mode, nullptr);  // down with the average strategies, up: best response (0) or average (1) for p
+    E.levels_only = true;  // every node's slots (river programs keep river rounds in shared memory)
+    try {
+        E.sweep(p, mode, nullptr);  // down with the average strategies, up: best response (0) or average (1) for p
+    } catch (...) {
+        E.levels_only = false;
+        throw;
+    }
+    E.levels_only = false;
     E.reach_valid = false;
     const int nh = E.plan.nh[p];
     const uint32_t cs = E.plan.node_cslot[node];
@@ -1036,7 +1169,14 @@ void GpuEngine::node_sweep_values(uint32_t node, int p, int mode, float* cfv, fl
 void GpuEngine::sweep_values(int p, int mode, const uint32_t* nodes, int n, float* out, uint8_t* ok) {
     EngineImpl& E = *d_;
     if (mode != 0 && mode != 1) throw Error("invalid argument: sweep mode");
-    E.sweep(p, mode, nullptr);
+    E.levels_only = true;
+    try {
+        E.sweep(p, mode, nullptr);
+    } catch (...) {
+        E.levels_only = false;
+        throw;
+    }
+    E.levels_only = false;
     E.reach_valid = false;
     const int nh = E.plan.nh[p];
     for (int k = 0; k < n; k++) {

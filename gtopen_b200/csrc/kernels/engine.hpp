@@ -18,7 +18,14 @@ namespace gtob {
 // nearest (an engine option: the layout and every other rule are I16's).
 enum ArenaFormat { kFmtF32 = 0, kFmtI16 = 1, kFmtFP8 = 2, kFmtI16SR = 3 };
 constexpr size_t kNodeScratchElems = 16384;  // 64 KiB of f32: the read_node_static limit
-enum EngineKind { kEngineFused = 0, kEnginePlain = 1, kEngineFused32 = 2, kEngineWarp = 3, kEngineStaged = 4 };
+enum EngineKind {
+    kEngineFused = 0,
+    kEnginePlain = 1,
+    kEngineFused32 = 2,
+    kEngineWarp = 3,
+    kEngineStaged = 4,
+    kEngineStagedRiver = 5
+};
 
 struct Profile {
     double ms[7];
@@ -49,7 +56,9 @@ class GpuEngine {
     // reference GPU kernels), kEngineWarp (one warp per action node, fold
     // children evaluated in place by the warp, showdowns one CTA each; f64),
     // kEngineStaged (one CTA per node staging its blocks and vectors in shared
-    // memory with bulk copies; fold children in place; f64).
+    // memory with bulk copies; fold children in place; exact sums),
+    // kEngineStagedRiver (the staged engine with river betting rounds solved
+    // by river programs, cfr_river.cuh).
     GpuEngine(const HostSolver& host, int fmt, int engine = 0);
     // One shard of a sharded spot: the top of the tree and every nshards-th
     // representative subtree below its chance nodes; `reducer` adds the
@@ -82,6 +91,7 @@ class GpuEngine {
     double iter_bytes() const;
     uint64_t upload_bytes() const;  // host-to-device bytes the constructor copied
     uint32_t iteration_kernels();   // kernels one iteration launches (the captured graph's kernel nodes)
+    uint32_t river_programs() const;  // river rounds the river kernel solves (0: level sweeps everywhere)
     // device arena exports for tests (reference layout, decoded f32)
     void export_arena(int which, int p, float* out);
     // One action node's block (reference layout, f32) through a static device

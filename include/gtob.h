@@ -45,8 +45,11 @@ extern "C" {
                                    in the warp; showdowns one CTA each; f64 terminal sums */
 #define GTOB_ENGINE_STAGED 4    /* one CTA per node staging its arena blocks and vectors in
                                    shared memory with bulk copies; fold children in place;
-                                   f64 terminal sums (nodes with more than 4 actions: the
+                                   exact terminal sums (nodes with more than 4 actions: the
                                    warp engine's kernels) */
+#define GTOB_ENGINE_STAGED_RIVER 5 /* the staged engine with every river betting round solved by
+                                   one CTA walking it depth first (river programs); the same
+                                   results bit for bit, slower on this device (see DESIGN) */
 #define GTOB_ARENA_REGRETS 0
 #define GTOB_ARENA_STRATEGY 1
 #define GTOB_ARENA_PREDICTIONS 2
@@ -86,6 +89,7 @@ typedef struct {
     uint64_t upload_bytes; /* host-to-device bytes copied by gtob_gpu_new (plan tables, arenas) */
     uint32_t iteration_kernels; /* kernel launches of one iteration (kernel nodes of its CUDA graph;
                                    reading it captures that graph if no iteration has run yet) */
+    uint32_t river_programs;    /* river betting rounds solved by river programs (0: level sweeps) */
 } gtob_gpu_info;
 
 /* Thread-local message of the last failed call (Result::Err text). */
