@@ -229,7 +229,25 @@ def workload_config(args, cfg):
                          "bench_spot": "reference bench_spot.json (Ks7h2d, 257 v 319)"}[args.workload],
             "board": cfg["board"], "arenas": ARENA_DESC[args.storage],
             "algo": "DCFR alpha 1.5 beta 0 gamma 2, alternating", "l2": "inputs larger than L2 (arenas GB-sized)",
-            "parallelism": "replica per GPU (weak scaling)", "engine": getattr(args, "engine", "fused")}
+            "parallelism": ("one spot sharded by turn card over the ranks, exact NCCL sums (strong scaling)"
+                            if getattr(args, "shard", False) else "replica per GPU (weak scaling)"),
+            "engine": getattr(args, "engine", "fused")}
+
+
+def make_engine(g, host, args, world, rank, storage=None):
+    """The engine of this rank: a replica of the whole spot, or with --shard
+    this rank's shard of the one spot (NCCL sums between the ranks, captured
+    in the iteration's graph; every rank builds it together)."""
+    fmt = DEVICE_FORMAT[storage or args.storage]
+    if not args.shard:
+        return g.GpuSolver(host, device_format=fmt, engine=args.engine)
+    nid = g.nccl_unique_id() if rank == 0 else None
+    if world > 1:
+        import torch.distributed as dist
+        box = [nid]
+        dist.broadcast_object_list(box, src=0)
+        nid = box[0]
+    return g.sharded_gpu_solver(host, rank, world, nid, device_format=fmt, engine=args.engine)
 
 
 def run_ours(args, world, rank, local):
@@ -240,7 +258,7 @@ def run_ours(args, world, rank, local):
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage=HOST_STORAGE[args.storage], algo="dcfr", use_iso=True)
     build_s = time.perf_counter() - t0
-    gpu = g.GpuSolver(host, device_format=DEVICE_FORMAT[args.storage], engine=args.engine)
+    gpu = make_engine(g, host, args, world, rank)
     info = gpu.info()
     gpu.iterate(args.warmup)
     gpu.synchronize()
@@ -251,7 +269,8 @@ def run_ours(args, world, rank, local):
     ck = clocks.stop()
     barrier(world)
     ms_max = allmax(ms, world)
-    value = world * args.steps / (ms_max / 1000.0)
+    # replicas: every rank's iterations count; shards: the ranks run one spot
+    value = (1 if args.shard else world) * args.steps / (ms_max / 1000.0)
     per_iter_s = ms / 1000.0 / args.steps
     peak, peak_kind = load_peak()
     achieved = info["iter_bytes"] / per_iter_s / 1e9
@@ -269,7 +288,7 @@ def run_ours(args, world, rank, local):
     if not args.no_e2e:
         barrier(world)
         t = time.perf_counter()
-        gpu2 = g.GpuSolver(host, device_format=DEVICE_FORMAT[args.storage], engine=args.engine)
+        gpu2 = make_engine(g, host, args, world, rank)
         t_new = time.perf_counter()
         gpu2.iterate(args.steps)
         gpu2.synchronize()
@@ -286,7 +305,7 @@ def run_ours(args, world, rank, local):
         b = HOST_BYTES[args.storage]
         arena_bytes = 2 * (spot.data_size[0] + spot.data_size[1]) * b
         up = gpu2.info()["upload_bytes"]
-        e2e = {"value": world * args.steps / dt_max, "unit": "iter/s",
+        e2e = {"value": (1 if args.shard else world) * args.steps / dt_max, "unit": "iter/s",
                "h2d_bytes_per_step": int(up / args.steps),
                "d2h_bytes_per_step": int((arena_bytes + 16) / args.steps),
                "includes": "GpuSolver::new (plan tables and, when the host solver has any, arenas uploaded; "
@@ -300,7 +319,9 @@ def run_ours(args, world, rank, local):
     # exploitability checked on the GPU every check_every iterations), the
     # f32 arenas' run beside it, and the plain f32 kernels' iteration time
     ttt = ttt_f32 = plain = None
-    if not args.no_ttt and rank == 0:
+    if not args.no_ttt and args.shard:  # every rank takes part in a sharded solve
+        ttt = time_to_target(g, cfg, args, factory=lambda host: make_engine(g, host, args, world, rank))
+    elif not args.no_ttt and rank == 0:
         ttt = time_to_target(g, cfg, args)
         if args.storage != "f32":
             ttt_f32 = time_to_target(g, cfg, args, storage="f32")
@@ -320,7 +341,7 @@ def run_ours(args, world, rank, local):
     # 1.25M nodes; exploitability checked every 10 iterations on the GPU, as
     # the reference CLI does), wall clock from GpuSolver::new
     ttt_spot = None
-    if not args.no_spot_ttt and rank == 0:
+    if not args.no_spot_ttt and rank == 0 and not args.shard:
         ttt_spot = time_to_target(g, make_config("bench_spot"), args)
         ttt_spot["spot"] = "reference bench_spot.json (Ks7h2d, 257 v 319 hands, 1,245,971 nodes)"
 
@@ -338,7 +359,8 @@ def run_ours(args, world, rank, local):
     line = {
         "metric": "CFR iterations/s (time-to-0.3%-pot exploitability & HBM GB/s vs peak)",
         "value": value, "unit": "iter/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "strong" if args.shard else "weak", "vs_baseline": None,
         "dtype": DTYPE[args.storage], "data": "synthetic (seeded spot)",
         "config": workload_config(args, cfg),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -394,8 +416,11 @@ def run_report(args, world, rank, local):
     t1 = time.perf_counter()
     batch = g.Batch([spots[i] for i in mine], storage=HOST_STORAGE[args.storage],
                     device_format=DEVICE_FORMAT[args.storage], engine=args.engine, keep_solvers=False)
-    batch.run(max_iterations=args.ttt_max, target_pct=args.target, check_every=20, workers=args.report_workers)
+    persistent = args.batch_mode == "persistent"
+    batch.run(max_iterations=args.ttt_max, target_pct=args.target, check_every=20, workers=args.report_workers,
+              persistent=persistent, window=args.report_window)
     run_s = allmax(time.perf_counter() - t1, world)
+    bstats = batch.stats() if persistent else None
     rows = batch.rows()
     bad = [r["error"] for r in rows if r["status"] != 0]
     if bad:
@@ -427,7 +452,10 @@ def run_report(args, world, rank, local):
                                "combos, weights U[0.2,1]), pot 100 stack 300, raise 2.5x, 2 raises, 1-3 bet sizes "
                                "from {33,50,75,125,a} (trees %d-%d nodes)" % (n, min(sizes), max(sizes)),
                    "arenas": ARENA_DESC[args.storage], "algo": "DCFR alpha 1.5 beta 0 gamma 2, alternating",
-                   "check_every": 20, "max_iterations": args.ttt_max, "workers": args.report_workers,
+                   "check_every": 20, "max_iterations": args.ttt_max,
+                   "batch": ("one persistent kernel launch per iteration of up to %d spots in flight "
+                             "(a (spot, step, node tile) work queue)" % args.report_window if persistent else
+                             "%d spots in flight, each on its own engine and CUDA graphs" % args.report_workers),
                    "parallelism": "flops dealt round-robin over ranks", "engine": args.engine},
         "report": {"reached_target": int(stats[1]), "flops": int(stats[3]), "iterations_total": int(stats[0]),
                    "worst_exploit_pct": float(stats[2]),
@@ -438,6 +466,9 @@ def run_report(args, world, rank, local):
                     build_s, pool._max_workers),
                 "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    if bstats:
+        line["persistent_kernel"] = bstats
+        line["gpu_launches"] = int(bstats["launches"])
     if not args.no_cpu_baseline:
         mid = int(np.argsort(sizes)[len(sizes) // 2])
         r = cpu_baseline(cfgs[mid], args.storage, max(1, args.cpu_steps), args.cpu_threads)
@@ -586,13 +617,16 @@ def run_leaf(args, world, rank, local):
     print(json.dumps(line), flush=True)
 
 
-def time_to_target(g, cfg, args, storage=None, engine=None):
+def time_to_target(g, cfg, args, storage=None, engine=None, factory=None):
     storage = storage or args.storage
     engine = engine or args.engine
     spot = g.Spot(cfg)
     host = g.Solver(spot, storage=HOST_STORAGE[storage], algo="dcfr", use_iso=True)
     t = time.perf_counter()
-    gpu = g.GpuSolver(host, device_format=DEVICE_FORMAT[storage], engine=engine)
+    if factory is not None:
+        gpu = factory(host)
+    else:
+        gpu = g.GpuSolver(host, device_format=DEVICE_FORMAT[storage], engine=engine)
     pot = cfg["tree"]["starting_pot"]
     pct = None
     while gpu.iteration < args.ttt_max:
@@ -637,9 +671,14 @@ def main():
     ap.add_argument("--leaf-check-iters", type=int, default=400)
     ap.add_argument("--report-flops", type=int, default=184)
     ap.add_argument("--report-workers", type=int, default=8)
+    ap.add_argument("--batch-mode", default="persistent", choices=["persistent", "concurrent"],
+                    help="report: one persistent kernel over the spots in flight, or an engine per spot")
+    ap.add_argument("--report-window", type=int, default=16, help="report: spots in flight on the persistent kernel")
     ap.add_argument("--storage", default="i16sr", choices=["i16sr", "compressed", "f32", "fp8"])
     ap.add_argument("--engine", default="staged", choices=["fused", "plain", "warp", "fused32", "staged", "staged_river"])
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--shard", action="store_true",
+                    help="split the one spot over the ranks by turn card (NCCL sums) instead of a replica per rank")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=3, help="timed CPU-oracle iterations (after one warm-up)")
     ap.add_argument("--cpu-threads", type=int, default=0)

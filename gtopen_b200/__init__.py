@@ -62,6 +62,15 @@ class BatchRow(C.Structure):
                 ("seconds", C.c_double), ("ev", C.c_double * 2)]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("launches", C.c_uint64), ("kernel_ms", C.c_double), ("tuned", C.c_int32), ("tile", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("grid", C.c_int32)]
+
+
+# gtob_reduce_fn: int (*)(void* user, float* values, size_t count)
+REDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_float), C.c_size_t)
+
+
 class Profile(C.Structure):
     _fields_ = [("ms", C.c_double * 7), ("launches", C.c_uint32 * 7)]
 
@@ -136,6 +145,7 @@ def lib():
         "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, I, C.POINTER(P)]),
         "gtob_nccl_unique_id": (I, [P]),
         "gtob_gpu_new_sharded": (I, [P, I, I, I, I, P, C.POINTER(P)]),
+        "gtob_gpu_new_sharded_host": (I, [P, I, I, I, I, REDUCE_FN, P, C.POINTER(P)]),
         "gtob_shards_new": (I, [P, I, I, I, C.POINTER(P)]),
         "gtob_shards_iterate": (I, [P, I]),
         "gtob_shards_exploitability": (I, [P, P, C.POINTER(D)]),
@@ -144,6 +154,8 @@ def lib():
         "gtob_shards_free": (None, [P]),
         "gtob_spot_shard_visited": (I, [P, I, I, I, P]),
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
+        "gtob_batch_run_persistent": (I, [P, U32, D, U32, I]),
+        "gtob_batch_stats_get": (I, [P, C.POINTER(BatchStats)]),
         "gtob_batch_size": (I, [P]),
         "gtob_batch_row_get": (I, [P, I, C.POINTER(BatchRow)]),
         "gtob_batch_root_cfv": (I, [P, I, I, P, I, C.POINTER(I)]),
@@ -610,6 +622,32 @@ def sharded_gpu_solver(solver, rank, world, nccl_id, device_format=None, engine=
     return gpu
 
 
+def sharded_gpu_solver_host(solver, rank, world, reduce_fn, device_format=None, engine="staged"):
+    """Shard `rank` of a spot split over `world` processes that sum over a
+    channel of the caller's own: reduce_fn(values) gets a float32 array (the
+    shard's values after a level of the up sweep) and must leave in it, in
+    place, the element-wise sum over every rank -- for example
+    torch.distributed.all_reduce on torch.from_numpy(values) in a gloo group.
+    Every rank makes the same calls in the same order."""
+    def tramp(user, ptr, count):
+        try:
+            reduce_fn(np.ctypeslib.as_array(ptr, shape=(int(count),)))
+            return 0
+        except BaseException:  # the error reaches the caller as a failed engine call
+            import traceback
+            traceback.print_exc()
+            return 1
+    cb = REDUCE_FN(tramp)
+    h = C.c_void_p()
+    _check(lib().gtob_gpu_new_sharded_host(solver._h, DEVICE_FORMAT[device_format], ENGINES[engine], int(rank),
+                                           int(world), cb, None, C.byref(h)))
+    gpu = GpuSolver.__new__(GpuSolver)
+    gpu._h = h
+    gpu.solver = solver
+    gpu._reduce_cb = cb  # the C side keeps the pointer: keep the thunk alive with the engine
+    return gpu
+
+
 class Shards:
     """Every shard of one spot in this process on the current device, summing
     the split subtrees' values on the host: the sharded computation on one GPU."""
@@ -672,8 +710,22 @@ class Batch:
             _LIB.gtob_batch_free(self._h)
             self._h = None
 
-    def run(self, max_iterations=300, target_pct=0.3, check_every=20, workers=8):
-        _check(lib().gtob_batch_run(self._h, int(max_iterations), float(target_pct), int(check_every), int(workers)))
+    def run(self, max_iterations=300, target_pct=0.3, check_every=20, workers=8, persistent=False, window=16):
+        """workers: spots in flight on their own engines and graphs; with
+        persistent=True, `window` spots in flight whose iterations run as one
+        persistent kernel launch each (gtob_batch_run_persistent)."""
+        if persistent:
+            _check(lib().gtob_batch_run_persistent(self._h, int(max_iterations), float(target_pct), int(check_every),
+                                                   int(window)))
+        else:
+            _check(lib().gtob_batch_run(self._h, int(max_iterations), float(target_pct), int(check_every),
+                                        int(workers)))
+
+    def stats(self):
+        """The last persistent run: launches, kernel_ms, tuned, tile, ctas_per_sm, grid."""
+        st = BatchStats()
+        _check(lib().gtob_batch_stats_get(self._h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in BatchStats._fields_}
 
     def rows(self):
         out = []

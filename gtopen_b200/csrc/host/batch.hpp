@@ -36,6 +36,24 @@ void run_batch(const std::vector<std::shared_ptr<Spot>>& spots, const std::vecto
                int algo, bool use_iso, int device_format, int engine, uint32_t max_iterations, double target_pct,
                uint32_t check_every, int workers, std::vector<BatchRow>& rows);
 
+// The batch on ONE persistent kernel (BatchKernel, cfr_batch.cuh): up to
+// `window` spots in flight, every iteration of all of them one launch; spots
+// leave at their checks (the same rule and the same per-spot iterations as
+// run_batch, so each row equals the spot solved alone) and a builder thread
+// keeps the next engines ready.  Shapes (records per ticket, CTAs per SM)
+// are tuned per size class from timed iterations and cached on disk
+// (GTOB_TUNE_CACHE or ~/.cache/gtob/batch_shapes.txt).  Staged engines only.
+struct BatchRunStats {
+    uint64_t launches = 0;   // batched iterations (one kernel launch each)
+    double kernel_ms = 0.0;  // device time of those launches (CUDA events)
+    int tuned = 0;           // size classes tuned in this run
+    int tile = 0, ctas_per_sm = 0, grid = 0;  // the last shape used
+};
+void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const std::vector<HostSolver*>& solvers,
+                          int storage, int algo, bool use_iso, int device_format, uint32_t max_iterations,
+                          double target_pct, uint32_t check_every, int window, std::vector<BatchRow>& rows,
+                          BatchRunStats* stats);
+
 // Per-hand compatible opponent reach mass (query.rs:463-488), f64.
 std::vector<double> valid_opp_sum(const Spot& spot, int p, const float* reach_o);
 

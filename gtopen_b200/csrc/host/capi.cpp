@@ -379,6 +379,16 @@ int gtob_gpu_new_sharded(const gtob_solver* v, int fmt, int engine, int rank, in
     *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt, engine, rank, world, red)};
     API_END
 }
+int gtob_gpu_new_sharded_host(const gtob_solver* v, int fmt, int engine, int rank, int world, gtob_reduce_fn fn,
+                              void* user, gtob_gpu** out) {
+    REQUIRE(v && fn && out && world >= 1 && rank >= 0 && rank < world && fmt >= -1 && fmt <= 3 &&
+            engine >= GTOB_ENGINE_FUSED && engine <= GTOB_ENGINE_STAGED_RIVER);
+    *out = nullptr;
+    API_BEGIN
+    auto red = make_callback_reducer(fn, user);
+    *out = new gtob_gpu{std::make_unique<GpuEngine>(*v->v, fmt, engine, rank, world, red)};
+    API_END
+}
 int gtob_shards_new(const gtob_solver* v, int fmt, int engine, int nshards, gtob_shards** out) {
     REQUIRE(v && out && nshards >= 1 && nshards <= 64 && fmt >= -1 && fmt <= 3 && engine >= GTOB_ENGINE_FUSED &&
             engine <= GTOB_ENGINE_STAGED_RIVER);
@@ -461,6 +471,7 @@ struct gtob_batch {
     std::vector<std::shared_ptr<Spot>> spots;
     std::vector<std::unique_ptr<gtob_solver>> solvers;  // empty entries when the batch keeps none
     std::vector<BatchRow> rows;
+    BatchRunStats stats;  // of the last persistent run
     int storage = 0, algo = 0, fmt = -1, engine = GTOB_ENGINE_STAGED;
     bool use_iso = true;
 };
@@ -495,6 +506,26 @@ int gtob_batch_run(gtob_batch* b, uint32_t max_iterations, double target_pct, ui
     run_batch(b->spots, hs, b->storage, b->algo, b->use_iso, b->fmt, b->engine, max_iterations, target_pct,
               check_every, workers, b->rows);
     API_END
+}
+int gtob_batch_run_persistent(gtob_batch* b, uint32_t max_iterations, double target_pct, uint32_t check_every,
+                              int window) {
+    REQUIRE(b && check_every > 0 && window > 0);
+    API_BEGIN
+    std::vector<HostSolver*> hs;
+    for (auto& v : b->solvers) hs.push_back(v ? v->v.get() : nullptr);
+    run_batch_persistent(b->spots, hs, b->storage, b->algo, b->use_iso, b->fmt, max_iterations, target_pct,
+                         check_every, window, b->rows, &b->stats);
+    API_END
+}
+int gtob_batch_stats_get(const gtob_batch* b, gtob_batch_stats* out) {
+    REQUIRE(b && out);
+    out->launches = b->stats.launches;
+    out->kernel_ms = b->stats.kernel_ms;
+    out->tuned = b->stats.tuned;
+    out->tile = b->stats.tile;
+    out->ctas_per_sm = b->stats.ctas_per_sm;
+    out->grid = b->stats.grid;
+    return GTOB_OK;
 }
 int gtob_batch_size(const gtob_batch* b) { return b ? (int)b->solvers.size() : 0; }
 int gtob_batch_row_get(const gtob_batch* b, int i, gtob_batch_row* out) {

@@ -80,6 +80,26 @@ class HostReducer : public ShardReducer {
     std::shared_ptr<HostExchange> x_;
     int shard_;
 };
+
+class CallbackReducer : public ShardReducer {
+  public:
+    CallbackReducer(HostReduceFn fn, void* user) : fn_(fn), user_(user) {}
+    void reduce(float* buf, size_t count, cudaStream_t stream) override {
+        host_.resize(count);
+        GTOB_CUDA_OK(cudaMemcpyAsync(host_.data(), buf, count * sizeof(float), cudaMemcpyDeviceToHost, stream));
+        GTOB_CUDA_OK(cudaStreamSynchronize(stream));
+        const int rc = fn_(user_, host_.data(), count);
+        if (rc != 0) throw Error("shard reduce callback failed (status " + std::to_string(rc) + ")");
+        GTOB_CUDA_OK(cudaMemcpyAsync(buf, host_.data(), count * sizeof(float), cudaMemcpyHostToDevice, stream));
+        GTOB_CUDA_OK(cudaStreamSynchronize(stream));
+    }
+    bool capturable() const override { return false; }
+
+  private:
+    HostReduceFn fn_;
+    void* user_;
+    std::vector<float> host_;
+};
 }  // namespace
 
 void nccl_unique_id(unsigned char* out) {
@@ -124,6 +144,10 @@ void HostExchange::exchange(int shard, float* buf, size_t count, cudaStream_t st
 }
 std::shared_ptr<ShardReducer> make_host_reducer(std::shared_ptr<HostExchange> x, int shard) {
     return std::make_shared<HostReducer>(std::move(x), shard);
+}
+std::shared_ptr<ShardReducer> make_callback_reducer(HostReduceFn fn, void* user) {
+    if (!fn) throw Error("invalid argument: reduce callback");
+    return std::make_shared<CallbackReducer>(fn, user);
 }
 
 }  // namespace gtob

@@ -44,4 +44,13 @@ class HostExchange {
 };
 std::shared_ptr<ShardReducer> make_host_reducer(std::shared_ptr<HostExchange> x, int shard);
 
+// Shards in separate processes that sum over a channel of the caller's own
+// (a torch.distributed group, MPI, sockets): reduce() copies the shard's
+// values to a host buffer, calls fn(user, values, count), which must leave
+// there the sum over every rank and return 0, and copies the sums back.  The
+// engine runs plain launches (the call synchronises on the host), and no
+// kernel ever waits on another rank.
+using HostReduceFn = int (*)(void* user, float* values, size_t count);
+std::shared_ptr<ShardReducer> make_callback_reducer(HostReduceFn fn, void* user);
+
 }  // namespace gtob

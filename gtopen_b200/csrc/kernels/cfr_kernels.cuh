@@ -549,7 +549,7 @@ __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* r
 }
 
 // ------------------------------------------------------------------ kernels
-__global__ void k_begin_iteration(unsigned* iter, float* disc, int algo) {
+__device__ __forceinline__ void begin_iteration(unsigned* iter, float* disc, int algo) {
     // cfr.rs:44-64, in f64 on the device from the device iteration counter
     const unsigned t = ++(*iter);
     const double td = (double)t;
@@ -564,6 +564,7 @@ __global__ void k_begin_iteration(unsigned* iter, float* disc, int algo) {
     }
     disc[2] = (float)(q * q);
 }
+__global__ void k_begin_iteration(unsigned* iter, float* disc, int algo) { begin_iteration(iter, disc, algo); }
 
 __global__ void k_copy_root(Dev d) {
     for (int q = 0; q < 2; q++)
@@ -594,8 +595,7 @@ __global__ void __launch_bounds__(kThreads) k_down_action(Dev d, Arenas ar, cons
 
 // Down sweep, chance edges: both players' reach with holders of the card zeroed.
 // qmask: the players whose reach is refreshed (bit q)
-__global__ void __launch_bounds__(kThreads) k_down_chance(Dev d, const EdgeItem* items, int qmask) {
-    const EdgeItem e = items[blockIdx.x];
+__device__ __forceinline__ void edge_down(const Dev& d, const EdgeItem& e, int qmask) {
     for (int q = 0; q < 2; q++) {
         if (!(qmask >> q & 1)) continue;
         const int nh = d.nh[q];
@@ -603,6 +603,9 @@ __global__ void __launch_bounds__(kThreads) k_down_chance(Dev d, const EdgeItem*
         float* cr = d.reach[q] + (size_t)e.crs[q] * d.rstr[q];
         for (int i = threadIdx.x; i < nh; i += blockDim.x) cr[i] = (d.mask[q][i] >> e.card & 1ull) ? 0.0f : pr[i];
     }
+}
+__global__ void __launch_bounds__(kThreads) k_down_chance(Dev d, const EdgeItem* items, int qmask) {
+    edge_down(d, items[blockIdx.x], qmask);
 }
 
 // Plain engine terminal kernels (exact sums): one CTA per terminal, result to its cfv slot.
@@ -631,11 +634,9 @@ __global__ void __launch_bounds__(kThreads) k_showdown(Dev d, const ShowItem* it
 // suit-permutation hand tables, skipping holders of the card, times
 // 1/divisor.  All-in runout children (showdowns) are evaluated in place (T
 // is the runout showdowns' accumulator type).
+// (kThreads threads; s_w: kWarps entries; dsm: the runout scratch)
 template <class T>
-__global__ void __launch_bounds__(kThreads) k_chance(Dev d, const ChanceItem* items, int p) {
-    extern __shared__ double dsm[];
-    __shared__ T s_w[kWarps];
-    const ChanceItem c = items[blockIdx.x];
+__device__ void chance_node(const Dev& d, const ChanceItem& c, int p, double* dsm, T* s_w) {
     const int nh = d.nh[p], o = 1 - p, nho = d.nh[o];
     float* out = d.cfv + (size_t)c.cslot * d.nh_max;
     if (c.nterm == 0) {
@@ -692,6 +693,12 @@ __global__ void __launch_bounds__(kThreads) k_chance(Dev d, const ChanceItem* it
         const int i = threadIdx.x + k * blockDim.x;
         if (i < nh) out[i] = acc[k] * c.inv;
     }
+}
+template <class T>
+__global__ void __launch_bounds__(kThreads) k_chance(Dev d, const ChanceItem* items, int p) {
+    extern __shared__ double dsm[];
+    __shared__ T s_w[kWarps];
+    chance_node<T>(d, items[blockIdx.x], p, dsm, s_w);
 }
 
 // Up sweep, action nodes.  EVAL = 0: CFR update (cfr.rs:469-531 with

@@ -270,14 +270,16 @@ __device__ __forceinline__ void s_block_max3(float& a, float& b, float& c, float
 // Fold summary of a staged opponent reach vector (game.rs:478-485), exact
 // sums (cfr_kernels.cuh): the vector's grid scale, the total and the
 // per-card sums.  Integer sums do not depend on their order, so every thread
-// takes hands j = tid, tid + 128, ... and adds each hand's grid value to its
-// two cards' sums with shared-memory atomics.  s_red: kSWarps entries;
+// takes hands j = tid, tid + NT, ... and adds each hand's grid value to its
+// two cards' sums with shared-memory atomics.  s_red: NT / 32 entries;
 // returns the total, *sc_out the scale.
+template <int NT = kSThreads>
 __device__ long long s_fold_sums(const Dev& d, int o, const float* ro, long long* S, long long* s_red, int* sc_out) {
+    constexpr int W = NT / 32;
     const int nho = d.nh[o];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float mx = 0.0f;
-    for (int j = threadIdx.x; j < nho; j += kSThreads) mx = fmaxf(mx, ro[j]);
+    for (int j = threadIdx.x; j < nho; j += NT) mx = fmaxf(mx, ro[j]);
     mx = warp_max(mx);
     float* fred = (float*)s_red;
     if (lane == 0) fred[warp] = mx;
@@ -285,11 +287,11 @@ __device__ long long s_fold_sums(const Dev& d, int o, const float* ro, long long
     __syncthreads();
     mx = fred[0];
 #pragma unroll
-    for (int k = 1; k < kSWarps; k++) mx = fmaxf(mx, fred[k]);
+    for (int k = 1; k < W; k++) mx = fmaxf(mx, fred[k]);
     const int sc = fix_scale(mx);
     long long t = 0;
     const uint32_t* hi = d.hinfo[o];
-    for (int j = threadIdx.x; j < nho; j += kSThreads) {
+    for (int j = threadIdx.x; j < nho; j += NT) {
         const long long q = fix_q(ro[j], sc);
         if (q) {
             const uint32_t h = hi[j];
@@ -305,7 +307,7 @@ __device__ long long s_fold_sums(const Dev& d, int o, const float* ro, long long
     __syncthreads();
     long long total = 0;
 #pragma unroll
-    for (int k = 0; k < kSWarps; k++) total += s_red[k];
+    for (int k = 0; k < W; k++) total += s_red[k];
     *sc_out = sc;
     return total;
 }
@@ -373,7 +375,7 @@ __host__ __device__ constexpr int fmt_bytes(int fmt) { return fmt == kDevF32 ? 4
 
 // Down sweep, one node per CTA: staged sigma source and parent reach; child
 // reach vectors written with coalesced stores (cfr.rs:469-531 push-down).
-template <int FMT, int NA>
+template <int FMT, int NA, int NT = kSThreads>
 __device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, const SNode& it, int mode,
                                              unsigned char* sm, int& s_flag) {
     const int a = (int)it.actor, nh = d.nh[a];
@@ -416,7 +418,7 @@ __device__ __forceinline__ void ks_down_node(const Dev& d, const Arenas& ar, con
     }
     if (!wait_staged(d, bar, &s_flag)) return;
     float sig[kSKA];
-    for (int i = threadIdx.x; i < nh; i += kSThreads) {
+    for (int i = threadIdx.x; i < nh; i += NT) {
         s_node_sigma<FMT>(d, loff, a, i, mode, b_reg, has_pred ? b_pred : nullptr, b_str, kr, kp, na, sig);
         const float p = pr[i];
 #pragma unroll
@@ -441,12 +443,14 @@ __global__ void __launch_bounds__(kSThreads) ks_down(Dev d, Arenas ar, const SNo
 // best_response.rs:69-121, 185-219 for EVAL = 1 with mode 0 BR / 1 average).
 // The node's fold child, if any, is evaluated here from the staged opponent
 // reach; every other child's cfv is staged from its slot.
-struct UpShared {  // static shared memory of ks_up
+template <int NT = kSThreads>
+struct UpSharedT {  // static shared memory of ks_up (NT threads)
     int flag;
     long long S[52];
-    long long dred[kSWarps];
-    float red[3 * kSWarps];
+    long long dred[NT / 32];
+    float red[3 * (NT / 32)];
 };
+using UpShared = UpSharedT<>;
 // The traverser's node once its children's values are staged (cv, row k at
 // cv + k * vstride) and, for the update, its regret / strategy-sum /
 // prediction blocks (b_reg, b_str, b_pred) and own reach (rp): a locked
@@ -652,9 +656,9 @@ __device__ __forceinline__ void s_mine_node(const Dev& d, const Arenas& ar, int 
         if (use_pred) ar.pscale[p][sidx] = (pmax > 0.0f && isfinite(pmax)) ? pmax : 0.0f;
     }
 }
-template <int FMT, int EVAL, int NA, bool MINE>
+template <int FMT, int EVAL, int NA, bool MINE, int NT = kSThreads>
 __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const SNode& it, int p, int mode,
-                                           unsigned char* sm, UpShared& us) {
+                                           unsigned char* sm, UpSharedT<NT>& us) {
     int& s_flag = us.flag;
     long long* s_S = us.S;
     long long* s_dred = us.dred;
@@ -732,11 +736,11 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     long long ftotal = 0;
     if (fk >= 0) {
         int fsc;
-        ftotal = s_fold_sums(d, o, ro, s_S, s_dred, &fsc);
+        ftotal = s_fold_sums<NT>(d, o, ro, s_S, s_dred, &fsc);
         // the fold child's values go where a staged child's cfv would be
         // (fold_value of cfr_kernels.cuh with the hand's cards and same combo
         // packed in one word)
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+        for (int i = threadIdx.x; i < nh; i += NT) {
             const uint32_t h = d.hinfo[p][i];
             const uint32_t sm_ = h >> 16;
             const float same_r = sm_ != 0xFFFFu ? ro[sm_] : 0.0f;
@@ -747,7 +751,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
     float* out = d.cfv + (size_t)it.cslot * d.nh_max;
 #define CHILD_V(k, i) (cv[(k) * vstride + (i)])
     if (!mine) {  // opponent node: sum of children
-        for (int i = threadIdx.x; i < nh; i += kSThreads) {
+        for (int i = threadIdx.x; i < nh; i += NT) {
             float acc = 0.0f;
 #pragma unroll
             for (int k = 0; k < kSKA; k++)
@@ -756,7 +760,7 @@ __device__ __forceinline__ void ks_up_node(const Dev& d, const Arenas& ar, const
         }
         return;
     }
-    s_mine_node<FMT, EVAL, NA, kSThreads>(d, ar, p, mode, loff, kr, kp, sscale, it.sidx, it.aoff, use_pred, b_reg,
+    s_mine_node<FMT, EVAL, NA, NT>(d, ar, p, mode, loff, kr, kp, sscale, it.sidx, it.aoff, use_pred, b_reg,
                                            b_str, b_pred, cv, vstride, rp, out, false, s_red);
 #undef CHILD_V
 }
@@ -1010,16 +1014,23 @@ __host__ __device__ inline unsigned show_pair_scratch_bytes(int nh_pad, int msor
 inline size_t show_pair_smem_bytes(int nh_pad, int msort) {
     return (size_t)show_pair_scratch_bytes(nh_pad, msort) + show_tab_layout(nh_pad).total;
 }
+// Static shared memory of one showdown batch (NT threads).
 template <int NT>
-__global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items, const ShowBatch* batches, int p,
-                                                    int msort) {
-    extern __shared__ __align__(16) unsigned char sm[];
-    __shared__ longlong2 s_w[NT / 32];
-    __shared__ int s_wf[NT / 32];
-    __shared__ float2 s_mx[NT / 32];
-    __shared__ int s_flag;
-    __shared__ ShowItem s_it[kShowBatch];
-    const ShowBatch bt = batches[blockIdx.x];
+struct ShowShared {
+    longlong2 w[NT / 32];
+    int wf[NT / 32];
+    float2 mx[NT / 32];
+    int flag;
+    ShowItem it[kShowBatch];
+};
+// One batch of showdowns (bt) on the whole CTA; sm: show_pair_smem_bytes of
+// dynamic shared memory.  Returns false when a copy failed (error bits set,
+// copies in flight drained).
+template <int NT>
+__device__ bool show_batch_run(const Dev& d, const ShowItem* items, const ShowBatch& bt, int p, int msort,
+                               unsigned char* sm, ShowShared<NT>& ss) {
+    int& s_flag = ss.flag;
+    ShowItem* s_it = ss.it;
     const int o = 1 - p;
     const int n = (int)bt.count, npairs = (n + 1) / 2;
     uint64_t* bars = (uint64_t*)sm;
@@ -1069,7 +1080,7 @@ __global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items,
                 mbar_wait(&bars[st], (unsigned)(q >> 1) & 1u);
                 if (q + 1 < npairs) mbar_wait(&bars[st ^ 1], (unsigned)((q + 1) >> 1) & 1u);
             }
-            return;
+            return false;
         }
         const int j0 = 2 * q;
         const bool two = j0 + 1 < n;
@@ -1078,11 +1089,19 @@ __global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items,
         const float* roA = rbuf + (size_t)(2 * st) * d.nh_pad;
         const float* roB = two ? roA + d.nh_pad : roA;
         cta_showdown2<NT>(tb, d.nh[o], msort, roA, roB, ia, ib, d.cfv + (size_t)ia.cslot * d.nh_max,
-                          two ? d.cfv + (size_t)ib.cslot * d.nh_max : nullptr, U, s_w, s_wf, s_mx);
+                          two ? d.cfv + (size_t)ib.cslot * d.nh_max : nullptr, U, ss.w, ss.wf, ss.mx);
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (threadIdx.x == 0 && q + 2 < npairs) issue(q + 2);
     }
+    return true;
+}
+template <int NT>
+__global__ void __launch_bounds__(NT) ks_show_pair(Dev d, const ShowItem* items, const ShowBatch* batches, int p,
+                                                    int msort) {
+    extern __shared__ __align__(16) unsigned char sm[];
+    __shared__ ShowShared<NT> ss;
+    show_batch_run<NT>(d, items, batches[blockIdx.x], p, msort, sm, ss);
 }
 
 }  // namespace gtob

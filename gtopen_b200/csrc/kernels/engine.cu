@@ -38,6 +38,7 @@
 #include "cfr_kernels.cuh"
 #include "cfr_staged.cuh"
 #include "cfr_river.cuh"
+#include "cfr_batch.cuh"
 #include "engine.hpp"
 
 namespace gtob {
@@ -1628,6 +1629,272 @@ bool vram_info_mb(uint64_t* free_mb, uint64_t* total_mb) {
     *free_mb = f / 1000000;
     *total_mb = t / 1000000;
     return true;
+}
+
+
+// ---------------------------------------------------------------------------
+// Batched engine (cfr_batch.cuh): many engines' CFR iterations in one
+// persistent kernel launch per iteration.
+
+struct BatchImpl {
+    std::vector<GpuEngine*> eng;
+    std::vector<EngineImpl*> E;
+    int fmt = -1;
+    BatchShape shape;
+    cudaStream_t stream = nullptr;
+    std::vector<void*> owned;  // device buffers of the current set
+    size_t bytes = 0;
+    BSpot* spots = nullptr;
+    BSeg* segs = nullptr;
+    unsigned* ctl = nullptr;
+    size_t nctl = 0;
+    int nseg = 0;
+    unsigned nticket = 0;
+    uint64_t nrecord = 0;
+    size_t smem = 0;
+    int grid = 0;
+    cudaGraphExec_t graph = nullptr;
+    unsigned h_ctl[4] = {0, 0, 0, 0};
+    ~BatchImpl() {
+        release();
+        if (stream) cudaStreamDestroy(stream);
+    }
+    void release() {
+        if (graph) {
+            cudaGraphExecDestroy(graph);
+            graph = nullptr;
+        }
+        for (void* p : owned) cudaFree(p);
+        owned.clear();
+        spots = nullptr;
+        segs = nullptr;
+        ctl = nullptr;
+        nseg = 0;
+        nticket = 0;
+        nrecord = 0;
+    }
+    template <int FMT>
+    static const void* kernel() { return (const void*)kb_iterate<FMT>; }
+    const void* kernel_fn() const {
+        return fmt == kFmtF32 ? kernel<kDevF32>() : fmt == kFmtFP8 ? kernel<kDevFP8>() : kernel<kDevI16>();
+    }
+    int occupancy() const {
+        int n = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_fn(), kBThreads, smem));
+        return n;
+    }
+    // One spot's iteration as steps of (kind, traverser / qmask, span, tile),
+    // the order of GpuEngine::iterate's graph: per traverser the discounts and
+    // root reach, the down sweep's levels (the opponent's reach), the
+    // showdowns of every level, the up sweep's levels deepest first.
+    struct SSpan {
+        int kind, p;
+        Span s;
+        int tile;
+    };
+    static std::vector<std::vector<SSpan>> steps_of(const EngineImpl& X, int tile) {
+        const Plan& P = X.plan;
+        const int L = P.num_levels;
+        std::vector<std::vector<SSpan>> st;
+        auto add = [&](std::vector<SSpan> v) {
+            std::vector<SSpan> keep;
+            for (auto& x : v)
+                if (x.s.count) keep.push_back(x);
+            if (!keep.empty()) st.push_back(std::move(keep));
+        };
+        for (int p = 0; p < 2; p++) {
+            std::vector<SSpan> first;
+            if (p == 0) first.push_back({kBBegin, 0, {0, 1}, 1});
+            first.push_back({kBRoot, 0, {0, 1}, 1});
+            add(first);
+            const int opp = 1 - p;
+            for (int l = 0; l < L; l++)
+                add({{kBDown, 0, P.act_span_actor[opp][l], tile}, {kBEdge, 1 << opp, P.edge_span[l], tile}});
+            std::vector<SSpan> shows;
+            for (int l = 0; l < L; l++) shows.push_back({kBShow, p, P.show_batch_span[l], 1});
+            add(shows);
+            for (int l = L - 1; l >= 0; l--)
+                add({{kBChance, p, P.chance_span[l], tile},
+                     {kBUpMine, p, P.act_span_actor[p][l], tile},
+                     {kBUpOpp, p, P.act_span_actor[opp][l], tile}});
+        }
+        return st;
+    }
+    void build() {
+        release();
+        if (eng.empty()) return;
+        if (!stream) CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        const int tile = std::max(1, std::min(shape.tile, 64));
+        std::vector<BSpot> hs(E.size());
+        smem = 16;
+        std::vector<std::vector<std::vector<SSpan>>> steps(E.size());
+        size_t kmax = 0;
+        for (size_t s = 0; s < E.size(); s++) {
+            const EngineImpl& X = *E[s];
+            BSpot& b = hs[s];
+            std::memset(&b, 0, sizeof(b));
+            b.d = X.d;
+            b.ar = X.ar;
+            b.snodes = X.snodes;
+            b.edge = X.edge;
+            b.show = X.show;
+            b.show_batch = X.show_batch;
+            b.chance = X.chance;
+            b.msort = (int)X.plan.max_sorted;
+            b.algo = X.algo;
+            smem = std::max({smem, X.st_mine_smem, X.st_opp_smem, X.st_down_smem, X.show_pair_smem, X.chance_smem});
+            steps[s] = steps_of(X, tile);
+            kmax = std::max(kmax, steps[s].size());
+        }
+        // segments ordered by step, then spot; a segment's tickets wait for
+        // the spot's tickets of its earlier steps
+        std::vector<BSeg> hg;
+        std::vector<uint32_t> before(E.size(), 0);  // tickets of the spot's steps so far
+        uint64_t t = 0;
+        for (size_t k = 0; k < kmax; k++) {
+            for (size_t s = 0; s < E.size(); s++) {
+                if (k >= steps[s].size()) continue;
+                uint32_t here = 0;
+                for (const SSpan& x : steps[s][k]) {
+                    BSeg g;
+                    std::memset(&g, 0, sizeof(g));
+                    g.first = (uint32_t)t;
+                    g.start = x.s.start;
+                    g.count = x.s.count;
+                    g.need = before[s];
+                    g.spot = (uint16_t)s;
+                    g.kind = (uint8_t)x.kind;
+                    g.p = (uint8_t)x.p;
+                    g.tile = (uint16_t)x.tile;
+                    const uint32_t nt = (x.s.count + (uint32_t)x.tile - 1) / (uint32_t)x.tile;
+                    nrecord += x.s.count;
+                    hg.push_back(g);
+                    t += nt;
+                    here += nt;
+                }
+                before[s] += here;
+            }
+        }
+        if (t >= 0xFFFFFFFFull) throw Error("batch: too many tickets in one iteration");
+        nticket = (unsigned)t;
+        nseg = (int)hg.size();
+        spots = dupload(hs, owned, &bytes);
+        segs = dupload(hg, owned, &bytes);
+        nctl = (size_t)kBCtlDone + E.size();
+        ctl = (unsigned*)dalloc(nctl * sizeof(unsigned), owned, &bytes);
+        set_smem(kernel_fn(), smem);
+        int dev = 0, nsm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        const int occ = occupancy();
+        if (occ < 1) throw Error("batch: the kernel does not fit an SM (" + std::to_string(smem) + " B shared memory)");
+        const int per = shape.ctas_per_sm > 0 ? std::min(shape.ctas_per_sm, occ) : occ;
+        grid = nsm * per;
+        // the iteration's graph: control words zeroed, then the kernel
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+        cudaMemsetAsync(ctl, 0, nctl * sizeof(unsigned), stream);
+        if (fmt == kFmtF32)
+            kb_iterate<kDevF32><<<grid, kBThreads, smem, stream>>>(spots, segs, nseg, nticket, ctl);
+        else if (fmt == kFmtFP8)
+            kb_iterate<kDevFP8><<<grid, kBThreads, smem, stream>>>(spots, segs, nseg, nticket, ctl);
+        else
+            kb_iterate<kDevI16><<<grid, kBThreads, smem, stream>>>(spots, segs, nseg, nticket, ctl);
+        const cudaError_t le = cudaGetLastError();
+        CK(cudaStreamEndCapture(stream, &g));
+        if (le != cudaSuccess) {
+            cudaGraphDestroy(g);
+            throw Error(std::string("cuda: ") + cudaGetErrorString(le) + " launching the batch kernel");
+        }
+        const cudaError_t ie = cudaGraphInstantiate(&graph, g, 0);
+        cudaGraphDestroy(g);
+        CK(ie);
+    }
+    // Every engine's own work done and its reach current (after an
+    // evaluation sweep an engine primes its reach first, as iterate does).
+    void ready() {
+        for (EngineImpl* X : E) {
+            X->prime();
+            CK(cudaStreamSynchronize(X->stream));
+        }
+    }
+    void finish(int n) {
+        CK(cudaMemcpyAsync(h_ctl, ctl, sizeof(h_ctl), cudaMemcpyDeviceToHost, stream));
+        CK(cudaStreamSynchronize(stream));
+        for (EngineImpl* X : E) X->iteration += (uint32_t)n;
+        if (h_ctl[kBCtlAbort]) {
+            for (EngineImpl* X : E) X->check_err();  // a copy's error, with its message
+            throw Error((h_ctl[kBCtlErr] & 4u) ? "timeout: a batched step waited too long for its spot's earlier steps"
+                                               : "timeout: the batched iteration stopped");
+        }
+    }
+};
+
+BatchKernel::BatchKernel() : d_(new BatchImpl()) {}
+BatchKernel::~BatchKernel() = default;
+
+std::string BatchKernel::unsupported(const GpuEngine& e) {
+    const EngineImpl& X = *e.d_;
+    if (!X.staged) return "the spot's engine is not the staged engine (nodes of more than 4 actions, or another kind)";
+    if (X.river) return "river programs are not batched";
+    if (X.leaf) return "depth-limited engines are not batched";
+    if (X.reducer) return "sharded engines are not batched";
+    if (!X.term64) return "f32 terminal sums are not batched";
+    for (const Span& s : X.plan.fold_span)
+        if (s.count) return "fold terminals with slots of their own are not batched";
+    return "";
+}
+void BatchKernel::configure(const std::vector<GpuEngine*>& engines, const BatchShape& shape) {
+    BatchImpl& B = *d_;
+    B.shape = shape;
+    if (engines.size() > 65535) throw Error("invalid argument: at most 65535 spots in one batch");
+    int fmt = -1;
+    for (GpuEngine* e : engines) {
+        if (!e) throw Error("invalid argument: null engine");
+        const std::string why = unsupported(*e);
+        if (!why.empty()) throw Error("invalid argument: " + why);
+        if (fmt >= 0 && e->d_->fmt != fmt) throw Error("invalid argument: the batch's engines differ in arena format");
+        fmt = e->d_->fmt;
+    }
+    B.eng = engines;
+    B.E.clear();
+    for (GpuEngine* e : engines) B.E.push_back(e->d_.get());
+    if (fmt >= 0) B.fmt = fmt;
+    B.build();
+}
+void BatchKernel::configure_shape(const BatchShape& s) {
+    d_->shape = s;
+    d_->build();
+}
+BatchShape BatchKernel::shape() const { return d_->shape; }
+int BatchKernel::max_ctas_per_sm() const { return d_->eng.empty() ? 0 : d_->occupancy(); }
+int BatchKernel::grid() const { return d_->grid; }
+size_t BatchKernel::tickets() const { return d_->nticket; }
+uint64_t BatchKernel::records() const { return d_->nrecord; }
+void BatchKernel::iterate(int n) {
+    BatchImpl& B = *d_;
+    if (B.eng.empty() || n <= 0) return;
+    B.ready();
+    for (int k = 0; k < n; k++) CK(cudaGraphLaunch(B.graph, B.stream));
+    B.finish(n);
+}
+double BatchKernel::time_iterations(int n) {
+    BatchImpl& B = *d_;
+    if (B.eng.empty() || n <= 0) return 0.0;
+    B.ready();
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    CK(cudaEventRecord(a, B.stream));
+    for (int k = 0; k < n; k++) CK(cudaGraphLaunch(B.graph, B.stream));
+    CK(cudaEventRecord(b, B.stream));
+    CK(cudaEventSynchronize(b));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    B.finish(n);
+    return ms;
 }
 
 }  // namespace gtob

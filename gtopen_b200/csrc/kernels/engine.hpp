@@ -7,6 +7,7 @@
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <vector>
 
 #include "../host/plan.hpp"
 #include "../host/solver.hpp"
@@ -128,7 +129,40 @@ class GpuEngine {
     void load_arenas(std::istream& in, HostSolver& host);
 
   private:
+    friend class BatchKernel;
     std::unique_ptr<EngineImpl> d_;
+};
+
+// Many spots' CFR iterations in ONE persistent kernel launch per iteration
+// (cfr_batch.cuh: a (spot, step, node-tile) work queue).  The engines stay
+// owned by the caller and must outlive their use here; all live on the
+// current device with one arena format, each a staged engine without river
+// programs, shards or a leaf network (unsupported() says why not).  An
+// iteration through the batch leaves every engine bit for bit as its own
+// iterate(1) would; the engines' other calls (exploitability, syncs,
+// queries) work between batched iterations as usual.
+struct BatchShape {
+    int tile = 4;         // node records per ticket (down, up, edge and chance steps)
+    int ctas_per_sm = 0;  // persistent CTAs per SM (0: as many as fit)
+};
+struct BatchImpl;
+class BatchKernel {
+  public:
+    BatchKernel();
+    ~BatchKernel();
+    static std::string unsupported(const GpuEngine& e);  // empty when the engine can join a batch
+    void configure(const std::vector<GpuEngine*>& engines, const BatchShape& s);
+    void configure_shape(const BatchShape& s);  // same engines, another shape
+    BatchShape shape() const;
+    int max_ctas_per_sm() const;  // resident CTAs per SM for the current engines' shared memory
+    int grid() const;
+    size_t tickets() const;       // tickets of one iteration
+    uint64_t records() const;     // node records of one iteration (independent of the shape)
+    void iterate(int n);          // n CFR iterations of every engine
+    double time_iterations(int n);  // ms (CUDA events on the batch stream)
+
+  private:
+    std::unique_ptr<BatchImpl> d_;
 };
 
 uint64_t estimate_vram(const Spot& spot);

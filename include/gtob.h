@@ -14,6 +14,7 @@
  */
 #ifndef GTOB_H
 #define GTOB_H
+#include <stddef.h>
 #include <stdint.h>
 #ifdef __cplusplus
 extern "C" {
@@ -279,6 +280,19 @@ int gtob_nccl_unique_id(unsigned char out[128]);
  * it with the same id (ncclCommInitRank: it returns once all have joined). */
 int gtob_gpu_new_sharded(const gtob_solver* solver, int device_format, int engine, int rank, int world,
                          const unsigned char id[128], gtob_gpu** out);
+/* Shard `rank` of `world` processes that sum over a channel of the caller's
+ * own instead of NCCL (a torch.distributed gloo group, MPI, sockets): after
+ * each level whose chance nodes add up split subtrees, the shard's `count`
+ * values are copied to a host buffer and fn(user, values, count) is called on
+ * the calling thread; it must leave there the element-wise sum over every
+ * rank and return 0 (non-zero fails the call with GTOB_EINVAL and that
+ * status).  Every rank must make the same calls in the same order (iterate,
+ * exploitability and the queries each reduce).  Plain launches, no graphs;
+ * no kernel waits on another rank.  No reference counterpart (the reference
+ * solves one spot on one GPU). */
+typedef int (*gtob_reduce_fn)(void* user, float* values, size_t count);
+int gtob_gpu_new_sharded_host(const gtob_solver* solver, int device_format, int engine, int rank, int world,
+                              gtob_reduce_fn fn, void* user, gtob_gpu** out);
 /* All nshards shards in this process on the current device, reducing on the
  * host (no graphs; each call below runs the shards on their own threads):
  * the whole sharded computation on one GPU, to check it against one engine. */
@@ -325,6 +339,28 @@ typedef struct {
 int gtob_batch_new(gtob_spot* const* spots, int n, int storage, int algo, int use_iso, int device_format, int engine,
                    int keep, gtob_batch** out);
 int gtob_batch_run(gtob_batch* batch, uint32_t max_iterations, double target_pct, uint32_t check_every, int workers);
+/* The same batch solved on ONE persistent kernel: every iteration of up to
+ * `window` spots in flight is a single launch (a CUDA graph of one kernel)
+ * whose CTAs take (spot, step, node tile) tickets from a device work queue;
+ * a ticket waits (bounded) only for its own spot's earlier steps.  Spots
+ * join as a builder thread readies their engines and leave at their checks
+ * (the same rule as gtob_batch_run), so every row equals the spot solved
+ * alone, bit for bit.  The kernel's shape -- node records per ticket, CTAs
+ * per SM -- is tuned per size class on the batch's first iterations (each
+ * trial is an ordinary iteration) and cached in GTOB_TUNE_CACHE or
+ * ~/.cache/gtob/batch_shapes.txt.  Staged engines only: the batch's engine
+ * argument is not used; a spot the kernel cannot take (nodes of more than 4
+ * actions) fails in its row.  No reference counterpart (solve_cli.rs's
+ * batch solves one spot at a time). */
+int gtob_batch_run_persistent(gtob_batch* batch, uint32_t max_iterations, double target_pct, uint32_t check_every,
+                              int window);
+typedef struct {
+    uint64_t launches;  /* batched iterations, one kernel launch each */
+    double kernel_ms;   /* their device time (CUDA events) */
+    int32_t tuned;      /* size classes tuned during the run */
+    int32_t tile, ctas_per_sm, grid;  /* the last shape (ctas_per_sm 0: as many as fit) and its grid */
+} gtob_batch_stats;
+int gtob_batch_stats_get(const gtob_batch* batch, gtob_batch_stats* out);
 int gtob_batch_size(const gtob_batch* batch);
 int gtob_batch_row_get(const gtob_batch* batch, int i, gtob_batch_row* out);
 /* spot i's root counterfactual values of the average strategies, per hand of
