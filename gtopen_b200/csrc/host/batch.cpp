@@ -223,7 +223,11 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
     BatchRunStats st;
     int device = 0;
     {
-        const cudaError_t rc = cudaGetDevice(&device);
+        // the device's context bound to this thread before any other thread
+        // builds engines: the engines' streams and buffers must belong to the
+        // context this thread launches in, for the whole run
+        cudaError_t rc = cudaGetDevice(&device);
+        if (rc == cudaSuccess) rc = cudaSetDevice(device);
         if (rc != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(rc));
     }
     // builder thread: engines for the spots in order, at most `window` built
@@ -265,6 +269,9 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
             built++;
             cv.notify_all();
         }
+        // stays until the run ends (the thread that built the engines outlives them)
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stop; });
     });
     struct Join {
         std::thread& t;
@@ -290,6 +297,8 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
     std::vector<double> cand_ms;
     size_t cand_next = 0;
     int cls = -1, fmt = -1;
+    const char* phase = "start";
+    try {
     for (;;) {
         {  // admit built spots while the window has room
             std::unique_lock<std::mutex> lk(mu);
@@ -329,6 +338,7 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
                 }
             }
             if (cand_next < cand.size()) shape = cand[cand_next];
+            phase = "configure";
             bk.configure(ptr, shape);
             changed = false;
         }
@@ -336,7 +346,9 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
         // shape while the class is being tuned: the shape changes no result,
         // so a trial iteration is an ordinary one)
         if (cand_next < cand.size()) {
+            phase = "configure a trial shape";
             bk.configure_shape(cand[cand_next]);
+            phase = "trial iteration";
             const double ms = bk.time_iterations(1);
             st.kernel_ms += ms;
             // per node record: the set may shrink while the class is tuned
@@ -350,6 +362,7 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
                 st.tuned++;
             }
         } else {
+            phase = "iteration";
             st.kernel_ms += bk.time_iterations(1);
         }
         st.launches++;
@@ -364,15 +377,17 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
         std::vector<double> pct(chk.size(), NAN);
         std::vector<std::string> err(chk.size());
         parallel_for(chk.size(), [&](size_t j) {
+            int stage = 0;
             try {
                 const cudaError_t r = cudaSetDevice(device);
                 if (r != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(r));
                 Live& L = live[chk[j]];
                 pct[j] = L.eng->exploitability(*L.host) / spots[L.idx]->config.tree.starting_pot * 100.0;
+                stage = 1;
                 if (pct[j] <= target_pct || L.eng->iteration() >= max_iterations)
                     finish_one(*L.eng, *L.host, L.shell == nullptr, pct[j], L.t0, rows[L.idx]);
             } catch (const std::exception& e) {
-                err[j] = e.what();
+                err[j] = std::string(e.what()) + (stage ? " (root values and sync)" : " (exploitability check)");
                 if (err[j].empty()) err[j] = "unknown error";
             }
         });
@@ -395,9 +410,13 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
             keep.push_back(std::move(live[k]));
         }
         if (changed) {
+            phase = "release finished spots";
             bk.configure({}, bk.shape());  // the kernel's set holds no freed engine
             live = std::move(keep);
         }
+    }
+    } catch (const std::exception& e) {
+        throw Error(std::string(e.what()) + " [persistent batch: " + phase + "]");
     }
     const BatchShape s = bk.shape();
     st.tile = s.tile;

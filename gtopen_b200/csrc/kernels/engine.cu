@@ -1813,6 +1813,9 @@ struct BatchImpl {
     // Every engine's own work done and its reach current (after an
     // evaluation sweep an engine primes its reach first, as iterate does).
     void ready() {
+        const cudaError_t pend = cudaGetLastError();
+        if (pend != cudaSuccess)
+            throw Error(std::string("cuda: ") + cudaGetErrorString(pend) + " (pending before the batched launch)");
         for (EngineImpl* X : E) {
             X->prime();
             CK(cudaStreamSynchronize(X->stream));
