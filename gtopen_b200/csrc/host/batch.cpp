@@ -203,6 +203,18 @@ int size_class(const std::vector<std::shared_ptr<Spot>>& spots, const std::vecto
     return n > 1.0 ? (int)std::floor(std::log2(n)) : 0;
 }
 
+bool trace_on() {
+    static const bool on = std::getenv("GTOB_BATCH_TRACE") != nullptr;
+    return on;
+}
+#define BTRACE(...)                                  \
+    do {                                             \
+        if (trace_on()) {                            \
+            std::fprintf(stderr, "[batch] " __VA_ARGS__); \
+            std::fflush(stderr);                     \
+        }                                            \
+    } while (0)
+
 struct Live {
     size_t idx;
     std::unique_ptr<HostSolver> shell;  // when the batch keeps no solver for this spot
@@ -264,6 +276,7 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
                 if (rows[i].error.empty()) rows[i].error = "unknown error";
                 L.eng.reset();
             }
+            BTRACE("built spot %zu engine %p err '%s'\n", i, (void*)L.eng.get(), rows[i].error.c_str());
             std::lock_guard<std::mutex> lk(mu);
             if (L.eng) ready.push_back(std::move(L));
             built++;
@@ -339,6 +352,7 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
             }
             if (cand_next < cand.size()) shape = cand[cand_next];
             phase = "configure";
+            for (auto& L : live) BTRACE("set: spot %zu engine %p it %u\n", L.idx, (void*)L.eng.get(), L.eng->iteration());
             bk.configure(ptr, shape);
             changed = false;
         }
@@ -382,6 +396,7 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
                 const cudaError_t r = cudaSetDevice(device);
                 if (r != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(r));
                 Live& L = live[chk[j]];
+                BTRACE("check spot %zu engine %p it %u\n", L.idx, (void*)L.eng.get(), L.eng->iteration());
                 pct[j] = L.eng->exploitability(*L.host) / spots[L.idx]->config.tree.starting_pot * 100.0;
                 stage = 1;
                 if (pct[j] <= target_pct || L.eng->iteration() >= max_iterations)
@@ -401,18 +416,19 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
                 drop[chk[j]] = true;
             }
         }
-        std::vector<Live> keep;
-        for (size_t k = 0; k < live.size(); k++) {
-            if (drop[k]) {
-                changed = true;
-                continue;
+        if (std::find(drop.begin(), drop.end(), true) != drop.end()) {
+            std::vector<Live> keep;
+            for (size_t k = 0; k < live.size(); k++) {
+                if (drop[k]) {
+                    BTRACE("drop spot %zu engine %p\n", live[k].idx, (void*)live[k].eng.get());
+                    continue;
+                }
+                keep.push_back(std::move(live[k]));
             }
-            keep.push_back(std::move(live[k]));
-        }
-        if (changed) {
             phase = "release finished spots";
-            bk.configure({}, bk.shape());  // the kernel's set holds no freed engine
-            live = std::move(keep);
+            bk.configure({}, bk.shape());  // the kernel's set holds no engine about to be freed
+            live = std::move(keep);        // the finished engines are freed here
+            changed = true;
         }
     }
     } catch (const std::exception& e) {
