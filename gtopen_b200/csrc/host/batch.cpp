@@ -242,20 +242,34 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
         if (rc == cudaSuccess) rc = cudaSetDevice(device);
         if (rc != cudaSuccess) throw Error(std::string("cuda: ") + cudaGetErrorString(rc));
     }
-    // builder thread: engines for the spots in order, at most `window` built
-    // ahead of the solve (a spot whose engine fails gets its error row)
+    // builder thread: engines for the spots in order, at most kPrefetch built
+    // ahead of the window, and each only once the device has room for it --
+    // its size predicted from the bytes per tree node of the engines built so
+    // far -- unless nothing else holds device memory (a spot whose engine
+    // fails gets its error row)
+    constexpr size_t kPrefetch = 2;
     std::mutex mu;
     std::condition_variable cv;
     std::deque<Live> ready;
-    size_t built = 0;  // spots the builder has finished with (engine ready or error row)
+    size_t built = 0;   // spots the builder has finished with (engine ready or error row)
+    size_t held = 0;    // engines alive (ready or in the window)
     bool stop = false;
+    double bytes_per_node = 0.0;  // of the engines built so far (0: none yet)
     std::thread builder([&] {
         const cudaError_t r = cudaSetDevice(device);
         for (size_t i = 0; i < solvers.size(); i++) {
             {
                 std::unique_lock<std::mutex> lk(mu);
-                cv.wait(lk, [&] { return stop || ready.size() < (size_t)window; });
-                if (stop) return;
+                for (;;) {
+                    if (stop) return;
+                    if (ready.size() < kPrefetch) {
+                        size_t fr = 0, tot = 0;
+                        const double need = bytes_per_node * (double)spots[i]->tree.size() * 1.15 + (1ull << 30);
+                        if (held == 0 || bytes_per_node <= 0.0 || (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (double)fr >= need))
+                            break;
+                    }
+                    cv.wait_for(lk, std::chrono::milliseconds(20));
+                }
             }
             Live L;
             L.idx = i;
@@ -278,7 +292,12 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
             }
             BTRACE("built spot %zu engine %p err '%s'\n", i, (void*)L.eng.get(), rows[i].error.c_str());
             std::lock_guard<std::mutex> lk(mu);
-            if (L.eng) ready.push_back(std::move(L));
+            if (L.eng) {
+                const double bpn = (double)L.eng->device_bytes() / (double)std::max<size_t>(spots[i]->tree.size(), 1);
+                bytes_per_node = std::max(bytes_per_node, bpn);
+                held++;
+                ready.push_back(std::move(L));
+            }
             built++;
             cv.notify_all();
         }
@@ -317,8 +336,25 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
             std::unique_lock<std::mutex> lk(mu);
             // an empty window (the start) fills up first, so that the first
             // set -- the one whose size class gets tuned -- is a full one
-            if (live.empty())
-                cv.wait(lk, [&] { return ready.size() >= (size_t)window || built == solvers.size(); });
+            // (or as full as device memory allows)
+            if (live.empty()) {
+                while (live.size() < (size_t)window && built < solvers.size()) {
+                    if (ready.empty()) {
+                        cv.wait_for(lk, std::chrono::milliseconds(20));
+                        // the builder waits for room that only this window's
+                        // start can give: start with what is there
+                        size_t fr = 0, tot = 0;
+                        if (ready.empty() && !live.empty() && cudaMemGetInfo(&fr, &tot) == cudaSuccess &&
+                            (double)fr < bytes_per_node * (double)spots[built]->tree.size() * 1.15 + (1ull << 30))
+                            break;
+                        continue;
+                    }
+                    live.push_back(std::move(ready.front()));
+                    ready.pop_front();
+                    changed = true;
+                    cv.notify_all();
+                }
+            }
             while (live.size() < (size_t)window && !ready.empty()) {
                 live.push_back(std::move(ready.front()));
                 ready.pop_front();
@@ -427,8 +463,14 @@ void run_batch_persistent(const std::vector<std::shared_ptr<Spot>>& spots, const
             }
             phase = "release finished spots";
             bk.configure({}, bk.shape());  // the kernel's set holds no engine about to be freed
+            const size_t freed = live.size() - keep.size();
             live = std::move(keep);        // the finished engines are freed here
             changed = true;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                held -= freed;
+            }
+            cv.notify_all();
         }
     }
     } catch (const std::exception& e) {
