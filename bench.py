@@ -582,28 +582,25 @@ def run_leaf(args, world, rank, local):
     check = LD.FullTreeCheck(g, cfg, iterations=args.leaf_check_iters)
     res = {}
     for name, n in (("trained", net), ("untrained", untrained)):
-        host = g.Solver(spot, storage="compressed", use_iso=False)
-        dl = g.dl_gpu_solver(host, n, device_format="f32")
-        t = time.perf_counter()
-        dl.iterate(args.leaf_dl_iters)
-        dl.synchronize()
-        dl_s = time.perf_counter() - t
-        e_cut = dl.exploitability(host) / cfg["tree"]["starting_pot"] * 100
-        strat = LD.dl_flop_strategies(g, dl, spot)
-        kern = dl.info()["iteration_kernels"]
-        dl.close()
-        l0, l1, ex = check.loss(strat)
-        res[name] = {"loss_pct_pot": [l0, l1], "loss_sum_pct_pot": l0 + l1, "locked_solve_exploit_pct": ex,
-                     "dl_iterations": args.leaf_dl_iters, "dl_s": dl_s, "dl_exploit_pct_cut_game": e_cut,
-                     "dl_iteration_kernels": kern}
+        r = LD.depth_limited_or_full(g, cfg, n, check, dl_iterations=args.leaf_dl_iters)
+        r.pop("strategies")
+        res[name] = r
+    # the non-learned leaf: the flop solved with the turn and river checked
+    # down (showdown equity of the ranges reaching each turn), judged the same way
+    t = time.perf_counter()
+    cd = LD.checkdown_flop_strategies(g, cfg, iterations=args.leaf_dl_iters)
+    c0, c1, cex = check.loss(cd)
+    res["checkdown"] = {"loss_pct": [c0, c1], "loss_sum_pct": c0 + c1, "locked_solve_exploit_pct": cex,
+                        "solve_s": time.perf_counter() - t}
     line = {"metric": "depth-limited flop solve (config 5): flop-strategy loss vs the full-tree solve, "
                       "trained vs untrained turn-leaf network",
-            "value": res["trained"]["loss_sum_pct_pot"], "unit": "% pot (sum over players)", "n_gpus": 1,
+            "value": res["trained"]["loss_sum_pct"], "unit": "% pot (sum over players)", "n_gpus": 1,
             "higher_is_better": False, "dtype": "bf16 (network), f32 (solve)", "data": "synthetic (seeded spots)",
             "config": {"workload": "dl_flop c5: flop %s, 1.94M-node full tree cut at 11 turn leaves, "
                                    "network 2705-1024x3-2652" % cfg["board"],
                        "training_spots": len(Xt), "validation_spots": nval},
-            "trained": res["trained"], "untrained": res["untrained"],
+            "trained": res["trained"], "untrained": res["untrained"], "checkdown_leaf": res["checkdown"],
+            "answer_path": res["trained"]["path"], "fallback_threshold_pct": LD.FALLBACK_PCT,
             "full_solve": {"iterations": check.iterations, "exploit_pct": check.full_exploit},
             "training": {"spots_generated": args.leaf_spots, "generate_s": gen_s,
                          "turn_solve_exploit_pct_mean": float(info["exploit_pct"].mean()),

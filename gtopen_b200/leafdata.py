@@ -19,6 +19,8 @@ Output row (LEAF_OUT = 2652): per player the combos' counterfactual values /
 (pot x the opponent's reach sum); only the combos of the player's hands are
 trained (mask 1).
 """
+import copy
+
 import numpy as np
 
 from . import workloads as W
@@ -247,6 +249,8 @@ class FullTreeCheck:
         gpu.iterate(self.iterations)
         v = [root_value(gpu, self.spot, p, self.pm) for p in (0, 1)]
         e = gpu.exploitability(self.host) / self.pot * 100
+        if not locks:  # the unlocked full solve: its flop strategies are the fallback's answer
+            self.full_strategies = dl_flop_strategies(self.g, gpu, self.spot)
         gpu.close()
         return v, e
 
@@ -261,3 +265,82 @@ class FullTreeCheck:
             ex.append(e)
         self.host.clear_locks()
         return out[0], out[1], ex
+
+
+# Config 5's rule: the depth-limited answer stands when committing to its flop
+# strategies costs the two players together at most this share of the pot on
+# the full tree; otherwise the full solve answers.
+FALLBACK_PCT = 0.5
+
+
+def depth_limited_or_full(g, cfg, net, check, dl_iterations=400, threshold_pct=FALLBACK_PCT, device_format="f32"):
+    """A depth-limited flop solve (turn leaves from `net`) with the full solve
+    as its judge and fallback: the flop strategies of the depth-limited
+    solve, their loss on the full tree (check: a FullTreeCheck of the same
+    config), and -- when the two losses add up to more than threshold_pct of
+    the pot -- the full solve's flop strategies as the answer instead.
+    Returns {"path": "depth-limited" or "full", "strategies", "loss_pct"
+    (both players' losses of the depth-limited strategies), "dl_s",
+    "dl_exploit_pct_cut_game", "locked_solve_exploit_pct"}."""
+    import time
+    spot = check.spot
+    host = g.Solver(spot, storage="compressed", use_iso=False)
+    dl = g.dl_gpu_solver(host, net, device_format=device_format)
+    t = time.perf_counter()
+    dl.iterate(dl_iterations)
+    dl.synchronize()
+    dl_s = time.perf_counter() - t
+    e_cut = dl.exploitability(host) / cfg["tree"]["starting_pot"] * 100
+    strat = dl_flop_strategies(g, dl, spot)
+    kern = dl.info()["iteration_kernels"]
+    dl.close()
+    l0, l1, ex = check.loss(strat)
+    full = l0 + l1 > threshold_pct
+    return {"path": "full" if full else "depth-limited",
+            "strategies": check.full_strategies if full else strat,
+            "loss_pct": [l0, l1], "loss_sum_pct": l0 + l1, "threshold_pct": threshold_pct,
+            "dl_iterations": dl_iterations, "dl_s": dl_s, "dl_exploit_pct_cut_game": e_cut,
+            "locked_solve_exploit_pct": ex, "dl_iteration_kernels": kern}
+
+
+def checkdown_config(cfg):
+    """The same flop with no betting on the turn and river: both players check
+    them down, so every turn and river chance node leads to showdowns only --
+    the non-learned leaf (showdown equity of the ranges reaching it)."""
+    c = copy.deepcopy(cfg)
+    for side in ("oop", "ip"):
+        for st in c["tree"][side][1:]:
+            st["bet"], st["raise"], st["donk"] = [], [], []
+    return c
+
+
+def flop_paths(spot):
+    """{action path from the root (child indices): node} of the flop action nodes."""
+    t = spot.tree()
+    ch = spot.children()
+    out, stack = {}, [(0, ())]
+    while stack:
+        n, key = stack.pop()
+        if t["kind"][n] != 0 or t["street"][n] != 0:
+            continue
+        out[key] = n
+        for k in range(int(t["nchild"][n])):
+            stack.append((int(ch[int(t["child_start"][n]) + k]), key + (k,)))
+    return out
+
+
+def checkdown_flop_strategies(g, cfg, iterations=400, device_format="f32"):
+    """The flop strategies of the checked-down tree (checkdown_config) solved
+    in full, keyed by the nodes of `cfg`'s own tree (the flop betting is the
+    same in both)."""
+    spot = g.Spot(checkdown_config(cfg))
+    host = g.Solver(spot, storage="compressed", use_iso=False)
+    gpu = g.GpuSolver(host, device_format=device_format)
+    gpu.iterate(iterations)
+    strat = dl_flop_strategies(g, gpu, spot)
+    gpu.close()
+    mine = flop_paths(spot)
+    full = flop_paths(g.Spot(cfg))
+    if set(mine) != set(full):
+        raise ValueError("the checked-down tree's flop differs from the full tree's")
+    return {full[k]: strat[mine[k]] for k in full}

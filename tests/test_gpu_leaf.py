@@ -84,11 +84,11 @@ def test_trained_network_gains_over_untrained():
     check = LD.FullTreeCheck(g, cfg, iterations=200)
     losses = {}
     for name, n in (("trained", net), ("untrained", untrained)):
-        dl = g.dl_gpu_solver(g.Solver(spot, storage="compressed", use_iso=False), n, device_format="f32")
-        dl.iterate(200)
-        strat = LD.dl_flop_strategies(g, dl, spot)
-        dl.close()
-        l0, l1, ex = check.loss(strat)
-        assert max(ex) < 0.5, ex
-        losses[name] = l0 + l1
+        r = LD.depth_limited_or_full(g, cfg, n, check, dl_iterations=200)
+        assert max(r["locked_solve_exploit_pct"]) < 0.5, r
+        losses[name] = r["loss_sum_pct"]
+        # config 5's rule: above 0.5% of the pot the full solve answers
+        assert r["path"] == ("full" if r["loss_sum_pct"] > LD.FALLBACK_PCT else "depth-limited"), r
+        if r["path"] == "full":
+            assert r["strategies"] is check.full_strategies
     assert losses["trained"] < 0.5 * losses["untrained"], losses

@@ -119,3 +119,19 @@ def test_dl_plan_cut():
     assert np.any(v & (t["kind"] == 1) & (t["street"] == 2))  # runouts deal the river too
     with pytest.raises(g.GtobError):
         g.dl_plan(g.Spot(W.turn_spot(g.evaluate7)))  # a turn spot has no turn leaves to cut
+
+
+def test_checkdown_tree_keeps_the_flop():
+    """The non-learned baseline's tree: the same flop betting (every flop
+    action node found by the same action path, with the same actor and
+    action count), and on the turn and river nothing but checks."""
+    cfg = LD.dl_flop_spot(g.evaluate7)
+    full, down = g.Spot(cfg), g.Spot(LD.checkdown_config(cfg))
+    pf, pd = LD.flop_paths(full), LD.flop_paths(down)
+    assert set(pf) == set(pd) and len(pf) > 10
+    tf, td = full.tree(), down.tree()
+    for k in pf:
+        assert tf["player"][pf[k]] == td["player"][pd[k]] and tf["nchild"][pf[k]] == td["nchild"][pd[k]], k
+    later = (td["kind"] == 0) & (td["street"] > 0)
+    assert later.any() and np.all(td["nchild"][later] == 1)
+    assert down.num_nodes < full.num_nodes // 10
