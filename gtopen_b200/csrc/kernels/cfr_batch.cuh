@@ -29,15 +29,19 @@
 // mbarriers are invalidated and its shared-memory accesses fenced for the
 // async proxy before the next record's copies are issued.
 //
-// The arithmetic is the staged engine's node functions at 256 threads: per
-// hand in registers, block maxima, and exact (integer) terminal sums, so the
-// results are bit-identical to the spot's own engine.
+// The arithmetic is the staged engine's node functions (the chance node's at
+// 128 threads instead of 256): per hand in registers, block maxima, and
+// exact (integer) terminal sums, so the results are bit-identical to the
+// spot's own engine.
 #pragma once
 #include "cfr_staged.cuh"
 
 namespace gtob {
 
-constexpr int kBThreads = kThreads;  // 256: the chance kernel's runout evaluator is written for this width
+// 128 threads, the staged node kernels' width: the CTA count per SM is set
+// by the largest shared-memory need over the record kinds (a showdown
+// batch's), so a narrow CTA keeps the most nodes in flight
+constexpr int kBThreads = kSThreads;
 enum BatchKind : uint32_t { kBBegin = 0, kBRoot = 1, kBDown = 2, kBEdge = 3, kBShow = 4, kBChance = 5, kBUpMine = 6,
                             kBUpOpp = 7 };
 
@@ -125,13 +129,13 @@ __device__ __forceinline__ void b_up(const BSpot& S, uint32_t r, int p, unsigned
 // One CFR iteration of every spot of the queue.  ctl: the launch's control
 // words (zeroed before the launch).
 template <int FMT>
-__global__ void __launch_bounds__(kBThreads, 2) kb_iterate(const BSpot* spots, const BSeg* segs, int nseg,
+__global__ void __launch_bounds__(kBThreads, 4) kb_iterate(const BSpot* spots, const BSeg* segs, int nseg,
                                                         unsigned nticket, unsigned* ctl) {
     extern __shared__ __align__(16) unsigned char sm[];
     __shared__ BSpot s_spot;
     __shared__ UpSharedT<kBThreads> us;
     __shared__ ShowShared<kBThreads> ss;
-    __shared__ long long s_cw[kWarps];
+    __shared__ long long s_cw[kBThreads / 32];
     __shared__ int s_flag;
     __shared__ unsigned s_t, s_seg, s_go;
     __shared__ int s_have;  // the spot in s_spot (-1: none yet)
@@ -182,7 +186,7 @@ __global__ void __launch_bounds__(kBThreads, 2) kb_iterate(const BSpot* spots, c
                 case kBDown: b_down<FMT>(S, r, sm, s_flag); break;
                 case kBEdge: edge_down(S.d, S.edge[r], p); break;
                 case kBShow: show_batch_run<kBThreads>(S.d, S.show, S.show_batch[r], p, S.msort, sm, ss); break;
-                case kBChance: chance_node<long long>(S.d, S.chance[r], p, (double*)sm, s_cw); break;
+                case kBChance: chance_node<long long, kBThreads>(S.d, S.chance[r], p, (double*)sm, s_cw); break;
                 case kBUpMine: b_up<FMT, true>(S, r, p, sm, us); break;
                 default: b_up<FMT, false>(S, r, p, sm, us); break;
             }

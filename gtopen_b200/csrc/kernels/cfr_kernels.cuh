@@ -211,6 +211,8 @@ __device__ __forceinline__ void requant16(float nr, float ns, float rk, float sk
     }
 }
 
+// Block reductions of an NT-thread CTA (sh: NT / 32 entries).
+template <int NT = kThreads>
 __device__ __forceinline__ float block_max(float v, float* sh) {  // order-independent
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     __syncthreads();
@@ -218,10 +220,10 @@ __device__ __forceinline__ float block_max(float v, float* sh) {  // order-indep
     __syncthreads();
     float m = sh[0];
 #pragma unroll
-    for (int k = 1; k < kWarps; k++) m = fmaxf(m, sh[k]);
+    for (int k = 1; k < NT / 32; k++) m = fmaxf(m, sh[k]);
     return m;
 }
-template <class T>
+template <class T, int NT = kThreads>
 __device__ __forceinline__ T block_sum(T v, T* sh) {  // fixed tree: deterministic
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -230,7 +232,7 @@ __device__ __forceinline__ T block_sum(T v, T* sh) {  // fixed tree: determinist
     __syncthreads();
     T s = 0;
 #pragma unroll
-    for (int k = 0; k < kWarps; k++) s += sh[k];
+    for (int k = 0; k < NT / 32; k++) s += sh[k];
     return s;
 }
 
@@ -377,14 +379,14 @@ __device__ __forceinline__ void node_sigma(const Dev& d, const Arenas& ar, const
 // per dependent load level instead of one per card.
 constexpr int kCardsPerWarp = (52 + kWarps - 1) / kWarps;
 
-// Scale of the exact sums over one opponent reach vector (all threads of a
-// kThreads CTA; 0 for the f32 accumulator).  sh: kWarps floats.
-template <class T>
+// Scale of the exact sums over one opponent reach vector (all threads of an
+// NT-thread CTA; 0 for the f32 accumulator).  sh: NT / 32 floats.
+template <class T, int NT = kThreads>
 __device__ __forceinline__ int vec_scale(const float* ro, int n, float* sh) {
     if (!Acc<T>::kExact) return 0;
     float m = 0.0f;
     for (int j = threadIdx.x; j < n; j += blockDim.x) m = fmaxf(m, ro[j]);
-    return fix_scale(block_max(m, sh));
+    return fix_scale(block_max<NT>(m, sh));
 }
 template <class T>
 __device__ T fold_sums(const Dev& d, int o, const float* ro, T* S, T* s_red, int& sc) {
@@ -434,11 +436,12 @@ __device__ void fold_write(const Dev& d, int p, const float* ro, T total, const 
     }
 }
 
-// Block exclusive scan of x[0..m) into out[0..m], out[m] = total (fixed order).
-template <class T>
+// Block exclusive scan of x[0..m) into out[0..m], out[m] = total (fixed
+// order; an NT-thread CTA, s_w: NT / 32 entries).
+template <class T, int NT = kThreads>
 __device__ void block_exclusive_scan(const T* x, T* out, int m, T* s_w) {
     const int tid = threadIdx.x;
-    const int chunk = (m + kThreads - 1) / kThreads;
+    const int chunk = (m + NT - 1) / NT;
     const int lo = min(tid * chunk, m), hi = min(lo + chunk, m);
     T local = 0;
     for (int k = lo; k < hi; k++) local += x[k];
@@ -458,10 +461,10 @@ __device__ void block_exclusive_scan(const T* x, T* out, int m, T* s_w) {
         out[k] = run;
         run += x[k];
     }
-    if (tid == kThreads - 1) {
+    if (tid == NT - 1) {
         T tot = 0;
 #pragma unroll
-        for (int k = 0; k < kWarps; k++) tot += s_w[k];
+        for (int k = 0; k < NT / 32; k++) tot += s_w[k];
         out[m] = tot;
     }
 }
@@ -470,8 +473,9 @@ __device__ void block_exclusive_scan(const T* x, T* out, int m, T* s_w) {
 // card-removal corrections.  Scratch `sh` (4m + 105 elements): R (sorted
 // opponent reach), P (exclusive prefix of R, P[m] = total), Q (per-card
 // exclusive prefixes, concatenated), S (per-card totals).  My hands absent
-// from the board's list get 0.  Ends with a barrier.
-template <class T>
+// from the board's list get 0.  Ends with a barrier.  NT threads (s_w: NT /
+// 32 entries); the exact sums make the result independent of NT.
+template <class T, int NT = kThreads>
 __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* ro, float win, float lose, float tie,
                               float* out, T* sh, T* s_w) {
     const int o = 1 - p;
@@ -485,15 +489,11 @@ __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* r
     T* S = Q + 2 * m + 52;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t c0 = coff[0];
-    const int sc = vec_scale<T>(ro, d.nh[o], (float*)s_w);
+    const int sc = vec_scale<T, NT>(ro, d.nh[o], (float*)s_w);
     if (threadIdx.x < 52) Q[(coff[threadIdx.x] - c0) + threadIdx.x] = 0;  // each card's exclusive prefix starts at 0
-#pragma unroll
-    for (int u = 0; u < kMaxHpt; u++) {
-        const int k = threadIdx.x + u * kThreads;
-        if (k < m) R[k] = Acc<T>::q(ro[sidx[k]], sc);
-    }
+    for (int k = threadIdx.x; k < m; k += NT) R[k] = Acc<T>::q(ro[sidx[k]], sc);
     __syncthreads();
-    block_exclusive_scan<T>(R, P, m, s_w);
+    block_exclusive_scan<T, NT>(R, P, m, s_w);
     // Per-card exclusive prefixes: whole card lists are packed into bins of
     // <= 64 entries (plan time), so one warp scans a bin as two 32-lane
     // chunks of a segmented scan (segments = cards) with no cross-warp carry.
@@ -501,7 +501,7 @@ __device__ void eval_showdown(const Dev& d, int p, uint32_t slot, const float* r
     const int nbins = (int)(d.bin_off[o][slot + 1] - d.bin_off[o][slot]) - 1;
     const uint16_t* bpos = cpos + c0;
     const uint8_t* bcard = d.ccard_card[o] + c0;
-    for (int b = warp; b < nbins; b += kWarps) {
+    for (int b = warp; b < nbins; b += NT / 32) {
         const uint32_t t0 = bs[b], t1 = bs[b + 1];
         T carry = 0;
 #pragma unroll
@@ -634,9 +634,11 @@ __global__ void __launch_bounds__(kThreads) k_showdown(Dev d, const ShowItem* it
 // suit-permutation hand tables, skipping holders of the card, times
 // 1/divisor.  All-in runout children (showdowns) are evaluated in place (T
 // is the runout showdowns' accumulator type).
-// (kThreads threads; s_w: kWarps entries; dsm: the runout scratch)
-template <class T>
+// (NT threads; s_w: NT / 32 entries; dsm: the runout scratch; nh <=
+// kMaxHpt * kThreads, which the engine checks)
+template <class T, int NT = kThreads>
 __device__ void chance_node(const Dev& d, const ChanceItem& c, int p, double* dsm, T* s_w) {
+    constexpr int HPT = kMaxHpt * kThreads / NT;  // hands per thread
     const int nh = d.nh[p], o = 1 - p, nho = d.nh[o];
     float* out = d.cfv + (size_t)c.cslot * d.nh_max;
     if (c.nterm == 0) {
@@ -657,9 +659,9 @@ __device__ void chance_node(const Dev& d, const ChanceItem& c, int p, double* ds
     float* rt = (float*)(scr + d.scr_elems);
     float* tv = rt + d.nh_pad;
     const float* ro = d.reach[o] + (size_t)c.rs[o] * d.rstr[o];
-    float acc[kMaxHpt];
+    float acc[HPT];
 #pragma unroll
-    for (int k = 0; k < kMaxHpt; k++) acc[k] = 0.0f;
+    for (int k = 0; k < HPT; k++) acc[k] = 0.0f;
     uint32_t have = kNoSlot;
     for (uint32_t t = c.cc_start; t < c.cc_start + c.cc_count; t++) {
         const CardEntry e = d.cards[t];
@@ -671,7 +673,7 @@ __device__ void chance_node(const Dev& d, const ChanceItem& c, int p, double* ds
                 for (int j = threadIdx.x; j < nho; j += blockDim.x) rt[j] = (d.mask[o][j] >> rep & 1ull) ? 0.0f : ro[j];
                 __syncthreads();
                 const TermInfo tm = d.terms[e.term];
-                eval_showdown<T>(d, p, tm.aux, rt, tm.twin, tm.tlose, tm.ttie, tv, scr, s_w);
+                eval_showdown<T, NT>(d, p, tm.aux, rt, tm.twin, tm.tlose, tm.ttie, tv, scr, s_w);
                 have = e.term;
             }
             src_v = tv;
@@ -679,8 +681,8 @@ __device__ void chance_node(const Dev& d, const ChanceItem& c, int p, double* ds
             src_v = d.cfv + (size_t)e.child_cslot * d.nh_max;
         }
 #pragma unroll
-        for (int k = 0; k < kMaxHpt; k++) {
-            const int i = threadIdx.x + k * blockDim.x;
+        for (int k = 0; k < HPT; k++) {
+            const int i = threadIdx.x + k * NT;
             if (i < nh && !(d.mask[p][i] >> card & 1ull)) {
                 const int src = e.perm ? (int)d.hperm[p][(size_t)e.perm * nh + i] : i;
                 acc[k] += src_v[src];
@@ -689,8 +691,8 @@ __device__ void chance_node(const Dev& d, const ChanceItem& c, int p, double* ds
         __syncthreads();  // tv / rt are rewritten by the next runout card
     }
 #pragma unroll
-    for (int k = 0; k < kMaxHpt; k++) {
-        const int i = threadIdx.x + k * blockDim.x;
+    for (int k = 0; k < HPT; k++) {
+        const int i = threadIdx.x + k * NT;
         if (i < nh) out[i] = acc[k] * c.inv;
     }
 }
