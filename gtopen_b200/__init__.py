@@ -144,6 +144,7 @@ def lib():
         "gtob_gpu_exploit_values": (I, [P, P, P, I, I, C.POINTER(NodeInfo)] + [P] * 8),
         "gtob_batch_new": (I, [C.POINTER(P), I, I, I, I, I, I, I, C.POINTER(P)]),
         "gtob_nccl_unique_id": (I, [P]),
+        "gtob_solver_path_view": (I, [P, P, I, C.c_char_p, U64, C.POINTER(U64)]),
         "gtob_gpu_new_sharded": (I, [P, I, I, I, I, P, C.POINTER(P)]),
         "gtob_gpu_new_sharded_host": (I, [P, I, I, I, I, REDUCE_FN, P, C.POINTER(P)]),
         "gtob_shards_new": (I, [P, I, I, I, C.POINTER(P)]),
@@ -383,6 +384,17 @@ class Solver:
     def num_locks(self):
         return lib().gtob_solver_num_locks(self._h)
 
+    def path_view(self, path):
+        """node_view's structure at the node `path` reaches (query.rs:353-461,
+        490-640), host only: node, node_type, street, board, pot, put, player,
+        actions (label, kind, amount), available_cards, locked, history."""
+        st = np.array(_path_steps(path) + [0], np.int32)
+        need = C.c_uint64()
+        _check(lib().gtob_solver_path_view(self._h, _ptr(st), len(st) - 1, None, 0, C.byref(need)))
+        buf = C.create_string_buffer(int(need.value))
+        _check(lib().gtob_solver_path_view(self._h, _ptr(st), len(st) - 1, buf, need.value, C.byref(need)))
+        return json.loads(buf.value.decode())
+
     def ensure_symmetric(self):
         _check(lib().gtob_solver_ensure_symmetric(self._h))
 
@@ -399,6 +411,19 @@ class Solver:
             header = json.loads(f.readline())
         spot = Spot(header["config"], lenient=True)
         return Solver(spot, storage=storage, _handle=h)
+
+
+def card_string(c):
+    """cards.rs card_to_string: rank then suit ("Ah", "2c")."""
+    return "23456789TJQKA"[c >> 2] + "cdhs"[c & 3]
+
+
+def combo_string(c1, c2):
+    """cards.rs:116-121 combo_to_string: the higher rank first, on equal ranks
+    the higher suit first."""
+    hi, lo = (c1, c2) if c1 > c2 else (c2, c1)
+    a, b = (hi, lo) if (hi >> 2) >= (lo >> 2) else (lo, hi)
+    return card_string(a) + card_string(b)
 
 
 def _path_steps(path):
@@ -548,6 +573,41 @@ class GpuSolver:
             na, h = info.num_actions, nh[info.player]
             out["strategy"] = strat[:na * h].reshape(na, h).copy()
             out["action_ev"] = aev[:na * h].reshape(na, h).copy()
+        return out
+
+    def node_view(self, path, solver=None):
+        """query.rs node_view (490-640) at the node `path` reaches, its numbers
+        from device memory (node_values) and its structure from the host
+        (Solver.path_view): the reference's NodeView fields, with per player
+        `hands` of combo, c1, c2, weight, reach, valid, eq, ev and, for the
+        actor, strategy and evs (None where the reference has None)."""
+        sv = solver or self.solver
+        view = sv.path_view(path)
+        vals = self.node_values(path, sv)
+        sp = sv.spot
+
+        def opt(x):
+            x = float(x)
+            return None if x != x else x
+        players = []
+        for p in (0, 1):
+            c1, c2, w, _ = sp.hands(p)
+            actor = view["node_type"] == "action" and view["player"] == p
+            hands = []
+            for i in range(sp.nh[p]):
+                h = {"combo": combo_string(int(c1[i]), int(c2[i])), "c1": int(c1[i]), "c2": int(c2[i]),
+                     "weight": float(w[i]), "reach": float(vals["reach"][p][i]), "valid": float(vals["valid"][p][i]),
+                     "eq": opt(vals["eq"][p][i]), "ev": opt(vals["ev"][p][i])}
+                if actor:
+                    h["strategy"] = [float(x) for x in vals["strategy"][:, i]]
+                    h["evs"] = [opt(x) for x in vals["action_ev"][:, i]]
+                hands.append(h)
+            players.append({"hands": hands})
+        out = {k: view[k] for k in ("node_type", "street", "board", "pot", "put", "player", "actions",
+                                    "available_cards")}
+        out["players"] = players
+        out["locked"] = view["locked"]
+        out["history"] = view["history"]
         return out
 
     def runouts(self, path, solver=None):

@@ -363,6 +363,19 @@ int gtob_gpu_exploit_values(gtob_gpu* g, const gtob_solver* v, const int* steps,
     if (averages) std::memcpy(averages, x.avg, sizeof(x.avg));
     API_END
 }
+int gtob_solver_path_view(const gtob_solver* v, const int* steps, int nsteps, char* out, uint64_t cap,
+                          uint64_t* needed) {
+    REQUIRE(v && needed && nsteps >= 0 && (steps || nsteps == 0) && (out || cap == 0));
+    API_BEGIN
+    const std::string js = path_view_json(*v->v, std::vector<int>(steps, steps + nsteps));
+    *needed = js.size() + 1;
+    if (cap > 0) {
+        const size_t k = std::min<size_t>(js.size(), (size_t)cap - 1);
+        std::memcpy(out, js.data(), k);
+        out[k] = 0;
+    }
+    API_END
+}
 int gtob_nccl_unique_id(unsigned char out[128]) {
     REQUIRE(out);
     API_BEGIN

@@ -1,7 +1,9 @@
 #include "query.hpp"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
+#include <cstdio>
 #include <limits>
 
 #include "../kernels/engine.hpp"
@@ -491,6 +493,165 @@ ExploitValues exploit_values(GpuEngine& eng, const HostSolver& host, const std::
         out.avg[0] = out.avg[1] = out.avg[2] = nan;
     }
     return out;
+}
+
+// ------------------------------------------------ node_view's structure
+namespace {
+// tree.rs:163-169: an integral amount as an integer, else two decimals
+std::string trim_num(double x) {
+    if (std::fabs(x - std::round(x)) < 1e-6) return std::to_string((long long)std::round(x));
+    char b[64];
+    std::snprintf(b, sizeof(b), "%.2f", x);
+    return b;
+}
+// an integral f64 printed as Rust's `{}` prints it (the bet label's percentage)
+std::string rust_int_f64(double x) {
+    if (x == 0.0) return std::signbit(x) ? "-0" : "0";
+    char b[64];
+    std::snprintf(b, sizeof(b), "%.0f", x);
+    return b;
+}
+const char* act_kind_name(int k) {
+    switch (k) {
+        case kFoldA: return "fold";
+        case kCheck: return "check";
+        case kCall: return "call";
+        case kBet: return "bet";
+        default: return "raise";
+    }
+}
+// query.rs:353-394 action_views
+json::Value action_views(const Spot& sp, uint32_t n) {
+    const Tree& t = sp.tree;
+    json::Value arr = json::Value::array();
+    if (t.kind[n] != kAction) return arr;
+    const double pot = t.put0[n] + t.put1[n];
+    const int me = t.player[n];
+    const TreeConfig& cfg = sp.config.tree;
+    for (int a = 0; a < t.nchild[n]; a++) {
+        const int k = t.act_kind[t.action_start[n] + a];
+        const double amt = t.act_amount[t.action_start[n] + a];
+        bool all_in = false;
+        if (k == kBet || k == kRaise) {
+            const uint32_t c = t.child(n, a);
+            const double put = me == 0 ? t.put0[c] : t.put1[c];
+            all_in = std::fabs(cfg.effective_stack - (put - cfg.starting_pot / 2.0)) < 1e-6;
+        }
+        std::string label;
+        switch (k) {
+            case kFoldA: label = "Fold"; break;
+            case kCheck: label = "Check"; break;
+            case kCall: label = "Call"; break;
+            case kBet:
+                label = all_in ? "All-in " + trim_num(amt)
+                               : "Bet " + trim_num(amt) + " (" + rust_int_f64(std::round(amt / pot * 100.0)) + "%)";
+                break;
+            default: label = all_in ? "All-in " + trim_num(amt) : "Raise " + trim_num(amt); break;
+        }
+        json::Value v = json::Value::object();
+        v.set("label", json::Value::string(label));
+        v.set("kind", json::Value::string(act_kind_name(k)));
+        v.set("amount", json::Value::number(k == kCall || k == kBet || k == kRaise ? amt : 0.0));
+        arr.arr.push_back(std::move(v));
+    }
+    return arr;
+}
+json::Value opt_int(bool has, long long v) { return has ? json::Value::integer(v) : json::Value(); }
+}  // namespace
+
+std::string path_view_json(const HostSolver& host, const std::vector<int>& steps) {
+    const Spot& sp = *host.spot;
+    const Tree& t = sp.tree;
+    const TreeConfig& cfg = sp.config.tree;
+    auto stack_of = [&](uint32_t n) {
+        const int p = t.player[n];
+        return cfg.effective_stack - ((p == 0 ? t.put0[n] : t.put1[n]) - cfg.starting_pot / 2.0);
+    };
+    json::Value history = json::Value::array();
+    std::vector<uint8_t> dealt;
+    uint32_t n = 0;
+    for (int st : steps) {  // query.rs:396-461 build_history, walk_path's checks
+        json::Value h = json::Value::object();
+        if (t.kind[n] == kAction && st >= 0) {
+            if (st >= t.nchild[n]) throw Error("invalid argument: action index out of range");
+            h.set("kind", json::Value::string("action"));
+            h.set("player", json::Value::integer(t.player[n]));
+            h.set("stack", json::Value::number(stack_of(n)));
+            h.set("pot", json::Value::number(t.put0[n] + t.put1[n]));
+            h.set("street", json::Value::integer(t.street[n]));
+            h.set("actions", action_views(sp, n));
+            h.set("chosen", json::Value::integer(st));
+            h.set("card", json::Value());
+            n = t.child(n, st);
+        } else if (t.kind[n] == kChance && st < 0) {
+            const int c = -1 - st;
+            if (c >= 52 || t.child(n, c) == kSentinel || std::find(dealt.begin(), dealt.end(), (uint8_t)c) != dealt.end())
+                throw Error("invalid argument: card " + std::to_string(c) + " cannot be dealt here");
+            h.set("kind", json::Value::string("card"));
+            h.set("player", json::Value());
+            h.set("stack", json::Value::number(0.0));
+            h.set("pot", json::Value::number(t.put0[n] + t.put1[n]));
+            h.set("street", json::Value::integer(t.street[n]));
+            h.set("actions", json::Value::array());
+            h.set("chosen", json::Value());
+            h.set("card", json::Value::string(card_name((uint8_t)c)));
+            dealt.push_back((uint8_t)c);
+            n = t.child(n, c);
+        } else {
+            throw Error("invalid argument: path step does not match node type");
+        }
+        history.arr.push_back(std::move(h));
+    }
+    const bool act = t.kind[n] == kAction;
+    {
+        json::Value h = json::Value::object();
+        h.set("kind", json::Value::string(act ? "action" : t.kind[n] == kChance ? "card" : "terminal"));
+        h.set("player", opt_int(act, t.player[n]));
+        h.set("stack", json::Value::number(act ? stack_of(n) : 0.0));
+        h.set("pot", json::Value::number(t.put0[n] + t.put1[n]));
+        h.set("street", json::Value::integer(t.street[n]));
+        h.set("actions", action_views(sp, n));
+        h.set("chosen", json::Value());
+        h.set("card", json::Value());
+        history.arr.push_back(std::move(h));
+    }
+    static const char* kTypes[4] = {"action", "chance", "terminal_fold", "terminal_showdown"};
+    json::Value v = json::Value::object();
+    v.set("node", json::Value::integer(n));
+    v.set("node_type", json::Value::string(t.kind[n] < 4 ? kTypes[t.kind[n]] : "?"));
+    v.set("street", json::Value::integer(t.street[n]));
+    json::Value board = json::Value::array();
+    for (uint8_t c : sp.board) board.arr.push_back(json::Value::string(card_name(c)));
+    for (uint8_t c : dealt) board.arr.push_back(json::Value::string(card_name(c)));
+    v.set("board", board);
+    v.set("pot", json::Value::number(t.put0[n] + t.put1[n]));
+    json::Value put = json::Value::array();
+    put.arr.push_back(json::Value::number(t.put0[n]));
+    put.arr.push_back(json::Value::number(t.put1[n]));
+    v.set("put", put);
+    v.set("player", opt_int(act, t.player[n]));
+    v.set("actions", action_views(sp, n));
+    if (t.kind[n] == kChance) {
+        json::Value cards = json::Value::array();
+        for (int c = 0; c < 52; c++)
+            if (t.child(n, c) != kSentinel && std::find(dealt.begin(), dealt.end(), (uint8_t)c) == dealt.end())
+                cards.arr.push_back(json::Value::string(card_name((uint8_t)c)));
+        v.set("available_cards", cards);
+    } else {
+        v.set("available_cards", json::Value());
+    }
+    // the lock lives on the orbit representative's node (query.rs:627-633)
+    bool locked = false;
+    {
+        std::array<uint8_t, 4> perm;
+        const std::vector<int> canon = host.canonical_steps(steps, &perm);
+        uint32_t m = 0;
+        for (int st : canon) m = st >= 0 ? t.child(m, st) : t.child(m, -1 - st);
+        locked = host.locks.count(m) > 0;
+    }
+    v.set("locked", json::Value::boolean(locked));
+    v.set("history", history);
+    return json::dump(v);
 }
 
 }  // namespace gtob

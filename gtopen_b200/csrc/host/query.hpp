@@ -6,6 +6,7 @@
 // the values from one average-strategy evaluation sweep per player.
 #pragma once
 #include <cstdint>
+#include <string>
 #include <vector>
 
 #include "solver.hpp"
@@ -59,6 +60,15 @@ Runouts runouts(GpuEngine& eng, const HostSolver& host, const std::vector<int>& 
 // remaining runouts of the board plus `dealt` (best_response.rs:292-386,
 // game.rs:580-653 sweep_buckets); NaN where no compatible mass.
 std::vector<float> equity(const Spot& sp, int p, const float* reach_o, const uint8_t* dealt, int nd);
+
+// node_view's structure at the node a path reaches, without the per-hand
+// numbers (query.rs:353-461, 490-640): node type, street, board (the spot's
+// cards and the dealt ones), pot and puts, actor, the action views (label,
+// kind, amount; tree.rs:139-169 labels), the cards a chance node can deal,
+// whether the node -- on its orbit representative -- is locked, and the
+// history bar (one step per node along the path, then the current node).  A
+// JSON object with the reference's field names; Option fields are null.
+std::string path_view_json(const HostSolver& host, const std::vector<int>& steps);
 
 // steps: action indices (>= 0) and dealt cards (-1 - card), from the root.
 // Through a suit-isomorphic branch the device holds the representative: its

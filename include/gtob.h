@@ -236,6 +236,17 @@ typedef struct {
 int gtob_gpu_node_values(gtob_gpu* gpu, const gtob_solver* solver, const int* steps, int nsteps, gtob_node_info* info,
                          float* reach0, float* reach1, float* valid0, float* valid1, float* eq0, float* eq1,
                          float* ev0, float* ev1, float* strategy, float* action_ev);
+/* node_view's structure (query.rs:353-461, 490-640) at the node a path
+ * reaches, without the per-hand numbers: a JSON object with the reference's
+ * field names -- node, node_type, street, board, pot, put, player (null off
+ * action nodes), actions [{label, kind, amount}] with tree.rs:139-169's
+ * labels, available_cards (chance nodes, else null), locked (on the orbit
+ * representative) and history (one step per path node, then the current
+ * node: kind, player, stack, pot, street, actions, chosen, card).  Host only.
+ * Writes at most cap bytes including the terminating NUL; *needed receives
+ * the full size (call again with a larger buffer when it exceeds cap). */
+int gtob_solver_path_view(const gtob_solver* solver, const int* steps, int nsteps, char* out, uint64_t cap,
+                          uint64_t* needed);
 /* runouts (query.rs:964-1106) at the chance node a path reaches: one row per
  * available card, descending -- the action frequencies at the following
  * action node (freqs[row * max_actions + a], reach-weighted), and per player
