@@ -610,6 +610,58 @@ class GpuSolver:
         out["history"] = view["history"]
         return out
 
+    def exploit_view(self, path, exploiter, solver=None):
+        """query.rs exploit_view (808-930): the ExploitView fields -- node_type,
+        exploiter, player, actions, locked, per hand of the exploiter combo,
+        c1, c2, weight, reach, valid, br_ev, cur_ev, gain and, where the
+        exploiter acts, br_strategy and evs; avg_br_ev / avg_cur_ev / avg_gain
+        -- numbers from device memory (exploit_values), structure from the host."""
+        sv = solver or self.solver
+        view = sv.path_view(path)
+        vals = self.exploit_values(path, exploiter, sv)
+        c1, c2, w, _ = sv.spot.hands(exploiter)
+
+        def opt(x):
+            x = float(x)
+            return None if x != x else x
+        actor = view["node_type"] == "action" and view["player"] == exploiter
+        hands = []
+        for i in range(sv.spot.nh[exploiter]):
+            h = {"combo": combo_string(int(c1[i]), int(c2[i])), "c1": int(c1[i]), "c2": int(c2[i]),
+                 "weight": float(w[i]), "reach": float(vals["reach"][i]), "valid": float(vals["valid"][i]),
+                 "br_ev": opt(vals["br_ev"][i]), "cur_ev": opt(vals["cur_ev"][i]), "gain": opt(vals["gain"][i])}
+            if actor:
+                h["br_strategy"] = [float(x) for x in vals["br_strategy"][:, i]]
+                h["evs"] = [opt(x) for x in vals["action_ev"][:, i]]
+            hands.append(h)
+        avg = [opt(x) for x in vals["averages"]]
+        return {"node_type": view["node_type"], "exploiter": int(exploiter), "player": view["player"],
+                "actions": view["actions"], "locked": view["locked"], "hands": hands,
+                "avg_br_ev": avg[0], "avg_cur_ev": avg[1], "avg_gain": avg[2]}
+
+    def runouts_report(self, path, solver=None):
+        """query.rs runouts (964-1106) as its RunoutsReport: actions (of the
+        action node after the first card, in descending card order, that
+        leads to one), player, pot and per card (descending) the card string,
+        freqs, eq and ev per player (None without mass)."""
+        sv = solver or self.solver
+        r = self.runouts(path, sv)
+
+        def opt(x):
+            x = float(x)
+            return None if x != x else x
+        actions = []
+        for row in r["rows"]:
+            v = sv.path_view(list(path) + [card_string(row["card"])])
+            if v["node_type"] == "action":
+                actions = v["actions"]
+                break
+        rows = [{"card": card_string(row["card"]), "freqs": [float(x) for x in row["freqs"]],
+                 "eq": [opt(row["eq"][0]), opt(row["eq"][1])], "ev": [opt(row["ev"][0]), opt(row["ev"][1])]}
+                for row in r["rows"]]
+        return {"actions": actions, "player": r["player"] if r["player"] >= 0 else None, "pot": r["pot"],
+                "rows": rows}
+
     def runouts(self, path, solver=None):
         """query.rs runouts at the chance node `path` reaches, from device
         memory: dict with player, pot and rows (card, freqs, eq, ev)."""

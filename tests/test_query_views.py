@@ -231,3 +231,53 @@ def test_node_view_composes_host_structure_and_device_numbers():
             assert "strategy" not in h0 and "evs" not in h0 and h0["ev"] == 1.0
     # combo strings: higher rank first, on equal ranks the higher suit first
     assert g.combo_string(0, 51) == "As2c" and g.combo_string(48, 51) == "AsAc"
+
+
+def _stub_gpu(sv, **methods):
+    gpu = g.GpuSolver.__new__(g.GpuSolver)
+    gpu._h = None
+    gpu.solver = sv
+    for k, f in methods.items():
+        setattr(gpu, k, f)
+    return gpu
+
+
+def test_exploit_view_and_runouts_report_compose():
+    """GpuSolver.exploit_view and runouts_report assembled from stand-in
+    device numbers: the reference's ExploitView and RunoutsReport fields."""
+    cfg = W.small_flop_spot()
+    spot = g.Spot(cfg)
+    sv = g.Solver(spot)
+    hv = sv.path_view([1])
+    na, p = len(hv["actions"]), hv["player"]
+    nh = spot.nh[p]
+
+    def fake_exploit(path, exploiter, solver=None):
+        z = np.ones(spot.nh[exploiter], np.float32)
+        gain = z.copy()
+        gain[0] = np.nan
+        return {"node": hv["node"], "kind": 0, "player": p, "reach": z, "valid": z * 2, "br_ev": z * 3,
+                "cur_ev": z * 2, "gain": gain, "averages": np.array([3, 2, np.nan], np.float32),
+                "br_strategy": np.eye(na, nh, dtype=np.float32), "action_ev": np.zeros((na, nh), np.float32)}
+    gpu = _stub_gpu(sv, exploit_values=fake_exploit)
+    ev = gpu.exploit_view([1], p)
+    assert set(ev) == {"node_type", "exploiter", "player", "actions", "locked", "hands", "avg_br_ev", "avg_cur_ev",
+                       "avg_gain"}
+    assert ev["actions"] == hv["actions"] and ev["avg_gain"] is None and ev["avg_br_ev"] == 3.0
+    assert ev["hands"][0]["gain"] is None and ev["hands"][0]["br_strategy"] == [1.0] + [0.0] * (na - 1)
+    other = gpu.exploit_view([1], 1 - p)
+    assert "br_strategy" not in other["hands"][0]
+
+    chance = [0, 0]  # check, check: the turn's chance node
+    cv = sv.path_view(chance)
+    assert cv["node_type"] == "chance"
+    cards = [("23456789TJQKA".index(c[0]) * 4 + "cdhs".index(c[1])) for c in cv["available_cards"]][::-1]
+
+    def fake_runouts(path, solver=None):
+        rows = [{"card": c, "freqs": np.full(2, 0.5, np.float32), "eq": [0.4, np.nan], "ev": [1.0, 2.0]}
+                for c in cards]
+        return {"player": 0, "num_actions": 2, "pot": 60.0, "rows": rows}
+    rep = _stub_gpu(sv, runouts=fake_runouts).runouts_report(chance)
+    assert rep["pot"] == 60.0 and rep["player"] == 0 and len(rep["rows"]) == len(cards)
+    assert rep["rows"][0]["card"] == g.card_string(cards[0]) and rep["rows"][0]["eq"] == [pytest.approx(0.4), None]
+    assert rep["actions"] == sv.path_view(chance + [g.card_string(cards[0])])["actions"]
