@@ -154,6 +154,7 @@ def lib():
         "gtob_shards_sync_to_cpu": (I, [P, P, I]),
         "gtob_shards_free": (None, [P]),
         "gtob_spot_shard_visited": (I, [P, I, I, I, P]),
+        "gtob_spot_batch_queue": (I, [C.POINTER(P), I, I, I, P, I, C.POINTER(I), C.POINTER(U64), C.POINTER(U64)]),
         "gtob_batch_run": (I, [P, U32, D, U32, I]),
         "gtob_batch_run_persistent": (I, [P, U32, D, U32, I]),
         "gtob_batch_stats_get": (I, [P, C.POINTER(BatchStats)]),
@@ -792,6 +793,24 @@ class Shards:
     def sync_to_cpu(self, solver=None, strategy_only=False):
         """Every shard's nodes into one host solver (GpuSolver.sync_to_cpu per shard)."""
         _check(lib().gtob_shards_sync_to_cpu(self._h, (solver or self.solver)._h, int(bool(strategy_only))))
+
+
+BATCH_SEGMENT = np.dtype([("first", np.uint64), ("start", np.uint32), ("count", np.uint32), ("need", np.uint32),
+                          ("spot", np.uint32), ("step", np.uint32), ("kind", np.int32), ("p", np.int32),
+                          ("tile", np.int32)])
+
+
+def batch_queue(spots, tile=4, use_iso=True):
+    """The persistent batch kernel's work queue for these spots, built on the
+    host (no GPU): (segments as a structured array, tickets, records)."""
+    arr = (C.c_void_p * len(spots))(*[sp._h for sp in spots])
+    n, nt, nr = C.c_int(), C.c_uint64(), C.c_uint64()
+    _check(lib().gtob_spot_batch_queue(arr, len(spots), int(use_iso), int(tile), None, 0, C.byref(n), C.byref(nt),
+                                       C.byref(nr)))
+    out = np.zeros(n.value, BATCH_SEGMENT)
+    _check(lib().gtob_spot_batch_queue(arr, len(spots), int(use_iso), int(tile), _ptr(out), n.value, C.byref(n),
+                                       C.byref(nt), C.byref(nr)))
+    return out, nt.value, nr.value
 
 
 def shard_visited(spot, shard, nshards, use_iso=True):

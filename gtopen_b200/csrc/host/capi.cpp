@@ -458,6 +458,26 @@ int gtob_shards_sync_to_cpu(gtob_shards* g, gtob_solver* v, int strategy_only) {
     API_END
 }
 void gtob_shards_free(gtob_shards* g) { delete g; }
+int gtob_spot_batch_queue(gtob_spot* const* spots, int n, int use_iso, int tile, gtob_batch_segment* out, int cap,
+                          int* nseg, uint64_t* ntickets, uint64_t* nrecords) {
+    REQUIRE(spots && n > 0 && tile >= 1 && cap >= 0 && (out || cap == 0) && nseg && ntickets && nrecords);
+    for (int i = 0; i < n; i++) REQUIRE(spots[i]);
+    API_BEGIN
+    std::vector<Plan> plans(n);
+    std::vector<const Plan*> ptr;
+    for (int i = 0; i < n; i++) {
+        plans[i] = build_plan(*spots[i]->s, use_iso != 0, kFuseFolds);
+        ptr.push_back(&plans[i]);
+    }
+    std::vector<BatchSegment> q;
+    *ntickets = batch_queue(ptr, tile, q, nrecords);
+    *nseg = (int)q.size();
+    for (int k = 0; k < std::min<int>(cap, (int)q.size()); k++) {
+        const BatchSegment& g = q[k];
+        out[k] = gtob_batch_segment{g.first, g.start, g.count, g.need, g.spot, g.step, g.kind, g.p, g.tile};
+    }
+    API_END
+}
 int gtob_spot_shard_visited(const gtob_spot* sp, int use_iso, int shard, int nshards, uint8_t* visited) {
     REQUIRE(sp && visited && nshards >= 1 && shard >= 0 && shard < nshards);
     API_BEGIN

@@ -782,4 +782,61 @@ Plan build_plan(const Spot& sp, bool use_iso, int fuse_mode, int shard, int nsha
     return P;
 }
 
+std::vector<std::vector<BatchSpan>> batch_steps(const Plan& P, int tile) {
+    const int L = P.num_levels;
+    std::vector<std::vector<BatchSpan>> st;
+    auto add = [&](std::vector<BatchSpan> v) {
+        std::vector<BatchSpan> keep;
+        for (auto& x : v)
+            if (x.s.count) keep.push_back(x);
+        if (!keep.empty()) st.push_back(std::move(keep));
+    };
+    for (int p = 0; p < 2; p++) {
+        std::vector<BatchSpan> first;
+        if (p == 0) first.push_back({kBBegin, 0, {0, 1}, 1});
+        first.push_back({kBRoot, 0, {0, 1}, 1});
+        add(first);
+        const int opp = 1 - p;
+        for (int l = 0; l < L; l++)
+            add({{kBDown, 0, P.act_span_actor[opp][l], tile}, {kBEdge, 1 << opp, P.edge_span[l], tile}});
+        std::vector<BatchSpan> shows;
+        for (int l = 0; l < L; l++) shows.push_back({kBShow, p, P.show_batch_span[l], 1});
+        add(shows);
+        for (int l = L - 1; l >= 0; l--)
+            add({{kBChance, p, P.chance_span[l], tile},
+                 {kBUpMine, p, P.act_span_actor[p][l], tile},
+                 {kBUpOpp, p, P.act_span_actor[opp][l], tile}});
+    }
+    return st;
+}
+
+uint64_t batch_queue(const std::vector<const Plan*>& plans, int tile, std::vector<BatchSegment>& out,
+                     uint64_t* records) {
+    tile = std::max(1, std::min(tile, 64));
+    std::vector<std::vector<std::vector<BatchSpan>>> steps(plans.size());
+    size_t kmax = 0;
+    for (size_t s = 0; s < plans.size(); s++) {
+        steps[s] = batch_steps(*plans[s], tile);
+        kmax = std::max(kmax, steps[s].size());
+    }
+    out.clear();
+    std::vector<uint32_t> before(plans.size(), 0);  // tickets of the spot's steps so far
+    uint64_t t = 0, rec = 0;
+    for (size_t k = 0; k < kmax; k++)
+        for (size_t s = 0; s < plans.size(); s++) {
+            if (k >= steps[s].size()) continue;
+            uint32_t here = 0;
+            for (const BatchSpan& x : steps[s][k]) {
+                const uint32_t nt = (x.s.count + (uint32_t)x.tile - 1) / (uint32_t)x.tile;
+                out.push_back({t, x.s.start, x.s.count, before[s], (uint32_t)s, (uint32_t)k, x.kind, x.p, x.tile});
+                t += nt;
+                here += nt;
+                rec += x.s.count;
+            }
+            before[s] += here;
+        }
+    if (records) *records = rec;
+    return t;
+}
+
 }  // namespace gtob

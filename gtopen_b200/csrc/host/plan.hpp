@@ -278,6 +278,40 @@ struct Plan {
     int river_depth = 0;                       // deepest river action node (root = 0), over all programs
 };
 
+// The batched iteration's work queue (the persistent multi-spot kernel,
+// kernels/cfr_batch.cuh).  A spot's CFR iteration is a list of steps in the
+// order of the level sweeps' launches -- per traverser p = 0, 1: the
+// iteration's discounts (p = 0 only) and the root reach; each level of the
+// down sweep (the opponent's action nodes and the chance edges); the
+// showdown batches of every level; each level of the up sweep, deepest
+// first (chance nodes, the traverser's and the opponent's action nodes) --
+// and a step is up to three spans of one kind of record (the staged engine's
+// node records, chance edges, showdown batches, chance nodes).  Records of
+// one step never depend on each other.
+enum BatchKind : uint32_t { kBBegin = 0, kBRoot = 1, kBDown = 2, kBEdge = 3, kBShow = 4, kBChance = 5, kBUpMine = 6,
+                            kBUpOpp = 7 };
+struct BatchSpan {
+    int kind, p;  // p: traverser (show, chance, up); edges: the players whose reach is refreshed (a mask)
+    Span s;
+    int tile;     // records per ticket
+};
+std::vector<std::vector<BatchSpan>> batch_steps(const Plan& P, int tile);
+// One queue segment: a span of one step of one spot, cut into tickets of
+// `tile` records.  Segments are ordered by step index, then spot, and a
+// segment's `need` counts the tickets of its spot's earlier steps -- all of
+// them numbered below the segment's first ticket, so a ticket only waits
+// on lower tickets.
+struct BatchSegment {
+    uint64_t first;  // first ticket
+    uint32_t start, count, need;
+    uint32_t spot, step;
+    int kind, p, tile;
+};
+// The queue of one batched iteration of the given plans; returns the ticket
+// count (*records: the node records it covers).
+uint64_t batch_queue(const std::vector<const Plan*>& plans, int tile, std::vector<BatchSegment>& out,
+                     uint64_t* records);
+
 // shard / nshards: the representative subtrees below the first chance nodes
 // are dealt round-robin over nshards plans, each keeping the whole tree above
 // them; the values of those subtrees' roots are summed over the shards

@@ -42,8 +42,7 @@ namespace gtob {
 // by the largest shared-memory need over the record kinds (a showdown
 // batch's), so a narrow CTA keeps the most nodes in flight
 constexpr int kBThreads = kSThreads;
-enum BatchKind : uint32_t { kBBegin = 0, kBRoot = 1, kBDown = 2, kBEdge = 3, kBShow = 4, kBChance = 5, kBUpMine = 6,
-                            kBUpOpp = 7 };
+// (BatchKind, the record kinds of a ticket: host/plan.hpp)
 
 // One spot as the batched kernel reads it (copied to shared memory when a
 // CTA starts a ticket of a spot other than its last one).

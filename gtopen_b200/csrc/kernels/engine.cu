@@ -1683,52 +1683,13 @@ struct BatchImpl {
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel_fn(), kBThreads, smem));
         return n;
     }
-    // One spot's iteration as steps of (kind, traverser / qmask, span, tile),
-    // the order of GpuEngine::iterate's graph: per traverser the discounts and
-    // root reach, the down sweep's levels (the opponent's reach), the
-    // showdowns of every level, the up sweep's levels deepest first.
-    struct SSpan {
-        int kind, p;
-        Span s;
-        int tile;
-    };
-    static std::vector<std::vector<SSpan>> steps_of(const EngineImpl& X, int tile) {
-        const Plan& P = X.plan;
-        const int L = P.num_levels;
-        std::vector<std::vector<SSpan>> st;
-        auto add = [&](std::vector<SSpan> v) {
-            std::vector<SSpan> keep;
-            for (auto& x : v)
-                if (x.s.count) keep.push_back(x);
-            if (!keep.empty()) st.push_back(std::move(keep));
-        };
-        for (int p = 0; p < 2; p++) {
-            std::vector<SSpan> first;
-            if (p == 0) first.push_back({kBBegin, 0, {0, 1}, 1});
-            first.push_back({kBRoot, 0, {0, 1}, 1});
-            add(first);
-            const int opp = 1 - p;
-            for (int l = 0; l < L; l++)
-                add({{kBDown, 0, P.act_span_actor[opp][l], tile}, {kBEdge, 1 << opp, P.edge_span[l], tile}});
-            std::vector<SSpan> shows;
-            for (int l = 0; l < L; l++) shows.push_back({kBShow, p, P.show_batch_span[l], 1});
-            add(shows);
-            for (int l = L - 1; l >= 0; l--)
-                add({{kBChance, p, P.chance_span[l], tile},
-                     {kBUpMine, p, P.act_span_actor[p][l], tile},
-                     {kBUpOpp, p, P.act_span_actor[opp][l], tile}});
-        }
-        return st;
-    }
     void build() {
         release();
         if (eng.empty()) return;
         if (!stream) CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
-        const int tile = std::max(1, std::min(shape.tile, 64));
         std::vector<BSpot> hs(E.size());
         smem = 16;
-        std::vector<std::vector<std::vector<SSpan>>> steps(E.size());
-        size_t kmax = 0;
+        std::vector<const Plan*> plans;
         for (size_t s = 0; s < E.size(); s++) {
             const EngineImpl& X = *E[s];
             BSpot& b = hs[s];
@@ -1743,37 +1704,24 @@ struct BatchImpl {
             b.msort = (int)X.plan.max_sorted;
             b.algo = X.algo;
             smem = std::max({smem, X.st_mine_smem, X.st_opp_smem, X.st_down_smem, X.show_pair_smem, X.chance_smem});
-            steps[s] = steps_of(X, tile);
-            kmax = std::max(kmax, steps[s].size());
+            plans.push_back(&X.plan);
         }
         // segments ordered by step, then spot; a segment's tickets wait for
-        // the spot's tickets of its earlier steps
-        std::vector<BSeg> hg;
-        std::vector<uint32_t> before(E.size(), 0);  // tickets of the spot's steps so far
-        uint64_t t = 0;
-        for (size_t k = 0; k < kmax; k++) {
-            for (size_t s = 0; s < E.size(); s++) {
-                if (k >= steps[s].size()) continue;
-                uint32_t here = 0;
-                for (const SSpan& x : steps[s][k]) {
-                    BSeg g;
-                    std::memset(&g, 0, sizeof(g));
-                    g.first = (uint32_t)t;
-                    g.start = x.s.start;
-                    g.count = x.s.count;
-                    g.need = before[s];
-                    g.spot = (uint16_t)s;
-                    g.kind = (uint8_t)x.kind;
-                    g.p = (uint8_t)x.p;
-                    g.tile = (uint16_t)x.tile;
-                    const uint32_t nt = (x.s.count + (uint32_t)x.tile - 1) / (uint32_t)x.tile;
-                    nrecord += x.s.count;
-                    hg.push_back(g);
-                    t += nt;
-                    here += nt;
-                }
-                before[s] += here;
-            }
+        // the spot's tickets of its earlier steps (host/plan.cpp)
+        std::vector<BatchSegment> q;
+        const uint64_t t = batch_queue(plans, shape.tile, q, &nrecord);
+        std::vector<BSeg> hg(q.size());
+        for (size_t k = 0; k < q.size(); k++) {
+            BSeg& g = hg[k];
+            std::memset(&g, 0, sizeof(g));
+            g.first = (uint32_t)q[k].first;
+            g.start = q[k].start;
+            g.count = q[k].count;
+            g.need = q[k].need;
+            g.spot = (uint16_t)q[k].spot;
+            g.kind = (uint8_t)q[k].kind;
+            g.p = (uint8_t)q[k].p;
+            g.tile = (uint16_t)q[k].tile;
         }
         if (t >= 0xFFFFFFFFull) throw Error("batch: too many tickets in one iteration");
         nticket = (unsigned)t;

@@ -318,6 +318,22 @@ int gtob_shards_export_arena(gtob_shards* shards, int which, int player, float* 
  * gtob_gpu_sync_to_cpu of each shard in turn */
 int gtob_shards_sync_to_cpu(gtob_shards* shards, gtob_solver* solver, int strategy_only);
 void gtob_shards_free(gtob_shards* shards);
+/* The persistent batch kernel's work queue for these spots, built on the host
+ * with no GPU (the staged engine's plans): one segment per span of one step of
+ * one spot, ordered by step then spot, with the ticket it starts at and the
+ * tickets of its spot's earlier steps it waits for (need).  kind: 0 discounts,
+ * 1 root reach, 2 down-sweep action nodes, 3 chance edges, 4 showdown
+ * batches, 5 chance nodes, 6 / 7 up-sweep action nodes of the traverser / its
+ * opponent; p: traverser (edges: mask of the players whose reach is
+ * refreshed).  *nseg, *ntickets and *nrecords receive the totals; at most cap
+ * segments are written.  It exists to check the queue's order on the CPU. */
+typedef struct {
+    uint64_t first;
+    uint32_t start, count, need, spot, step;
+    int32_t kind, p, tile;
+} gtob_batch_segment;
+int gtob_spot_batch_queue(gtob_spot* const* spots, int n, int use_iso, int tile, gtob_batch_segment* out, int cap,
+                          int* nseg, uint64_t* ntickets, uint64_t* nrecords);
 /* The plan partition without a GPU: visited[node] = 1 for every node shard
  * `shard` of `nshards` visits (staged engine's plan). */
 int gtob_spot_shard_visited(const gtob_spot* spot, int use_iso, int shard, int nshards, uint8_t* visited);
