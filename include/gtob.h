@@ -326,7 +326,8 @@ void gtob_shards_free(gtob_shards* shards);
  * batches, 5 chance nodes, 6 / 7 up-sweep action nodes of the traverser / its
  * opponent; p: traverser (edges: mask of the players whose reach is
  * refreshed).  *nseg, *ntickets and *nrecords receive the totals; at most cap
- * segments are written.  It exists to check the queue's order on the CPU. */
+ * segments are written.  It exists to check the queue's order on the CPU; no
+ * reference counterpart. */
 typedef struct {
     uint64_t first;
     uint32_t start, count, need, spot, step;

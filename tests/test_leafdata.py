@@ -135,3 +135,54 @@ def test_checkdown_tree_keeps_the_flop():
     later = (td["kind"] == 0) & (td["street"] > 0)
     assert later.any() and np.all(td["nchild"][later] == 1)
     assert down.num_nodes < full.num_nodes // 10
+
+
+def test_depth_limited_or_full_applies_the_threshold():
+    """Config 5's rule with stand-ins for the engine (no GPU): the depth-limited
+    answer stands at or below 0.5% of the pot summed over both players, and
+    above it the full solve's flop strategies answer."""
+    class FakeGpu:
+        def iterate(self, n):
+            pass
+
+        def synchronize(self):
+            pass
+
+        def exploitability(self, host):
+            return 0.1
+
+        def info(self):
+            return {"iteration_kernels": 60}
+
+        def close(self):
+            pass
+
+    class FakeG:
+        def Solver(self, *a, **k):
+            return object()
+
+        def dl_gpu_solver(self, *a, **k):
+            return FakeGpu()
+
+        def node_strategy(self, gpu, n, na, pl):
+            return np.full((na, 3), 1.0 / na, np.float32)
+
+    class FakeCheck:
+        def __init__(self, losses):
+            self.spot = g.Spot(LD.dl_flop_spot(g.evaluate7))
+            self.losses = losses
+            self.full_strategies = {"full": True}
+
+        def loss(self, strat):
+            return self.losses[0], self.losses[1], [0.05, 0.05]
+
+    cfg = {"tree": {"starting_pot": 100.0}}
+    for losses, path in (((0.2, 0.3), "depth-limited"), ((0.3, 0.25), "full"), ((4.7, 3.5), "full")):
+        chk = FakeCheck(losses)
+        r = LD.depth_limited_or_full(FakeG(), cfg, None, chk, dl_iterations=10)
+        assert r["path"] == path, (losses, r["path"])
+        assert r["loss_sum_pct"] == pytest.approx(sum(losses))
+        if path == "full":
+            assert r["strategies"] is chk.full_strategies
+        else:
+            assert r["strategies"] is not chk.full_strategies and len(r["strategies"]) > 10
