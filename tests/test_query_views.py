@@ -281,3 +281,23 @@ def test_exploit_view_and_runouts_report_compose():
     assert rep["pot"] == 60.0 and rep["player"] == 0 and len(rep["rows"]) == len(cards)
     assert rep["rows"][0]["card"] == g.card_string(cards[0]) and rep["rows"][0]["eq"] == [pytest.approx(0.4), None]
     assert rep["actions"] == sv.path_view(chance + [g.card_string(cards[0])])["actions"]
+
+
+def test_stack_sized_turn_bet_is_labelled_all_in():
+    """The reference's runouts_labels_allin_bets (tests/convergence.rs:847-873)
+    on the host side: on Th9h2c with 60 behind and a 60%-pot turn bet, the
+    turn node after the report's first card (the highest available) offers
+    the bet labelled "All-in" -- the label the runouts report copies from
+    that node's action bar."""
+    empty = {"bet": [], "raise": []}
+    cfg = {"board": "Th9h2c", "range_oop": "QQ,JJ,TT", "range_ip": "AA,KK",
+           "tree": {"starting_pot": 100.0, "effective_stack": 60.0,
+                    "oop": [dict(empty), {"bet": W.sizes("60"), "raise": []}, dict(empty)],
+                    "ip": [dict(empty), dict(empty), dict(empty)]}}
+    sv = g.Solver(g.Spot(cfg))
+    chance = [0, 0]
+    cv = sv.path_view(chance)
+    assert cv["node_type"] == "chance"
+    first = cv["available_cards"][-1]  # the report's rows run from the highest card down
+    labels = [a["label"] for a in sv.path_view(chance + [first])["actions"]]
+    assert labels == ["Check", "All-in 60"], labels
