@@ -177,10 +177,44 @@ ARENA_DESC = {"compressed": "i16/u16 per-node scale, round to nearest (store.rs)
 HOST_BYTES = {"compressed": 2, "i16sr": 2, "f32": 4, "fp8": 4}
 
 
+def host_cpus():
+    """(physical cores, logical CPUs, model name) of the CPUs this process may
+    run on (its affinity mask; /proc/cpuinfo's physical id / core id pairs)."""
+    try:
+        allowed = os.sched_getaffinity(0)
+    except (AttributeError, OSError):
+        allowed = set(range(os.cpu_count() or 1))
+    cores, model, cpu = set(), "", None
+    phys = core = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f.read().splitlines() + [""]:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "processor":
+                    cpu = int(v)
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    core = v
+                elif k == "model name" and not model:
+                    model = v
+                elif not line.strip():
+                    if cpu is not None and cpu in allowed:
+                        cores.add((phys, core) if core is not None else ("cpu", cpu))
+                    cpu = phys = core = None
+    except OSError:
+        pass
+    return max(1, len(cores) or len(allowed)), len(allowed), model
+
+
 def cpu_baseline(cfg, storage, steps, threads=None):
-    """The oracle (reference CPU engine restated, pruning on) on the host cores."""
+    """The oracle (reference CPU engine restated, pruning on) on the host
+    cores: one thread per physical core unless told otherwise, the reference
+    CLI's default (SOLVER_THREADS, README.md: SMT hurts this workload)."""
     from oracle import pyoracle as po
-    n = threads or os.cpu_count() or 1
+    phys, logical, _ = host_cpus()
+    n = threads or phys
     po.set_threads(n)
     t0 = time.perf_counter()
     spot = po.Spot(cfg)
@@ -192,7 +226,8 @@ def cpu_baseline(cfg, storage, steps, threads=None):
         t = time.perf_counter()
         sv.iterate(1)
         times.append(time.perf_counter() - t)
-    return {"iter_s": times, "build_s": build_s, "cores": n}
+    return {"iter_s": times, "build_s": build_s, "cores": n, "physical_cores": phys, "logical_cpus": logical,
+            "cpu_model": host_cpus()[2]}
 
 
 def run_reference(args, world, rank):
@@ -213,6 +248,8 @@ def run_reference(args, world, rank):
         "vs_baseline": None, "dtype": DTYPE[args.storage], "data": "synthetic (seeded spot)",
         "config": workload_config(args, cfg),
         "cpu_baseline": {"value": value, "unit": "iter/s", "cores": r["cores"], "kind": "port",
+                         "cpu_model": r["cpu_model"], "physical_cores": r["physical_cores"],
+                         "logical_cpus": r["logical_cpus"],
                          "sample": "%d full DCFR iterations of the workload on the CPU oracle "
                                    "(reference cfr.rs semantics, pruning on, OpenMP over chance cards)" % len(timed)},
         "e2e": {"value": value, "unit": "iter/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -353,7 +390,8 @@ def run_ours(args, world, rank, local):
         r = cpu_baseline(cfg, args.storage, args.cpu_steps + 1, args.cpu_threads)
         timed = r["iter_s"][1:]  # the first iteration is the warm-up
         v = len(timed) / sum(timed)
-        base = {"value": v, "unit": "iter/s", "cores": r["cores"], "kind": "port",
+        base = {"value": v, "unit": "iter/s", "cores": r["cores"], "kind": "port", "cpu_model": r["cpu_model"],
+                "physical_cores": r["physical_cores"], "logical_cpus": r["logical_cpus"],
                 "sample": "%d DCFR iterations of the same spot after 1 warm-up iteration on the CPU oracle "
                           "(reference cfr.rs semantics, %s arenas, pruning on, OpenMP over chance cards); "
                           "spot build %.1fs excluded" % (len(timed), ARENA_DESC[args.storage], r["build_s"])}
